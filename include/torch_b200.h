@@ -1,0 +1,128 @@
+/*
+ * torch_b200: B200 (sm_100a) implementation of the TORCH operator-split
+ * radiation-hydrodynamics timestep, behind a plain C ABI.
+ *
+ * The entry points replace the Fluid/Integrators step of the reference:
+ *
+ *   trg_create         Torch::initialise (src/Torch/Torch.cpp:29-144) followed by
+ *                      the Torch::run prologue (src/Torch/Torch.cpp:245-264).
+ *                      Input: the raw Lua parameters (TorchParameters,
+ *                      src/Torch/Parameters.hpp:25-97, before
+ *                      TorchParameters::initialise) and the initial primitive
+ *                      fields in cgs, as DataReader::readGrid
+ *                      (src/IO/DataReader.cpp:70-125) or the Lua setup callback
+ *                      (src/Torch/Torch.cpp:192-228) would produce them.
+ *   trg_full_step      Torch::fullStep(dt_next_checkpoint)
+ *                      (src/Torch/Torch.cpp:389-418) plus the currentTime advance
+ *                      of Torch::run (src/Torch/Torch.cpp:285-286).
+ *   trg_run_steps      nsteps consecutive trg_full_step calls enqueued without a
+ *                      host round trip between steps.
+ *   trg_component      one phase of one Integrator (src/Integrators/Integrator.hpp:26-29:
+ *                      preTimeStepCalculations / calculateTimeStep / integrate /
+ *                      updateSourceTerms) or of the Fluid bookkeeping
+ *                      (Fluid::globalQfromU+fixPrimitives, advSolution+fixSolution,
+ *                      src/Fluid/Fluid.cpp:80-170), for callers that drive the
+ *                      operator split themselves.
+ *   trg_get_state /    read or replace the cell state (code units, SoA, flat
+ *   trg_set_conserved  index i + nx*(j + ny*k), Grid::flatIndex, src/Fluid/Grid.cpp:153-155).
+ *   trg_last_error     the text of the last failure (the reference throws
+ *                      std::runtime_error with a message, src/main.cpp:101-105).
+ *
+ * Conventions: every call returns 0 on success or a TRG_ERR_* code; the
+ * context owns all device memory; one context per host thread, all work on the
+ * context's own CUDA stream.  Field order for U and Q is DEN, PRE (total energy
+ * E in U), HII, ADV, VEL0, VEL1, VEL2 (src/Torch/Common.hpp:23-34); R is
+ * HII_A, TAU, TAU_A, DTAU, DTAU_A, HEAT; T is COL_DEN, DCOL_DEN, HEAT, RATE.
+ */
+#ifndef TORCH_B200_H
+#define TORCH_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TRG_OK 0
+#define TRG_ERR_ARG 1          /* invalid argument or unsupported parameter */
+#define TRG_ERR_CUDA 2         /* a CUDA runtime call failed */
+#define TRG_ERR_NAN 3          /* checkValues / fixSolution found an invalid state */
+#define TRG_ERR_PICARD 4       /* implicit ionisation solve did not converge */
+#define TRG_ERR_DT 5           /* invalid radiation time step */
+#define TRG_ERR_FLUX 6         /* Riemann solver produced a NaN HII flux */
+#define TRG_ERR_OOM 7          /* device allocation failed */
+
+#define TRG_PRECISION_FP64 0   /* every kernel in FP64, reference operation order, no FMA */
+#define TRG_PRECISION_FP32 1   /* hydro in FP32 (compensated E - KE), FP64 for ionisation, dt, sums */
+
+/* Raw run parameters: the values of the Lua Parameters table (cgs where the
+ * reference keeps cgs).  Enum values follow src/Torch/Common.hpp. */
+typedef struct trg_params {
+	double dscale, pscale, tscale;
+	int spatial_order, temporal_order;
+	double tmax;
+	int radiation_on, cooling_on;
+	int nd;
+	int ncells[3];
+	double side_length;
+	int geometry;                /* 0 cartesian, 1 cylindrical, 2 spherical */
+	int left_bc[3], right_bc[3]; /* 0 free, 1 reflecting, 2 outflow, 3 inflow, 4 periodic */
+	double gamma, dfloor, tfloor;
+	int riemann;                 /* 0 HLLC, 1 RotatedHLLC, 2 HLL */
+	int limiter;                 /* 0 monotonised_central, 1 superbee, 2 minmod, 3 maxmod, 4 leer, 5 ospre, 6 albada */
+	double K1, K2, K3, K4;
+	double photoion_xsec, alphaB, tau0, minX, THI, THII, mass_frac_h;
+	int rt_scheme;               /* 0 implicit */
+	int collisions_on;
+	int coupling;                /* 0 tti, 1 neq, 2 off */
+	double heating_amp, thermo_hii_switch;
+	int thermo_subcycling, min_temp_initial_state;
+	int star_on;
+	int star_pos[3];
+	int face_snap[3];
+	double photon_energy, photon_rate, mass_loss_rate, wind_velocity, wind_temperature;
+	int wind_cell_radius;
+	int precision;               /* TRG_PRECISION_* */
+	int device;                  /* CUDA device ordinal */
+} trg_params;
+
+typedef struct trg_ctx trg_ctx;
+
+/* Component ids and phases for trg_component (ComponentID, src/Torch/Torch.hpp:29). */
+#define TRG_COMP_HYDRO 0
+#define TRG_COMP_RAD 1
+#define TRG_COMP_THERMO 2
+#define TRG_COMP_FLUID 3
+#define TRG_PHASE_PRE 0         /* Integrator::preTimeStepCalculations */
+#define TRG_PHASE_DT 1          /* Integrator::calculateTimeStep (returns dt in *out) */
+#define TRG_PHASE_INTEGRATE 2   /* Integrator::integrate(dt) */
+#define TRG_PHASE_SOURCES 3     /* Integrator::updateSourceTerms(dt) (accumulates UDOT) */
+#define TRG_PHASE_Q_FROM_U 4    /* FLUID: globalQfromU + fixPrimitives */
+#define TRG_PHASE_ADVANCE 5     /* FLUID: advSolution(dt) + fixSolution */
+
+/* den..v2: initial primitives in cgs over the interior cells (N each); v1, v2
+ * and grav ([3][N], cgs) may be NULL for zero.  ncells/side_length describe
+ * the grid (for a text snapshot, side_length = dx * ncells[0] as
+ * DataReader::readDataParameters derives it). */
+int trg_create(const trg_params* p, const double* den, const double* pre, const double* hii,
+               const double* v0, const double* v1, const double* v2, const double* grav,
+               trg_ctx** out);
+int trg_full_step(trg_ctx* c, double dt_next_checkpoint, double* dt_taken);
+int trg_run_steps(trg_ctx* c, int nsteps, double dt_next_checkpoint, double* dts_out);
+int trg_component(trg_ctx* c, int comp, int phase, double dt, double* out);
+/* Any pointer may be NULL.  U, Q: [7][N]; R: [6][N]; T: [4][N]; Tmin: [N]. */
+int trg_get_state(trg_ctx* c, double* U, double* Q, double* R, double* T, double* Tmin);
+int trg_set_conserved(trg_ctx* c, const double* U);
+int trg_synchronize(trg_ctx* c);
+double trg_time(const trg_ctx* c);
+double trg_dt_max(const trg_ctx* c);
+long trg_ncells(const trg_ctx* c);
+/* Kernel launches issued by this context since creation (for accounting). */
+long long trg_kernel_launches(const trg_ctx* c);
+const char* trg_last_error(const trg_ctx* c);
+void trg_destroy(trg_ctx* c);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

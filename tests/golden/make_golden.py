@@ -1,0 +1,44 @@
+"""Generates the golden fixtures in tests/golden/ by running the reference.
+
+Usage (needs the reference tree and oracle/_ref/torch_ref, i.e. this build
+container):  python tests/golden/make_golden.py
+
+For each case of tests/cases.py it writes <case>.npz holding the exact Lua
+parameter text and initial-condition text the reference read, the number of
+full steps, and the reference's final U, Q, R, T, T_min and dt history.
+"""
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import cases  # noqa: E402
+import oracle  # noqa: E402
+from torch_b200 import config  # noqa: E402
+
+
+def make(name):
+    with tempfile.TemporaryDirectory() as d:
+        tp, ic, text, steps = cases.build(name, d)
+        params = config.to_lua(tp)
+        ppath = os.path.join(d, "params.lua")
+        with open(ppath, "w") as f:
+            f.write(params)
+        ref = oracle.run_reference(ppath, os.path.join(d, "ic_000.txt"), steps, d)
+    out = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(out, params_lua=np.array(params), ic_text=np.array(text), steps=np.array(steps),
+                        U=ref.U, Q=ref.Q, R=ref.R, T=ref.T, Tmin=ref.Tmin, dts=ref.dts, time=np.array(ref.time))
+    print(f"{name}: {steps} steps, {ic.den.size} cells -> {os.path.relpath(out, ROOT)} "
+          f"({os.path.getsize(out) // 1024} KiB)")
+
+
+if __name__ == "__main__":
+    for name in (sys.argv[1:] or list(cases.CASES)):
+        make(name)

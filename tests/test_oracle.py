@@ -1,0 +1,85 @@
+"""The CPU oracle (plain-C restatement) pinned against the reference.
+
+* golden fixtures produced by the reference build (tests/golden/*.npz):
+  the oracle must reproduce them bit for bit;
+* when the reference build is available (this container), fresh runs of the
+  reference itself on further cases, including the full shipped config 1.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import common
+import oracle
+from torch_b200 import config
+
+
+@pytest.mark.parametrize("name", common.golden_names())
+def test_oracle_matches_golden_bitwise(name):
+    tp, ic, steps, ref = common.load_golden(name)
+    o = oracle.Oracle(tp, ic)
+    for _ in range(steps):
+        o.full_step()
+    got = common.state_dict(o.state())
+    assert np.array_equal(np.array(o.dts), ref["dts"])
+    for (g, fname), err in common.compare_states(got, ref, ic.nd).items():
+        f = common.FIELD_NAMES[g].index(fname)
+        assert np.array_equal(got[g][f], ref[g][f]), f"{name} {g}.{fname} differs (relL1 {err:.3e})"
+
+
+def _reference_or_skip():
+    if oracle.build_reference() is None:
+        pytest.skip("reference build unavailable")
+
+
+def test_oracle_matches_reference_config1_full():
+    """The shipped 150x200 cylindrical rad-hydro setup, 20 full steps."""
+    _reference_or_skip()
+    import cases
+    with tempfile.TemporaryDirectory() as d:
+        tp, ic, text, steps = cases.build("blister_full", d)
+        ppath = os.path.join(d, "p.lua")
+        with open(ppath, "w") as f:
+            f.write(config.to_lua(tp))
+        ref = oracle.run_reference(ppath, os.path.join(d, "ic_000.txt"), steps, d)
+    o = oracle.Oracle(tp, ic)
+    for _ in range(steps):
+        o.full_step()
+    st = o.state()
+    assert np.array_equal(np.array(o.dts), ref.dts)
+    for g in ("U", "Q", "R", "T"):
+        a, b = getattr(st, g), getattr(ref, g)
+        for f in range(a.shape[0]):
+            if common.inplane(g, f, 2):
+                assert np.array_equal(a[f], b[f]), (g, f)
+
+
+def test_reference_params_match_lua_front_end():
+    """parse_parameters reads the shipped config exactly like src/main.cpp."""
+    _reference_or_skip()
+    import subprocess
+    path = os.path.join(oracle.REF_TREE, "config", "torch-config.lua")
+    out = subprocess.run([oracle.REF_BIN, f"--params={path}", "--print-params"], capture_output=True,
+                         text=True, check=True).stdout
+    ref = {}
+    for line in out.splitlines():
+        k, *v = line.split()
+        ref[k] = v
+    tp = config.parse_parameters(path)
+    assert float(ref["tmax"][0]) == tp.tmax
+    assert float(ref["side_length"][0]) == tp.sideLength
+    assert [int(x) for x in ref["ncells"]] == list(tp.ncells)
+    assert ref["right_bc"] == list(tp.rightBC)
+    assert int(ref["radiation_on"][0]) == tp.radiation_on and int(ref["cooling_on"][0]) == tp.cooling_on
+    assert [int(x) for x in ref["star_pos"]] == list(tp.star_position)
+    assert float(ref["photon_rate"][0]) == tp.photonRate
+    assert ref["riemann"][0] == tp.riemannSolver and ref["limiter"][0] == tp.slopeLimiter
+
+
+def test_causal_order_covers_grid_once():
+    tp, ic, steps, _ = common.load_golden("hii3d_offcentre")
+    o = oracle.Oracle(tp, ic)
+    order = o.causal_order()
+    assert len(order) == o.N and len(set(order.tolist())) == o.N

@@ -1,0 +1,248 @@
+"""torch_b200: B200-native TORCH operator-split timestep behind a C ABI.
+
+The compute path is ``libtorch_b200.so`` (hand-written sm_100a CUDA kernels,
+built in-tree by ``torch_b200/csrc/Makefile``).  This module binds its C ABI
+(``include/torch_b200.h``) with ctypes and mirrors the reference's driver
+interface (``Torch::initialise`` / ``Torch::fullStep`` / ``Torch::run``,
+src/Torch/Torch.cpp) so that Python callers and the tests drive it like the
+reference.  There is no CPU fallback: if the library is missing or no GPU is
+present, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import config
+from .config import CONDITION, GEOMETRY, TorchParameters, enum_value
+
+__all__ = ["Torch", "TrgError", "library_path", "load_library", "TorchParameters", "config"]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_NAME = "libtorch_b200.so"
+
+PRECISION_FP64 = 0
+PRECISION_FP32 = 1
+
+COMP_HYDRO, COMP_RAD, COMP_THERMO, COMP_FLUID = 0, 1, 2, 3
+PHASE_PRE, PHASE_DT, PHASE_INTEGRATE, PHASE_SOURCES, PHASE_Q_FROM_U, PHASE_ADVANCE = 0, 1, 2, 3, 4, 5
+
+ERROR_NAMES = {1: "TRG_ERR_ARG", 2: "TRG_ERR_CUDA", 3: "TRG_ERR_NAN", 4: "TRG_ERR_PICARD",
+               5: "TRG_ERR_DT", 6: "TRG_ERR_FLUX", 7: "TRG_ERR_OOM"}
+
+
+class TrgError(RuntimeError):
+    """A failing torch_b200 call (the reference throws std::runtime_error)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERROR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class TrgParams(C.Structure):
+    """ctypes mirror of ``trg_params`` (include/torch_b200.h)."""
+    _fields_ = [
+        ("dscale", C.c_double), ("pscale", C.c_double), ("tscale", C.c_double),
+        ("spatial_order", C.c_int), ("temporal_order", C.c_int),
+        ("tmax", C.c_double),
+        ("radiation_on", C.c_int), ("cooling_on", C.c_int),
+        ("nd", C.c_int), ("ncells", C.c_int * 3),
+        ("side_length", C.c_double),
+        ("geometry", C.c_int), ("left_bc", C.c_int * 3), ("right_bc", C.c_int * 3),
+        ("gamma", C.c_double), ("dfloor", C.c_double), ("tfloor", C.c_double),
+        ("riemann", C.c_int), ("limiter", C.c_int),
+        ("K1", C.c_double), ("K2", C.c_double), ("K3", C.c_double), ("K4", C.c_double),
+        ("photoion_xsec", C.c_double), ("alphaB", C.c_double), ("tau0", C.c_double),
+        ("minX", C.c_double), ("THI", C.c_double), ("THII", C.c_double), ("mass_frac_h", C.c_double),
+        ("rt_scheme", C.c_int), ("collisions_on", C.c_int), ("coupling", C.c_int),
+        ("heating_amp", C.c_double), ("thermo_hii_switch", C.c_double),
+        ("thermo_subcycling", C.c_int), ("min_temp_initial_state", C.c_int),
+        ("star_on", C.c_int), ("star_pos", C.c_int * 3), ("face_snap", C.c_int * 3),
+        ("photon_energy", C.c_double), ("photon_rate", C.c_double), ("mass_loss_rate", C.c_double),
+        ("wind_velocity", C.c_double), ("wind_temperature", C.c_double),
+        ("wind_cell_radius", C.c_int),
+        ("precision", C.c_int),
+        ("device", C.c_int),
+    ]
+
+
+def library_path() -> str:
+    return os.path.join(HERE, _LIB_NAME)
+
+
+_lib = None
+
+# (name, restype, argtypes) for every entry point of include/torch_b200.h
+_SIGNATURES = [
+    ("trg_create", C.c_int, [C.POINTER(TrgParams)] + [C.c_void_p] * 7 + [C.POINTER(C.c_void_p)]),
+    ("trg_full_step", C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_double)]),
+    ("trg_run_steps", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_void_p]),
+    ("trg_component", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_double)]),
+    ("trg_get_state", C.c_int, [C.c_void_p] + [C.c_void_p] * 5),
+    ("trg_set_conserved", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("trg_synchronize", C.c_int, [C.c_void_p]),
+    ("trg_time", C.c_double, [C.c_void_p]),
+    ("trg_dt_max", C.c_double, [C.c_void_p]),
+    ("trg_ncells", C.c_long, [C.c_void_p]),
+    ("trg_kernel_launches", C.c_longlong, [C.c_void_p]),
+    ("trg_last_error", C.c_char_p, [C.c_void_p]),
+    ("trg_destroy", None, [C.c_void_p]),
+]
+
+
+def load_library():
+    """Loads libtorch_b200.so from the package directory (raises if absent)."""
+    global _lib
+    if _lib is None:
+        path = library_path()
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is missing: build it with `make -C torch_b200/csrc` "
+                                    "(there is no CPU fallback)")
+        lib = C.CDLL(path)
+        for name, res, args in _SIGNATURES:
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def make_params(tp: TorchParameters, side_length: float, ncells, precision: int = PRECISION_FP64,
+                device: int = 0) -> TrgParams:
+    p = TrgParams()
+    p.dscale, p.pscale, p.tscale = tp.dscale, tp.pscale, tp.tscale
+    p.spatial_order, p.temporal_order = tp.spatialOrder, tp.temporalOrder
+    p.tmax = tp.tmax
+    p.radiation_on, p.cooling_on = int(tp.radiation_on), int(tp.cooling_on)
+    p.nd = 1 if ncells[1] == 1 else (2 if ncells[2] == 1 else 3)
+    for i in range(3):
+        p.ncells[i] = int(ncells[i])
+        p.left_bc[i] = enum_value(CONDITION, tp.leftBC[i])
+        p.right_bc[i] = enum_value(CONDITION, tp.rightBC[i])
+        p.star_pos[i] = tp.star_position[i]
+        p.face_snap[i] = int(tp.faceSnap[i])
+    p.side_length = side_length
+    p.geometry = enum_value(GEOMETRY, tp.geometry)
+    p.gamma, p.dfloor, p.tfloor = tp.heatCapacityRatio, tp.dfloor, tp.tfloor
+    p.riemann, p.limiter = tp.riemann_id(), tp.limiter_id()
+    p.K1, p.K2, p.K3, p.K4 = tp.K1, tp.K2, tp.K3, tp.K4
+    p.photoion_xsec, p.alphaB, p.tau0 = tp.photoIonCrossSection, tp.alphaB, tp.tau0
+    p.minX, p.THI, p.THII, p.mass_frac_h = tp.minX, tp.THI, tp.THII, tp.massFractionH
+    p.rt_scheme, p.collisions_on, p.coupling = tp.scheme_id(), int(tp.collisions_on), tp.coupling_id()
+    p.heating_amp, p.thermo_hii_switch = tp.heatingAmplification, tp.thermoHII_Switch
+    p.thermo_subcycling, p.min_temp_initial_state = int(tp.thermoSubcycling), int(tp.minTempInitialState)
+    p.star_on = int(tp.star_on)
+    p.photon_energy, p.photon_rate = tp.photonEnergy, tp.photonRate
+    p.mass_loss_rate, p.wind_velocity = tp.massLossRate, tp.windVelocity
+    p.wind_temperature, p.wind_cell_radius = tp.windTemperature, tp.windCellRadius
+    p.precision = precision
+    p.device = device
+    return p
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+@dataclass
+class State:
+    U: np.ndarray
+    Q: np.ndarray
+    R: np.ndarray
+    T: np.ndarray
+    Tmin: np.ndarray
+    time: float
+    dts: np.ndarray
+
+
+class Torch:
+    """One run on one GPU: ``Torch::initialise`` then ``full_step`` calls.
+
+    ``ic`` is a ``config.InitialConditions`` (primitives in cgs, as the
+    reference's DataReader or Lua setup provides them).
+    """
+
+    def __init__(self, tp: TorchParameters, ic, precision: int = PRECISION_FP64, device: int = 0):
+        self.lib = load_library()
+        self.N = int(np.prod(ic.ncells))
+        p = make_params(tp, ic.side_length, ic.ncells, precision, device)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in
+                (ic.den, ic.pre, ic.hii, ic.vel[0], ic.vel[1], ic.vel[2])]
+        grav = getattr(ic, "grav", None)
+        garr = None if grav is None else np.ascontiguousarray(grav, dtype=np.float64)
+        ctx = C.c_void_p()
+        rc = self.lib.trg_create(C.byref(p), *[_ptr(a) for a in arrs], _ptr(garr), C.byref(ctx))
+        self.ctx = ctx.value
+        if rc != 0:
+            msg = self.lib.trg_last_error(self.ctx).decode() if self.ctx else "trg_create failed"
+            self.close()
+            raise TrgError(rc, msg)
+        self.dts = []
+
+    def _check(self, rc):
+        if rc != 0:
+            raise TrgError(rc, self.lib.trg_last_error(self.ctx).decode())
+
+    @property
+    def dt_max(self) -> float:
+        return self.lib.trg_dt_max(self.ctx)
+
+    def full_step(self, dt_next_checkpoint: Optional[float] = None) -> float:
+        """Torch::fullStep (src/Torch/Torch.cpp:389-418); returns dt."""
+        if dt_next_checkpoint is None:
+            dt_next_checkpoint = self.dt_max
+        dt = C.c_double(0)
+        self._check(self.lib.trg_full_step(self.ctx, dt_next_checkpoint, C.byref(dt)))
+        self.dts.append(dt.value)
+        return dt.value
+
+    def run_steps(self, nsteps: int, dt_next_checkpoint: Optional[float] = None) -> np.ndarray:
+        """nsteps full steps enqueued back to back; returns their dt values."""
+        if dt_next_checkpoint is None:
+            dt_next_checkpoint = self.dt_max
+        out = np.zeros(max(nsteps, 1))
+        self._check(self.lib.trg_run_steps(self.ctx, nsteps, dt_next_checkpoint, _ptr(out)))
+        self.dts.extend(out[:nsteps].tolist())
+        return out[:nsteps]
+
+    def component(self, comp: int, phase: int, dt: float = 0.0) -> float:
+        out = C.c_double(0)
+        self._check(self.lib.trg_component(self.ctx, comp, phase, dt, C.byref(out)))
+        return out.value
+
+    def state(self) -> State:
+        N = self.N
+        U = np.zeros((7, N)); Q = np.zeros((7, N)); R = np.zeros((6, N)); T = np.zeros((4, N)); Tm = np.zeros(N)
+        self._check(self.lib.trg_get_state(self.ctx, _ptr(U), _ptr(Q), _ptr(R), _ptr(T), _ptr(Tm)))
+        return State(U, Q, R, T, Tm, self.lib.trg_time(self.ctx), np.array(self.dts))
+
+    def set_conserved(self, U: np.ndarray):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        self._check(self.lib.trg_set_conserved(self.ctx, _ptr(U)))
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.trg_kernel_launches(self.ctx))
+
+    def synchronize(self):
+        self._check(self.lib.trg_synchronize(self.ctx))
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.trg_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -426,3 +426,39 @@ def read_initial_conditions(path: str) -> InitialConditions:
     for d in range(nd):
         vel[d, flat[ok]] = rows[ok, nd + 3 + d]
     return InitialConditions(t, ncells, nd, dx, side, den, pre, hii, vel)
+
+
+def to_lua(tp: TorchParameters) -> str:
+    """Writes the Parameters table that parse_parameters reads back (and that
+    the reference's own parseParameters reads, src/main.cpp:126-208)."""
+    def lit(v):
+        if isinstance(v, bool):
+            return "true" if v else "false"
+        if isinstance(v, str):
+            return '"' + v.replace('"', '\\"') + '"'
+        if isinstance(v, int):
+            return str(v)
+        return repr(float(v))
+
+    sections: Dict[str, List[str]] = {}
+    for section, key, attr, kind, idx in _KEYS:
+        v = getattr(tp, attr)
+        if idx is not None:
+            v = v[idx]
+        sections.setdefault(section, []).append(f"\t\t{key} = {lit(v)},")
+    out = ["Parameters = {"]
+    for section, lines in sections.items():
+        out.append(f"\t{section} = {{")
+        out.extend(lines)
+        out.append("\t},")
+    out.append("}")
+    return "\n".join(out) + "\n"
+
+
+def make_initial_conditions(ncells, dx: float, den, pre, hii, vel, time: float = 0.0) -> InitialConditions:
+    """In-memory initial conditions with side_length = dx * ncells[0]."""
+    nx, ny, nz = ncells
+    nd = 1 if ny == 1 else (2 if nz == 1 else 3)
+    vel = np.asarray(vel, dtype=np.float64)
+    return InitialConditions(time, tuple(ncells), nd, dx, dx * nx, np.asarray(den, np.float64),
+                             np.asarray(pre, np.float64), np.asarray(hii, np.float64), vel)

@@ -1,0 +1,428 @@
+// C ABI and step orchestration (Torch::fullStep / subStep / hydroStep,
+// src/Torch/Torch.cpp:352-418) for torch_b200.
+//
+// All device memory belongs to the context; all work is enqueued on the
+// context's stream.  Time-step values stay on the device between kernels
+// (the dt reduction writes them, the integrators read them), so a sequence of
+// steps needs no host round trip.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/torch_b200.h"
+#include "setup.h"
+#include "trg_kernels.h"
+
+using namespace trg;
+
+namespace {
+constexpr int COMP_HYDRO = 0, COMP_RAD = 1, COMP_THERMO = 2;
+}
+
+struct trg_ctx {
+	trg_params raw;
+	HostSetup hs;
+	Params P;
+	State S;
+	cudaStream_t stream = nullptr;
+	Tables* d_tables = nullptr;
+	int* d_sweep_all = nullptr;
+	int* d_sweep_nonwind = nullptr;
+	int* d_wind = nullptr;
+	std::vector<void*> allocs;
+	int first_time = 1;
+	int rad_once_pending = 1;
+	int stepCounter = 0;
+	long long steps = 0;
+	long long launches = 0;
+	int dt_hist_cap = 0;
+	std::string err;
+};
+
+namespace {
+
+int set_error(trg_ctx* c, int code, const std::string& msg) {
+	if (c) c->err = msg;
+	return code;
+}
+
+#define CUDA_TRY(call)                                                                                  \
+	do {                                                                                                \
+		cudaError_t e_ = (call);                                                                        \
+		if (e_ != cudaSuccess)                                                                          \
+			return set_error(c, e_ == cudaErrorMemoryAllocation ? TRG_ERR_OOM : TRG_ERR_CUDA,         \
+			                 std::string(#call) + ": " + cudaGetErrorString(e_));                         \
+	} while (0)
+
+template <typename T>
+int dalloc(trg_ctx* c, T** p, size_t count) {
+	void* v = nullptr;
+	CUDA_TRY(cudaMalloc(&v, count * sizeof(T) + 16));
+	c->allocs.push_back(v);
+	*p = static_cast<T*>(v);
+	return 0;
+}
+
+inline unsigned grid_for(long long n, int block) { return (unsigned)((n + block - 1) / block); }
+
+#define LAUNCH(kernel, n, block, ...)                                                        \
+	do {                                                                                     \
+		if ((n) > 0) {                                                                       \
+			kernel<<<grid_for((n), (block)), (block), 0, c->stream>>>(__VA_ARGS__);          \
+			c->launches++;                                                                   \
+		}                                                                                    \
+	} while (0)
+
+void q_from_u(trg_ctx* c, const double* Usrc, int fix) { LAUNCH(k_q_from_u_fp64, c->P.N, 256, c->P, c->S, Usrc, fix); }
+
+void colden_sweep(trg_ctx* c) {
+	const auto& off = c->hs.off_all;
+	for (size_t s = 0; s + 1 < off.size(); ++s) {
+		int count = (int)(off[s + 1] - off[s]);
+		LAUNCH(k_colden_shell_fp64, count, 128, c->P, c->S, c->d_sweep_all + off[s], count);
+	}
+}
+
+void thermo_pre(trg_ctx* c) {
+	// Thermodynamics::preTimeStepCalculations: column densities, then rates.
+	if (c->P.star_on) colden_sweep(c);
+	LAUNCH(k_thermo_rates_fp64, c->P.N, 256, c->P, c->S);
+}
+
+void rad_pre(trg_ctx* c) { LAUNCH(k_rad_heating_fp64, c->P.N, 256, c->P, c->S); }
+
+void comp_pre(trg_ctx* c, int comp) {
+	if (comp == COMP_RAD) rad_pre(c);
+	else if (comp == COMP_THERMO) thermo_pre(c);
+}
+
+void hydro_fluxes(trg_ctx* c) {
+	for (int d = 0; d < c->P.nd; ++d) LAUNCH(k_faces_fp64, c->S.nfaces[d], 128, c->P, c->S, d);
+}
+
+void rad_integrate(trg_ctx* c, double h) {
+	// Radiation::transferRadiation (Radiation.cpp:569-651)
+	if (c->P.star_on) {
+		int nw = (int)c->hs.wind_cells.size();
+		LAUNCH(k_rad_wind_reset, nw, 128, c->P, c->S, c->d_wind, nw);
+		const auto& off = c->hs.off_nonwind;
+		for (size_t s = 0; s + 1 < off.size(); ++s) {
+			int count = (int)(off[s + 1] - off[s]);
+			LAUNCH(k_rad_shell_fp64, count, 128, c->P, c->S, c->d_sweep_nonwind + off[s], count, h,
+			       (const double*)nullptr);
+		}
+	} else {
+		LAUNCH(k_rad_no_star_fp64, c->P.N, 256, c->P, c->S, h);
+	}
+}
+
+void sub_step(trg_ctx* c, double h, bool hasCalculatedHeatFlux, int comp) {
+	// Torch::subStep, Torch.cpp:352-364
+	if (!hasCalculatedHeatFlux) {
+		q_from_u(c, c->S.U, 1);
+		comp_pre(c, comp);
+	}
+	switch (comp) {
+	case COMP_HYDRO:
+		hydro_fluxes(c);
+		LAUNCH(k_hydro_update_fp64, c->P.N, 256, c->P, c->S, h, (const double*)c->S.U, c->S.U, 0);
+		break;
+	case COMP_RAD:
+		rad_integrate(c, h);
+		LAUNCH(k_rad_update_fp64, c->P.N, 256, c->P, c->S, h, 0);
+		break;
+	default:
+		LAUNCH(k_thermo_integrate_fp64, c->P.N, 256, c->P, c->S, h);
+		LAUNCH(k_thermo_update_fp64, c->P.N, 256, c->P, c->S, h, 0);
+		break;
+	}
+}
+
+void hydro_step(trg_ctx* c) {
+	// Torch::hydroStep (hasCalculatedHeatFlux = true), Torch.cpp:366-387: the
+	// saved state W is the untouched U; the predictor writes U1.
+	hydro_fluxes(c);
+	LAUNCH(k_hydro_update_fp64, c->P.N, 256, c->P, c->S, 0.5, (const double*)c->S.U, c->S.U1, 0);
+	q_from_u(c, c->S.U1, 0);
+	hydro_fluxes(c);
+	LAUNCH(k_hydro_update_fp64, c->P.N, 256, c->P, c->S, 1.0, (const double*)c->S.U, c->S.U, 0);
+}
+
+void time_step(trg_ctx* c, double dt_next) {
+	// Torch::calculateTimeStep and the min with dt_next_checkpoint (Torch.cpp:304-339, :394)
+	int step = c->steps < c->dt_hist_cap ? (int)c->steps : -1;
+	if (c->first_time) {
+		LAUNCH(k_dt_finalize, 1, 1, c->P, c->S, dt_next, 1, step);
+		c->first_time = 0;
+		return;
+	}
+	long long first_cell = -1;
+	if (c->P.radiation_on && c->P.star_on && c->P.K1 != 0.0 && c->rad_once_pending) {
+		first_cell = c->hs.first_nonwind_cell;
+		c->rad_once_pending = 0;
+	}
+	LAUNCH(k_dt_reset, 1, 1, c->P, c->S);
+	LAUNCH(k_dt_reduce_fp64, c->P.N, 256, c->P, c->S, first_cell);
+	LAUNCH(k_dt_finalize, 1, 1, c->P, c->S, dt_next, 0, step);
+}
+
+void enqueue_full_step(trg_ctx* c, double dt_next) {
+	// Torch::fullStep, Torch.cpp:389-418
+	q_from_u(c, c->S.U, 1);
+	if (c->P.cooling_on) thermo_pre(c);
+	if (c->P.radiation_on) rad_pre(c);
+	time_step(c, dt_next);
+	const int ncomps = c->hs.nactive;
+	if (ncomps == 1) {
+		hydro_step(c);
+	} else {
+		c->stepCounter = (c->stepCounter + 1) % ncomps;
+		for (int i = 0; i < ncomps; ++i) {
+			double h = (i == ncomps - 1) ? 1.0 : 0.5;
+			sub_step(c, h, i == 0, c->hs.active[(i + c->stepCounter) % ncomps]);
+		}
+		for (int i = ncomps - 2; i >= 0; --i) sub_step(c, 0.5, false, c->hs.active[(i + c->stepCounter) % ncomps]);
+	}
+	LAUNCH(k_time_advance, 1, 1, c->S);
+	c->steps++;
+}
+
+int check_device_error(trg_ctx* c) {
+	CUDA_TRY(cudaGetLastError());
+	unsigned e = 0;
+	CUDA_TRY(cudaMemcpyAsync(&e, c->S.err, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	if (e & ERRB_FLUX) return set_error(c, TRG_ERR_FLUX, "Riemann solver: HII flux is NaN");
+	if (e & ERRB_PICARD) return set_error(c, TRG_ERR_PICARD, "update_HIIfrac: implicit method not converging");
+	if (e & ERRB_DT) return set_error(c, TRG_ERR_DT, "Radiation::calculateTimeStep: invalid timestep");
+	if (e & ERRB_NAN) return set_error(c, TRG_ERR_NAN, "checkValues/fixSolution: invalid cell state");
+	return TRG_OK;
+}
+
+int ensure_dt_hist(trg_ctx* c, long long needed) {
+	if (needed <= c->dt_hist_cap) return 0;
+	int cap = (int)std::max<long long>(needed, 2LL * c->dt_hist_cap + 1024);
+	double* nh = nullptr;
+	if (dalloc(c, &nh, cap)) return TRG_ERR_OOM;
+	if (c->S.dt_hist && c->steps > 0)
+		CUDA_TRY(cudaMemcpyAsync(nh, c->S.dt_hist, sizeof(double) * std::min<long long>(c->steps, c->dt_hist_cap),
+		                         cudaMemcpyDeviceToDevice, c->stream));
+	c->S.dt_hist = nh;
+	c->dt_hist_cap = cap;
+	return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int trg_create(const trg_params* p, const double* den, const double* pre, const double* hii, const double* v0,
+               const double* v1, const double* v2, const double* grav, trg_ctx** out) {
+	if (!p || !out) return TRG_ERR_ARG;
+	*out = nullptr;
+	trg_ctx* c = new trg_ctx();
+	c->raw = *p;
+	if (p->precision != TRG_PRECISION_FP64 && p->precision != TRG_PRECISION_FP32) {
+		c->err = "unknown precision";
+		*out = c;
+		return TRG_ERR_ARG;
+	}
+	std::string why = host_setup(*p, den, pre, hii, v0, v1, v2, grav, c->hs);
+	if (!why.empty()) {
+		c->err = why;
+		*out = c;
+		return TRG_ERR_ARG;
+	}
+	*out = c;
+	c->P = c->hs.P;
+	const long long N = c->P.N;
+	CUDA_TRY(cudaSetDevice(p->device));
+	CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+	State& S = c->S;
+	std::memset(&S, 0, sizeof(S));
+	int rc = 0;
+	rc |= dalloc(c, &S.U, 7 * N);
+	rc |= dalloc(c, &S.Q, 7 * N);
+	rc |= dalloc(c, &S.U1, 7 * N);
+	rc |= dalloc(c, &S.UDOT, 7 * N);
+	rc |= dalloc(c, &S.R, 6 * N);
+	rc |= dalloc(c, &S.T, 4 * N);
+	rc |= dalloc(c, &S.Tmin, N);
+	rc |= dalloc(c, &S.ds, N);
+	rc |= dalloc(c, &S.shellVol, N);
+	rc |= dalloc(c, &S.err, 1);
+	rc |= dalloc(c, &S.scal, 8);
+	if (c->hs.has_grav) rc |= dalloc(c, &S.grav, 3 * N);
+	for (int d = 0; d < 3; ++d) {
+		int n = d == 0 ? c->P.nx : (d == 1 ? c->P.ny : c->P.nz);
+		S.nfaces[d] = (N / n) * (n + 1);
+		if (d < c->P.nd) rc |= dalloc(c, &S.F[d], 7 * S.nfaces[d]);
+	}
+	rc |= dalloc(c, &c->d_tables, 1);
+	rc |= dalloc(c, &c->d_sweep_all, c->hs.sweep_all.size() + 1);
+	rc |= dalloc(c, &c->d_sweep_nonwind, c->hs.sweep_nonwind.size() + 1);
+	rc |= dalloc(c, &c->d_wind, c->hs.wind_cells.size() + 1);
+	if (rc) return rc;
+	S.tables = c->d_tables;
+	cudaStream_t st = c->stream;
+	CUDA_TRY(cudaMemcpyAsync(S.U, c->hs.U.data(), 7 * N * sizeof(double), cudaMemcpyHostToDevice, st));
+	CUDA_TRY(cudaMemcpyAsync(S.Q, c->hs.Q.data(), 7 * N * sizeof(double), cudaMemcpyHostToDevice, st));
+	CUDA_TRY(cudaMemcpyAsync(S.R, c->hs.R.data(), 6 * N * sizeof(double), cudaMemcpyHostToDevice, st));
+	CUDA_TRY(cudaMemcpyAsync(S.T, c->hs.T.data(), 4 * N * sizeof(double), cudaMemcpyHostToDevice, st));
+	CUDA_TRY(cudaMemcpyAsync(S.Tmin, c->hs.Tmin.data(), N * sizeof(double), cudaMemcpyHostToDevice, st));
+	CUDA_TRY(cudaMemcpyAsync(S.ds, c->hs.ds.data(), N * sizeof(double), cudaMemcpyHostToDevice, st));
+	CUDA_TRY(cudaMemcpyAsync(S.shellVol, c->hs.shellVol.data(), N * sizeof(double), cudaMemcpyHostToDevice, st));
+	if (c->hs.has_grav)
+		CUDA_TRY(cudaMemcpyAsync(S.grav, c->hs.grav.data(), 3 * N * sizeof(double), cudaMemcpyHostToDevice, st));
+	CUDA_TRY(cudaMemsetAsync(S.UDOT, 0, 7 * N * sizeof(double), st));
+	CUDA_TRY(cudaMemsetAsync(S.U1, 0, 7 * N * sizeof(double), st));
+	CUDA_TRY(cudaMemsetAsync(S.err, 0, sizeof(unsigned), st));
+	CUDA_TRY(cudaMemsetAsync(S.scal, 0, 8 * sizeof(double), st));
+	CUDA_TRY(cudaMemcpyAsync(c->d_tables, &c->hs.tables, sizeof(Tables), cudaMemcpyHostToDevice, st));
+	if (!c->hs.sweep_all.empty())
+		CUDA_TRY(cudaMemcpyAsync(c->d_sweep_all, c->hs.sweep_all.data(), c->hs.sweep_all.size() * sizeof(int),
+		                         cudaMemcpyHostToDevice, st));
+	if (!c->hs.sweep_nonwind.empty())
+		CUDA_TRY(cudaMemcpyAsync(c->d_sweep_nonwind, c->hs.sweep_nonwind.data(),
+		                         c->hs.sweep_nonwind.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+	if (!c->hs.wind_cells.empty())
+		CUDA_TRY(cudaMemcpyAsync(c->d_wind, c->hs.wind_cells.data(), c->hs.wind_cells.size() * sizeof(int),
+		                         cudaMemcpyHostToDevice, st));
+	if ((rc = ensure_dt_hist(c, 1024))) return rc;
+	// Torch::run prologue (Torch.cpp:245-264): Q from U with floors, and the
+	// column-density ray trace of fillHeatingArrays (Thermodynamics.cpp:420-421).
+	q_from_u(c, S.U, 1);
+	if (c->P.star_on) colden_sweep(c);
+	// the host copies of the initial fields are no longer needed
+	std::vector<double>().swap(c->hs.U);
+	std::vector<double>().swap(c->hs.Q);
+	std::vector<double>().swap(c->hs.R);
+	std::vector<double>().swap(c->hs.T);
+	std::vector<double>().swap(c->hs.grav);
+	return check_device_error(c);
+}
+
+int trg_full_step(trg_ctx* c, double dt_next_checkpoint, double* dt_taken) {
+	if (!c) return TRG_ERR_ARG;
+	int rc = ensure_dt_hist(c, c->steps + 1);
+	if (rc) return rc;
+	enqueue_full_step(c, dt_next_checkpoint);
+	if ((rc = check_device_error(c))) return rc;
+	if (dt_taken) {
+		CUDA_TRY(cudaMemcpy(dt_taken, c->S.scal, sizeof(double), cudaMemcpyDeviceToHost));
+	}
+	return TRG_OK;
+}
+
+int trg_run_steps(trg_ctx* c, int nsteps, double dt_next_checkpoint, double* dts_out) {
+	if (!c || nsteps < 0) return TRG_ERR_ARG;
+	long long first = c->steps;
+	int rc = ensure_dt_hist(c, c->steps + nsteps);
+	if (rc) return rc;
+	for (int s = 0; s < nsteps; ++s) enqueue_full_step(c, dt_next_checkpoint);
+	if ((rc = check_device_error(c))) return rc;
+	if (dts_out && nsteps > 0)
+		CUDA_TRY(cudaMemcpy(dts_out, c->S.dt_hist + first, sizeof(double) * nsteps, cudaMemcpyDeviceToHost));
+	return TRG_OK;
+}
+
+int trg_component(trg_ctx* c, int comp, int phase, double dt, double* out) {
+	if (!c) return TRG_ERR_ARG;
+	// The phase kernels read dt from the device scalar: stage the caller's dt.
+	CUDA_TRY(cudaMemcpyAsync(c->S.scal, &dt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+	switch (phase) {
+	case TRG_PHASE_PRE:
+		if (comp == TRG_COMP_THERMO) thermo_pre(c);
+		else if (comp == TRG_COMP_RAD) rad_pre(c);
+		break;
+	case TRG_PHASE_DT: {
+		LAUNCH(k_dt_reset, 1, 1, c->P, c->S);
+		long long first_cell = -1;
+		if (comp == TRG_COMP_RAD && c->P.radiation_on && c->P.star_on && c->P.K1 != 0.0 && c->rad_once_pending) {
+			first_cell = c->hs.first_nonwind_cell;
+			c->rad_once_pending = 0;
+		}
+		LAUNCH(k_dt_reduce_fp64, c->P.N, 256, c->P, c->S, first_cell);
+		double mins[3];
+		CUDA_TRY(cudaMemcpyAsync(mins, c->S.scal + 2, sizeof(mins), cudaMemcpyDeviceToHost, c->stream));
+		CUDA_TRY(cudaStreamSynchronize(c->stream));
+		double v = c->P.dt_max;
+		if (comp == TRG_COMP_HYDRO) v = mins[0] < v ? mins[0] : v;
+		else if (comp == TRG_COMP_RAD) v = (c->P.star_on && mins[1] < v) ? mins[1] : v;
+		else if (comp == TRG_COMP_THERMO) v = mins[2] < v ? mins[2] : v;
+		if (out) *out = v;
+		break;
+	}
+	case TRG_PHASE_INTEGRATE:
+		if (comp == TRG_COMP_HYDRO) hydro_fluxes(c);
+		else if (comp == TRG_COMP_RAD) rad_integrate(c, 1.0);
+		else if (comp == TRG_COMP_THERMO) LAUNCH(k_thermo_integrate_fp64, c->P.N, 256, c->P, c->S, 1.0);
+		break;
+	case TRG_PHASE_SOURCES:
+		if (comp == TRG_COMP_HYDRO)
+			LAUNCH(k_hydro_update_fp64, c->P.N, 256, c->P, c->S, 1.0, (const double*)c->S.U, c->S.U, 1);
+		else if (comp == TRG_COMP_RAD) LAUNCH(k_rad_update_fp64, c->P.N, 256, c->P, c->S, 1.0, 1);
+		else if (comp == TRG_COMP_THERMO) LAUNCH(k_thermo_update_fp64, c->P.N, 256, c->P, c->S, 1.0, 1);
+		break;
+	case TRG_PHASE_Q_FROM_U:
+		q_from_u(c, c->S.U, 1);
+		break;
+	case TRG_PHASE_ADVANCE:
+		LAUNCH(k_advance_fp64, c->P.N, 256, c->P, c->S, dt);
+		break;
+	default:
+		return set_error(c, TRG_ERR_ARG, "unknown phase");
+	}
+	return check_device_error(c);
+}
+
+int trg_get_state(trg_ctx* c, double* U, double* Q, double* R, double* T, double* Tmin) {
+	if (!c) return TRG_ERR_ARG;
+	const long long N = c->P.N;
+	cudaStream_t st = c->stream;
+	if (U) CUDA_TRY(cudaMemcpyAsync(U, c->S.U, 7 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
+	if (Q) CUDA_TRY(cudaMemcpyAsync(Q, c->S.Q, 7 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
+	if (R) CUDA_TRY(cudaMemcpyAsync(R, c->S.R, 6 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
+	if (T) CUDA_TRY(cudaMemcpyAsync(T, c->S.T, 4 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
+	if (Tmin) CUDA_TRY(cudaMemcpyAsync(Tmin, c->S.Tmin, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+	CUDA_TRY(cudaStreamSynchronize(st));
+	return TRG_OK;
+}
+
+int trg_set_conserved(trg_ctx* c, const double* U) {
+	if (!c || !U) return TRG_ERR_ARG;
+	CUDA_TRY(cudaMemcpyAsync(c->S.U, U, 7 * c->P.N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+	return TRG_OK;
+}
+
+int trg_synchronize(trg_ctx* c) {
+	if (!c) return TRG_ERR_ARG;
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	return check_device_error(c);
+}
+
+double trg_time(const trg_ctx* c) {
+	if (!c || !c->S.scal) return 0;
+	double t = 0;
+	cudaStreamSynchronize(c->stream);
+	cudaMemcpy(&t, c->S.scal + 1, sizeof(double), cudaMemcpyDeviceToHost);
+	return t;
+}
+
+double trg_dt_max(const trg_ctx* c) { return c ? c->hs.dt_max : 0; }
+long trg_ncells(const trg_ctx* c) { return c ? (long)c->P.N : 0; }
+long long trg_kernel_launches(const trg_ctx* c) { return c ? c->launches : 0; }
+const char* trg_last_error(const trg_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+void trg_destroy(trg_ctx* c) {
+	if (!c) return;
+	if (c->stream) cudaStreamSynchronize(c->stream);
+	for (void* p : c->allocs) cudaFree(p);
+	if (c->stream) cudaStreamDestroy(c->stream);
+	delete c;
+}
+
+}  // extern "C"

@@ -1,0 +1,971 @@
+// FP64 kernels of the operator-split step (the plain-FP64 form).
+//
+// Compiled with --fmad=false: every kernel reproduces the reference's FP64
+// arithmetic in the reference's operation order, so that results match the
+// CPU oracle to the last bit except where a CUDA transcendental (exp, log,
+// pow) differs from the host libm by an ulp.
+//
+// Layout: SoA, field-major, interior cells only, flat index i + nx*(j + ny*k).
+// Ghost cells are not stored: boundary conditions are applied while loading
+// (Grid::applyBCs, Grid.cpp:649-836, restated by map_ghost below).
+#include "trg_device.cuh"
+#include "trg_kernels.h"
+
+namespace trg {
+
+// ------------------------------------------------------------------ limiters
+__device__ __forceinline__ double minmod(double a, double b) { return (a * b > 0) ? (fabs(a) < fabs(b) ? a : b) : 0; }
+__device__ __forceinline__ double maxmod(double a, double b) { return (a * b > 0) ? (fabs(a) > fabs(b) ? a : b) : 0; }
+
+// SlopeLimiter::calculate variants, SlopeLimiter.cpp:5-54.
+__device__ __forceinline__ double limiter(int kind, double a, double b) {
+	switch (kind) {
+	case 0: return minmod((a + b) / 2.0, minmod(2.0 * a, 2.0 * b));
+	case 1: return maxmod(minmod(b, 2.0 * a), minmod(2.0 * b, a));
+	case 2: return minmod(a, b);
+	case 3: return maxmod(a, b);
+	case 4: {
+		if (b == 0) return 0;
+		double r = fabs(a / b);
+		return (a + b * r) / (1.0 + r);
+	}
+	case 5: return (a * b <= 1.0e-30) ? 0 : 1.5 * b * (a * a + a * b) / (a * a + a * b + b * b);
+	default: return a * b <= 1.0e-30 ? 0 : a * b * (a + b) / (a * a + b * b);
+	}
+}
+
+// ----------------------------------------------------------- Riemann solvers
+// characteristicWaveSpeeds (Einfeldt), Riemann.cpp:27-42.
+__device__ __forceinline__ void wave_speeds(double a_l2, double a_r2, const double* Ql, const double* Qr, int dim,
+                                            double& Sl, double& Sr) {
+	double sqrtrho_l = sqrt(Ql[DEN]);
+	double sqrtrho_r = sqrt(Qr[DEN]);
+	double u_tilde = (sqrtrho_l * Ql[VEL + dim] + sqrtrho_r * Qr[VEL + dim]) / (sqrtrho_l + sqrtrho_r);
+	double nu2 = 0.5 * sqrtrho_r * sqrtrho_l / ((sqrtrho_l + sqrtrho_r) * (sqrtrho_l + sqrtrho_r));
+	double dsqrd = (sqrtrho_l * a_l2 + sqrtrho_r * a_r2) / (sqrtrho_l + sqrtrho_r);
+	dsqrd += nu2 * (Qr[VEL + dim] - Ql[VEL + dim]) * (Qr[VEL + dim] - Ql[VEL + dim]);
+	double d = sqrt(dsqrd);
+	Sl = u_tilde - d;
+	Sr = u_tilde + d;
+}
+
+// HartenLaxLeerContactSolver::solve, Riemann.cpp:52-104.
+__device__ void hllc(double* F, const double* Ql, const double* Qr, double a_l2, double a_r2, double gamma, int nd, int dim) {
+	double S_l, S_r;
+	wave_speeds(a_l2, a_r2, Ql, Qr, dim, S_l, S_r);
+	if (S_l >= 0) {
+		FfromQ(F, Ql, gamma, nd, dim);
+	} else if (S_r <= 0) {
+		FfromQ(F, Qr, gamma, nd, dim);
+	} else {
+		double S_c = Qr[PRE] - Ql[PRE];
+		S_c += Ql[DEN] * Ql[VEL + dim] * (S_l - Ql[VEL + dim]);
+		S_c -= Qr[DEN] * Qr[VEL + dim] * (S_r - Qr[VEL + dim]);
+		S_c /= (Ql[DEN] * (S_l - Ql[VEL + dim]) - Qr[DEN] * (S_r - Qr[VEL + dim]));
+		const double* Qlr = (S_c >= 0) ? Ql : Qr;
+		double S_lr = (S_c >= 0) ? S_l : S_r;
+		double U_lr[7] = {0, 0, 0, 0, 0, 0, 0}, F_lr[7] = {0, 0, 0, 0, 0, 0, 0}, U_c[7] = {0, 0, 0, 0, 0, 0, 0};
+		UfromQ(U_lr, Qlr, gamma, nd);
+		FfromQ(F_lr, Qlr, gamma, nd, dim);
+		double A_lr = Qlr[DEN] * (S_lr - Qlr[VEL + dim]) / (S_lr - S_c);
+		U_c[DEN] = A_lr;
+		for (int id = 0; id < nd; ++id) U_c[VEL + id] = A_lr * Qlr[VEL + id];
+		U_c[VEL + dim] = A_lr * S_c;
+		U_c[PRE] = A_lr * ((U_lr[PRE] / Qlr[DEN]) +
+		                   (S_c - Qlr[VEL + dim]) * (S_c + Qlr[PRE] / (Qlr[DEN] * (S_lr - Qlr[VEL + dim]))));
+		U_c[HII] = A_lr * Qlr[HII];
+		U_c[ADV] = A_lr * Qlr[ADV];
+		for (int i = 0; i < NU; ++i) F[i] = F_lr[i] + S_lr * (U_c[i] - U_lr[i]);
+		if (nd < 3) F[VEL + 2] = 0;
+		if (nd < 2) F[VEL + 1] = 0;
+	}
+}
+
+// HartenLaxLeerSolver::solve, Riemann.cpp:108-140.
+__device__ void hll(double* F, const double* Ql, const double* Qr, double a_l2, double a_r2, double gamma, int nd, int dim) {
+	double S_l, S_r;
+	wave_speeds(a_l2, a_r2, Ql, Qr, dim, S_l, S_r);
+	if (S_r <= 0) {
+		FfromQ(F, Qr, gamma, nd, dim);
+	} else if (S_l >= 0) {
+		FfromQ(F, Ql, gamma, nd, dim);
+	} else {
+		double U_l[7] = {0, 0, 0, 0, 0, 0, 0}, U_r[7] = {0, 0, 0, 0, 0, 0, 0};
+		double F_l[7] = {0, 0, 0, 0, 0, 0, 0}, F_r[7] = {0, 0, 0, 0, 0, 0, 0};
+		UfromQ(U_l, Ql, gamma, nd);
+		UfromQ(U_r, Qr, gamma, nd);
+		FfromQ(F_l, Ql, gamma, nd, dim);
+		FfromQ(F_r, Qr, gamma, nd, dim);
+		for (int i = 0; i < NU; ++i)
+			F[i] = (S_r * F_l[i] - S_l * F_r[i] + S_l * S_r * (U_r[i] - U_l[i])) / (S_r - S_l);
+	}
+}
+
+// 3-vector helpers with the reduction order of the reference's vendored
+// Eigen 3.2.1 (x + (y + z) for dot/norm; v /= s multiplies by 1/s; matrix
+// coefficients accumulate (a + b) + c).
+__device__ __forceinline__ void cross3(const double* a, const double* b, double* r) {
+	r[0] = a[1] * b[2] - a[2] * b[1];
+	r[1] = a[2] * b[0] - a[0] * b[2];
+	r[2] = a[0] * b[1] - a[1] * b[0];
+}
+__device__ __forceinline__ double dot3(const double* a, const double* b) { return a[0] * b[0] + (a[1] * b[1] + a[2] * b[2]); }
+__device__ __forceinline__ double norm3(const double* a) { return sqrt(dot3(a, a)); }
+__device__ __forceinline__ void normalize3(double* a) {
+	double r = 1.0 / norm3(a);
+	a[0] *= r; a[1] *= r; a[2] *= r;
+}
+
+// getRotationFromA2B, Riemann.cpp:161-171 (Rodrigues: I + [v]x + (1-c)/s^2 [v]x^2).
+__device__ __forceinline__ void rotation_a2b(const double* A, const double* B, double R[3][3]) {
+	double v[3];
+	cross3(A, B, v);
+	double s = norm3(v);
+	double cc = dot3(A, B);
+	double vx[3][3] = {{0, -v[2], v[1]}, {v[2], 0, -v[0]}, {-v[1], v[0], 0}};
+	double k = (1.0 - cc) / (s * s);
+	double kvx[3][3];
+#pragma unroll
+	for (int i = 0; i < 3; ++i)
+#pragma unroll
+		for (int j = 0; j < 3; ++j) kvx[i][j] = k * vx[i][j];
+#pragma unroll
+	for (int i = 0; i < 3; ++i)
+#pragma unroll
+		for (int j = 0; j < 3; ++j) {
+			double prod = kvx[i][0] * vx[0][j] + kvx[i][1] * vx[1][j] + kvx[i][2] * vx[2][j];
+			R[i][j] = ((i == j ? 1.0 : 0.0) + vx[i][j]) + prod;
+		}
+}
+
+// rotate, Riemann.cpp:154-159.
+__device__ __forceinline__ void rotate(const double R[3][3], double* v) {
+	double x = v[VEL + 0], y = v[VEL + 1], z = v[VEL + 2];
+#pragma unroll
+	for (int i = 0; i < 3; ++i) v[VEL + i] = R[i][0] * x + R[i][1] * y + R[i][2] * z;
+}
+
+// RotatedHartenLaxLeerSolver::solve (Nishikawa & Kitamura 2008), Riemann.cpp:181-244.
+__device__ void rotated_hllc(double* F, const double* Ql, const double* Qr, double a_l2, double a_r2, double gamma, int nd,
+                             int dim) {
+	bool pureHLLC = false, pureHLL = false;
+	double d[3] = {dim == 0 ? 1.0 : 0.0, dim == 1 ? 1.0 : 0.0, dim == 2 ? 1.0 : 0.0};
+	double n1[3] = {Qr[VEL + 0] - Ql[VEL + 0], Qr[VEL + 1] - Ql[VEL + 1], Qr[VEL + 2] - Ql[VEL + 2]};
+	double n2[3] = {0, 0, 0}, t[3];
+	if (n1[dim] < 0)
+		for (int i = 0; i < 3; ++i) n1[i] = -1.0 * n1[i];
+	if (norm3(n1) < 1.0e-6)
+		pureHLLC = true;
+	else {
+		normalize3(n1);
+		cross3(n1, d, t);
+		if (norm3(t) == 0)
+			pureHLL = true;
+		else {
+			cross3(t, n1, n2);
+			if (norm3(n2) == 0)
+				pureHLL = true;
+			else {
+				if (n2[dim] < 0)
+					for (int i = 0; i < 3; ++i) n2[i] = -1.0 * n2[i];
+				normalize3(n2);
+				cross3(n2, d, t);
+				if (norm3(t) == 0) pureHLLC = true;
+			}
+		}
+	}
+	if (!pureHLLC && !pureHLL) {
+		double F1[7] = {0, 0, 0, 0, 0, 0, 0}, F2[7] = {0, 0, 0, 0, 0, 0, 0};
+		double QlR[7], QrR[7], Rm[3][3];
+		for (int i = 0; i < NU; ++i) { QlR[i] = Ql[i]; QrR[i] = Qr[i]; }
+		rotation_a2b(n1, d, Rm);
+		rotate(Rm, QlR);
+		rotate(Rm, QrR);
+		hll(F1, QlR, QrR, a_l2, a_r2, gamma, nd, dim);
+		rotation_a2b(d, n1, Rm);
+		rotate(Rm, QlR);
+		rotate(Rm, QrR);
+		rotate(Rm, F1);
+		rotation_a2b(n2, d, Rm);
+		rotate(Rm, QlR);
+		rotate(Rm, QrR);
+		hllc(F2, QlR, QrR, a_l2, a_r2, gamma, nd, dim);
+		rotation_a2b(d, n2, Rm);
+		rotate(Rm, F2);
+		double w1 = fabs(dot3(d, n1)), w2 = fabs(dot3(d, n2));
+		for (int iu = 0; iu < NU; ++iu) F[iu] = w1 * F1[iu] + w2 * F2[iu];
+	} else if (pureHLL)
+		hll(F, Ql, Qr, a_l2, a_r2, gamma, nd, dim);
+	else
+		hllc(F, Ql, Qr, a_l2, a_r2, gamma, nd, dim);
+}
+
+// ------------------------------------------------------------- hydro faces
+// Ghost position p (< 0 or >= n) along dim -> interior source index and the
+// velocity rule of Grid::applyBCs (Grid.cpp:649-836).  Layer k = 1 is adjacent.
+__device__ __forceinline__ void load_line(const Params& P, const double* __restrict__ Q, long long base, long long stride,
+                                          int n, int dim, int pos, double* q) {
+	int src = pos, cond = -1, side = 0;
+	if (pos < 0) {
+		int k = -pos;
+		cond = P.lbc[dim];
+		src = cond == BC_PERIODIC ? n - k : (cond == BC_REFLECTING ? k : 0);
+	} else if (pos >= n) {
+		int k = pos - n + 1;
+		cond = P.rbc[dim];
+		side = 1;
+		src = cond == BC_PERIODIC ? k - 1 : (cond == BC_REFLECTING ? n - 1 - k : n - 1);
+	}
+	long long id = base + (long long)src * stride;
+#pragma unroll
+	for (int f = 0; f < NU; ++f) q[f] = __ldg(&Q[(long long)f * P.N + id]);
+	if (cond >= 0) {
+		double v = q[VEL + dim];
+		if (cond == BC_INFLOW) {
+			if (side == 0 ? v < 0 : v > 0) q[VEL + dim] = -1.0 * v;
+		} else if (cond == BC_OUTFLOW) {
+			if (side == 0 ? v > 0 : v < 0) q[VEL + dim] = -1.0 * v;
+		} else if (cond == BC_REFLECTING) {
+			q[VEL + dim] = -v;
+		}
+	}
+}
+
+// Hydrodynamics::calcFluxes (Hydro.cpp:91-115) with the reconstruction of
+// Hydro.cpp:44-67: one thread per face along dim; face f lies between line
+// positions f-1 and f.
+__global__ void __launch_bounds__(128) k_faces_fp64(Params P, State S, int dim) {
+	long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (t >= S.nfaces[dim]) return;
+	int n = ncell(P, dim), f;
+	long long base, stride;
+	if (dim == 0) {
+		f = (int)(t % (n + 1));
+		long long rest = t / (n + 1);
+		base = rest * P.nx;
+		stride = 1;
+	} else if (dim == 1) {
+		int i = (int)(t % P.nx);
+		long long rest = t / P.nx;
+		f = (int)(rest % (n + 1));
+		long long k = rest / (n + 1);
+		base = i + (long long)P.nx * P.ny * k;
+		stride = P.nx;
+	} else {
+		long long plane = (long long)P.nx * P.ny;
+		f = (int)(t / plane);
+		base = t % plane;
+		stride = plane;
+	}
+	double Ls[7], Rs[7], Fv[7];
+	if (P.order == 1) {
+		double a[7], b[7], c[7], e[7];
+		load_line(P, S.Q, base, stride, n, dim, f - 2, a);
+		load_line(P, S.Q, base, stride, n, dim, f - 1, b);
+		load_line(P, S.Q, base, stride, n, dim, f, c);
+		load_line(P, S.Q, base, stride, n, dim, f + 1, e);
+#pragma unroll
+		for (int iq = 0; iq < NU; ++iq) {
+			// QR of the cell at f-1 and QL of the cell at f (Hydro.cpp:44-50)
+			double sl = limiter(P.limiter, b[iq] - a[iq], c[iq] - b[iq]);
+			Ls[iq] = b[iq] + 0.5 * sl;
+			double sr = limiter(P.limiter, c[iq] - b[iq], e[iq] - c[iq]);
+			Rs[iq] = c[iq] - 0.5 * sr;
+		}
+	} else {
+		load_line(P, S.Q, base, stride, n, dim, f - 1, Ls);
+		load_line(P, S.Q, base, stride, n, dim, f, Rs);
+	}
+	double a_l2 = P.gamma * Ls[PRE] / Ls[DEN];
+	double a_r2 = P.gamma * Rs[PRE] / Rs[DEN];
+#pragma unroll
+	for (int i = 0; i < NU; ++i) Fv[i] = 0;
+	if (P.riemann == RS_HLLC) hllc(Fv, Ls, Rs, a_l2, a_r2, P.gamma, P.nd, dim);
+	else if (P.riemann == RS_HLL) hll(Fv, Ls, Rs, a_l2, a_r2, P.gamma, P.nd, dim);
+	else rotated_hllc(Fv, Ls, Rs, a_l2, a_r2, P.gamma, P.nd, dim);
+	if (Fv[HII] != Fv[HII]) atomicOr(S.err, ERRB_FLUX);
+	double* Fd = S.F[dim];
+	long long nf = S.nfaces[dim];
+#pragma unroll
+	for (int i = 0; i < NU; ++i) Fd[(long long)i * nf + t] = Fv[i];
+}
+
+__device__ __forceinline__ void face_ids(const Params& P, const int* ijk, int dim, long long& l, long long& r) {
+	if (dim == 0) {
+		l = ijk[0] + (long long)(P.nx + 1) * (ijk[1] + (long long)P.ny * ijk[2]);
+		r = l + 1;
+	} else if (dim == 1) {
+		l = ijk[0] + (long long)P.nx * (ijk[1] + (long long)(P.ny + 1) * ijk[2]);
+		r = l + P.nx;
+	} else {
+		l = ijk[0] + (long long)P.nx * (ijk[1] + (long long)P.ny * ijk[2]);
+		r = l + (long long)P.nx * P.ny;
+	}
+}
+
+// Hydrodynamics::updateSourceTerms (Hydro.cpp:117-156) with
+// Star::injectEnergyMomentum (Star.cpp:57-68) into udot[7].
+__device__ __forceinline__ void hydro_udot(const Params& P, const State& S, long long id, const int* ijk, const double* xc,
+                                           const double* Ubase, double* udot) {
+	double vol = cell_volume(P, xc[0]);
+#pragma unroll
+	for (int i = 0; i < NU; ++i) udot[i] = 0;
+	for (int dim = 0; dim < P.nd; ++dim) {
+		long long fl, fr;
+		face_ids(P, ijk, dim, fl, fr);
+		double al = face_area(P, xc, dim, 0), ar = face_area(P, xc, dim, 1);
+		const double* Fd = S.F[dim];
+		long long nf = S.nfaces[dim];
+#pragma unroll
+		for (int i = 0; i < NU; ++i) {
+			udot[i] += (al / vol) * Fd[(long long)i * nf + fl];
+			udot[i] -= (ar / vol) * Fd[(long long)i * nf + fr];
+		}
+	}
+	for (int i = 0; i < 3; ++i) {
+		double g = S.grav ? S.grav[(long long)i * P.N + id] : 0.0;
+		udot[VEL + i] += g;
+		udot[PRE] += FLD(S.Q, VEL + i, id) * g;
+	}
+	if (P.geometry == G_CYL) {
+		double r = P.dx[0] * xc[0];
+		udot[VEL + 0] += FLD(S.Q, PRE, id) / r;
+	} else if (P.geometry == G_SPH) {
+		double area1 = face_area(P, xc, 0, 1), area2 = face_area(P, xc, 0, 0);
+		double r = vol / (area1 - area2);
+		udot[VEL + 0] += FLD(S.Q, PRE, id) / r;
+	}
+	if (P.star_on && P.mdot != 0 && is_wind(P, id, ijk, xc)) {
+		udot[DEN] += P.mdot;
+		udot[PRE] += P.edot;
+		udot[HII] += (FLD(Ubase, HII, id) / FLD(Ubase, DEN, id)) * P.mdot;
+		udot[ADV] += P.mdot;
+	}
+}
+
+// Hydro update: UDOT from the face fluxes, then Fluid::advSolution (Fluid.cpp:80-87)
+// from Ubase and Fluid::fixSolution, written to Uout (may alias Ubase).
+// mode 1 accumulates UDOT into S.UDOT instead (component-phase interface).
+__global__ void __launch_bounds__(256) k_hydro_update_fp64(Params P, State S, double h, const double* Ubase, double* Uout,
+                                                          int mode) {
+	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	int ijk[3];
+	double xc[3], udot[7];
+	cell_ijk(P, id, ijk);
+	cell_xc(P, ijk, xc);
+	hydro_udot(P, S, id, ijk, xc, Ubase, udot);
+	if (mode == 1) {
+		for (int i = 0; i < NU; ++i) FLD(S.UDOT, i, id) += udot[i];
+		return;
+	}
+	double dt = h * S.scal[0];
+	double u[7];
+#pragma unroll
+	for (int i = 0; i < NU; ++i) u[i] = FLD(Ubase, i, id) + dt * udot[i];
+	if (!fix_solution(P, u)) atomicOr(S.err, ERRB_NAN);
+#pragma unroll
+	for (int i = 0; i < NU; ++i) FLD(Uout, i, id) = u[i];
+}
+
+// Fluid::globalQfromU (+ fixPrimitives), Fluid.cpp:138-165, with the Q half of
+// Torch::checkValues (Torch.cpp:420-443).
+__global__ void __launch_bounds__(256) k_q_from_u_fp64(Params P, State S, const double* Usrc, int fix) {
+	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	double u[7], q[7];
+#pragma unroll
+	for (int i = 0; i < NU; ++i) { u[i] = FLD(Usrc, i, id); q[i] = FLD(S.Q, i, id); }
+	QfromU(q, u, P.gamma, P.nd);
+	if (fix) fix_primitives(P, q, u[DEN]);
+	bool bad = q[DEN] == 0 || q[PRE] == 0;
+#pragma unroll
+	for (int i = 0; i < NU; ++i) {
+		bad |= (u[i] != u[i]) || isinf(u[i]);
+		FLD(S.Q, i, id) = q[i];
+	}
+	if (bad) atomicOr(S.err, ERRB_NAN);
+}
+
+// advSolution(dt) + fixSolution over the UDOT array (component-phase interface).
+__global__ void __launch_bounds__(256) k_advance_fp64(Params P, State S, double dt) {
+	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	double u[7];
+	for (int i = 0; i < NU; ++i) {
+		u[i] = FLD(S.U, i, id) + dt * FLD(S.UDOT, i, id);
+		FLD(S.UDOT, i, id) = 0;
+	}
+	if (!fix_solution(P, u)) atomicOr(S.err, ERRB_NAN);
+	for (int i = 0; i < NU; ++i) FLD(S.U, i, id) = u[i];
+}
+
+// ------------------------------------------------------------------ radiation
+// Radiation.cpp:243-251.
+__device__ __forceinline__ double photoionisation_rate(double nHI, double T, double delT, double shellVol, double photonRate) {
+	if (nHI == 0 || shellVol == 0) return 0.0;
+	double emT = exp(-T);
+	double emdT = exp(-delT);
+	return photonRate * emT * (1.0 - emdT) / (nHI * shellVol);
+}
+
+// Voronov (1997) fit, Radiation.cpp:231-237.
+__device__ __forceinline__ double collisional_ionisation_rate(const Params& P, double T) {
+	if (!P.collisions_on || T < 5.0e3) return 0.0;
+	double U = P.voronov_DE / T;
+	return P.voronov_A * (1. + P.voronov_P * sqrt(U)) * exp(P.voronov_K * log(U) - U) / (P.voronov_X + U);
+}
+
+// Radiation::doric, Radiation.cpp:140-179.
+__device__ __forceinline__ void doric(double dt, double& HII_avg, double& HII, double Api, double nHII_aB, double nHII_Aci) {
+	double xeq, inv_ti, epsilon = 1.0e-8;
+	double HII_old = HII;
+	if (nHII_aB == 0.0) xeq = 1.0;
+	else xeq = (Api + nHII_Aci) / (Api + nHII_Aci + nHII_aB);
+	inv_ti = Api + nHII_Aci + nHII_aB;
+	if (dt * inv_ti < 1.0e-8) {
+		HII = HII_old;
+		HII = smax(smin(HII, 1.0), 0.0);
+		if (1.0 - HII < epsilon) HII = 1.0 - epsilon;
+		HII_avg = HII;
+	} else {
+		double e = exp(-dt * inv_ti);
+		HII = xeq + (HII_old - xeq) * e;
+		HII = smax(smin(HII, 1.0), 0.0);
+		if (1.0 - HII < epsilon) HII = 1.0 - epsilon;
+		HII_avg = xeq + (HII_old - xeq) * (1.0 - e) / (dt * inv_ti);
+		HII_avg = smax(smin(HII_avg, 1.0), 0.0);
+		if (1.0 - HII_avg < epsilon) HII_avg = 1.0 - epsilon;
+	}
+}
+
+// C2-Ray upwind neighbours and weights (Grid::calculateNearestNeighbours,
+// Grid.cpp:922-952) computed on the fly.  A neighbour outside the interior
+// (a ghost cell or none in the reference) contributes zero optical depth and
+// is returned as -1.
+__device__ __forceinline__ void neighbours(const Params& P, const int* ijk, const double* xc, long long* nb, double* w) {
+	int plane = 0;
+	double dmax = 0;
+	for (int i = 0; i < P.nd; ++i) {
+		double dd = fabs(xc[i] - P.sxc[i]);
+		if (dd > dmax) { dmax = dd; plane = i; }
+	}
+	int irot[3] = {(plane + 1) % 3, (plane + 2) % 3, plane % 3};
+	double d[3];
+	int s[3], LR[3];
+	for (int i = 0; i < 3; i++) {
+		d[i] = xc[irot[i]] - P.sxc[irot[i]];
+		s[i] = d[i] < -1.0 / 10.0 ? -1 : 1;
+		LR[i] = fabs(d[i]) < 1.0 / 10.0 ? 0 : s[i];
+	}
+	const int off[4][3] = {{0, 0, -LR[2]}, {0, -LR[1], -LR[2]}, {-LR[0], 0, -LR[2]}, {-LR[0], -LR[1], -LR[2]}};
+	for (int n = 0; n < 4; ++n) {
+		int t[3] = {ijk[0], ijk[1], ijk[2]};
+		for (int r = 0; r < 3; ++r) t[irot[r]] += off[n][r];
+		bool in = t[0] >= 0 && t[0] < P.nx && t[1] >= 0 && t[1] < P.ny && t[2] >= 0 && t[2] < P.nz;
+		nb[n] = in ? flat_id(P, t[0], t[1], t[2]) : -1;
+	}
+	double ic0 = (int)xc[irot[0]] - 0.5 * (s[2] * d[0] / d[2]);
+	double ic1 = (int)xc[irot[1]] - 0.5 * (s[2] * d[1] / d[2]);
+	double delta0 = fabs(2.0 * ic0 - 2.0 * (int)xc[irot[0]] + s[0]);
+	double delta1 = fabs(2.0 * ic1 - 2.0 * (int)xc[irot[1]] + s[1]);
+	w[0] = (fabs(d[2]) > 0.9) ? delta0 * delta1 : 0;
+	w[1] = ((fabs(d[1]) > 0.9) && (fabs(d[2]) > 0.9)) ? delta0 * (1.0 - delta1) : 0;
+	w[2] = ((fabs(d[0]) > 0.9) && (fabs(d[2]) > 0.9)) ? (1.0 - delta0) * delta1 : 0;
+	w[3] = ((fabs(d[0]) > 0.9) && (fabs(d[1]) > 0.9) && (fabs(d[2]) > 0.9)) ? (1.0 - delta0) * (1.0 - delta1) : 0;
+}
+
+__device__ __forceinline__ double dist2_cells(const Params& P, const double* xc) {
+	double d2 = 0;
+	for (int i = 0; i < P.nd; ++i) d2 += (xc[i] - P.sxc[i]) * (xc[i] - P.sxc[i]);
+	return d2;
+}
+
+// Radiation::updateTauSC, Radiation.cpp:353-373.
+__device__ __forceinline__ double tau_sc(const Params& P, const State& S, const long long* nb, const double* w0, int rt, int rd) {
+	double tau[4] = {0, 0, 0, 0}, w[4];
+	for (int i = 0; i < 4; ++i) {
+		if (nb[i] >= 0) tau[i] = FLD(S.R, rt, nb[i]) + FLD(S.R, rd, nb[i]);
+		w[i] = w0[i] / smax(P.tau0, tau[i]);
+	}
+	double sum_w = w[0] + w[1] + w[2] + w[3];
+	double newtau = 0.0;
+	for (int i = 0; i < 4; ++i) {
+		w[i] = w[i] / sum_w;
+		newtau += w[i] * tau[i];
+	}
+	return newtau;
+}
+
+// Wind cells of Radiation::transferRadiation, Radiation.cpp:590-598.
+__global__ void k_rad_wind_reset(Params P, State S, const int* __restrict__ cells, int count) {
+	int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= count) return;
+	long long id = cells[t];
+	FLD(S.R, R_TAU, id) = 0;
+	FLD(S.R, R_TAU_A, id) = 0;
+	FLD(S.R, R_DTAU, id) = 0;
+	FLD(S.R, R_DTAU_A, id) = 0;
+	FLD(S.Q, HII, id) = 1;
+	FLD(S.R, R_HII_A, id) = 1;
+}
+
+// One shell of the causal sweep of Radiation::transferRadiation
+// (Radiation.cpp:600-612): tau interpolation, the implicit HII update
+// (update_HIIfrac, :375-478) and the new optical depths.  Every cell of a
+// shell reads only cells of inner shells, so a shell is fully parallel.
+__global__ void __launch_bounds__(128) k_rad_shell_fp64(Params P, State S, const int* __restrict__ cells, int count,
+                                                       double h, const double* __restrict__ hii_start) {
+	int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= count) return;
+	long long id = cells[t];
+	int ijk[3];
+	double xc[3];
+	cell_ijk(P, id, ijk);
+	cell_xc(P, ijk, xc);
+	double dist2 = dist2_cells(P, xc);
+	if (dist2 > 0.95) {
+		long long nb[4];
+		double w[4];
+		neighbours(P, ijk, xc, nb, w);
+		FLD(S.R, R_TAU, id) = tau_sc(P, S, nb, w, R_TAU, R_DTAU);
+		FLD(S.R, R_TAU_A, id) = tau_sc(P, S, nb, w, R_TAU_A, R_DTAU_A);
+	} else {
+		FLD(S.R, R_TAU, id) = 0;
+		FLD(S.R, R_TAU_A, id) = 0;
+	}
+	const double dt = h * S.scal[0];
+	// Radiation::isStar (Radiation.cpp:682-684): z compares an int with a double.
+	bool star = (int)xc[0] == (int)P.sxc[0] && (int)xc[1] == (int)P.sxc[1] && (double)(int)xc[2] == P.sxc[2];
+	double q_den = FLD(S.Q, DEN, id), q_pre = FLD(S.Q, PRE, id), q_hii = FLD(S.Q, HII, id);
+	double ds = S.ds[id];
+	if (star) {
+		FLD(S.R, R_HEAT, id) = 0;
+		FLD(S.Q, HII, id) = 1;
+		FLD(S.R, R_HII_A, id) = 1;
+	} else {
+		double n_H = P.X * q_den / P.hydrogenMass;
+		double A_pi = 0;
+		double x_new = q_hii;
+		double HII_avg = hii_start ? hii_start[id] : x_new;
+		double T = calc_temperature(P, q_hii, q_pre, q_den);
+		double alphaB = spline_eval(S.tables->rad_recomb, T);
+		double A_ci = collisional_ionisation_rate(P, T);
+		double tau_avg = FLD(S.R, R_TAU_A, id);
+		double shellVol = S.shellVol[id];
+		double HII_avg_old;
+		int niter = 0, miter = 0;
+		bool converged = false;
+		while (!converged) {
+			niter++;
+			HII_avg_old = HII_avg;
+			x_new = q_hii;
+			double dtau_avg = (1.0 - HII_avg) * n_H * P.photoIonXsec * ds;
+			double nHI = (1.0 - HII_avg) * n_H;
+			A_pi = photoionisation_rate(nHI, tau_avg, dtau_avg, shellVol, P.photonRate);
+			double nHII_aB = HII_avg * n_H * alphaB;
+			double nHII_Aci = HII_avg * n_H * A_ci;
+			doric(dt, HII_avg, x_new, A_pi, nHII_aB, nHII_Aci);
+			if ((fabs((HII_avg - HII_avg_old) / HII_avg) < 1.0e-3 || (HII_avg < 1.0e-5) || A_pi == 0)) converged = true;
+			if (niter > 10005) {
+				miter++;
+				niter = 0;
+				HII_avg = 0.5 * (HII_avg + HII_avg_old);
+			}
+			if (miter > 5 || x_new != x_new) {
+				atomicOr(S.err, ERRB_PICARD);
+				break;
+			}
+		}
+		FLD(S.R, R_HII_A, id) = HII_avg;
+		FLD(S.Q, HII, id) = x_new;
+		if (x_new > 0.001) FLD(S.Q, ADV, id) = 1;
+	}
+	double nH = P.X * q_den / P.hydrogenMass;
+	FLD(S.R, R_DTAU, id) = (1.0 - FLD(S.Q, HII, id)) * nH * P.photoIonXsec * ds;
+	FLD(S.R, R_DTAU_A, id) = (1.0 - FLD(S.R, R_HII_A, id)) * nH * P.photoIonXsec * ds;
+}
+
+// Star off: Radiation::transferRadiation else-branch (Radiation.cpp:638-650), interior cells.
+__global__ void k_rad_no_star_fp64(Params P, State S, double h) {
+	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	const double dt = h * S.scal[0];
+	double x_new = FLD(S.Q, HII, id), x_dummy = x_new;
+	double n_H = P.X * FLD(S.Q, DEN, id) / P.hydrogenMass;
+	double T = calc_temperature(P, FLD(S.Q, HII, id), FLD(S.Q, PRE, id), FLD(S.Q, DEN, id));
+	double nHII_aB = x_new * n_H * spline_eval(S.tables->rad_recomb, T);
+	double nHII_Aci = x_new * n_H * collisional_ionisation_rate(P, T);
+	doric(dt, x_new, x_dummy, 0, nHII_aB, nHII_Aci);
+	FLD(S.Q, HII, id) = x_new;
+}
+
+// Radiation::preTimeStepCalculations (photoheating), Radiation.cpp:257-296, non-wind cells.
+__global__ void __launch_bounds__(256) k_rad_heating_fp64(Params P, State S) {
+	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	int ijk[3];
+	double xc[3];
+	cell_ijk(P, id, ijk);
+	cell_xc(P, ijk, xc);
+	if (is_wind(P, id, ijk, xc)) return;
+	double q_hii = FLD(S.Q, HII, id), q_pre = FLD(S.Q, PRE, id), q_den = FLD(S.Q, DEN, id);
+	double Tmin = S.Tmin[id];
+	double n_H = (P.X * q_den / P.hydrogenMass);
+	double excessEnergy = P.photonEnergy - P.rydbergEnergy;
+	double T = calc_temperature(P, q_hii, q_pre, q_den);
+	double nHI = (1.0 - q_hii) * n_H;
+	double A_pi = photoionisation_rate(nHI, FLD(S.R, R_TAU, id), FLD(S.R, R_DTAU, id), S.shellVol[id], P.photonRate);
+	double photoion = n_H * (1.0 - q_hii) * A_pi * excessEnergy;
+	double rate_rc = spline_eval(S.tables->rad_cool, T);
+	double recombination = q_hii * q_hii * n_H * n_H * P.boltzmannConst * T * rate_rc;
+	double collisions = q_hii * (1.0 - q_hii) * n_H * n_H * collisional_ionisation_rate(P, T);
+	double rate = photoion - recombination - collisions;
+	double softrate = rate;
+	if (T < Tmin + 200 && rate < 0.0) softrate = smin(0.0, softrate * (T - Tmin) / 200.0);
+	softrate *= P.heating_amp;
+	FLD(S.R, R_HEAT, id) = softrate;
+	if (rate != rate) atomicOr(S.err, ERRB_NAN);
+}
+
+// Radiation::updateSourceTerms (Radiation.cpp:653-680) then advSolution + fixSolution.
+__global__ void __launch_bounds__(256) k_rad_update_fp64(Params P, State S, double h, int mode) {
+	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	const double dt = h * S.scal[0];
+	double u[7], udot[7] = {0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+	for (int i = 0; i < NU; ++i) u[i] = FLD(S.U, i, id);
+	if (P.star_on) {
+		double q_hii = FLD(S.Q, HII, id), q_den = FLD(S.Q, DEN, id), q_adv = FLD(S.Q, ADV, id);
+		if (P.coupling == CP_TTI) {
+			double mu_inv_new = P.X * (q_hii + 1.0) + (1.0 - P.X) * 0.25;
+			double T_new = P.THI + (P.THII - P.THI) * q_hii;
+			double pre_new = P.specificGasConstant * mu_inv_new * q_den * T_new;
+			double ke = 0.0;
+			for (int dim = 0; dim < P.nd; ++dim) ke += 0.5 * u[VEL + dim] * u[VEL + dim] / u[DEN];
+			double E_new = pre_new / (P.gamma - 1.0) + ke;
+			udot[PRE] += (E_new - u[PRE]) / dt;
+		} else if (P.coupling == CP_NEQ) {
+			udot[PRE] += FLD(S.R, R_HEAT, id);
+		}
+		udot[HII] += (q_hii * q_den - u[HII]) / dt;
+		udot[ADV] += (q_adv * q_den - u[ADV]) / dt;
+	}
+	if (mode == 1) {
+		for (int i = 0; i < NU; ++i) FLD(S.UDOT, i, id) += udot[i];
+		return;
+	}
+#pragma unroll
+	for (int i = 0; i < NU; ++i) u[i] = u[i] + dt * udot[i];
+	if (!fix_solution(P, u)) atomicOr(S.err, ERRB_NAN);
+#pragma unroll
+	for (int i = 0; i < NU; ++i) FLD(S.U, i, id) = u[i];
+}
+
+// ----------------------------------------------------------- thermodynamics
+// Henney et al. (2009) heating and cooling, Thermodynamics.cpp:113-211.
+__device__ __forceinline__ double th_imlc(const Params& P, double ne, double T) {
+	return P.imlc * P.z0 * ne * ne * exp(-P.T1 / T - (P.T2 / T) * (P.T2 / T));
+}
+__device__ __forceinline__ double th_nmlc(const Params& P, double ne, double nn, double T) {
+	return P.nmlc * P.z0 * ne * nn * exp(-P.T3 / T - (P.T4 / T) * (P.T4 / T));
+}
+__device__ __forceinline__ double th_ciec(const Params& P, double ne, double T) {
+	if (T > P.ciec_minT) {
+		double cie_rate = P.ciec * ne * ne * P.z0 * exp(-0.63 * log(T)) * (1.0 - exp(-pow(1.0e-5 * T, 1.63)));
+		double smoothing = smin(1.0, (T - 5.0e4) / (2.0e4));
+		return cie_rate * smoothing;
+	}
+	return 0;
+}
+__device__ __forceinline__ double th_nmc(const Params& P, double nH, double x, double T) {
+	double T0 = 70.0 + 220.0 * pow(nH / P.n0, 0.2);
+	return P.nmc * (1.0 - x) * (1.0 - x) * pow(nH, 1.6) * sqrt(T) * exp(-T0 / T);
+}
+__device__ __forceinline__ double th_cxhi(const Params& P, const State& S, double nH, double x, double T) {
+	double rate = spline_eval(S.tables->th_cxhi, log10(T));
+	return x * (1.0 - x) * nH * nH * exp((2.302585093 * rate) - ((T / P.cxhi_damp) * (T / P.cxhi_damp)));
+}
+__device__ __forceinline__ double th_fuvh(const Params& P, double nH, double Av, double F) {
+	return P.fuvh_a * nH * F * exp(-1.9 * Av) / (P.fuvh_b + P.fuvh_c * F * exp(-1.9 * Av) / nH);
+}
+__device__ __forceinline__ double th_irh(const Params& P, double nH, double Av, double F) {
+	return P.irh_a * nH * F * exp(-0.05 * Av) * exp(-2.0 * log(1.0 + P.irh_b / nH));
+}
+__device__ __forceinline__ double soft_landing(double rate, double T, double T_min) {
+	double result = rate;
+	if (rate < 0.0) {
+		if (T <= T_min) result = 0;
+		else if (T <= T_min + 200) result = rate * (T - T_min) / 200;
+	}
+	return result;
+}
+__device__ __forceinline__ double th_cooling(const Params& P, const State& S, double heat, double ne, double nn, double nH,
+                                             double x, double T) {
+	double r = heat;
+	r -= th_imlc(P, ne, T);
+	r -= th_nmlc(P, ne, nn, T);
+	r -= th_cxhi(P, S, nH, x, T);
+	r -= th_ciec(P, ne, T);
+	r -= th_nmc(P, nH, x, T);
+	return r;
+}
+
+// One shell of Thermodynamics::rayTrace / updateColDen (Thermodynamics.cpp:339-417).
+__global__ void __launch_bounds__(128) k_colden_shell_fp64(Params P, State S, const int* __restrict__ cells, int count) {
+	int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= count) return;
+	long long id = cells[t];
+	int ijk[3];
+	double xc[3];
+	cell_ijk(P, id, ijk);
+	cell_xc(P, ijk, xc);
+	double dist2 = dist2_cells(P, xc);
+	double newcolden = 0.0;
+	if (dist2 > 0.95 * 0.95) {
+		long long nb[4];
+		double w0[4], colden[4] = {0, 0, 0, 0}, w[4];
+		neighbours(P, ijk, xc, nb, w0);
+		for (int i = 0; i < 4; ++i) {
+			if (nb[i] >= 0) colden[i] = FLD(S.T, T_COL_DEN, nb[i]) + FLD(S.T, T_DCOL_DEN, nb[i]);
+			w[i] = colden[i] == 0 ? 0 : w0[i] / colden[i];
+		}
+		double sum_w = w[0] + w[1] + w[2] + w[3];
+		for (int i = 0; i < 4 && sum_w != 0; ++i) {
+			w[i] = w[i] / sum_w;
+			newcolden += w[i] * colden[i];
+		}
+	}
+	FLD(S.T, T_COL_DEN, id) = newcolden;
+	FLD(S.T, T_DCOL_DEN, id) = (FLD(S.Q, DEN, id) / P.hydrogenMass) * S.ds[id];
+}
+
+// Thermodynamics::preTimeStepCalculations rates, Thermodynamics.cpp:224-263, non-wind cells.
+__global__ void __launch_bounds__(256) k_thermo_rates_fp64(Params P, State S) {
+	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	int ijk[3];
+	double xc[3];
+	cell_ijk(P, id, ijk);
+	cell_xc(P, ijk, xc);
+	if (is_wind(P, id, ijk, xc)) return;
+	if (FLD(S.Q, ADV, id) < P.thermo_hii_switch) {
+		FLD(S.T, T_RATE, id) = 0;
+		return;
+	}
+	double q_den = FLD(S.Q, DEN, id), x = FLD(S.Q, HII, id), q_pre = FLD(S.Q, PRE, id);
+	double nH = P.X * q_den / P.hydrogenMass;
+	double ne = nH * (x);
+	double nn = nH * (1.0 - x);
+	double T = calc_temperature(P, x, q_pre, q_den);
+	double rsqrd = 0, F_FUV = 0;
+	if (P.star_on) {
+		for (int i = 0; i < P.nd; ++i) rsqrd += (xc[i] - P.sxc[i]) * (xc[i] - P.sxc[i]) * P.dx[i] * P.dx[i];
+		double Q_FUV = 0.5 * P.photonRate;
+		F_FUV = rsqrd != 0 ? Q_FUV / (1.2e7 * 4 * P.pi * rsqrd) : 0;
+	}
+	double Av_FUV = 1.086 * P.dustXsec * FLD(S.T, T_COL_DEN, id);
+	double rate = 0;
+	rate += th_fuvh(P, nH, Av_FUV, F_FUV);
+	rate += th_irh(P, nH, Av_FUV, F_FUV);
+	rate += P.crh * nH;
+	FLD(S.T, T_HEAT, id) = rate;
+	rate = th_cooling(P, S, rate, ne, nn, nH, x, T);
+	rate = soft_landing(rate, T, S.Tmin[id]);
+	FLD(S.T, T_RATE, id) = P.heating_amp * rate;
+}
+
+// Thermodynamics::integrate (pressure subcycling), Thermodynamics.cpp:266-337, non-wind cells.
+__global__ void __launch_bounds__(256) k_thermo_integrate_fp64(Params P, State S, double h) {
+	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N || !P.thermo_subcycling) return;
+	int ijk[3];
+	double xc[3];
+	cell_ijk(P, id, ijk);
+	cell_xc(P, ijk, xc);
+	if (is_wind(P, id, ijk, xc)) return;
+	if (FLD(S.Q, ADV, id) < P.thermo_hii_switch) {
+		FLD(S.T, T_RATE, id) = 0;
+		return;
+	}
+	const double dt = h * S.scal[0];
+	double qden = FLD(S.Q, DEN, id), qpre = FLD(S.Q, PRE, id), x = FLD(S.Q, HII, id);
+	double Tmin = S.Tmin[id];
+	double rate0 = FLD(S.T, T_RATE, id), heat = FLD(S.T, T_HEAT, id);
+	double nH = P.X * qden / P.hydrogenMass;
+	double ne = nH * (x);
+	double nn = nH * (1.0 - x);
+	double dti = fabs(0.10 * FLD(S.U, PRE, id) / rate0);
+	double mu_inv = P.X * (x + 1.0) + (1.0 - P.X) * 0.25;
+	double pre2temp = 1.0 / (mu_inv * P.specificGasConstant * qden);
+	double temp2pre = (mu_inv * P.specificGasConstant * qden);
+	double rate2dpre = smin(dt, dti) * (P.gamma - 1.0);
+	double dpre2rate = 1.0 / rate2dpre;
+	double pressure = qpre + rate0 * rate2dpre;
+	double subT = pressure * pre2temp;
+	if (pressure < P.pfloor || subT < Tmin) {
+		double pfl = smax(Tmin * temp2pre, P.pfloor);
+		subT = pfl * pre2temp;
+		pressure = pfl;
+	}
+	if (dt > dti) {
+		double dtdti = dt / dti;
+		int nsteps = dtdti - (int)dtdti > 0 ? (int)(dtdti + 1.0) : (int)(dtdti + 0.5);
+		--nsteps;
+		for (int i = 0; i < nsteps; ++i) {
+			double r = th_cooling(P, S, heat, ne, nn, nH, x, subT);
+			r = P.heating_amp * soft_landing(r, subT, Tmin);
+			pressure += r * rate2dpre;
+			subT = pressure * pre2temp;
+			if (pressure < P.pfloor || subT < Tmin) {
+				double pfl = smax(Tmin * temp2pre, P.pfloor);
+				subT = pfl * pre2temp;
+				pressure = pfl;
+			}
+		}
+	}
+	FLD(S.T, T_RATE, id) = (pressure - qpre) * dpre2rate;
+}
+
+// Thermodynamics::updateSourceTerms (Thermodynamics.cpp:478-485) then advSolution + fixSolution.
+__global__ void __launch_bounds__(256) k_thermo_update_fp64(Params P, State S, double h, int mode) {
+	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	int ijk[3];
+	double xc[3];
+	cell_ijk(P, id, ijk);
+	cell_xc(P, ijk, xc);
+	double udot_pre = 0;
+	if (!is_wind(P, id, ijk, xc)) {
+		udot_pre += FLD(S.T, T_RATE, id);
+		FLD(S.T, T_RATE, id) = 0;
+		FLD(S.T, T_HEAT, id) = 0;
+	}
+	if (mode == 1) {
+		FLD(S.UDOT, PRE, id) += udot_pre;
+		return;
+	}
+	const double dt = h * S.scal[0];
+	double u[7];
+#pragma unroll
+	for (int i = 0; i < NU; ++i) u[i] = FLD(S.U, i, id) + dt * (i == PRE ? udot_pre : 0.0);
+	if (!fix_solution(P, u)) atomicOr(S.err, ERRB_NAN);
+#pragma unroll
+	for (int i = 0; i < NU; ++i) FLD(S.U, i, id) = u[i];
+}
+
+// ----------------------------------------------------------------- time step
+__device__ __forceinline__ unsigned long long dbits(double v) { return (unsigned long long)__double_as_longlong(v); }
+
+__device__ __forceinline__ double block_min(double v) {
+	__shared__ double red[32];
+	for (int o = 16; o > 0; o >>= 1) v = smin(v, __shfl_down_sync(0xffffffffu, v, o));
+	int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+	if (lane == 0) red[wid] = v;
+	__syncthreads();
+	if (wid == 0) {
+		int nw = (blockDim.x + 31) >> 5;
+		v = lane < nw ? red[lane] : 1.0e308;
+		for (int o = 16; o > 0; o >>= 1) v = smin(v, __shfl_down_sync(0xffffffffu, v, o));
+	}
+	return v;
+}
+
+// Hydrodynamics::calculateTimeStep (Hydro.cpp:77-89), Radiation::calculateTimeStep
+// (Radiation.cpp:298-351) and Thermodynamics::calculateTimeStep
+// (Thermodynamics.cpp:463-476) as one pass.  Minima of positive doubles are
+// exact and order independent; they are combined with atomicMin on the bit
+// pattern.  first_cell: the first non-wind cell in causal order on the first
+// radiation call (the reference's static `once`), else -1.
+__global__ void __launch_bounds__(256) k_dt_reduce_fp64(Params P, State S, long long first_cell) {
+	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	double th = 1.0e308, tr = 1.0e308, tt = 1.0e308;
+	if (id < P.N) {
+		double q_den = FLD(S.Q, DEN, id), q_pre = FLD(S.Q, PRE, id), q_hii = FLD(S.Q, HII, id);
+		double inv_t = 0;
+		double ss = sqrt(P.gamma * q_pre / q_den);
+		for (int dim = 0; dim < P.nd; ++dim) inv_t += (fabs(FLD(S.Q, VEL + dim, id)) + ss) / P.dx[dim];
+		if (inv_t == 0) inv_t = 1.0 / P.dt_max;
+		th = 0.5 / inv_t;
+		int ijk[3];
+		double xc[3];
+		cell_ijk(P, id, ijk);
+		cell_xc(P, ijk, xc);
+		if (P.radiation_on && P.star_on && !is_wind(P, id, ijk, xc)) {
+			double dt_max = P.dt_max;
+			double dtc = dt_max, dt1 = dt_max, dt2 = dt_max, dt3 = dt_max, dt4 = dt_max;
+			if (P.coupling == CP_NEQ) {
+				double heat = FLD(S.R, R_HEAT, id);
+				if (heat != 0) dtc = fabs(FLD(S.U, PRE, id) / heat);
+			}
+			if (P.K1 != 0.0) {
+				double T = calc_temperature(P, q_hii, q_pre, q_den);
+				if (id == first_cell)
+					dt1 = P.K1 * P.hydrogenMass / (P.X * q_den * spline_eval(S.tables->rad_recomb, T));
+				else if (q_hii != 0)
+					dt1 = P.K1 * P.hydrogenMass / (P.X * q_den * q_hii * spline_eval(S.tables->rad_recomb, T));
+			}
+			if (P.K3 != 0.0 || P.K4 != 0.0) {
+				double nH = P.X * q_den / P.hydrogenMass;
+				double nHI = (1.0 - q_hii) * nH;
+				double A_pi = photoionisation_rate(nHI, FLD(S.R, R_TAU, id), FLD(S.R, R_DTAU, id), S.shellVol[id], P.photonRate);
+				double Tq = calc_temperature(P, q_hii, q_pre, q_den);
+				double A_ci = collisional_ionisation_rate(P, Tq);
+				double A_rr = spline_eval(S.tables->rad_recomb, Tq);
+				double fracRate = (1.0 - q_hii) * (A_pi + q_hii * nH * A_ci) - q_hii * q_hii * nH * A_rr;
+				if (P.K3 != 0.0 && fracRate != 0.0) dt3 = P.K3 * smax(0.05, 1.0 - q_hii) / fabs(fracRate);
+				if (P.K4 != 0.0 && fracRate != 0.0) dt4 = P.K4 * 1.0 / fabs(fracRate);
+			}
+			tr = smin(dt_max, smin(dtc, smin(dt1, smin(dt2, smin(dt3, dt4)))));
+			if (tr == 0.0 || tr != tr || isinf(tr)) atomicOr(S.err, ERRB_DT);
+		}
+		if (P.cooling_on) {
+			double rate = FLD(S.T, T_RATE, id);
+			if (rate != 0) {
+				double frac = P.thermo_subcycling ? 1.0 : 0.1;
+				tt = fabs(frac * FLD(S.U, PRE, id) / rate);
+			}
+		}
+	}
+	th = block_min(th);
+	__syncthreads();
+	tr = block_min(tr);
+	__syncthreads();
+	tt = block_min(tt);
+	if (threadIdx.x == 0) {
+		unsigned long long* slots = reinterpret_cast<unsigned long long*>(S.scal + 2);
+		atomicMin(&slots[0], dbits(th));
+		atomicMin(&slots[1], dbits(tr));
+		atomicMin(&slots[2], dbits(tt));
+	}
+}
+
+// Torch::calculateTimeStep + the dt of Torch::fullStep (Torch.cpp:304-339, :394).
+__global__ void k_dt_finalize(Params P, State S, double dt_next, int first_time, int step) {
+	double dt;
+	if (first_time) {
+		dt = P.dt_max * 1.0e-20;
+	} else {
+		double dt_hydro = smin(S.scal[2], P.dt_max);
+		double dt_rad = dt_hydro, dt_thermo = dt_hydro;
+		if (P.radiation_on) dt_rad = P.star_on ? smin(P.dt_max, S.scal[3]) : P.dt_max;
+		if (P.cooling_on) dt_thermo = smin(P.dt_max, S.scal[4]);
+		dt = smin(smin(dt_hydro, dt_rad), dt_thermo);
+	}
+	dt = smin(dt_next, dt);
+	S.scal[0] = dt;
+	if (S.dt_hist && step >= 0) S.dt_hist[step] = dt;
+}
+
+__global__ void k_time_advance(State S) { S.scal[1] += S.scal[0]; }
+
+__global__ void k_dt_reset(Params P, State S) {
+	unsigned long long big = (unsigned long long)__double_as_longlong(P.dt_max);
+	unsigned long long* slots = reinterpret_cast<unsigned long long*>(S.scal + 2);
+	slots[0] = big;
+	slots[1] = big;
+	slots[2] = big;
+}
+
+}  // namespace trg

@@ -1,0 +1,214 @@
+// Device-side types and FP64 physics shared by the kernels of torch_b200.
+//
+// Every routine restates a reference TORCH routine (cited beside it) with the
+// same operation order; the translation units that include this header are
+// compiled with --fmad=false so that each a*b+c rounds twice, as on the
+// reference's x86-64 build.  Transcendentals (exp, log, log10, pow) are CUDA's.
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "trg_types.h"
+
+namespace trg {
+
+#define FLD(a, f, i) ((a)[(long long)(f) * P.N + (i)])
+
+__device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
+
+__device__ __forceinline__ void cell_ijk(const Params& P, long long id, int* ijk) {
+	ijk[0] = (int)(id % P.nx);
+	ijk[1] = (int)((id / P.nx) % P.ny);
+	ijk[2] = (int)(id / ((long long)P.nx * P.ny));
+}
+__device__ __forceinline__ long long flat_id(const Params& P, int i, int j, int k) {
+	return i + (long long)P.nx * (j + (long long)P.ny * k);
+}
+// Grid::buildCells (Grid.cpp:525-548): centre at index + 0.5 for dims < nd, 0 beyond.
+__device__ __forceinline__ void cell_xc(const Params& P, const int* ijk, double* xc) {
+	for (int i = 0; i < 3; ++i) xc[i] = (double)ijk[i];
+	for (int i = 0; i < P.nd; ++i) xc[i] += 0.5;
+}
+__device__ __forceinline__ int ncell(const Params& P, int d) { return d == 0 ? P.nx : (d == 1 ? P.ny : P.nz); }
+
+// Grid::computeCellVolume, Grid.cpp:876-905.
+__device__ __forceinline__ double cell_volume(const Params& P, double rc) {
+	const double PI = 3.14159265359;
+	double volume = 0, r1, r2;
+	if (P.geometry == G_CART) {
+		volume = 1.0;
+		for (int i = 0; i < P.nd; ++i) volume *= P.dx[i];
+	} else if (P.geometry == G_CYL) {
+		r2 = rc * P.dx[0] + 0.5 * P.dx[0];
+		r1 = rc * P.dx[0] - 0.5 * P.dx[0];
+		volume = PI * (r2 - r1) * (r2 + r1);
+		if (P.nd >= 2) volume *= P.dx[1];
+	} else if (P.geometry == G_SPH) {
+		r2 = rc * P.dx[0] + 0.5 * P.dx[0];
+		r1 = rc * P.dx[0] - 0.5 * P.dx[0];
+		volume = 4.0 * PI * (r2 - r1) * (r2 * r2 + r1 * r2 + r1 * r1) / 3.0;
+	}
+	return volume;
+}
+
+// Grid::computeJoinArea, Grid.cpp:846-874.
+__device__ __forceinline__ double join_area(const Params& P, const double* xj, int dim) {
+	const double PI = 3.14159265359;
+	double area = 0, r1, r2;
+	if (P.geometry == G_CART) {
+		area = 1.0;
+		for (int i = 0; i < P.nd; ++i)
+			if (i != dim) area *= P.dx[i];
+	} else if (P.geometry == G_CYL) {
+		if (dim == 0) {
+			r1 = xj[0] * P.dx[0];
+			area = 2.0 * PI * r1;
+			if (P.nd >= 2) area *= P.dx[1];
+		} else if (dim == 1) {
+			r1 = xj[0] * P.dx[0] - 0.5 * P.dx[0];
+			r2 = xj[0] * P.dx[0] + 0.5 * P.dx[0];
+			area = PI * (r2 - r1) * (r2 + r1);
+		}
+	} else if (P.geometry == G_SPH) {
+		r1 = xj[0] * P.dx[0];
+		area = 4.0 * PI * r1 * r1;
+	}
+	return area;
+}
+
+// Face on the left (side 0) or right (side 1) of a cell along dim; the join
+// coordinate is the right-hand cell's centre minus half a cell (Grid.cpp:405-411).
+__device__ __forceinline__ double face_area(const Params& P, const double* xc, int dim, int side) {
+	double xj[3] = {xc[0], xc[1], xc[2]};
+	xj[dim] += side ? 0.5 : -0.5;
+	return join_area(P, xj, dim);
+}
+
+// Fluid::initialiseGrid wind test, Fluid.cpp:41-53.
+__device__ __forceinline__ bool is_wind(const Params& P, long long id, const int* ijk, const double* xc) {
+	double dist2 = 0;
+	for (int i = 0; i < P.nd; ++i)
+		dist2 += ((int)xc[i] - P.star_pos[i]) * (xc[i] - P.star_pos[i]);
+	return dist2 <= (double)(P.wind_radius * P.wind_radius) || id == P.star_cell;
+}
+
+// ---------------------------------------------------------------- algebra
+// GridCell.cpp:163-213.
+__device__ __forceinline__ void UfromQ(double* u, const double* q, double gamma, int nd) {
+	double ke = 0;
+	u[DEN] = q[DEN];
+	for (int dim = 0; dim < nd; ++dim) {
+		u[VEL + dim] = q[VEL + dim] * q[DEN];
+		ke += 0.5 * q[DEN] * q[VEL + dim] * q[VEL + dim];
+	}
+	u[PRE] = q[PRE] / (gamma - 1.0) + ke;
+	u[HII] = q[HII] * q[DEN];
+	u[ADV] = q[ADV] * q[DEN];
+}
+
+__device__ __forceinline__ void QfromU(double* q, const double* u, double gamma, int nd) {
+	q[DEN] = u[DEN];
+	double ke = 0;
+	for (int dim = 0; dim < nd; ++dim) {
+		q[VEL + dim] = u[VEL + dim] / u[DEN];
+		ke += 0.5 * u[VEL + dim] * u[VEL + dim] / u[DEN];
+	}
+	q[PRE] = (u[PRE] - ke) * (gamma - 1.0);
+	q[HII] = u[HII] / u[DEN];
+	q[ADV] = u[ADV] / u[DEN];
+}
+
+__device__ __forceinline__ void FfromQ(double* f, const double* q, double gamma, int nd, int dim) {
+	f[DEN] = q[DEN] * q[VEL + dim];
+	double ke = 0;
+	for (int id = 0; id < nd; ++id) {
+		ke += q[VEL + id] * q[VEL + id];
+		int c = (dim + id) % nd;
+		f[VEL + c] = q[DEN] * q[VEL + c] * q[VEL + dim];
+	}
+	ke *= 0.5 * q[DEN];
+	f[VEL + dim] += q[PRE];
+	double g2 = gamma / (gamma - 1.0);
+	f[PRE] = q[VEL + dim] * (g2 * q[PRE] + ke);
+	f[HII] = q[DEN] * q[VEL + dim] * q[HII];
+	f[ADV] = q[DEN] * q[VEL + dim] * q[ADV];
+}
+
+// Fluid::calcTemperature, Fluid.cpp:71-74.
+__device__ __forceinline__ double calc_temperature(const Params& P, double hii, double pre, double den) {
+	double mu_inv = P.X * (hii + 1.0) + (1.0 - P.X) * 0.25;
+	return (pre / den) * (1.0 / mu_inv) / P.specificGasConstant;
+}
+
+// Fluid::fixPrimitives for one cell, Fluid.cpp:138-150 (floor uses U[DEN]).
+__device__ __forceinline__ void fix_primitives(const Params& P, double* q, double u_den) {
+	q[HII] = smax(smin(q[HII], 1.0), 0.0);
+	q[ADV] = smax(smin(q[ADV], 1.0), 0.0);
+	q[DEN] = smax(q[DEN], P.dfloor);
+	q[PRE] = smax(q[PRE], P.pfloor);
+	double mu_inv = P.X * (q[HII] + 1.0) + (1.0 - P.X) * 0.25;
+	double temperature = q[PRE] / (mu_inv * P.specificGasConstant * q[DEN]);
+	if (temperature < P.tfloor)
+		q[PRE] = mu_inv * P.specificGasConstant * u_den * P.tfloor;
+}
+
+// Fluid::fixSolution for one cell, Fluid.cpp:89-136.  Returns false on the
+// conditions under which the reference throws.
+__device__ __forceinline__ bool fix_solution(const Params& P, double* u) {
+	if (!isfinite(u[DEN]) || !isfinite(u[PRE])) return false;
+	double hii = smax(smin(u[HII] / u[DEN], 1.0), 0.0);
+	double adv = smax(smin(u[ADV] / u[DEN], 1.0), 0.0);
+	double v[3] = {0, 0, 0};
+	double den = smax(u[DEN], P.dfloor);
+	for (int dim = 0; dim < P.nd; ++dim) v[dim] = u[VEL + dim] / u[DEN];
+	double ke = 0.0;
+	for (int dim = 0; dim < P.nd; ++dim) ke += v[dim] * v[dim];
+	ke *= 0.5 * u[DEN];
+	double pre = (u[PRE] - ke) * (P.gamma - 1.0);
+	ke *= den / u[DEN];
+	if (pre < P.pfloor) pre = P.pfloor;
+	double mu_inv = P.X * (hii + 1.0) + (1.0 - P.X) * 0.25;
+	double temperature = pre / (mu_inv * P.specificGasConstant * den);
+	if (temperature < P.tfloor) pre = mu_inv * P.specificGasConstant * den * P.tfloor;
+	u[DEN] = den;
+	u[PRE] = pre / (P.gamma - 1.0) + ke;
+	u[HII] = hii * den;
+	u[ADV] = adv * den;
+	for (int dim = 0; dim < P.nd; ++dim) u[VEL + dim] = den * v[dim];
+	if (u[DEN] == 0 || u[PRE] == 0) return false;
+	for (int f = 0; f < NU; ++f)
+		if (u[f] != u[f] || isinf(u[f])) return false;
+	return true;
+}
+
+// ---------------------------------------------------------------- splines
+// SplineData::splint (SplineData.cpp:57-81) and the two interpolate() forms.
+__device__ __forceinline__ double splint(const Spline& s, double x2) {
+	int klo = 0, khi = s.n - 1, k;
+	while (khi - klo > 1) {
+		k = (khi + klo) >> 1;
+		if (s.x[k] > x2) khi = k;
+		else klo = k;
+	}
+	double h = s.x[khi] - s.x[klo];
+	double a = (s.x[khi] - x2) / h;
+	double b = (x2 - s.x[klo]) / h;
+	return a * s.y[klo] + b * s.y[khi] + ((a * a * a - a) * s.y2[klo] + (b * b * b - b) * s.y2[khi]) * (h * h) / 6.0;
+}
+
+__device__ __forceinline__ double spline_eval(const Spline& s, double x) {
+	int n = s.n;
+	if (s.log_mode) {
+		if (x > s.x[n - 1]) return s.y[n - 1] + s.max_slope * (x - s.x[n - 1]);
+		else if (x < s.x[0]) return s.y[0] + s.min_slope * (x - s.x[0]);
+		return splint(s, x);
+	}
+	if (x > s.x[n - 1]) return s.y[n - 1] * pow(x / s.x[n - 1], s.max_slope);
+	else if (x < s.x[0]) return s.y[0] * pow(x / s.x[0], s.min_slope);
+	return splint(s, x);
+}
+
+}  // namespace trg

@@ -1,0 +1,80 @@
+// Plain data types shared by host set-up code and device kernels of torch_b200.
+#pragma once
+
+#include <cstdint>
+
+namespace trg {
+
+enum { DEN = 0, PRE = 1, HII = 2, ADV = 3, VEL = 4, NU = 7 };
+enum { R_HII_A = 0, R_TAU, R_TAU_A, R_DTAU, R_DTAU_A, R_HEAT, NR };
+enum { T_COL_DEN = 0, T_DCOL_DEN, T_HEAT, T_RATE, NT };
+enum { G_CART = 0, G_CYL = 1, G_SPH = 2 };
+enum { BC_FREE = 0, BC_REFLECTING = 1, BC_OUTFLOW = 2, BC_INFLOW = 3, BC_PERIODIC = 4 };
+enum { CP_TTI = 0, CP_NEQ = 1, CP_OFF = 2 };
+enum { RS_HLLC = 0, RS_ROTATED = 1, RS_HLL = 2 };
+
+// Device error word bits (host maps them to TRG_ERR_*).
+enum : unsigned {
+	ERRB_NAN = 1u, ERRB_PICARD = 2u, ERRB_DT = 4u, ERRB_FLUX = 8u,
+};
+
+// Cubic spline table (SplineData, src/Integrators/SplineData.cpp) built on the host.
+struct Spline {
+	int n, log_mode;
+	double min_slope, max_slope;
+	double x[32], y[32], y2[32];
+};
+
+struct Tables {
+	Spline rad_recomb, rad_cool, th_cxhi, th_recomb;
+};
+
+// Code-unit parameters of one run (the reference's Constants, TorchParameters
+// after initialise(), Star, Thermodynamics constants).
+struct Params {
+	int nd, nx, ny, nz;
+	long long N;
+	int geometry, order, ng;
+	int lbc[3], rbc[3];
+	int riemann, limiter;
+	double dx[3];
+	double gamma, X;
+	double hydrogenMass, specificGasConstant, boltzmannConst, rydbergEnergy, dustXsec, pi;
+	double voronov_A, voronov_X, voronov_K, voronov_P, voronov_DE;
+	double dt_max, dfloor, pfloor, tfloor;
+	double photoIonXsec, photonEnergy, photonRate;
+	double tau0, THI, THII, heating_amp, thermo_hii_switch;
+	double K1, K2, K3, K4;
+	int radiation_on, cooling_on, star_on, collisions_on, coupling, thermo_subcycling;
+	int star_pos[3];
+	int wind_radius;     // Star::windCellRadius when the star is on, else 0
+	long long star_cell; // flat index of the star cell or -1
+	double sxc[3];       // Star::xc
+	double mdot, edot;
+	// thermodynamics constants (Thermodynamics::initialise, Thermodynamics.cpp:24-57)
+	double z0, T1, T2, T3, T4, imlc, nmlc, ciec_minT, ciec, cxhi_damp, n0, nmc;
+	double fuvh_a, fuvh_b, fuvh_c, irh_a, irh_b, crh;
+};
+
+// Device pointers of one context (FP64 state).
+struct State {
+	double* U;      // [7][N]
+	double* Q;      // [7][N]
+	double* U1;     // [7][N] scratch (RK2 intermediate state)
+	double* UDOT;   // [7][N] (component-phase interface only)
+	double* R;      // [6][N]
+	double* T;      // [4][N]
+	double* Tmin;   // [N]
+	double* ds;     // [N]
+	double* shellVol;
+	double* grav;   // [3][N] or nullptr
+	double* F[3];   // face fluxes per dimension [7][faces]
+	long long nfaces[3];
+	const Tables* tables;
+	unsigned* err;
+	// scalars: [0] dt, [1] time, [2..4] per-component dt minima (as uint64 bits)
+	double* scal;
+	double* dt_hist;
+};
+
+}  // namespace trg
