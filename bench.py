@@ -1,0 +1,362 @@
+"""Benchmark of the TORCH full step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload sedov|hii] [--n 256] [--precision fp32|fp64]
+
+Default workload: the 256^3 hydro-only Sedov blast (rho = 1e-20 g/cm^3,
+P = 1e-12 dyn/cm^2, 1e51 erg in a 3-cell sphere, outflow boundaries,
+albada-limited piecewise-linear reconstruction, rotated HLLC, RK2).  A step is
+one Torch::fullStep over the whole grid; the metric is cell updates per
+second (cells x full steps / time).  Inputs (7 x 256^3 cells) are far larger
+than the 126 MB L2, so no flush is needed between steps.
+
+One JSON line on rank 0.  Under torchrun (N > 1) every rank advances its own
+replica of the workload on its own GPU (the step does not shard in this
+build: "replicas only"), times are max-reduced over ranks, and value is the
+whole-job rate.  --impl reference times the reference's own CPU code (the
+unmodified reference build oracle/_ref/torch_ref, or the C restatement when
+that binary is absent) on the host cores, on a bounded sample of the same
+workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s/GPU full step 256^3"
+UNIT = "cell-updates/s"
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_PATH) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def build_workload(name, n):
+    from torch_b200 import workloads
+    if name == "sedov":
+        return workloads.sedov(n=n)
+    if name == "hii":
+        return workloads.hii_region(n=n)
+    raise ValueError(name)
+
+
+def workload_config(name, n, precision, replicas):
+    base = {"workload": f"{name} {n}^3", "cells": n ** 3, "precision": precision,
+            "parallelism": f"replicas x{replicas}", "l2": "inputs larger than L2 (no flush)"}
+    if name == "sedov":
+        base.update({"setup": "hydro-only Sedov blast, rho 1e-20, P 1e-12, E 1e51 erg in r<=3dx, outflow",
+                     "reconstruction": "piecewise-linear albada (spatial_order 1)", "riemann": "RotatedHLLC",
+                     "time": "RK2 midpoint", "gamma": 1.67, "side_pc": 2.0})
+    else:
+        base.update({"setup": "HII region, lognormal n (mean 1e3, sigma_ln 0.5, k^-11/3, seed 12345), "
+                              "Q=1e49/s star at centre, radiation+cooling, T=100 K",
+                     "time": "operator split H/T/R", "side_pc": 2.0})
+    return base
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() in ("active", "1", "yes"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, value, local):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------- CPU legs
+def _write_case(d, tp, ic):
+    from torch_b200 import config
+    pp = os.path.join(d, "params.lua")
+    with open(pp, "w") as f:
+        f.write(config.to_lua(tp))
+    icp = os.path.join(d, "ic_000.txt")
+    config.write_initial_conditions(icp, ic.ncells, ic.dx, ic.den, ic.pre, ic.hii, ic.vel)
+    return pp, icp
+
+
+def cpu_sample(workload, n_sample, steps, procs):
+    """Times the reference CPU code on `procs` independent replicas of a bounded
+    sample (n_sample^3 cells, `steps` full steps each) on the host cores.
+    Returns (cell-updates/s, kind, cores, description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    tp, ic = build_workload(workload, n_sample)
+    ref_bin = oracle.REF_BIN if os.path.exists(oracle.REF_BIN) else None
+    cells = int(np.prod(ic.ncells))
+    with tempfile.TemporaryDirectory() as d:
+        pp, icp = _write_case(d, tp, ic)
+        if ref_bin:
+            t0 = time.perf_counter()
+            ps = [subprocess.Popen([ref_bin, f"--params={pp}", f"--ic={icp}", f"--steps={steps}"],
+                                   cwd=d, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL) for _ in range(procs)]
+            rcs = [p.wait() for p in ps]
+            wall = time.perf_counter() - t0
+            if any(rcs):
+                raise RuntimeError(f"reference sample failed: {rcs}")
+            kind = "reference"
+        else:
+            from torch_b200 import config
+            ic2 = config.read_initial_conditions(icp)
+            t0 = time.perf_counter()
+            o = oracle.Oracle(tp, ic2)
+            for _ in range(steps):
+                o.full_step()
+            wall = time.perf_counter() - t0
+            procs = 1
+            kind = "port"
+    rate = cells * steps * procs / wall
+    desc = (f"{workload} {n_sample}^3, {steps} full steps x {procs} independent single-rank processes "
+            f"({'reference build, MPI absent: one rank each' if kind == 'reference' else 'C restatement'}); "
+            f"includes set-up")
+    return rate, kind, procs, desc
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return 0
+    procs = max(1, min(os.cpu_count() or 1, 16))
+    n_sample = 48 if args.workload == "sedov" else 32
+    per_step = []
+    total_steps = args.warmup + args.steps
+    t0 = time.perf_counter()
+    rate, kind, cores, desc = cpu_sample(args.workload, n_sample, max(1, total_steps), procs)
+    wall = time.perf_counter() - t0
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / max(1, total_steps),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args.workload, args.n, "fp64", 1),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------- GPU leg
+def run_ours(args, world, rank, local, pg):
+    import torch
+    import torch_b200
+
+    precision = torch_b200.PRECISION_FP32 if args.precision == "fp32" else torch_b200.PRECISION_FP64
+    tp, ic = build_workload(args.workload, args.n)
+    N = int(np.prod(ic.ncells))
+    sim = torch_b200.Torch(tp, ic, precision=precision, device=local)
+    dt_next = sim.dt_max
+    stream = torch.cuda.ExternalStream(sim.stream_handle(), device=f"cuda:{local}")
+
+    # warm-up (the first step is the reference's dt_max*1e-20 start step)
+    sim.run_steps(args.warmup)
+    launches0 = sim.kernel_launches()
+    sim.profile(True)
+    clocks = ClockSampler(local)
+    barrier(pg)
+    torch.cuda.synchronize(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    sim.enqueue_steps(args.steps, dt_next)
+    ev1.record(stream)
+    sim.synchronize()
+    torch.cuda.synchronize(local)
+    barrier(pg)
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    launches = sim.kernel_launches() - launches0
+    prof = {}
+    for name in ("k_hydro_stage_fp32", "k_faces_fp64", "k_hydro_update_fp64", "k_q_from_u", "k_dt_reduce",
+                 "k_rad_shell", "k_colden_shell", "k_thermo"):
+        t, c = sim.profile_read(name)
+        if c:
+            prof[name] = (t, c)
+    sim.profile(False)
+    ms_max = max_over_ranks(pg, ms, local)
+    value = N * args.steps * world / (ms_max / 1e3)
+
+    # roofline of the dominant hydro kernel
+    peak, peak_kind = hbm_peak()
+    if "k_hydro_stage_fp32" in prof:
+        kname = "k_hydro_stage_fp32"
+        # algorithmic bytes per cell per RK2 step in FP32: 140 B over two stage launches
+        alg_per_launch = 140.0 * N / 2.0
+    else:
+        kname = "k_faces_fp64"
+        # FP64 plain form, per face-flux launch (one per dimension, 2 stages):
+        # reads the 7 primitive fields once (8 B each) and writes 7 flux fields
+        alg_per_launch = (7 * 8 + 7 * 8) * N
+    tot_ms, count = prof.get(kname, (0.0, 0))
+    avg_ms = tot_ms / count if count else float("nan")
+    achieved = alg_per_launch / (avg_ms / 1e3) / 1e9 if count else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            with open(tpath) as f:
+                traffic = json.load(f).get(f"{kname}:{args.workload}:{args.n}")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "kernel": kname, "peak_source": peak_kind, "avg_launch_ms": avg_ms, "launches": count,
+                "algorithmic_bytes_per_launch": alg_per_launch}
+    kernel_share = {k: {"ms": v[0], "launches": v[1], "share": v[0] / max(1e-9, sum(x[0] for x in prof.values()))}
+                    for k, v in prof.items()}
+
+    # end to end: host buffers through the C ABI, copies inside the timed region
+    e2e = None
+    if args.e2e_steps > 0:
+        st = sim.state()
+        U_host = torch.from_numpy(st.U).pin_memory()
+        U_out = torch.empty_like(U_host).pin_memory()
+        Un = U_host.numpy()
+        Uo = U_out.numpy()
+        barrier(pg)
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            sim.set_conserved(Un)
+            sim.full_step(dt_next)
+            sim.lib.trg_get_state(sim.ctx, Uo.ctypes.data_as(torch_b200.C.c_void_p), None, None, None, None)
+        wall = time.perf_counter() - t0
+        wall = max_over_ranks(pg, wall, local)
+        e2e = {"value": N * args.e2e_steps * world / wall, "unit": UNIT,
+               "h2d_bytes_per_step": int(Un.nbytes), "d2h_bytes_per_step": int(Uo.nbytes),
+               "steps": args.e2e_steps, "note": "per step: pinned H2D of U, trg_full_step, D2H of U"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            rate, kind, cores, desc = cpu_sample(args.workload, 48 if args.workload == "sedov" else 32,
+                                                 args.cpu_steps, max(1, min(os.cpu_count() or 1, 16)))
+            cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc}
+        except Exception as e:  # a missing CPU baseline must not hide the GPU number
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable", "sample": str(e)[:200]}
+    sim.close()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if precision else "f64", "data": "synthetic",
+            "config": workload_config(args.workload, args.n, args.precision, world),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clk, "kernels": kernel_share,
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["sedov", "hii"], default="sedov")
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp64")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-steps", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local, pg = dist_setup()
+    try:
+        if args.impl == "reference":
+            return run_reference_arm(args, rank)
+        return run_ours(args, world, rank, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -119,6 +119,20 @@ double trg_dt_max(const trg_ctx* c);
 long trg_ncells(const trg_ctx* c);
 /* Kernel launches issued by this context since creation (for accounting). */
 long long trg_kernel_launches(const trg_ctx* c);
+
+/* Measurement hooks (no counterpart in the reference, which has no timers):
+ *   trg_enqueue_steps  like trg_run_steps but returns right after enqueuing,
+ *                      without waiting or checking the device error word
+ *                      (call trg_synchronize afterwards);
+ *   trg_stream         the context's cudaStream_t, for events recorded by the caller;
+ *   trg_profile_enable when on, every kernel launch is bracketed by CUDA events
+ *                      on the context's stream;
+ *   trg_profile_read   total milliseconds and launch count of the kernels whose
+ *                      name contains `name` since profiling was enabled. */
+int trg_enqueue_steps(trg_ctx* c, int nsteps, double dt_next_checkpoint);
+void* trg_stream(const trg_ctx* c);
+int trg_profile_enable(trg_ctx* c, int on);
+int trg_profile_read(trg_ctx* c, const char* name, double* total_ms, long long* launches);
 const char* trg_last_error(const trg_ctx* c);
 void trg_destroy(trg_ctx* c);
 

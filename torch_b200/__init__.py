@@ -91,6 +91,10 @@ _SIGNATURES = [
     ("trg_kernel_launches", C.c_longlong, [C.c_void_p]),
     ("trg_last_error", C.c_char_p, [C.c_void_p]),
     ("trg_destroy", None, [C.c_void_p]),
+    ("trg_enqueue_steps", C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    ("trg_stream", C.c_void_p, [C.c_void_p]),
+    ("trg_profile_enable", C.c_int, [C.c_void_p, C.c_int]),
+    ("trg_profile_read", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
 ]
 
 
@@ -208,6 +212,24 @@ class Torch:
         self._check(self.lib.trg_run_steps(self.ctx, nsteps, dt_next_checkpoint, _ptr(out)))
         self.dts.extend(out[:nsteps].tolist())
         return out[:nsteps]
+
+    def enqueue_steps(self, nsteps: int, dt_next_checkpoint: Optional[float] = None):
+        """Enqueues nsteps full steps and returns at once (see synchronize())."""
+        if dt_next_checkpoint is None:
+            dt_next_checkpoint = self.dt_max
+        self._check(self.lib.trg_enqueue_steps(self.ctx, nsteps, dt_next_checkpoint))
+
+    def stream_handle(self) -> int:
+        return int(self.lib.trg_stream(self.ctx) or 0)
+
+    def profile(self, on: bool):
+        self._check(self.lib.trg_profile_enable(self.ctx, int(on)))
+
+    def profile_read(self, name: str):
+        ms = C.c_double(0)
+        n = C.c_longlong(0)
+        self._check(self.lib.trg_profile_read(self.ctx, name.encode(), C.byref(ms), C.byref(n)))
+        return ms.value, n.value
 
     def component(self, comp: int, phase: int, dt: float = 0.0) -> float:
         out = C.c_double(0)

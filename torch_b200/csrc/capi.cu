@@ -40,6 +40,12 @@ struct trg_ctx {
 	long long launches = 0;
 	int dt_hist_cap = 0;
 	std::string err;
+	// optional per-launch CUDA-event timing
+	bool profiling = false;
+	struct Rec { const char* name; cudaEvent_t a, b; };
+	std::vector<Rec> recs;
+	std::vector<cudaEvent_t> event_pool;
+	std::vector<std::pair<std::string, std::pair<double, long long>>> prof_totals;
 };
 
 namespace {
@@ -68,10 +74,41 @@ int dalloc(trg_ctx* c, T** p, size_t count) {
 
 inline unsigned grid_for(long long n, int block) { return (unsigned)((n + block - 1) / block); }
 
+cudaEvent_t pool_event(trg_ctx* c) {
+	if (!c->event_pool.empty()) {
+		cudaEvent_t e = c->event_pool.back();
+		c->event_pool.pop_back();
+		return e;
+	}
+	cudaEvent_t e = nullptr;
+	cudaEventCreate(&e);
+	return e;
+}
+
+// Folds completed event pairs into per-kernel totals (the stream must be idle).
+void profile_collect(trg_ctx* c) {
+	for (auto& r : c->recs) {
+		float ms = 0;
+		cudaEventElapsedTime(&ms, r.a, r.b);
+		bool found = false;
+		for (auto& t : c->prof_totals)
+			if (t.first == r.name) { t.second.first += ms; t.second.second += 1; found = true; break; }
+		if (!found) c->prof_totals.push_back({r.name, {(double)ms, 1LL}});
+		c->event_pool.push_back(r.a);
+		c->event_pool.push_back(r.b);
+	}
+	c->recs.clear();
+}
+
 #define LAUNCH(kernel, n, block, ...)                                                        \
 	do {                                                                                     \
 		if ((n) > 0) {                                                                       \
+			cudaEvent_t ea_ = nullptr, eb_ = nullptr;                                        \
+			if (c->profiling) { ea_ = pool_event(c); eb_ = pool_event(c);                    \
+			                    cudaEventRecord(ea_, c->stream); }                           \
 			kernel<<<grid_for((n), (block)), (block), 0, c->stream>>>(__VA_ARGS__);          \
+			if (c->profiling) { cudaEventRecord(eb_, c->stream);                             \
+			                    c->recs.push_back({#kernel, ea_, eb_}); }                    \
 			c->launches++;                                                                   \
 		}                                                                                    \
 	} while (0)
@@ -195,10 +232,12 @@ int check_device_error(trg_ctx* c) {
 	unsigned e = 0;
 	CUDA_TRY(cudaMemcpyAsync(&e, c->S.err, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
 	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	// checkValues runs before every integrator in the reference, so an invalid
+	// state is reported ahead of the failures it causes downstream.
+	if (e & ERRB_NAN) return set_error(c, TRG_ERR_NAN, "checkValues/fixSolution: invalid cell state");
 	if (e & ERRB_FLUX) return set_error(c, TRG_ERR_FLUX, "Riemann solver: HII flux is NaN");
 	if (e & ERRB_PICARD) return set_error(c, TRG_ERR_PICARD, "update_HIIfrac: implicit method not converging");
 	if (e & ERRB_DT) return set_error(c, TRG_ERR_DT, "Radiation::calculateTimeStep: invalid timestep");
-	if (e & ERRB_NAN) return set_error(c, TRG_ERR_NAN, "checkValues/fixSolution: invalid cell state");
 	return TRG_OK;
 }
 
@@ -329,6 +368,39 @@ int trg_run_steps(trg_ctx* c, int nsteps, double dt_next_checkpoint, double* dts
 	return TRG_OK;
 }
 
+int trg_enqueue_steps(trg_ctx* c, int nsteps, double dt_next_checkpoint) {
+	if (!c || nsteps < 0) return TRG_ERR_ARG;
+	int rc = ensure_dt_hist(c, c->steps + nsteps);
+	if (rc) return rc;
+	for (int s = 0; s < nsteps; ++s) enqueue_full_step(c, dt_next_checkpoint);
+	CUDA_TRY(cudaGetLastError());
+	return TRG_OK;
+}
+
+void* trg_stream(const trg_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int trg_profile_enable(trg_ctx* c, int on) {
+	if (!c) return TRG_ERR_ARG;
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	profile_collect(c);
+	if (on && !c->profiling) c->prof_totals.clear();
+	c->profiling = on != 0;
+	return TRG_OK;
+}
+
+int trg_profile_read(trg_ctx* c, const char* name, double* total_ms, long long* launches) {
+	if (!c || !name) return TRG_ERR_ARG;
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	profile_collect(c);
+	double ms = 0;
+	long long n = 0;
+	for (auto& t : c->prof_totals)
+		if (t.first.find(name) != std::string::npos) { ms += t.second.first; n += t.second.second; }
+	if (total_ms) *total_ms = ms;
+	if (launches) *launches = n;
+	return TRG_OK;
+}
+
 int trg_component(trg_ctx* c, int comp, int phase, double dt, double* out) {
 	if (!c) return TRG_ERR_ARG;
 	// The phase kernels read dt from the device scalar: stage the caller's dt.
@@ -420,6 +492,8 @@ const char* trg_last_error(const trg_ctx* c) { return c ? c->err.c_str() : "null
 void trg_destroy(trg_ctx* c) {
 	if (!c) return;
 	if (c->stream) cudaStreamSynchronize(c->stream);
+	profile_collect(c);
+	for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
 	for (void* p : c->allocs) cudaFree(p);
 	if (c->stream) cudaStreamDestroy(c->stream);
 	delete c;

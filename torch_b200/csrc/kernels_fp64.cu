@@ -377,13 +377,17 @@ __global__ void __launch_bounds__(256) k_q_from_u_fp64(Params P, State S, const 
 #pragma unroll
 	for (int i = 0; i < NU; ++i) { u[i] = FLD(Usrc, i, id); q[i] = FLD(S.Q, i, id); }
 	QfromU(q, u, P.gamma, P.nd);
-	if (fix) fix_primitives(P, q, u[DEN]);
-	bool bad = q[DEN] == 0 || q[PRE] == 0;
+	bool bad = false;
+	if (fix) {
+		// Torch::checkValues runs where Q was just rebuilt with floors; the
+		// RK2 predictor's Q(U*) (fix == 0) is not checked by the reference.
+		fix_primitives(P, q, u[DEN]);
+		bad = q[DEN] == 0 || q[PRE] == 0;
 #pragma unroll
-	for (int i = 0; i < NU; ++i) {
-		bad |= (u[i] != u[i]) || isinf(u[i]);
-		FLD(S.Q, i, id) = q[i];
+		for (int i = 0; i < NU; ++i) bad |= (u[i] != u[i]) || isinf(u[i]);
 	}
+#pragma unroll
+	for (int i = 0; i < NU; ++i) FLD(S.Q, i, id) = q[i];
 	if (bad) atomicOr(S.err, ERRB_NAN);
 }
 
@@ -485,7 +489,9 @@ __device__ __forceinline__ double dist2_cells(const Params& P, const double* xc)
 __device__ __forceinline__ double tau_sc(const Params& P, const State& S, const long long* nb, const double* w0, int rt, int rd) {
 	double tau[4] = {0, 0, 0, 0}, w[4];
 	for (int i = 0; i < 4; ++i) {
-		if (nb[i] >= 0) tau[i] = FLD(S.R, rt, nb[i]) + FLD(S.R, rd, nb[i]);
+		// A zero-weight neighbour contributes 0 * tau = 0 whatever its tau, and
+		// may belong to the shell being swept: it is not read.
+		if (nb[i] >= 0 && w0[i] != 0) tau[i] = FLD(S.R, rt, nb[i]) + FLD(S.R, rd, nb[i]);
 		w[i] = w0[i] / smax(P.tau0, tau[i]);
 	}
 	double sum_w = w[0] + w[1] + w[2] + w[3];
@@ -728,7 +734,7 @@ __global__ void __launch_bounds__(128) k_colden_shell_fp64(Params P, State S, co
 		double w0[4], colden[4] = {0, 0, 0, 0}, w[4];
 		neighbours(P, ijk, xc, nb, w0);
 		for (int i = 0; i < 4; ++i) {
-			if (nb[i] >= 0) colden[i] = FLD(S.T, T_COL_DEN, nb[i]) + FLD(S.T, T_DCOL_DEN, nb[i]);
+			if (nb[i] >= 0 && w0[i] != 0) colden[i] = FLD(S.T, T_COL_DEN, nb[i]) + FLD(S.T, T_DCOL_DEN, nb[i]);
 			w[i] = colden[i] == 0 ? 0 : w0[i] / colden[i];
 		}
 		double sum_w = w[0] + w[1] + w[2] + w[3];

@@ -185,9 +185,9 @@ void next_causal(const Geo& g, const int* from, const int* src, int* nxt) {
 	if (!g.within(nxt) && dir[0] == 1 && dir[1] == -1 && dir[2] == -1 && nd > 2) { jump(1, 1, 1); dir[0] = -1; }
 }
 
-// Upwind neighbour offsets of Grid::calculateNearestNeighbours (Grid.cpp:922-952),
-// used here only to verify the shell order.
-void neighbour_cells(const Params& P, const int* ijk, const double* xc, long long* nb) {
+// Upwind neighbours and weights of Grid::calculateNearestNeighbours
+// (Grid.cpp:922-952), used here only to verify the shell order.
+void neighbour_cells(const Params& P, const int* ijk, const double* xc, long long* nb, double* w) {
 	int plane = 0;
 	double dmax = 0;
 	for (int i = 0; i < P.nd; ++i) {
@@ -195,11 +195,12 @@ void neighbour_cells(const Params& P, const int* ijk, const double* xc, long lon
 		if (dd > dmax) { dmax = dd; plane = i; }
 	}
 	int irot[3] = {(plane + 1) % 3, (plane + 2) % 3, plane % 3};
-	int LR[3];
+	double d[3];
+	int s[3], LR[3];
 	for (int i = 0; i < 3; i++) {
-		double d = xc[irot[i]] - P.sxc[irot[i]];
-		int s = d < -1.0 / 10.0 ? -1 : 1;
-		LR[i] = std::fabs(d) < 1.0 / 10.0 ? 0 : s;
+		d[i] = xc[irot[i]] - P.sxc[irot[i]];
+		s[i] = d[i] < -1.0 / 10.0 ? -1 : 1;
+		LR[i] = std::fabs(d[i]) < 1.0 / 10.0 ? 0 : s[i];
 	}
 	const int off[4][3] = {{0, 0, -LR[2]}, {0, -LR[1], -LR[2]}, {-LR[0], 0, -LR[2]}, {-LR[0], -LR[1], -LR[2]}};
 	for (int n = 0; n < 4; ++n) {
@@ -208,6 +209,14 @@ void neighbour_cells(const Params& P, const int* ijk, const double* xc, long lon
 		bool in = t[0] >= 0 && t[0] < P.nx && t[1] >= 0 && t[1] < P.ny && t[2] >= 0 && t[2] < P.nz;
 		nb[n] = in ? t[0] + (long long)P.nx * (t[1] + (long long)P.ny * t[2]) : -1;
 	}
+	double ic0 = (int)xc[irot[0]] - 0.5 * (s[2] * d[0] / d[2]);
+	double ic1 = (int)xc[irot[1]] - 0.5 * (s[2] * d[1] / d[2]);
+	double delta0 = std::fabs(2.0 * ic0 - 2.0 * (int)xc[irot[0]] + s[0]);
+	double delta1 = std::fabs(2.0 * ic1 - 2.0 * (int)xc[irot[1]] + s[1]);
+	w[0] = (std::fabs(d[2]) > 0.9) ? delta0 * delta1 : 0;
+	w[1] = ((std::fabs(d[1]) > 0.9) && (std::fabs(d[2]) > 0.9)) ? delta0 * (1.0 - delta1) : 0;
+	w[2] = ((std::fabs(d[0]) > 0.9) && (std::fabs(d[2]) > 0.9)) ? (1.0 - delta0) * delta1 : 0;
+	w[3] = ((std::fabs(d[0]) > 0.9) && (std::fabs(d[1]) > 0.9) && (std::fabs(d[2]) > 0.9)) ? (1.0 - delta0) * (1.0 - delta1) : 0;
 }
 
 }  // namespace
@@ -429,10 +438,15 @@ std::string host_setup(const trg_params& p, const double* den, const double* pre
 		out.R[R_DTAU_A * N + id] = (1.0 - out.R[R_HII_A * N + id]) * nH * P.photoIonXsec * ds;
 	}
 
-	// Shell order: key = max-norm distance L from the star in cell units; shell
-	// 0 holds L <= 0.5 (no upwind reads), shell ceil(L) otherwise.  Every
-	// upwind neighbour of a cell lies at L' <= L - 1 (or L' = 0.5 when L = 1),
-	// so it sits in an earlier shell; this is checked below.
+	// Shell order.  Key = 2L, L the max-norm distance from the star in cell
+	// units (cell and star centres sit on integers or half-integers, so 2L is
+	// an integer).  An upwind neighbour with a non-zero weight always has a
+	// smaller key: it is one cell nearer along the dominant axis, and a
+	// neighbour left level with the cell along another axis ties only when
+	// that axis is as far from the star as the dominant one, in which case its
+	// weight is exactly zero (delta = 0 in calculateNearestNeighbours).  The
+	// kernels skip zero-weight neighbours (their contribution is 0 * finite),
+	// so each shell reads only finished inner shells.  Checked below.
 	std::vector<int> shell_of(N);
 	int nshell = 0;
 	for (long long id = 0; id < N; ++id) {
@@ -441,7 +455,7 @@ std::string host_setup(const trg_params& p, const double* den, const double* pre
 		g.xc(id, xc, ijk);
 		double L = 0;
 		for (int i = 0; i < P.nd; ++i) L = std::max(L, std::fabs(xc[i] - P.sxc[i]));
-		int s = L <= 0.5 ? 0 : (int)std::ceil(L);
+		int s = (int)std::lround(2.0 * L);
 		shell_of[id] = s;
 		nshell = std::max(nshell, s + 1);
 	}
@@ -453,9 +467,22 @@ std::string host_setup(const trg_params& p, const double* den, const double* pre
 		for (int i = 0; i < P.nd; ++i) d2 += (xc[i] - P.sxc[i]) * (xc[i] - P.sxc[i]);
 		if (!(d2 > 0.95 * 0.95)) continue;
 		long long nb[4];
-		neighbour_cells(P, ijk, xc, nb);
+		double w[4];
+		neighbour_cells(P, ijk, xc, nb, w);
 		for (int k = 0; k < 4; ++k)
-			if (nb[k] >= 0 && shell_of[nb[k]] >= shell_of[id]) return "internal: shell order violates a sweep dependency";
+			if (nb[k] >= 0 && w[k] != 0 && shell_of[nb[k]] >= shell_of[id])
+				return "internal: shell order violates a sweep dependency";
+	}
+	// drop empty shells (odd keys are empty for a cell-centred star)
+	{
+		std::vector<int> remap(nshell, -1);
+		std::vector<char> used(nshell, 0);
+		for (long long id = 0; id < N; ++id) used[shell_of[id]] = 1;
+		int k = 0;
+		for (int s = 0; s < nshell; ++s)
+			if (used[s]) remap[s] = k++;
+		for (long long id = 0; id < N; ++id) shell_of[id] = remap[shell_of[id]];
+		nshell = k;
 	}
 	std::vector<long long> cnt_all(nshell + 1, 0), cnt_nw(nshell + 1, 0);
 	for (long long id = 0; id < N; ++id) {
