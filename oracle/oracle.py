@@ -19,6 +19,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+LIB_PM_PATH = os.path.join(HERE, "_build", "liboracle_pm.so")
 REF_BIN = os.path.join(HERE, "_ref", "torch_ref")
 REF_TREE = "/root/reference"
 
@@ -47,13 +48,14 @@ class OrcParams(C.Structure):
     ]
 
 
-def build(quiet: bool = True) -> str:
+def build(quiet: bool = True, portable_math: bool = False) -> str:
     """Compiles the C restatement (make -C oracle) if it is missing or stale."""
     src = os.path.join(HERE, "torch_oracle.c")
-    if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+    path = LIB_PM_PATH if portable_math else LIB_PATH
+    if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
         subprocess.run(["make", "-C", HERE], check=True,
                        stdout=subprocess.DEVNULL if quiet else None)
-    return LIB_PATH
+    return path
 
 
 def build_reference(quiet: bool = True) -> Optional[str]:
@@ -67,13 +69,13 @@ def build_reference(quiet: bool = True) -> Optional[str]:
     return REF_BIN if os.path.exists(REF_BIN) else None
 
 
-_lib = None
+_libs = {}
 
 
-def _load():
-    global _lib
-    if _lib is None:
-        _lib = C.CDLL(build())
+def _load(portable_math: bool = False):
+    if portable_math not in _libs:
+        _lib = C.CDLL(build(portable_math=portable_math))
+        _libs[portable_math] = _lib
         _lib.orc_create.restype = C.c_void_p
         _lib.orc_create.argtypes = [C.POINTER(OrcParams)] + [C.c_void_p] * 7 + [C.c_char_p, C.c_int]
         _lib.orc_full_step.restype = C.c_int
@@ -90,7 +92,7 @@ def _load():
         _lib.orc_destroy.argtypes = [C.c_void_p]
         _lib.orc_causal_order.restype = C.c_long
         _lib.orc_causal_order.argtypes = [C.c_void_p, C.c_void_p, C.c_long]
-    return _lib
+    return _libs[portable_math]
 
 
 def params_struct(tp, side_length: Optional[float] = None, ncells=None) -> OrcParams:
@@ -142,10 +144,14 @@ class State:
 
 
 class Oracle:
-    """The C restatement, driven like Torch::run (one context per run)."""
+    """The C restatement, driven like Torch::run (one context per run).
 
-    def __init__(self, tp, ic):
-        lib = _load()
+    portable_math=False: host libm, bit-exact with the reference build.
+    portable_math=True: the IEEE-only exp/log/log10/pow that the FP64 GPU
+    kernels use, i.e. the GPU's bit-exact CPU twin."""
+
+    def __init__(self, tp, ic, portable_math: bool = False):
+        lib = _load(portable_math)
         self.N = int(np.prod(ic.ncells))
         p = params_struct(tp, side_length=ic.side_length, ncells=ic.ncells)
         err = C.create_string_buffer(512)

@@ -9,6 +9,24 @@
 
 #include <math.h>
 #include <stdarg.h>
+
+/* Transcendentals of the step.  Default: the host libm (as the reference).
+ * With ORACLE_PORTABLE_MATH: the IEEE-only implementations of
+ * torch_b200/csrc/trg_math.h, which the FP64 GPU kernels use too - that build
+ * is the GPU's bit-exact CPU twin.  Set-up code (tables, unit conversion)
+ * always uses the host libm, like both the reference and the GPU library. */
+#ifdef ORACLE_PORTABLE_MATH
+#include "../torch_b200/csrc/trg_math.h"
+#define m_exp trg_exp
+#define m_log trg_log
+#define m_log10 trg_log10
+#define m_pow trg_pow
+#else
+#define m_exp exp
+#define m_log log
+#define m_log10 log10
+#define m_pow pow
+#endif
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -147,8 +165,8 @@ static double spline_eval(const spline_t* s, double x) {
 		else if (x < s->x[0]) return s->y[0] + s->min_slope * (x - s->x[0]);
 		return splint(s, x);
 	}
-	if (x > s->x[n - 1]) return s->y[n - 1] * pow(x / s->x[n - 1], s->max_slope);
-	else if (x < s->x[0]) return s->y[0] * pow(x / s->x[0], s->min_slope);
+	if (x > s->x[n - 1]) return s->y[n - 1] * m_pow(x / s->x[n - 1], s->max_slope);
+	else if (x < s->x[0]) return s->y[0] * m_pow(x / s->x[0], s->min_slope);
 	return splint(s, x);
 }
 
@@ -917,8 +935,8 @@ static double hydro_dt(orc_ctx* c) {
 static double photoionisation_rate(double nHI, double T, double delT, double shellVol, double photonRate) {
 	/* Radiation.cpp:243-251 */
 	if (nHI == 0 || shellVol == 0) return 0.0;
-	double emT = exp(-T);
-	double emdT = exp(-delT);
+	double emT = m_exp(-T);
+	double emdT = m_exp(-delT);
 	return photonRate * emT * (1.0 - emdT) / (nHI * shellVol);
 }
 
@@ -926,7 +944,7 @@ static double collisional_ionisation_rate(const orc_ctx* c, double T) {
 	/* Radiation.cpp:231-237 */
 	if (!c->p.collisions_on || T < 5.0e3) return 0.0;
 	double U = c->voronov_DE / T;
-	return c->voronov_A * (1. + c->voronov_P * sqrt(U)) * exp(c->voronov_K * log(U) - U) / (c->voronov_X + U);
+	return c->voronov_A * (1. + c->voronov_P * sqrt(U)) * m_exp(c->voronov_K * m_log(U) - U) / (c->voronov_X + U);
 }
 
 static void doric(double dt, double* HII_avg, double* HII, double Api, double nHII_aB, double nHII_Aci) {
@@ -942,7 +960,7 @@ static void doric(double dt, double* HII_avg, double* HII, double Api, double nH
 		if (1.0 - *HII < epsilon) *HII = 1.0 - epsilon;
 		*HII_avg = *HII;
 	} else {
-		double e = exp(-dt * inv_ti);
+		double e = m_exp(-dt * inv_ti);
 		*HII = xeq + (HII_old - xeq) * e;
 		*HII = smax(smin(*HII, 1.0), 0.0);
 		if (1.0 - *HII < epsilon) *HII = 1.0 - epsilon;
@@ -1164,15 +1182,15 @@ static double flux_fuv(const orc_ctx* c, double Q_FUV, double dist_sqrd) {
 	return dist_sqrd != 0 ? Q_FUV / (1.2e7 * 4 * c->pi * dist_sqrd) : 0;
 }
 static double imlc(const orc_ctx* c, double ne, double T) {
-	return c->imlc * c->z0 * ne * ne * exp(-c->T1 / T - (c->T2 / T) * (c->T2 / T));
+	return c->imlc * c->z0 * ne * ne * m_exp(-c->T1 / T - (c->T2 / T) * (c->T2 / T));
 }
 static double nmlc(const orc_ctx* c, double ne, double nn, double T) {
-	return c->nmlc * c->z0 * ne * nn * exp(-c->T3 / T - (c->T4 / T) * (c->T4 / T));
+	return c->nmlc * c->z0 * ne * nn * m_exp(-c->T3 / T - (c->T4 / T) * (c->T4 / T));
 }
 static double ciec(const orc_ctx* c, double ne, double T) {
 	/* Thermodynamics.cpp:135-143 */
 	if (T > c->ciec_minT) {
-		double cie_rate = c->ciec * ne * ne * c->z0 * exp(-0.63 * log(T)) * (1.0 - exp(-pow(1.0e-5 * T, 1.63)));
+		double cie_rate = c->ciec * ne * ne * c->z0 * m_exp(-0.63 * m_log(T)) * (1.0 - m_exp(-m_pow(1.0e-5 * T, 1.63)));
 		double smoothing = smin(1.0, (T - 5.0e4) / (2.0e4));
 		return cie_rate * smoothing;
 	}
@@ -1180,19 +1198,19 @@ static double ciec(const orc_ctx* c, double ne, double T) {
 }
 static double nmc(const orc_ctx* c, double nH, double x, double T) {
 	/* Thermodynamics.cpp:146-149 */
-	double T0 = 70.0 + 220.0 * pow(nH / c->n0, 0.2);
-	return c->nmc * (1.0 - x) * (1.0 - x) * pow(nH, 1.6) * sqrt(T) * exp(-T0 / T);
+	double T0 = 70.0 + 220.0 * m_pow(nH / c->n0, 0.2);
+	return c->nmc * (1.0 - x) * (1.0 - x) * m_pow(nH, 1.6) * sqrt(T) * m_exp(-T0 / T);
 }
 static double cxhi(const orc_ctx* c, double nH, double x, double T) {
 	/* Thermodynamics.cpp:161-166 */
-	double rate = spline_eval(&c->th_cxhi, log10(T));
-	return x * (1.0 - x) * nH * nH * exp((2.302585093 * rate) - ((T / c->cxhi_damp) * (T / c->cxhi_damp)));
+	double rate = spline_eval(&c->th_cxhi, m_log10(T));
+	return x * (1.0 - x) * nH * nH * m_exp((2.302585093 * rate) - ((T / c->cxhi_damp) * (T / c->cxhi_damp)));
 }
 static double fuvh(const orc_ctx* c, double nH, double Av, double F) {
-	return c->fuvh_a * nH * F * exp(-1.9 * Av) / (c->fuvh_b + c->fuvh_c * F * exp(-1.9 * Av) / nH);
+	return c->fuvh_a * nH * F * m_exp(-1.9 * Av) / (c->fuvh_b + c->fuvh_c * F * m_exp(-1.9 * Av) / nH);
 }
 static double irh(const orc_ctx* c, double nH, double Av, double F) {
-	return c->irh_a * nH * F * exp(-0.05 * Av) * exp(-2.0 * log(1.0 + c->irh_b / nH));
+	return c->irh_a * nH * F * m_exp(-0.05 * Av) * m_exp(-2.0 * m_log(1.0 + c->irh_b / nH));
 }
 static double soft_landing(double rate, double T, double T_min) {
 	/* Thermodynamics.cpp:202-211 */

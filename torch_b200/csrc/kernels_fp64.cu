@@ -1,9 +1,9 @@
 // FP64 kernels of the operator-split step (the plain-FP64 form).
 //
 // Compiled with --fmad=false: every kernel reproduces the reference's FP64
-// arithmetic in the reference's operation order, so that results match the
-// CPU oracle to the last bit except where a CUDA transcendental (exp, log,
-// pow) differs from the host libm by an ulp.
+// arithmetic in the reference's operation order.  exp/log/log10/pow come from
+// trg_math.h (IEEE +-*/ only), which the CPU oracle can share, so that the
+// GPU and CPU runs agree to the last bit.
 //
 // Layout: SoA, field-major, interior cells only, flat index i + nx*(j + ny*k).
 // Ghost cells are not stored: boundary conditions are applied while loading
@@ -408,8 +408,8 @@ __global__ void __launch_bounds__(256) k_advance_fp64(Params P, State S, double 
 // Radiation.cpp:243-251.
 __device__ __forceinline__ double photoionisation_rate(double nHI, double T, double delT, double shellVol, double photonRate) {
 	if (nHI == 0 || shellVol == 0) return 0.0;
-	double emT = exp(-T);
-	double emdT = exp(-delT);
+	double emT = trg_exp(-T);
+	double emdT = trg_exp(-delT);
 	return photonRate * emT * (1.0 - emdT) / (nHI * shellVol);
 }
 
@@ -417,7 +417,7 @@ __device__ __forceinline__ double photoionisation_rate(double nHI, double T, dou
 __device__ __forceinline__ double collisional_ionisation_rate(const Params& P, double T) {
 	if (!P.collisions_on || T < 5.0e3) return 0.0;
 	double U = P.voronov_DE / T;
-	return P.voronov_A * (1. + P.voronov_P * sqrt(U)) * exp(P.voronov_K * log(U) - U) / (P.voronov_X + U);
+	return P.voronov_A * (1. + P.voronov_P * sqrt(U)) * trg_exp(P.voronov_K * trg_log(U) - U) / (P.voronov_X + U);
 }
 
 // Radiation::doric, Radiation.cpp:140-179.
@@ -433,7 +433,7 @@ __device__ __forceinline__ void doric(double dt, double& HII_avg, double& HII, d
 		if (1.0 - HII < epsilon) HII = 1.0 - epsilon;
 		HII_avg = HII;
 	} else {
-		double e = exp(-dt * inv_ti);
+		double e = trg_exp(-dt * inv_ti);
 		HII = xeq + (HII_old - xeq) * e;
 		HII = smax(smin(HII, 1.0), 0.0);
 		if (1.0 - HII < epsilon) HII = 1.0 - epsilon;
@@ -672,32 +672,32 @@ __global__ void __launch_bounds__(256) k_rad_update_fp64(Params P, State S, doub
 // ----------------------------------------------------------- thermodynamics
 // Henney et al. (2009) heating and cooling, Thermodynamics.cpp:113-211.
 __device__ __forceinline__ double th_imlc(const Params& P, double ne, double T) {
-	return P.imlc * P.z0 * ne * ne * exp(-P.T1 / T - (P.T2 / T) * (P.T2 / T));
+	return P.imlc * P.z0 * ne * ne * trg_exp(-P.T1 / T - (P.T2 / T) * (P.T2 / T));
 }
 __device__ __forceinline__ double th_nmlc(const Params& P, double ne, double nn, double T) {
-	return P.nmlc * P.z0 * ne * nn * exp(-P.T3 / T - (P.T4 / T) * (P.T4 / T));
+	return P.nmlc * P.z0 * ne * nn * trg_exp(-P.T3 / T - (P.T4 / T) * (P.T4 / T));
 }
 __device__ __forceinline__ double th_ciec(const Params& P, double ne, double T) {
 	if (T > P.ciec_minT) {
-		double cie_rate = P.ciec * ne * ne * P.z0 * exp(-0.63 * log(T)) * (1.0 - exp(-pow(1.0e-5 * T, 1.63)));
+		double cie_rate = P.ciec * ne * ne * P.z0 * trg_exp(-0.63 * trg_log(T)) * (1.0 - trg_exp(-trg_pow(1.0e-5 * T, 1.63)));
 		double smoothing = smin(1.0, (T - 5.0e4) / (2.0e4));
 		return cie_rate * smoothing;
 	}
 	return 0;
 }
 __device__ __forceinline__ double th_nmc(const Params& P, double nH, double x, double T) {
-	double T0 = 70.0 + 220.0 * pow(nH / P.n0, 0.2);
-	return P.nmc * (1.0 - x) * (1.0 - x) * pow(nH, 1.6) * sqrt(T) * exp(-T0 / T);
+	double T0 = 70.0 + 220.0 * trg_pow(nH / P.n0, 0.2);
+	return P.nmc * (1.0 - x) * (1.0 - x) * trg_pow(nH, 1.6) * sqrt(T) * trg_exp(-T0 / T);
 }
 __device__ __forceinline__ double th_cxhi(const Params& P, const State& S, double nH, double x, double T) {
-	double rate = spline_eval(S.tables->th_cxhi, log10(T));
-	return x * (1.0 - x) * nH * nH * exp((2.302585093 * rate) - ((T / P.cxhi_damp) * (T / P.cxhi_damp)));
+	double rate = spline_eval(S.tables->th_cxhi, trg_log10(T));
+	return x * (1.0 - x) * nH * nH * trg_exp((2.302585093 * rate) - ((T / P.cxhi_damp) * (T / P.cxhi_damp)));
 }
 __device__ __forceinline__ double th_fuvh(const Params& P, double nH, double Av, double F) {
-	return P.fuvh_a * nH * F * exp(-1.9 * Av) / (P.fuvh_b + P.fuvh_c * F * exp(-1.9 * Av) / nH);
+	return P.fuvh_a * nH * F * trg_exp(-1.9 * Av) / (P.fuvh_b + P.fuvh_c * F * trg_exp(-1.9 * Av) / nH);
 }
 __device__ __forceinline__ double th_irh(const Params& P, double nH, double Av, double F) {
-	return P.irh_a * nH * F * exp(-0.05 * Av) * exp(-2.0 * log(1.0 + P.irh_b / nH));
+	return P.irh_a * nH * F * trg_exp(-0.05 * Av) * trg_exp(-2.0 * trg_log(1.0 + P.irh_b / nH));
 }
 __device__ __forceinline__ double soft_landing(double rate, double T, double T_min) {
 	double result = rate;

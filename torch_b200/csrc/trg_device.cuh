@@ -3,13 +3,14 @@
 // Every routine restates a reference TORCH routine (cited beside it) with the
 // same operation order; the translation units that include this header are
 // compiled with --fmad=false so that each a*b+c rounds twice, as on the
-// reference's x86-64 build.  Transcendentals (exp, log, log10, pow) are CUDA's.
+// reference's x86-64 build.  Transcendentals come from trg_math.h.
 #pragma once
 
 #include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "trg_math.h"
 #include "trg_types.h"
 
 namespace trg {
@@ -206,8 +207,8 @@ __device__ __forceinline__ double spline_eval(const Spline& s, double x) {
 		else if (x < s.x[0]) return s.y[0] + s.min_slope * (x - s.x[0]);
 		return splint(s, x);
 	}
-	if (x > s.x[n - 1]) return s.y[n - 1] * pow(x / s.x[n - 1], s.max_slope);
-	else if (x < s.x[0]) return s.y[0] * pow(x / s.x[0], s.min_slope);
+	if (x > s.x[n - 1]) return s.y[n - 1] * trg_pow(x / s.x[n - 1], s.max_slope);
+	else if (x < s.x[0]) return s.y[0] * trg_pow(x / s.x[0], s.min_slope);
 	return splint(s, x);
 }
 
