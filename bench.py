@@ -222,25 +222,18 @@ def run_reference_arm(args, rank):
 
 
 # ----------------------------------------------------------------- GPU leg
-def run_ours(args, world, rank, local, pg):
+def time_form(args, precision, tp, ic, local, pg, profile_names, stream_mod):
+    """Times K full steps of one precision form; returns (ms, launches, prof, sim)."""
     import torch
     import torch_b200
-
-    precision = torch_b200.PRECISION_FP32 if args.precision == "fp32" else torch_b200.PRECISION_FP64
-    tp, ic = build_workload(args.workload, args.n)
-    N = int(np.prod(ic.ncells))
     sim = torch_b200.Torch(tp, ic, precision=precision, device=local)
     dt_next = sim.dt_max
     stream = torch.cuda.ExternalStream(sim.stream_handle(), device=f"cuda:{local}")
-
-    # warm-up (the first step is the reference's dt_max*1e-20 start step)
-    sim.run_steps(args.warmup)
+    sim.run_steps(args.warmup)  # the first step is the reference's dt_max*1e-20 start step
     launches0 = sim.kernel_launches()
     sim.profile(True)
-    clocks = ClockSampler(local)
     barrier(pg)
     torch.cuda.synchronize(local)
-    clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     sim.enqueue_steps(args.steps, dt_next)
@@ -248,29 +241,59 @@ def run_ours(args, world, rank, local, pg):
     sim.synchronize()
     torch.cuda.synchronize(local)
     barrier(pg)
-    clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
     launches = sim.kernel_launches() - launches0
     prof = {}
-    for name in ("k_hydro_stage_fp32", "k_faces_fp64", "k_hydro_update_fp64", "k_q_from_u", "k_dt_reduce",
-                 "k_rad_shell", "k_colden_shell", "k_thermo"):
+    for name in profile_names:
         t, c = sim.profile_read(name)
         if c:
             prof[name] = (t, c)
     sim.profile(False)
-    ms_max = max_over_ranks(pg, ms, local)
+    return ms, launches, prof, sim
+
+
+PROFILE_NAMES = ("k_hydro_stage_fp32", "k_faces_fp64", "k_hydro_update_fp64", "k_q_from_u", "k_dt_reduce",
+                 "k_dt_finalize", "k_dt_reset", "k_time_advance", "k_rad_shell", "k_colden_shell", "k_thermo",
+                 "k_rad_heating", "k_rad_update", "k_rad_wind")
+
+
+def run_ours(args, world, rank, local, pg):
+    import torch
+    import torch_b200
+
+    tp, ic = build_workload(args.workload, args.n)
+    N = int(np.prod(ic.ncells))
+    forms = ["fp32", "fp64"] if args.precision == "both" else [args.precision]
+    results = {}
+    clocks = ClockSampler(local)
+    clocks.start()
+    sims = {}
+    for form in forms:
+        prec = torch_b200.PRECISION_FP32 if form == "fp32" else torch_b200.PRECISION_FP64
+        ms, launches, prof, sim = time_form(args, prec, tp, ic, local, pg, PROFILE_NAMES, None)
+        ms = max_over_ranks(pg, ms, local)
+        results[form] = (ms, launches, prof)
+        sims[form] = sim
+    clk = clocks.stop()
+    head = forms[0]
+    ms_max, launches, prof = results[head]
     value = N * args.steps * world / (ms_max / 1e3)
+    sim = sims[head]
+    for form, s in sims.items():
+        if form != head:
+            s.close()
 
     # roofline of the dominant hydro kernel
     peak, peak_kind = hbm_peak()
-    if "k_hydro_stage_fp32" in prof:
+    if head == "fp32":
         kname = "k_hydro_stage_fp32"
-        # algorithmic bytes per cell per RK2 step in FP32: 140 B over two stage launches
+        # algorithmic bytes per cell per RK2 step in FP32: stage 1 reads U0 (28 B) and
+        # writes U* (28 B); stage 2 reads U* and U0 and writes U1 (84 B): 140 B per two launches
         alg_per_launch = 140.0 * N / 2.0
     else:
         kname = "k_faces_fp64"
         # FP64 plain form, per face-flux launch (one per dimension, 2 stages):
-        # reads the 7 primitive fields once (8 B each) and writes 7 flux fields
+        # reads the 7 primitive fields (8 B each) and writes 7 flux fields
         alg_per_launch = (7 * 8 + 7 * 8) * N
     tot_ms, count = prof.get(kname, (0.0, 0))
     avg_ms = tot_ms / count if count else float("nan")
@@ -285,14 +308,20 @@ def run_ours(args, world, rank, local, pg):
             traffic = None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                "kernel": kname, "peak_source": peak_kind, "avg_launch_ms": avg_ms, "launches": count,
-                "algorithmic_bytes_per_launch": alg_per_launch}
-    kernel_share = {k: {"ms": v[0], "launches": v[1], "share": v[0] / max(1e-9, sum(x[0] for x in prof.values()))}
-                    for k, v in prof.items()}
+                "kernel": kname, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "avg_launch_ms": avg_ms, "launches": count, "algorithmic_bytes_per_launch": alg_per_launch}
+    total_prof = sum(x[0] for x in prof.values())
+    kernel_share = {k: {"ms": v[0], "launches": v[1], "share": v[0] / max(1e-9, total_prof)} for k, v in prof.items()}
+    other = {}
+    for form in forms[1:]:
+        ms_o, l_o, p_o = results[form]
+        other[f"plain_{form}"] = {"value": N * args.steps * world / (ms_o / 1e3), "ms_per_step": ms_o / args.steps,
+                                  "gpu_launches": int(l_o)}
 
     # end to end: host buffers through the C ABI, copies inside the timed region
     e2e = None
     if args.e2e_steps > 0:
+        dt_next = sim.dt_max
         st = sim.state()
         U_host = torch.from_numpy(st.U).pin_memory()
         U_out = torch.empty_like(U_host).pin_memory()
@@ -308,7 +337,9 @@ def run_ours(args, world, rank, local, pg):
         wall = max_over_ranks(pg, wall, local)
         e2e = {"value": N * args.e2e_steps * world / wall, "unit": UNIT,
                "h2d_bytes_per_step": int(Un.nbytes), "d2h_bytes_per_step": int(Uo.nbytes),
-               "steps": args.e2e_steps, "note": "per step: pinned H2D of U, trg_full_step, D2H of U"}
+               "steps": args.e2e_steps,
+               "note": "per step through the C ABI: pinned H2D of U (FP64), trg_full_step, D2H of U (FP64)"}
+    sim.close()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -318,17 +349,17 @@ def run_ours(args, world, rank, local, pg):
             cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc}
         except Exception as e:  # a missing CPU baseline must not hide the GPU number
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable", "sample": str(e)[:200]}
-    sim.close()
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if precision else "f64", "data": "synthetic",
-            "config": workload_config(args.workload, args.n, args.precision, world),
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if head == "fp32" else "f64",
+            "data": "synthetic", "config": workload_config(args.workload, args.n, head, world),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk, "kernels": kernel_share,
         }
+        line.update(other)
         print(json.dumps(line), flush=True)
     return 0
 
@@ -341,7 +372,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["sedov", "hii"], default="sedov")
     ap.add_argument("--n", type=int, default=256)
-    ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp64")
+    ap.add_argument("--precision", choices=["both", "fp32", "fp64"], default="both")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -1,0 +1,73 @@
+"""FP32 form of the hydro pass against the FP64 form (which is bit-exact with
+the CPU oracle): per-field relative L1 error of density and pressure, the
+figure the FP32 form is judged by (north star: <= 1e-4 against FP64)."""
+import numpy as np
+import pytest
+
+import common
+import torch_b200
+from torch_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def run(tp, ic, steps, precision):
+    t = torch_b200.Torch(tp, ic, precision=precision)
+    t.run_steps(steps)
+    s = t.state()
+    t.close()
+    return s
+
+
+def errors(tp, ic, steps):
+    a = run(tp, ic, steps, torch_b200.PRECISION_FP32)
+    b = run(tp, ic, steps, torch_b200.PRECISION_FP64)
+    Pa = a.Q[1]
+    Pb = b.Q[1]
+    return common.rel_l1(a.U[0], b.U[0]), common.rel_l1(Pa, Pb), common.rel_l1(a.U[1], b.U[1]), a, b
+
+
+def test_fp32_sedov3d_error_vs_fp64():
+    tp, ic = workloads.sedov(n=48)
+    ed, ep, eE, a, b = errors(tp, ic, 60)
+    print(f"sedov48 60 steps: den {ed:.2e} pre {ep:.2e} E {eE:.2e}")
+    assert ed <= 1e-4 and ep <= 1e-4 and eE <= 1e-4
+
+
+def test_fp32_sedov2d_cylindrical_error_vs_fp64():
+    import dataclasses
+    tp, ic = workloads.sedov(n=64, nd=2)
+    tp = dataclasses.replace(tp, geometry="cylindrical")
+    ed, ep, eE, a, b = errors(tp, ic, 60)
+    print(f"sedov2d-cyl 60 steps: den {ed:.2e} pre {ep:.2e}")
+    assert ed <= 1e-4 and ep <= 1e-4
+
+
+@pytest.mark.parametrize("riemann,limiter,order", [("HLLC", "minmod", 1), ("HLL", "superbee", 0),
+                                                   ("RotatedHLLC", "monotonised_central", 1)])
+def test_fp32_solver_variants(riemann, limiter, order):
+    tp, ic = workloads.sedov(n=24, riemann=riemann, limiter=limiter, order=order)
+    rng = np.random.default_rng(3)
+    for d in range(3):
+        ic.vel[d] = rng.normal(0, 2e5, ic.den.size)
+    ed, ep, eE, a, b = errors(tp, ic, 20)
+    assert ed <= 1e-4 and ep <= 1e-3, (ed, ep)
+
+
+def test_fp32_conserves_mass_periodic():
+    import dataclasses
+    tp, ic = workloads.sedov(n=32)
+    tp = dataclasses.replace(tp, leftBC=("periodic",) * 3, rightBC=("periodic",) * 3)
+    t = torch_b200.Torch(tp, ic, precision=torch_b200.PRECISION_FP32)
+    m0 = t.state().U[0].astype(np.float64).sum()
+    t.run_steps(30)
+    m1 = t.state().U[0].astype(np.float64).sum()
+    t.close()
+    assert abs(m1 / m0 - 1) < 1e-5
+
+
+def test_fp32_non_multiple_tile_sizes():
+    """Grids that are not multiples of the 32 x 8 tile or of the z chunk."""
+    tp, ic = workloads.sedov(n=37)
+    ed, ep, eE, a, b = errors(tp, ic, 15)
+    assert ed <= 1e-4 and ep <= 1e-4

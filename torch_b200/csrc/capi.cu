@@ -32,6 +32,11 @@ struct trg_ctx {
 	int* d_sweep_all = nullptr;
 	int* d_sweep_nonwind = nullptr;
 	int* d_wind = nullptr;
+	// FP32 form: conserved state U0/U1 and the RK2 intermediate U*
+	bool fp32 = false;
+	float* U32 = nullptr;
+	float* U32s = nullptr;
+	int zchunk = 64;
 	std::vector<void*> allocs;
 	int first_time = 1;
 	int rad_once_pending = 1;
@@ -206,7 +211,32 @@ void time_step(trg_ctx* c, double dt_next) {
 	LAUNCH(k_dt_finalize, 1, 1, c->P, c->S, dt_next, 0, step);
 }
 
+void enqueue_full_step_fp32(trg_ctx* c, double dt_next) {
+	// Hydro-only Torch::fullStep in the FP32 form: dt comes from the CFL minimum
+	// the previous corrector reduced (FP64), the two RK2 stages are one fused
+	// kernel each.
+	int step = c->steps < c->dt_hist_cap ? (int)c->steps : -1;
+	LAUNCH(k_dt_finalize, 1, 1, c->P, c->S, dt_next, c->first_time, step);
+	c->first_time = 0;
+	LAUNCH(k_dt_reset, 1, 1, c->P, c->S);
+	auto stage = [&](int st, const float* Uq, const float* Ub, float* Uo) {
+		cudaEvent_t ea = nullptr, eb = nullptr;
+		if (c->profiling) { ea = pool_event(c); eb = pool_event(c); cudaEventRecord(ea, c->stream); }
+		launch_hydro_stage_fp32(st, c->P, c->S, Uq, Ub, Uo, c->zchunk, c->stream);
+		if (c->profiling) { cudaEventRecord(eb, c->stream); c->recs.push_back({"k_hydro_stage_fp32", ea, eb}); }
+		c->launches++;
+	};
+	stage(1, c->U32, c->U32, c->U32s);
+	stage(2, c->U32s, c->U32, c->U32);
+	LAUNCH(k_time_advance, 1, 1, c->S);
+	c->steps++;
+}
+
 void enqueue_full_step(trg_ctx* c, double dt_next) {
+	if (c->fp32) {
+		enqueue_full_step_fp32(c, dt_next);
+		return;
+	}
 	// Torch::fullStep, Torch.cpp:389-418
 	q_from_u(c, c->S.U, 1);
 	if (c->P.cooling_on) thermo_pre(c);
@@ -331,6 +361,14 @@ int trg_create(const trg_params* p, const double* den, const double* pre, const 
 		CUDA_TRY(cudaMemcpyAsync(c->d_wind, c->hs.wind_cells.data(), c->hs.wind_cells.size() * sizeof(int),
 		                         cudaMemcpyHostToDevice, st));
 	if ((rc = ensure_dt_hist(c, 1024))) return rc;
+	if (p->precision == TRG_PRECISION_FP32) {
+		if (c->hs.nactive != 1 || c->P.nd < 2)
+			return set_error(c, TRG_ERR_ARG, "the FP32 form runs hydro-only steps on 2-D and 3-D grids");
+		c->fp32 = true;
+		if ((rc = dalloc(c, &c->U32, 7 * N)) || (rc = dalloc(c, &c->U32s, 7 * N))) return rc;
+		LAUNCH(k_f64_to_f32, 7 * N, 256, S.U, c->U32, 7 * N);
+		CUDA_TRY(cudaMemsetAsync(c->U32s, 0, 7 * N * sizeof(float), st));
+	}
 	// Torch::run prologue (Torch.cpp:245-264): Q from U with floors, and the
 	// column-density ray trace of fillHeatingArrays (Thermodynamics.cpp:420-421).
 	q_from_u(c, S.U, 1);
@@ -403,6 +441,7 @@ int trg_profile_read(trg_ctx* c, const char* name, double* total_ms, long long* 
 
 int trg_component(trg_ctx* c, int comp, int phase, double dt, double* out) {
 	if (!c) return TRG_ERR_ARG;
+	if (c->fp32) return set_error(c, TRG_ERR_ARG, "per-component phases are provided by the FP64 form");
 	// The phase kernels read dt from the device scalar: stage the caller's dt.
 	CUDA_TRY(cudaMemcpyAsync(c->S.scal, &dt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
 	switch (phase) {
@@ -455,6 +494,11 @@ int trg_get_state(trg_ctx* c, double* U, double* Q, double* R, double* T, double
 	if (!c) return TRG_ERR_ARG;
 	const long long N = c->P.N;
 	cudaStream_t st = c->stream;
+	if (c->fp32) {
+		// expose the FP32 state as FP64 (Q = QfromU without floors)
+		LAUNCH(k_f32_to_f64, 7 * N, 256, c->U32, c->S.U, 7 * N);
+		q_from_u(c, c->S.U, 0);
+	}
 	if (U) CUDA_TRY(cudaMemcpyAsync(U, c->S.U, 7 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
 	if (Q) CUDA_TRY(cudaMemcpyAsync(Q, c->S.Q, 7 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
 	if (R) CUDA_TRY(cudaMemcpyAsync(R, c->S.R, 6 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -467,6 +511,7 @@ int trg_get_state(trg_ctx* c, double* U, double* Q, double* R, double* T, double
 int trg_set_conserved(trg_ctx* c, const double* U) {
 	if (!c || !U) return TRG_ERR_ARG;
 	CUDA_TRY(cudaMemcpyAsync(c->S.U, U, 7 * c->P.N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+	if (c->fp32) LAUNCH(k_f64_to_f32, 7 * c->P.N, 256, c->S.U, c->U32, 7 * c->P.N);
 	return TRG_OK;
 }
 

@@ -1,3 +1,567 @@
-// FP32 performance-form kernels (filled in below the FP64 parity form).
+// FP32 performance form of the hydro pass: one fused kernel per RK2 stage.
+//
+// Per stage and cell: Q = QfromU(U) (+ fixPrimitives in the predictor),
+// albada-limited piecewise-linear reconstruction, rotated HLLC-HLL flux on
+// every face, flux divergence with the geometric source terms and wind
+// injection, the Euler update and fixSolution - the work of
+// Hydrodynamics::integrate/updateSourceTerms + Fluid::advSolution/fixSolution
+// (src/Integrators/Hydro.cpp:31-156, src/Fluid/Fluid.cpp:80-136) - in one pass
+// over HBM: the predictor reads U0 and writes U*, the corrector reads U* and
+// U0 and writes U1, and also reduces the next CFL time step (FP64, Hydro.cpp:77-89).
+//
+// Tiling: a CTA owns a 32 x 8 column of cells and marches along z, keeping the
+// primitives of five consecutive z-planes (the stencil of the z faces) in a
+// shared-memory ring; x/y halos of two cells are loaded with each plane.  Every
+// cell is read from HBM once per CTA (plus the 2-cell x/y halos, which other
+// CTAs share through L2), and every face flux is evaluated once.
+//
+// The rotated solver is written in directional form: HLL with normal n1 and
+// HLLC with normal n2 are the reference's rotate / 1-D solve / rotate-back
+// sequences (Riemann.cpp:181-244) without the rotation matrices, since the HLL
+// and HLLC fluxes are rotation invariant.
+//
+// Pressure from total energy uses a compensated subtraction: the kinetic
+// energy is formed as a float pair with error-free products and sums, so that
+// E - KE loses no more than E's own rounding.
+#include <cuda_runtime.h>
+
 #include "trg_device.cuh"
 #include "trg_kernels.h"
+
+namespace trg {
+namespace f32 {
+
+constexpr int BX = 32, BY = 8, HALO = 2;
+constexpr int SX = BX + 2 * HALO, SY = BY + 2 * HALO;
+constexpr int NPLANE = 5;
+
+struct Prim {
+	float d, p, x, a, v[3];
+};
+
+__device__ __forceinline__ float fminf_(float a, float b) { return (b < a) ? b : a; }
+__device__ __forceinline__ float fmaxf_(float a, float b) { return (a < b) ? b : a; }
+
+// error-free transformations
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+	s = a + b;
+	float bb = s - a;
+	e = (a - (s - bb)) + (b - bb);
+}
+__device__ __forceinline__ void two_prod(float a, float b, float& p, float& e) {
+	p = a * b;
+	e = fmaf(a, b, -p);
+}
+
+// Q from U with the compensated E - KE.  KE = 0.5 |m|^2 / rho as a float pair.
+__device__ __forceinline__ Prim prim_from_cons(const float* u, float gamma, int nd) {
+	Prim q;
+	q.d = u[DEN];
+	float inv = 1.0f / u[DEN];
+	float s = 0.f, se = 0.f;
+	for (int k = 0; k < 3; ++k) {
+		q.v[k] = k < nd ? u[VEL + k] * inv : 0.f;
+		if (k < nd) {
+			float p, pe, t, te;
+			two_prod(u[VEL + k], u[VEL + k], p, pe);
+			two_sum(s, p, t, te);
+			s = t;
+			se += pe + te;
+		}
+	}
+	// ke = 0.5 (s + se) / rho as (kh, kl)
+	float kh = s * inv;
+	float r = fmaf(-kh, u[DEN], s);  // exact remainder of s / rho
+	float kl = (r + se) * inv;
+	kh *= 0.5f;
+	kl *= 0.5f;
+	float dh, dl;
+	two_sum(u[PRE], -kh, dh, dl);
+	q.p = (dh + (dl - kl)) * (gamma - 1.0f);
+	q.x = u[HII] * inv;
+	q.a = u[ADV] * inv;
+	return q;
+}
+
+__device__ __forceinline__ void fix_prim(const Params& P, Prim& q, float u_den) {
+	q.x = fmaxf_(fminf_(q.x, 1.f), 0.f);
+	q.a = fmaxf_(fminf_(q.a, 1.f), 0.f);
+	q.d = fmaxf_(q.d, (float)P.dfloor);
+	q.p = fmaxf_(q.p, (float)P.pfloor);
+	float mu_inv = (float)P.X * (q.x + 1.f) + (1.f - (float)P.X) * 0.25f;
+	float Rg = (float)P.specificGasConstant;
+	float temperature = q.p / (mu_inv * Rg * q.d);
+	if (temperature < (float)P.tfloor) q.p = mu_inv * Rg * u_den * (float)P.tfloor;
+}
+
+// Fluid::fixSolution in FP32 (compensated kinetic energy as in prim_from_cons).
+__device__ __forceinline__ bool fix_cons(const Params& P, float* u) {
+	if (!isfinite(u[DEN]) || !isfinite(u[PRE])) return false;
+	float inv = 1.0f / u[DEN];
+	float hii = fmaxf_(fminf_(u[HII] * inv, 1.f), 0.f);
+	float adv = fmaxf_(fminf_(u[ADV] * inv, 1.f), 0.f);
+	float den = fmaxf_(u[DEN], (float)P.dfloor);
+	float v[3] = {0.f, 0.f, 0.f};
+	for (int k = 0; k < P.nd; ++k) v[k] = u[VEL + k] * inv;
+	Prim q = prim_from_cons(u, (float)P.gamma, P.nd);
+	float pre = q.p;
+	float ke = 0.f;
+	for (int k = 0; k < P.nd; ++k) ke += v[k] * v[k];
+	ke *= 0.5f * den;
+	float pfloor = (float)P.pfloor;
+	if (pre < pfloor) pre = pfloor;
+	float mu_inv = (float)P.X * (hii + 1.f) + (1.f - (float)P.X) * 0.25f;
+	float Rg = (float)P.specificGasConstant;
+	float temperature = pre / (mu_inv * Rg * den);
+	if (temperature < (float)P.tfloor) pre = mu_inv * Rg * den * (float)P.tfloor;
+	u[DEN] = den;
+	u[PRE] = pre / ((float)P.gamma - 1.f) + ke;
+	u[HII] = hii * den;
+	u[ADV] = adv * den;
+	for (int k = 0; k < P.nd; ++k) u[VEL + k] = den * v[k];
+	if (u[DEN] == 0.f || u[PRE] == 0.f) return false;
+	for (int f = 0; f < NU; ++f)
+		if (!isfinite(u[f])) return false;
+	return true;
+}
+
+__device__ __forceinline__ float albada(float a, float b) {
+	float ab = a * b;
+	return ab <= 1.0e-30f ? 0.f : ab * (a + b) / (a * a + b * b);
+}
+__device__ __forceinline__ float minmod_(float a, float b) {
+	return (a * b > 0) ? (fabsf(a) < fabsf(b) ? a : b) : 0.f;
+}
+__device__ __forceinline__ float maxmod_(float a, float b) {
+	return (a * b > 0) ? (fabsf(a) > fabsf(b) ? a : b) : 0.f;
+}
+__device__ __forceinline__ float limiter32(int kind, float a, float b) {
+	switch (kind) {
+	case 0: return minmod_((a + b) * 0.5f, minmod_(2.f * a, 2.f * b));
+	case 1: return maxmod_(minmod_(b, 2.f * a), minmod_(2.f * b, a));
+	case 2: return minmod_(a, b);
+	case 3: return maxmod_(a, b);
+	case 4: {
+		if (b == 0) return 0.f;
+		float r = fabsf(a / b);
+		return (a + b * r) / (1.f + r);
+	}
+	case 5: return (a * b <= 1.0e-30f) ? 0.f : 1.5f * b * (a * a + a * b) / (a * a + a * b + b * b);
+	default: return albada(a, b);
+	}
+}
+
+// Reconstructed face states: left = QR of cell c1 from (c0,c1,c2),
+// right = QL of cell c2 from (c1,c2,c3) (Hydro.cpp:44-50).
+__device__ __forceinline__ void reconstruct(int lim, const Prim& c0, const Prim& c1, const Prim& c2, const Prim& c3,
+                                            Prim& L, Prim& R) {
+#define REC(field)                                                                      \
+	{                                                                                   \
+		float sl = limiter32(lim, c1.field - c0.field, c2.field - c1.field);            \
+		float sr = limiter32(lim, c2.field - c1.field, c3.field - c2.field);            \
+		L.field = c1.field + 0.5f * sl;                                                 \
+		R.field = c2.field - 0.5f * sr;                                                 \
+	}
+	REC(d) REC(p) REC(x) REC(a) REC(v[0]) REC(v[1]) REC(v[2])
+#undef REC
+}
+
+struct Flux {
+	float f[7];
+};
+
+// Physical flux and conserved state of a primitive state along unit normal n.
+__device__ __forceinline__ void flux_n(const Prim& q, const float* n, float g1inv, float& un, float* U, float* F) {
+	un = q.v[0] * n[0] + q.v[1] * n[1] + q.v[2] * n[2];
+	float ke = 0.5f * q.d * (q.v[0] * q.v[0] + q.v[1] * q.v[1] + q.v[2] * q.v[2]);
+	float E = q.p * g1inv + ke;
+	float mflux = q.d * un;
+	U[DEN] = q.d;
+	U[PRE] = E;
+	U[HII] = q.d * q.x;
+	U[ADV] = q.d * q.a;
+	F[DEN] = mflux;
+	F[PRE] = (E + q.p) * un;
+	F[HII] = mflux * q.x;
+	F[ADV] = mflux * q.a;
+	for (int k = 0; k < 3; ++k) {
+		U[VEL + k] = q.d * q.v[k];
+		F[VEL + k] = mflux * q.v[k] + q.p * n[k];
+	}
+}
+
+// Einfeldt speeds along n (characteristicWaveSpeeds, Riemann.cpp:27-42).
+__device__ __forceinline__ void speeds_n(const Prim& L, const Prim& R, float unL, float unR, float gamma, float& SL,
+                                         float& SR) {
+	float sl = sqrtf(L.d), sr = sqrtf(R.d);
+	float inv = 1.f / (sl + sr);
+	float ut = (sl * unL + sr * unR) * inv;
+	float nu2 = 0.5f * sr * sl * inv * inv;
+	float aL2 = gamma * L.p / L.d, aR2 = gamma * R.p / R.d;
+	float d2 = (sl * aL2 + sr * aR2) * inv + nu2 * (unR - unL) * (unR - unL);
+	float dd = sqrtf(d2);
+	SL = ut - dd;
+	SR = ut + dd;
+}
+
+__device__ __forceinline__ void hll_n(const Prim& L, const Prim& R, const float* n, float gamma, float g1inv, float* F) {
+	float UL[7], FL[7], UR[7], FR[7], unL, unR, SL, SR;
+	flux_n(L, n, g1inv, unL, UL, FL);
+	flux_n(R, n, g1inv, unR, UR, FR);
+	speeds_n(L, R, unL, unR, gamma, SL, SR);
+	if (SR <= 0) {
+		for (int i = 0; i < 7; ++i) F[i] = FR[i];
+	} else if (SL >= 0) {
+		for (int i = 0; i < 7; ++i) F[i] = FL[i];
+	} else {
+		float inv = 1.f / (SR - SL);
+		for (int i = 0; i < 7; ++i) F[i] = (SR * FL[i] - SL * FR[i] + SL * SR * (UR[i] - UL[i])) * inv;
+	}
+}
+
+__device__ __forceinline__ void hllc_n(const Prim& L, const Prim& R, const float* n, float gamma, float g1inv, float* F) {
+	float UL[7], FL[7], UR[7], FR[7], unL, unR, SL, SR;
+	flux_n(L, n, g1inv, unL, UL, FL);
+	flux_n(R, n, g1inv, unR, UR, FR);
+	speeds_n(L, R, unL, unR, gamma, SL, SR);
+	if (SL >= 0) {
+		for (int i = 0; i < 7; ++i) F[i] = FL[i];
+	} else if (SR <= 0) {
+		for (int i = 0; i < 7; ++i) F[i] = FR[i];
+	} else {
+		float mL = L.d * (SL - unL), mR = R.d * (SR - unR);
+		float Sc = (R.p - L.p + mL * unL - mR * unR) / (mL - mR);
+		bool left = Sc >= 0;
+		const Prim& K = left ? L : R;
+		const float* UK = left ? UL : UR;
+		const float* FK = left ? FL : FR;
+		float SK = left ? SL : SR, unK = left ? unL : unR;
+		float mK = K.d * (SK - unK);
+		float A = mK / (SK - Sc);
+		float Us[7];
+		Us[DEN] = A;
+		Us[PRE] = A * (UK[PRE] / K.d + (Sc - unK) * (Sc + K.p / mK));
+		Us[HII] = A * K.x;
+		Us[ADV] = A * K.a;
+		for (int k = 0; k < 3; ++k) Us[VEL + k] = A * (K.v[k] + (Sc - unK) * n[k]);
+		for (int i = 0; i < 7; ++i) F[i] = FK[i] + SK * (Us[i] - UK[i]);
+	}
+}
+
+// Rotated HLLC-HLL flux through a face with normal e_dim (Riemann.cpp:181-244).
+__device__ __forceinline__ void riemann32(int kind, const Prim& L, const Prim& R, int dim, float gamma, float* F) {
+	const float g1inv = 1.f / (gamma - 1.f);
+	float d[3] = {dim == 0 ? 1.f : 0.f, dim == 1 ? 1.f : 0.f, dim == 2 ? 1.f : 0.f};
+	if (kind == RS_HLLC) { hllc_n(L, R, d, gamma, g1inv, F); return; }
+	if (kind == RS_HLL) { hll_n(L, R, d, gamma, g1inv, F); return; }
+	float n1[3] = {R.v[0] - L.v[0], R.v[1] - L.v[1], R.v[2] - L.v[2]};
+	if (n1[dim] < 0) { n1[0] = -n1[0]; n1[1] = -n1[1]; n1[2] = -n1[2]; }
+	float nn = n1[0] * n1[0] + n1[1] * n1[1] + n1[2] * n1[2];
+	if (nn < 1.0e-12f) { hllc_n(L, R, d, gamma, g1inv, F); return; }
+	float inv = rsqrtf(nn);
+	n1[0] *= inv; n1[1] *= inv; n1[2] *= inv;
+	// t = n1 x d, n2 = t x n1 = d - (n1.d) n1
+	float c = n1[dim];
+	float n2[3] = {d[0] - c * n1[0], d[1] - c * n1[1], d[2] - c * n1[2]};
+	float n2n = n2[0] * n2[0] + n2[1] * n2[1] + n2[2] * n2[2];
+	if (n2n <= 1.0e-14f) { hll_n(L, R, d, gamma, g1inv, F); return; }   // n1 parallel to d
+	float inv2 = rsqrtf(n2n);
+	n2[0] *= inv2; n2[1] *= inv2; n2[2] *= inv2;
+	if (fabsf(c) <= 1.0e-7f) { hllc_n(L, R, d, gamma, g1inv, F); return; }  // n1 normal to d: n2 = d
+	float F1[7], F2[7];
+	hll_n(L, R, n1, gamma, g1inv, F1);
+	hllc_n(L, R, n2, gamma, g1inv, F2);
+	float w1 = fabsf(c), w2 = fabsf(n2[dim]);
+	for (int i = 0; i < 7; ++i) F[i] = w1 * F1[i] + w2 * F2[i];
+}
+
+struct SmemQ {
+	float v[NPLANE][7][SY][SX];
+};
+
+// Source position (with the boundary rule) of coordinate c along dim.
+__device__ __forceinline__ int bc_src(const Params& P, int dim, int c, int n, int& flip_cond, int& side) {
+	flip_cond = -1;
+	side = 0;
+	if (c < 0) {
+		int k = -c;
+		flip_cond = P.lbc[dim];
+		return flip_cond == BC_PERIODIC ? n - k : (flip_cond == BC_REFLECTING ? k : 0);
+	}
+	if (c >= n) {
+		int k = c - n + 1;
+		flip_cond = P.rbc[dim];
+		side = 1;
+		return flip_cond == BC_PERIODIC ? k - 1 : (flip_cond == BC_REFLECTING ? n - 1 - k : n - 1);
+	}
+	return c;
+}
+
+__device__ __forceinline__ void apply_flip(Prim& q, int dim, int cond, int side) {
+	if (cond < 0) return;
+	float v = q.v[dim];
+	if (cond == BC_INFLOW) {
+		if (side == 0 ? v < 0 : v > 0) q.v[dim] = -v;
+	} else if (cond == BC_OUTFLOW) {
+		if (side == 0 ? v > 0 : v < 0) q.v[dim] = -v;
+	} else if (cond == BC_REFLECTING) {
+		q.v[dim] = -v;
+	}
+}
+
+// Loads plane z (global index, may be a ghost plane) of the CTA's x/y box into ring slot.
+template <int STAGE>
+__device__ __forceinline__ void load_plane(const Params& P, const float* __restrict__ U, SmemQ& s, int slot, int x0, int y0,
+                                           int z) {
+	int zc, zside;
+	int zs = P.nd > 2 ? bc_src(P, 2, z, P.nz, zc, zside) : 0;
+	if (P.nd <= 2) zc = -1;
+	const long long N = P.N;
+	for (int idx = threadIdx.x; idx < SX * SY; idx += blockDim.x) {
+		int ly = idx / SX, lx = idx - ly * SX;
+		bool xh = lx < HALO || lx >= HALO + BX, yh = ly < HALO || ly >= HALO + BY;
+		if (xh && yh) continue;  // corners: never part of a stencil
+		int gx = x0 + lx - HALO, gy = y0 + ly - HALO;
+		int xc, xside, yc, yside;
+		int xs = bc_src(P, 0, gx, P.nx, xc, xside);
+		int ys = P.nd > 1 ? bc_src(P, 1, gy, P.ny, yc, yside) : 0;
+		if (P.nd <= 1) yc = -1;
+		if (xs < 0 || xs >= P.nx || ys < 0 || ys >= P.ny) continue;  // tile beyond a ragged grid edge
+		long long id = xs + (long long)P.nx * (ys + (long long)P.ny * zs);
+		float u[7];
+#pragma unroll
+		for (int f = 0; f < 7; ++f) u[f] = __ldg(&U[f * N + id]);
+		Prim q = prim_from_cons(u, (float)P.gamma, P.nd);
+		if (STAGE == 1) fix_prim(P, q, u[DEN]);
+		apply_flip(q, 0, xc, xside);
+		if (P.nd > 1) apply_flip(q, 1, yc, yside);
+		if (P.nd > 2) apply_flip(q, 2, zc, zside);
+		s.v[slot][DEN][ly][lx] = q.d;
+		s.v[slot][PRE][ly][lx] = q.p;
+		s.v[slot][HII][ly][lx] = q.x;
+		s.v[slot][ADV][ly][lx] = q.a;
+		s.v[slot][VEL + 0][ly][lx] = q.v[0];
+		s.v[slot][VEL + 1][ly][lx] = q.v[1];
+		s.v[slot][VEL + 2][ly][lx] = q.v[2];
+	}
+}
+
+__device__ __forceinline__ Prim get(const SmemQ& s, int slot, int ly, int lx) {
+	Prim q;
+	q.d = s.v[slot][DEN][ly][lx];
+	q.p = s.v[slot][PRE][ly][lx];
+	q.x = s.v[slot][HII][ly][lx];
+	q.a = s.v[slot][ADV][ly][lx];
+	q.v[0] = s.v[slot][VEL + 0][ly][lx];
+	q.v[1] = s.v[slot][VEL + 1][ly][lx];
+	q.v[2] = s.v[slot][VEL + 2][ly][lx];
+	return q;
+}
+
+__device__ __forceinline__ double dmin_(double a, double b) { return (b < a) ? b : a; }
+
+}  // namespace f32
+
+using namespace f32;
+
+// One RK2 stage (STAGE 1: predictor with floors on Q, h = 1/2; STAGE 2:
+// corrector on Q(U*), h = 1, plus the next step's CFL minimum).
+// Ubase: the state the Euler update starts from (U0 in both stages);
+// Uq: the state the primitives come from (U0, then U*); Uout: result.
+template <int STAGE>
+__global__ void __launch_bounds__(BX* BY, 2)
+    k_hydro_stage_fp32(Params P, State S, const float* __restrict__ Uq, const float* __restrict__ Ubase,
+                       float* __restrict__ Uout, int zchunk) {
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	SmemQ& s = *reinterpret_cast<SmemQ*>(smem_raw);
+	float* Fx = reinterpret_cast<float*>(smem_raw + sizeof(SmemQ));   // [7][BY][BX+1]
+	float* Fy = Fx + 7 * BY * (BX + 1);                                  // [7][BY+1][BX]
+	const int tx = threadIdx.x % BX, ty = threadIdx.x / BX;
+	const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY;
+	const int z0 = blockIdx.z * zchunk;
+	const int z1 = min(z0 + zchunk, P.nz);
+	const int nd = P.nd;
+	const float gamma = (float)P.gamma;
+	const double dt = (STAGE == 1 ? 0.5 : 1.0) * S.scal[0];
+	const float dtf = (float)dt;
+	const long long N = P.N;
+	const int gx = x0 + tx, gy = y0 + ty;
+	const bool active = gx < P.nx && gy < P.ny;
+	double tmin = 1.0e308;
+	bool bad = false;
+
+	// preload planes z0-2 .. z0+1 (ring slots by z mod 5)
+	auto slot_of = [](int z) { return ((z % NPLANE) + NPLANE) % NPLANE; };
+	if (nd > 2) {
+		for (int z = z0 - 2; z <= z0 + 1; ++z) load_plane<STAGE>(P, Uq, s, slot_of(z), x0, y0, z);
+	} else {
+		load_plane<STAGE>(P, Uq, s, 0, x0, y0, 0);
+	}
+	__syncthreads();
+
+	float Fzm[7];
+	if (nd > 2 && active) {
+		// flux through the face z0 - 1/2
+		Prim c0 = get(s, slot_of(z0 - 2), ty + HALO, tx + HALO), c1 = get(s, slot_of(z0 - 1), ty + HALO, tx + HALO);
+		Prim c2 = get(s, slot_of(z0), ty + HALO, tx + HALO), c3 = get(s, slot_of(z0 + 1), ty + HALO, tx + HALO);
+		Prim L, R;
+		if (P.order == 1) reconstruct(P.limiter, c0, c1, c2, c3, L, R);
+		else { L = c1; R = c2; }
+		riemann32(P.riemann, L, R, 2, gamma, Fzm);
+	}
+
+	for (int z = z0; z < z1; ++z) {
+		const int sc = nd > 2 ? slot_of(z) : 0;
+		if (nd > 2) {
+			load_plane<STAGE>(P, Uq, s, slot_of(z + 2), x0, y0, z + 2);
+			__syncthreads();
+		}
+		// x faces of plane z: (BX+1) x BY
+		for (int f = threadIdx.x; f < (BX + 1) * BY; f += blockDim.x) {
+			int fy = f / (BX + 1), fx = f - fy * (BX + 1);
+			if (x0 + fx > P.nx || y0 + fy >= P.ny) continue;
+			int ly = fy + HALO;
+			Prim c0 = get(s, sc, ly, fx), c1 = get(s, sc, ly, fx + 1), c2 = get(s, sc, ly, fx + 2), c3 = get(s, sc, ly, fx + 3);
+			Prim L, R;
+			float F[7];
+			if (P.order == 1) reconstruct(P.limiter, c0, c1, c2, c3, L, R);
+			else { L = c1; R = c2; }
+			riemann32(P.riemann, L, R, 0, gamma, F);
+#pragma unroll
+			for (int i = 0; i < 7; ++i) Fx[(i * BY + fy) * (BX + 1) + fx] = F[i];
+		}
+		if (nd > 1) {
+			for (int f = threadIdx.x; f < BX * (BY + 1); f += blockDim.x) {
+				int fy = f / BX, fx = f - fy * BX;
+				if (x0 + fx >= P.nx || y0 + fy > P.ny) continue;
+				int lx = fx + HALO;
+				Prim c0 = get(s, sc, fy, lx), c1 = get(s, sc, fy + 1, lx), c2 = get(s, sc, fy + 2, lx), c3 = get(s, sc, fy + 3, lx);
+				Prim L, R;
+				float F[7];
+				if (P.order == 1) reconstruct(P.limiter, c0, c1, c2, c3, L, R);
+				else { L = c1; R = c2; }
+				riemann32(P.riemann, L, R, 1, gamma, F);
+#pragma unroll
+				for (int i = 0; i < 7; ++i) Fy[(i * (BY + 1) + fy) * BX + fx] = F[i];
+			}
+		}
+		float Fzp[7];
+		if (nd > 2 && active) {
+			Prim c0 = get(s, slot_of(z - 1), ty + HALO, tx + HALO), c1 = get(s, sc, ty + HALO, tx + HALO);
+			Prim c2 = get(s, slot_of(z + 1), ty + HALO, tx + HALO), c3 = get(s, slot_of(z + 2), ty + HALO, tx + HALO);
+			Prim L, R;
+			if (P.order == 1) reconstruct(P.limiter, c0, c1, c2, c3, L, R);
+			else { L = c1; R = c2; }
+			riemann32(P.riemann, L, R, 2, gamma, Fzp);
+		}
+		__syncthreads();
+		if (active) {
+			const long long id = gx + (long long)P.nx * (gy + (long long)P.ny * z);
+			int ijk[3] = {gx, gy, z};
+			double xc[3];
+			cell_xc(P, ijk, xc);
+			// areas / volume (Grid.cpp:846-905) in FP64, once per cell
+			double vol = cell_volume(P, xc[0]);
+			float udot[7] = {0, 0, 0, 0, 0, 0, 0};
+			{
+				float al = (float)(face_area(P, xc, 0, 0) / vol), ar = (float)(face_area(P, xc, 0, 1) / vol);
+#pragma unroll
+				for (int i = 0; i < 7; ++i)
+					udot[i] += al * Fx[(i * BY + ty) * (BX + 1) + tx] - ar * Fx[(i * BY + ty) * (BX + 1) + tx + 1];
+			}
+			if (nd > 1) {
+				float al = (float)(face_area(P, xc, 1, 0) / vol), ar = (float)(face_area(P, xc, 1, 1) / vol);
+#pragma unroll
+				for (int i = 0; i < 7; ++i)
+					udot[i] += al * Fy[(i * (BY + 1) + ty) * BX + tx] - ar * Fy[(i * (BY + 1) + ty + 1) * BX + tx];
+			}
+			if (nd > 2) {
+				float al = (float)(face_area(P, xc, 2, 0) / vol), ar = (float)(face_area(P, xc, 2, 1) / vol);
+#pragma unroll
+				for (int i = 0; i < 7; ++i) udot[i] += al * Fzm[i] - ar * Fzp[i];
+			}
+			Prim qc = get(s, sc, ty + HALO, tx + HALO);
+			if (S.grav) {
+				for (int k = 0; k < 3; ++k) {
+					float g = (float)S.grav[(long long)k * N + id];
+					udot[VEL + k] += g;
+					udot[PRE] += qc.v[k] * g;
+				}
+			}
+			if (P.geometry == G_CYL) {
+				udot[VEL + 0] += qc.p / (float)(P.dx[0] * xc[0]);
+			} else if (P.geometry == G_SPH) {
+				double r = vol / (face_area(P, xc, 0, 1) - face_area(P, xc, 0, 0));
+				udot[VEL + 0] += qc.p / (float)r;
+			}
+			float ub[7];
+#pragma unroll
+			for (int i = 0; i < 7; ++i) ub[i] = Ubase[i * N + id];
+			if (P.star_on && P.mdot != 0 && is_wind(P, id, ijk, xc)) {
+				float mdot = (float)P.mdot;
+				udot[DEN] += mdot;
+				udot[PRE] += (float)P.edot;
+				udot[HII] += (ub[HII] / ub[DEN]) * mdot;
+				udot[ADV] += mdot;
+			}
+			float u[7];
+#pragma unroll
+			for (int i = 0; i < 7; ++i) u[i] = ub[i] + dtf * udot[i];
+			bad |= !fix_cons(P, u);
+#pragma unroll
+			for (int i = 0; i < 7; ++i) Uout[i * N + id] = u[i];
+			if (STAGE == 2) {
+				// the next step's CFL limit from Q(U1) with floors (Torch::fullStep:
+				// globalQfromU + fixPrimitives, then Hydrodynamics::calculateTimeStep)
+				Prim q = prim_from_cons(u, gamma, nd);
+				fix_prim(P, q, u[DEN]);
+				double ss = sqrt(P.gamma * (double)q.p / (double)q.d);
+				double inv_t = 0;
+				for (int k = 0; k < nd; ++k) inv_t += (fabs((double)q.v[k]) + ss) / P.dx[k];
+				if (inv_t == 0) inv_t = 1.0 / P.dt_max;
+				tmin = dmin_(tmin, 0.5 / inv_t);
+			}
+		}
+		if (nd > 2)
+#pragma unroll
+			for (int i = 0; i < 7; ++i) Fzm[i] = Fzp[i];
+		__syncthreads();
+	}
+	if (bad) atomicOr(S.err, ERRB_NAN);
+	if (STAGE == 2) {
+		for (int o = 16; o > 0; o >>= 1) tmin = dmin_(tmin, __shfl_down_sync(0xffffffffu, tmin, o));
+		if ((threadIdx.x & 31) == 0) {
+			unsigned long long* slots = reinterpret_cast<unsigned long long*>(S.scal + 2);
+			atomicMin(&slots[0], (unsigned long long)__double_as_longlong(tmin));
+		}
+	}
+}
+
+size_t hydro_stage_fp32_smem() {
+	return sizeof(SmemQ) + sizeof(float) * 7 * (BY * (BX + 1) + (BY + 1) * BX);
+}
+
+void launch_hydro_stage_fp32(int stage, const Params& P, const State& S, const float* Uq, const float* Ubase,
+                             float* Uout, int zchunk, cudaStream_t stream) {
+	size_t smem = hydro_stage_fp32_smem();
+	dim3 grid((P.nx + BX - 1) / BX, (P.ny + BY - 1) / BY, (P.nz + zchunk - 1) / zchunk);
+	if (stage == 1) {
+		cudaFuncSetAttribute(k_hydro_stage_fp32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+		k_hydro_stage_fp32<1><<<grid, BX * BY, smem, stream>>>(P, S, Uq, Ubase, Uout, zchunk);
+	} else {
+		cudaFuncSetAttribute(k_hydro_stage_fp32<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+		k_hydro_stage_fp32<2><<<grid, BX * BY, smem, stream>>>(P, S, Uq, Ubase, Uout, zchunk);
+	}
+}
+
+// FP64 <-> FP32 state conversion (entry to / exit from the FP32 form).
+__global__ void k_f64_to_f32(const double* __restrict__ a, float* __restrict__ b, long long n) {
+	long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (i < n) b[i] = (float)a[i];
+}
+__global__ void k_f32_to_f64(const float* __restrict__ a, double* __restrict__ b, long long n) {
+	long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (i < n) b[i] = (double)a[i];
+}
+
+}  // namespace trg

@@ -21,4 +21,10 @@ __global__ void k_dt_reduce_fp64(Params P, State S, long long first_cell);
 __global__ void k_dt_finalize(Params P, State S, double dt_next, int first_time, int step);
 __global__ void k_time_advance(State S);
 __global__ void k_dt_reset(Params P, State S);
+// FP32 form of the hydro pass (kernels_fp32.cu)
+void launch_hydro_stage_fp32(int stage, const Params& P, const State& S, const float* Uq, const float* Ubase,
+                             float* Uout, int zchunk, cudaStream_t stream);
+size_t hydro_stage_fp32_smem();
+__global__ void k_f64_to_f32(const double* a, float* b, long long n);
+__global__ void k_f32_to_f64(const float* a, double* b, long long n);
 }  // namespace trg
