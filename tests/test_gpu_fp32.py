@@ -19,11 +19,18 @@ def run(tp, ic, steps, precision):
     return s
 
 
+def pressure(U, gamma, nd):
+    """P = (E - |m|^2 / (2 rho)) (gamma - 1) from the conserved state (FP64)."""
+    ke = sum(U[4 + k] ** 2 for k in range(nd)) / (2.0 * U[0])
+    return (U[1] - ke) * (gamma - 1.0)
+
+
 def errors(tp, ic, steps):
     a = run(tp, ic, steps, torch_b200.PRECISION_FP32)
     b = run(tp, ic, steps, torch_b200.PRECISION_FP64)
-    Pa = a.Q[1]
-    Pb = b.Q[1]
+    nd = ic.nd
+    Pa = pressure(a.U, tp.heatCapacityRatio, nd)
+    Pb = pressure(b.U, tp.heatCapacityRatio, nd)
     return common.rel_l1(a.U[0], b.U[0]), common.rel_l1(Pa, Pb), common.rel_l1(a.U[1], b.U[1]), a, b
 
 

@@ -365,6 +365,17 @@ int trg_create(const trg_params* p, const double* den, const double* pre, const 
 		if (c->hs.nactive != 1 || c->P.nd < 2)
 			return set_error(c, TRG_ERR_ARG, "the FP32 form runs hydro-only steps on 2-D and 3-D grids");
 		c->fp32 = true;
+		{
+			// z chunk per CTA: aim for about four waves of two 256-thread CTAs per SM
+			int dev_sms = 148;
+			cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, p->device);
+			long long tiles = (long long)((c->P.nx + 31) / 32) * ((c->P.ny + 7) / 8);
+			long long want = 4LL * 2 * dev_sms;
+			long long nchunks = (want + tiles - 1) / tiles;
+			if (nchunks < 1) nchunks = 1;
+			int zc = (int)((c->P.nz + nchunks - 1) / nchunks);
+			c->zchunk = zc < 16 ? 16 : zc;
+		}
 		if ((rc = dalloc(c, &c->U32, 7 * N)) || (rc = dalloc(c, &c->U32s, 7 * N))) return rc;
 		LAUNCH(k_f64_to_f32, 7 * N, 256, S.U, c->U32, 7 * N);
 		CUDA_TRY(cudaMemsetAsync(c->U32s, 0, 7 * N * sizeof(float), st));

@@ -59,6 +59,7 @@ __device__ __forceinline__ Prim prim_from_cons(const float* u, float gamma, int 
 	q.d = u[DEN];
 	float inv = 1.0f / u[DEN];
 	float s = 0.f, se = 0.f;
+#pragma unroll
 	for (int k = 0; k < 3; ++k) {
 		q.v[k] = k < nd ? u[VEL + k] * inv : 0.f;
 		if (k < nd) {
@@ -101,12 +102,13 @@ __device__ __forceinline__ bool fix_cons(const Params& P, float* u) {
 	float hii = fmaxf_(fminf_(u[HII] * inv, 1.f), 0.f);
 	float adv = fmaxf_(fminf_(u[ADV] * inv, 1.f), 0.f);
 	float den = fmaxf_(u[DEN], (float)P.dfloor);
-	float v[3] = {0.f, 0.f, 0.f};
-	for (int k = 0; k < P.nd; ++k) v[k] = u[VEL + k] * inv;
-	Prim q = prim_from_cons(u, (float)P.gamma, P.nd);
+	const int nd = P.nd;
+	float v[3];
+#pragma unroll
+	for (int k = 0; k < 3; ++k) v[k] = k < nd ? u[VEL + k] * inv : 0.f;
+	Prim q = prim_from_cons(u, (float)P.gamma, nd);
 	float pre = q.p;
-	float ke = 0.f;
-	for (int k = 0; k < P.nd; ++k) ke += v[k] * v[k];
+	float ke = (v[0] * v[0] + v[1] * v[1]) + v[2] * v[2];
 	ke *= 0.5f * den;
 	float pfloor = (float)P.pfloor;
 	if (pre < pfloor) pre = pfloor;
@@ -118,11 +120,14 @@ __device__ __forceinline__ bool fix_cons(const Params& P, float* u) {
 	u[PRE] = pre / ((float)P.gamma - 1.f) + ke;
 	u[HII] = hii * den;
 	u[ADV] = adv * den;
-	for (int k = 0; k < P.nd; ++k) u[VEL + k] = den * v[k];
+#pragma unroll
+	for (int k = 0; k < 3; ++k)
+		if (k < nd) u[VEL + k] = den * v[k];
 	if (u[DEN] == 0.f || u[PRE] == 0.f) return false;
-	for (int f = 0; f < NU; ++f)
-		if (!isfinite(u[f])) return false;
-	return true;
+	bool ok = true;
+#pragma unroll
+	for (int f = 0; f < NU; ++f) ok &= isfinite(u[f]);
+	return ok;
 }
 
 __device__ __forceinline__ float albada(float a, float b) {
@@ -249,30 +254,33 @@ __device__ __forceinline__ void hllc_n(const Prim& L, const Prim& R, const float
 }
 
 // Rotated HLLC-HLL flux through a face with normal e_dim (Riemann.cpp:181-244).
+// No array is indexed with the run-time dim, so everything stays in registers.
 __device__ __forceinline__ void riemann32(int kind, const Prim& L, const Prim& R, int dim, float gamma, float* F) {
 	const float g1inv = 1.f / (gamma - 1.f);
-	float d[3] = {dim == 0 ? 1.f : 0.f, dim == 1 ? 1.f : 0.f, dim == 2 ? 1.f : 0.f};
+	const float d[3] = {dim == 0 ? 1.f : 0.f, dim == 1 ? 1.f : 0.f, dim == 2 ? 1.f : 0.f};
 	if (kind == RS_HLLC) { hllc_n(L, R, d, gamma, g1inv, F); return; }
 	if (kind == RS_HLL) { hll_n(L, R, d, gamma, g1inv, F); return; }
 	float n1[3] = {R.v[0] - L.v[0], R.v[1] - L.v[1], R.v[2] - L.v[2]};
-	if (n1[dim] < 0) { n1[0] = -n1[0]; n1[1] = -n1[1]; n1[2] = -n1[2]; }
+	float c = n1[0] * d[0] + n1[1] * d[1] + n1[2] * d[2];
+	float sgn = c < 0 ? -1.f : 1.f;  // orient n1 . d >= 0
 	float nn = n1[0] * n1[0] + n1[1] * n1[1] + n1[2] * n1[2];
-	if (nn < 1.0e-12f) { hllc_n(L, R, d, gamma, g1inv, F); return; }
-	float inv = rsqrtf(nn);
+	if (nn < 1.0e-12f) { hllc_n(L, R, d, gamma, g1inv, F); return; }  // |dv| < 1e-6
+	float inv = sgn * rsqrtf(nn);
 	n1[0] *= inv; n1[1] *= inv; n1[2] *= inv;
-	// t = n1 x d, n2 = t x n1 = d - (n1.d) n1
-	float c = n1[dim];
+	c = n1[0] * d[0] + n1[1] * d[1] + n1[2] * d[2];
+	// n2 = (n1 x d) x n1 = d - (n1 . d) n1, already oriented with n2 . d >= 0
 	float n2[3] = {d[0] - c * n1[0], d[1] - c * n1[1], d[2] - c * n1[2]};
 	float n2n = n2[0] * n2[0] + n2[1] * n2[1] + n2[2] * n2[2];
 	if (n2n <= 1.0e-14f) { hll_n(L, R, d, gamma, g1inv, F); return; }   // n1 parallel to d
+	if (c <= 1.0e-7f) { hllc_n(L, R, d, gamma, g1inv, F); return; }     // n1 normal to d: n2 = d
 	float inv2 = rsqrtf(n2n);
 	n2[0] *= inv2; n2[1] *= inv2; n2[2] *= inv2;
-	if (fabsf(c) <= 1.0e-7f) { hllc_n(L, R, d, gamma, g1inv, F); return; }  // n1 normal to d: n2 = d
 	float F1[7], F2[7];
 	hll_n(L, R, n1, gamma, g1inv, F1);
 	hllc_n(L, R, n2, gamma, g1inv, F2);
-	float w1 = fabsf(c), w2 = fabsf(n2[dim]);
-	for (int i = 0; i < 7; ++i) F[i] = w1 * F1[i] + w2 * F2[i];
+	float w2 = n2[0] * d[0] + n2[1] * d[1] + n2[2] * d[2];
+#pragma unroll
+	for (int i = 0; i < 7; ++i) F[i] = c * F1[i] + w2 * F2[i];
 }
 
 struct SmemQ {
@@ -364,11 +372,28 @@ __device__ __forceinline__ double dmin_(double a, double b) { return (b < a) ? b
 
 using namespace f32;
 
+// Reconstruction + Riemann solve for one face (the single call site of the
+// solver in the kernel keeps the instruction footprint small).
+template <int LIM, int RS>
+__device__ __forceinline__ void face_flux(int order, int lim_rt, int rs_rt, const Prim& c0, const Prim& c1, const Prim& c2,
+                                          const Prim& c3, int dim, float gamma, float* F) {
+	Prim L, R;
+	if (order == 1) {
+		const int lim = LIM >= 0 ? LIM : lim_rt;
+		reconstruct(lim, c0, c1, c2, c3, L, R);
+	} else {
+		L = c1;
+		R = c2;
+	}
+	riemann32(RS >= 0 ? RS : rs_rt, L, R, dim, gamma, F);
+}
+
 // One RK2 stage (STAGE 1: predictor with floors on Q, h = 1/2; STAGE 2:
 // corrector on Q(U*), h = 1, plus the next step's CFL minimum).
 // Ubase: the state the Euler update starts from (U0 in both stages);
 // Uq: the state the primitives come from (U0, then U*); Uout: result.
-template <int STAGE>
+// LIM / RS: limiter and Riemann solver fixed at compile time (-1: chosen at run time).
+template <int STAGE, int LIM, int RS>
 __global__ void __launch_bounds__(BX* BY, 2)
     k_hydro_stage_fp32(Params P, State S, const float* __restrict__ Uq, const float* __restrict__ Ubase,
                        float* __restrict__ Uout, int zchunk) {
@@ -376,21 +401,39 @@ __global__ void __launch_bounds__(BX* BY, 2)
 	SmemQ& s = *reinterpret_cast<SmemQ*>(smem_raw);
 	float* Fx = reinterpret_cast<float*>(smem_raw + sizeof(SmemQ));   // [7][BY][BX+1]
 	float* Fy = Fx + 7 * BY * (BX + 1);                                  // [7][BY+1][BX]
+	float* Fz = Fy + 7 * (BY + 1) * BX;                                  // [2][7][BY][BX]
 	const int tx = threadIdx.x % BX, ty = threadIdx.x / BX;
 	const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY;
 	const int z0 = blockIdx.z * zchunk;
-	const int z1 = min(z0 + zchunk, P.nz);
 	const int nd = P.nd;
+	const int z1 = nd > 2 ? min(z0 + zchunk, P.nz) : 1;
 	const float gamma = (float)P.gamma;
 	const double dt = (STAGE == 1 ? 0.5 : 1.0) * S.scal[0];
 	const float dtf = (float)dt;
 	const long long N = P.N;
 	const int gx = x0 + tx, gy = y0 + ty;
 	const bool active = gx < P.nx && gy < P.ny;
+	const int order = P.order, lim_rt = P.limiter, rs_rt = P.riemann;
+	// face counts of one plane (x faces, y faces, z faces at z + 1/2)
+	const int nfx = (BX + 1) * BY, nfy = nd > 1 ? BX * (BY + 1) : 0, nfz = nd > 2 ? BX * BY : 0;
 	double tmin = 1.0e308;
 	bool bad = false;
 
-	// preload planes z0-2 .. z0+1 (ring slots by z mod 5)
+	// geometry of this thread's cell column: cartesian factors are uniform
+	float axl = 0, axr = 0, ayl = 0, ayr = 0, azl = 0, azr = 0, rgeo = 0;
+	int ijk[3] = {gx, gy, 0};
+	double xc[3];
+	cell_xc(P, ijk, xc);
+	{
+		double vol = cell_volume(P, xc[0]);
+		axl = (float)(face_area(P, xc, 0, 0) / vol);
+		axr = (float)(face_area(P, xc, 0, 1) / vol);
+		if (nd > 1) { ayl = (float)(face_area(P, xc, 1, 0) / vol); ayr = (float)(face_area(P, xc, 1, 1) / vol); }
+		if (nd > 2) { azl = (float)(face_area(P, xc, 2, 0) / vol); azr = (float)(face_area(P, xc, 2, 1) / vol); }
+		if (P.geometry == G_CYL) rgeo = (float)(1.0 / (P.dx[0] * xc[0]));
+		else if (P.geometry == G_SPH) rgeo = (float)((face_area(P, xc, 0, 1) - face_area(P, xc, 0, 0)) / vol);
+	}
+
 	auto slot_of = [](int z) { return ((z % NPLANE) + NPLANE) % NPLANE; };
 	if (nd > 2) {
 		for (int z = z0 - 2; z <= z0 + 1; ++z) load_plane<STAGE>(P, Uq, s, slot_of(z), x0, y0, z);
@@ -398,87 +441,80 @@ __global__ void __launch_bounds__(BX* BY, 2)
 		load_plane<STAGE>(P, Uq, s, 0, x0, y0, 0);
 	}
 	__syncthreads();
-
-	float Fzm[7];
-	if (nd > 2 && active) {
-		// flux through the face z0 - 1/2
+	if (nd > 2) {
+		// flux through the face z0 - 1/2 into Fz[0]
 		Prim c0 = get(s, slot_of(z0 - 2), ty + HALO, tx + HALO), c1 = get(s, slot_of(z0 - 1), ty + HALO, tx + HALO);
 		Prim c2 = get(s, slot_of(z0), ty + HALO, tx + HALO), c3 = get(s, slot_of(z0 + 1), ty + HALO, tx + HALO);
-		Prim L, R;
-		if (P.order == 1) reconstruct(P.limiter, c0, c1, c2, c3, L, R);
-		else { L = c1; R = c2; }
-		riemann32(P.riemann, L, R, 2, gamma, Fzm);
+		float F[7];
+		face_flux<LIM, RS>(order, lim_rt, rs_rt, c0, c1, c2, c3, 2, gamma, F);
+#pragma unroll
+		for (int i = 0; i < 7; ++i) Fz[i * BX * BY + threadIdx.x] = F[i];
 	}
 
 	for (int z = z0; z < z1; ++z) {
 		const int sc = nd > 2 ? slot_of(z) : 0;
+		const int zb = (z - z0) & 1;  // Fz buffer holding the face z - 1/2
 		if (nd > 2) {
 			load_plane<STAGE>(P, Uq, s, slot_of(z + 2), x0, y0, z + 2);
 			__syncthreads();
 		}
-		// x faces of plane z: (BX+1) x BY
-		for (int f = threadIdx.x; f < (BX + 1) * BY; f += blockDim.x) {
-			int fy = f / (BX + 1), fx = f - fy * (BX + 1);
-			if (x0 + fx > P.nx || y0 + fy >= P.ny) continue;
-			int ly = fy + HALO;
-			Prim c0 = get(s, sc, ly, fx), c1 = get(s, sc, ly, fx + 1), c2 = get(s, sc, ly, fx + 2), c3 = get(s, sc, ly, fx + 3);
-			Prim L, R;
-			float F[7];
-			if (P.order == 1) reconstruct(P.limiter, c0, c1, c2, c3, L, R);
-			else { L = c1; R = c2; }
-			riemann32(P.riemann, L, R, 0, gamma, F);
-#pragma unroll
-			for (int i = 0; i < 7; ++i) Fx[(i * BY + fy) * (BX + 1) + fx] = F[i];
-		}
-		if (nd > 1) {
-			for (int f = threadIdx.x; f < BX * (BY + 1); f += blockDim.x) {
-				int fy = f / BX, fx = f - fy * BX;
-				if (x0 + fx >= P.nx || y0 + fy > P.ny) continue;
-				int lx = fx + HALO;
-				Prim c0 = get(s, sc, fy, lx), c1 = get(s, sc, fy + 1, lx), c2 = get(s, sc, fy + 2, lx), c3 = get(s, sc, fy + 3, lx);
-				Prim L, R;
-				float F[7];
-				if (P.order == 1) reconstruct(P.limiter, c0, c1, c2, c3, L, R);
-				else { L = c1; R = c2; }
-				riemann32(P.riemann, L, R, 1, gamma, F);
-#pragma unroll
-				for (int i = 0; i < 7; ++i) Fy[(i * (BY + 1) + fy) * BX + fx] = F[i];
+		for (int f = threadIdx.x; f < nfx + nfy + nfz; f += blockDim.x) {
+			int dim, a, b;
+			Prim c0, c1, c2, c3;
+			if (f < nfx) {
+				dim = 0;
+				b = f / (BX + 1);
+				a = f - b * (BX + 1);
+				if (x0 + a > P.nx || y0 + b >= P.ny) continue;
+				int ly = b + HALO;
+				c0 = get(s, sc, ly, a); c1 = get(s, sc, ly, a + 1); c2 = get(s, sc, ly, a + 2); c3 = get(s, sc, ly, a + 3);
+			} else if (f < nfx + nfy) {
+				dim = 1;
+				int g = f - nfx;
+				b = g / BX;
+				a = g - b * BX;
+				if (x0 + a >= P.nx || y0 + b > P.ny) continue;
+				int lx = a + HALO;
+				c0 = get(s, sc, b, lx); c1 = get(s, sc, b + 1, lx); c2 = get(s, sc, b + 2, lx); c3 = get(s, sc, b + 3, lx);
+			} else {
+				dim = 2;
+				int g = f - nfx - nfy;
+				b = g / BX;
+				a = g - b * BX;
+				if (x0 + a >= P.nx || y0 + b >= P.ny) continue;
+				int lx = a + HALO, ly = b + HALO;
+				c0 = get(s, slot_of(z - 1), ly, lx); c1 = get(s, sc, ly, lx);
+				c2 = get(s, slot_of(z + 1), ly, lx); c3 = get(s, slot_of(z + 2), ly, lx);
 			}
-		}
-		float Fzp[7];
-		if (nd > 2 && active) {
-			Prim c0 = get(s, slot_of(z - 1), ty + HALO, tx + HALO), c1 = get(s, sc, ty + HALO, tx + HALO);
-			Prim c2 = get(s, slot_of(z + 1), ty + HALO, tx + HALO), c3 = get(s, slot_of(z + 2), ty + HALO, tx + HALO);
-			Prim L, R;
-			if (P.order == 1) reconstruct(P.limiter, c0, c1, c2, c3, L, R);
-			else { L = c1; R = c2; }
-			riemann32(P.riemann, L, R, 2, gamma, Fzp);
+			float F[7];
+			face_flux<LIM, RS>(order, lim_rt, rs_rt, c0, c1, c2, c3, dim, gamma, F);
+			if (dim == 0) {
+#pragma unroll
+				for (int i = 0; i < 7; ++i) Fx[(i * BY + b) * (BX + 1) + a] = F[i];
+			} else if (dim == 1) {
+#pragma unroll
+				for (int i = 0; i < 7; ++i) Fy[(i * (BY + 1) + b) * BX + a] = F[i];
+			} else {
+#pragma unroll
+				for (int i = 0; i < 7; ++i) Fz[((zb ^ 1) * 7 + i) * BX * BY + b * BX + a] = F[i];
+			}
 		}
 		__syncthreads();
 		if (active) {
 			const long long id = gx + (long long)P.nx * (gy + (long long)P.ny * z);
-			int ijk[3] = {gx, gy, z};
-			double xc[3];
-			cell_xc(P, ijk, xc);
-			// areas / volume (Grid.cpp:846-905) in FP64, once per cell
-			double vol = cell_volume(P, xc[0]);
-			float udot[7] = {0, 0, 0, 0, 0, 0, 0};
-			{
-				float al = (float)(face_area(P, xc, 0, 0) / vol), ar = (float)(face_area(P, xc, 0, 1) / vol);
+			float udot[7];
 #pragma unroll
-				for (int i = 0; i < 7; ++i)
-					udot[i] += al * Fx[(i * BY + ty) * (BX + 1) + tx] - ar * Fx[(i * BY + ty) * (BX + 1) + tx + 1];
-			}
+			for (int i = 0; i < 7; ++i)
+				udot[i] = axl * Fx[(i * BY + ty) * (BX + 1) + tx] - axr * Fx[(i * BY + ty) * (BX + 1) + tx + 1];
 			if (nd > 1) {
-				float al = (float)(face_area(P, xc, 1, 0) / vol), ar = (float)(face_area(P, xc, 1, 1) / vol);
 #pragma unroll
 				for (int i = 0; i < 7; ++i)
-					udot[i] += al * Fy[(i * (BY + 1) + ty) * BX + tx] - ar * Fy[(i * (BY + 1) + ty + 1) * BX + tx];
+					udot[i] += ayl * Fy[(i * (BY + 1) + ty) * BX + tx] - ayr * Fy[(i * (BY + 1) + ty + 1) * BX + tx];
 			}
 			if (nd > 2) {
-				float al = (float)(face_area(P, xc, 2, 0) / vol), ar = (float)(face_area(P, xc, 2, 1) / vol);
 #pragma unroll
-				for (int i = 0; i < 7; ++i) udot[i] += al * Fzm[i] - ar * Fzp[i];
+				for (int i = 0; i < 7; ++i)
+					udot[i] += azl * Fz[(zb * 7 + i) * BX * BY + threadIdx.x] - azr * Fz[((zb ^ 1) * 7 + i) * BX * BY + threadIdx.x];
 			}
 			Prim qc = get(s, sc, ty + HALO, tx + HALO);
 			if (S.grav) {
@@ -488,21 +524,22 @@ __global__ void __launch_bounds__(BX* BY, 2)
 					udot[PRE] += qc.v[k] * g;
 				}
 			}
-			if (P.geometry == G_CYL) {
-				udot[VEL + 0] += qc.p / (float)(P.dx[0] * xc[0]);
-			} else if (P.geometry == G_SPH) {
-				double r = vol / (face_area(P, xc, 0, 1) - face_area(P, xc, 0, 0));
-				udot[VEL + 0] += qc.p / (float)r;
-			}
+			if (P.geometry == G_CYL) udot[VEL + 0] += qc.p * rgeo;
+			else if (P.geometry == G_SPH) udot[VEL + 0] += qc.p * rgeo;
 			float ub[7];
 #pragma unroll
 			for (int i = 0; i < 7; ++i) ub[i] = Ubase[i * N + id];
-			if (P.star_on && P.mdot != 0 && is_wind(P, id, ijk, xc)) {
-				float mdot = (float)P.mdot;
-				udot[DEN] += mdot;
-				udot[PRE] += (float)P.edot;
-				udot[HII] += (ub[HII] / ub[DEN]) * mdot;
-				udot[ADV] += mdot;
+			if (P.star_on && P.mdot != 0) {
+				int cijk[3] = {gx, gy, z};
+				double cxc[3];
+				cell_xc(P, cijk, cxc);
+				if (is_wind(P, id, cijk, cxc)) {
+					float mdot = (float)P.mdot;
+					udot[DEN] += mdot;
+					udot[PRE] += (float)P.edot;
+					udot[HII] += (ub[HII] / ub[DEN]) * mdot;
+					udot[ADV] += mdot;
+				}
 			}
 			float u[7];
 #pragma unroll
@@ -517,14 +554,13 @@ __global__ void __launch_bounds__(BX* BY, 2)
 				fix_prim(P, q, u[DEN]);
 				double ss = sqrt(P.gamma * (double)q.p / (double)q.d);
 				double inv_t = 0;
-				for (int k = 0; k < nd; ++k) inv_t += (fabs((double)q.v[k]) + ss) / P.dx[k];
+#pragma unroll
+				for (int k = 0; k < 3; ++k)
+					if (k < nd) inv_t += (fabs((double)q.v[k]) + ss) / P.dx[k];
 				if (inv_t == 0) inv_t = 1.0 / P.dt_max;
 				tmin = dmin_(tmin, 0.5 / inv_t);
 			}
 		}
-		if (nd > 2)
-#pragma unroll
-			for (int i = 0; i < 7; ++i) Fzm[i] = Fzp[i];
 		__syncthreads();
 	}
 	if (bad) atomicOr(S.err, ERRB_NAN);
@@ -538,19 +574,30 @@ __global__ void __launch_bounds__(BX* BY, 2)
 }
 
 size_t hydro_stage_fp32_smem() {
-	return sizeof(SmemQ) + sizeof(float) * 7 * (BY * (BX + 1) + (BY + 1) * BX);
+	return sizeof(SmemQ) + sizeof(float) * 7 * (BY * (BX + 1) + (BY + 1) * BX + 2 * BX * BY);
+}
+
+template <int STAGE, int LIM, int RS>
+static void launch_one(const Params& P, const State& S, const float* Uq, const float* Ubase, float* Uout, int zchunk,
+                       cudaStream_t stream) {
+	size_t smem = hydro_stage_fp32_smem();
+	int zc = P.nd > 2 ? zchunk : 1;
+	dim3 grid((P.nx + BX - 1) / BX, (P.ny + BY - 1) / BY, P.nd > 2 ? (P.nz + zc - 1) / zc : 1);
+	cudaFuncSetAttribute(k_hydro_stage_fp32<STAGE, LIM, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	k_hydro_stage_fp32<STAGE, LIM, RS><<<grid, BX * BY, smem, stream>>>(P, S, Uq, Ubase, Uout, zc);
 }
 
 void launch_hydro_stage_fp32(int stage, const Params& P, const State& S, const float* Uq, const float* Ubase,
                              float* Uout, int zchunk, cudaStream_t stream) {
-	size_t smem = hydro_stage_fp32_smem();
-	dim3 grid((P.nx + BX - 1) / BX, (P.ny + BY - 1) / BY, (P.nz + zchunk - 1) / zchunk);
+	// the reference's configured and default pair (albada, RotatedHLLC) is compiled
+	// with both fixed; any other pair takes the run-time switches
+	bool fast = P.limiter == 6 && P.riemann == RS_ROTATED;
 	if (stage == 1) {
-		cudaFuncSetAttribute(k_hydro_stage_fp32<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-		k_hydro_stage_fp32<1><<<grid, BX * BY, smem, stream>>>(P, S, Uq, Ubase, Uout, zchunk);
+		if (fast) launch_one<1, 6, RS_ROTATED>(P, S, Uq, Ubase, Uout, zchunk, stream);
+		else launch_one<1, -1, -1>(P, S, Uq, Ubase, Uout, zchunk, stream);
 	} else {
-		cudaFuncSetAttribute(k_hydro_stage_fp32<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-		k_hydro_stage_fp32<2><<<grid, BX * BY, smem, stream>>>(P, S, Uq, Ubase, Uout, zchunk);
+		if (fast) launch_one<2, 6, RS_ROTATED>(P, S, Uq, Ubase, Uout, zchunk, stream);
+		else launch_one<2, -1, -1>(P, S, Uq, Ubase, Uout, zchunk, stream);
 	}
 }
 
