@@ -377,7 +377,7 @@ int trg_create(const trg_params* p, const double* den, const double* pre, const 
 			c->zchunk = zc < 16 ? 16 : zc;
 		}
 		if ((rc = dalloc(c, &c->U32, 7 * N)) || (rc = dalloc(c, &c->U32s, 7 * N))) return rc;
-		LAUNCH(k_f64_to_f32, 7 * N, 256, S.U, c->U32, 7 * N);
+		LAUNCH(k_f64_to_f32, 7 * N, 256, c->P, S.U, c->U32);
 		CUDA_TRY(cudaMemsetAsync(c->U32s, 0, 7 * N * sizeof(float), st));
 	}
 	// Torch::run prologue (Torch.cpp:245-264): Q from U with floors, and the
@@ -507,7 +507,7 @@ int trg_get_state(trg_ctx* c, double* U, double* Q, double* R, double* T, double
 	cudaStream_t st = c->stream;
 	if (c->fp32) {
 		// expose the FP32 state as FP64 (Q = QfromU without floors)
-		LAUNCH(k_f32_to_f64, 7 * N, 256, c->U32, c->S.U, 7 * N);
+		LAUNCH(k_f32_to_f64, 7 * N, 256, c->P, c->U32, c->S.U);
 		q_from_u(c, c->S.U, 0);
 	}
 	if (U) CUDA_TRY(cudaMemcpyAsync(U, c->S.U, 7 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -522,7 +522,7 @@ int trg_get_state(trg_ctx* c, double* U, double* Q, double* R, double* T, double
 int trg_set_conserved(trg_ctx* c, const double* U) {
 	if (!c || !U) return TRG_ERR_ARG;
 	CUDA_TRY(cudaMemcpyAsync(c->S.U, U, 7 * c->P.N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-	if (c->fp32) LAUNCH(k_f64_to_f32, 7 * c->P.N, 256, c->S.U, c->U32, 7 * c->P.N);
+	if (c->fp32) LAUNCH(k_f64_to_f32, 7 * c->P.N, 256, c->P, c->S.U, c->U32);
 	return TRG_OK;
 }
 

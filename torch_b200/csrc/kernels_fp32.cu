@@ -39,6 +39,15 @@ struct Prim {
 	float d, p, x, a, v[3];
 };
 
+// Floors and constants in the FP32 form's scaled units (state / reference value).
+struct Scaled {
+	float dfloor, pfloor, tfloor, Rg, X, gamma;
+	int nd;
+	__device__ explicit Scaled(const Params& P)
+		: dfloor((float)(P.dfloor / P.f32_rho0)), pfloor((float)(P.pfloor / P.f32_p0)), tfloor((float)P.tfloor),
+		  Rg((float)(P.specificGasConstant * P.f32_rho0 / P.f32_p0)), X((float)P.X), gamma((float)P.gamma), nd(P.nd) {}
+};
+
 __device__ __forceinline__ float fminf_(float a, float b) { return (b < a) ? b : a; }
 __device__ __forceinline__ float fmaxf_(float a, float b) { return (a < b) ? b : a; }
 
@@ -84,40 +93,37 @@ __device__ __forceinline__ Prim prim_from_cons(const float* u, float gamma, int 
 	return q;
 }
 
-__device__ __forceinline__ void fix_prim(const Params& P, Prim& q, float u_den) {
+__device__ __forceinline__ void fix_prim(const Scaled& P, Prim& q, float u_den) {
 	q.x = fmaxf_(fminf_(q.x, 1.f), 0.f);
 	q.a = fmaxf_(fminf_(q.a, 1.f), 0.f);
-	q.d = fmaxf_(q.d, (float)P.dfloor);
-	q.p = fmaxf_(q.p, (float)P.pfloor);
-	float mu_inv = (float)P.X * (q.x + 1.f) + (1.f - (float)P.X) * 0.25f;
-	float Rg = (float)P.specificGasConstant;
-	float temperature = q.p / (mu_inv * Rg * q.d);
-	if (temperature < (float)P.tfloor) q.p = mu_inv * Rg * u_den * (float)P.tfloor;
+	q.d = fmaxf_(q.d, P.dfloor);
+	q.p = fmaxf_(q.p, P.pfloor);
+	float mu_inv = P.X * (q.x + 1.f) + (1.f - P.X) * 0.25f;
+	float temperature = q.p / (mu_inv * P.Rg * q.d);
+	if (temperature < P.tfloor) q.p = mu_inv * P.Rg * u_den * P.tfloor;
 }
 
 // Fluid::fixSolution in FP32 (compensated kinetic energy as in prim_from_cons).
-__device__ __forceinline__ bool fix_cons(const Params& P, float* u) {
+__device__ __forceinline__ bool fix_cons(const Scaled& P, float* u) {
 	if (!isfinite(u[DEN]) || !isfinite(u[PRE])) return false;
 	float inv = 1.0f / u[DEN];
 	float hii = fmaxf_(fminf_(u[HII] * inv, 1.f), 0.f);
 	float adv = fmaxf_(fminf_(u[ADV] * inv, 1.f), 0.f);
-	float den = fmaxf_(u[DEN], (float)P.dfloor);
+	float den = fmaxf_(u[DEN], P.dfloor);
 	const int nd = P.nd;
 	float v[3];
 #pragma unroll
 	for (int k = 0; k < 3; ++k) v[k] = k < nd ? u[VEL + k] * inv : 0.f;
-	Prim q = prim_from_cons(u, (float)P.gamma, nd);
+	Prim q = prim_from_cons(u, P.gamma, nd);
 	float pre = q.p;
 	float ke = (v[0] * v[0] + v[1] * v[1]) + v[2] * v[2];
 	ke *= 0.5f * den;
-	float pfloor = (float)P.pfloor;
-	if (pre < pfloor) pre = pfloor;
-	float mu_inv = (float)P.X * (hii + 1.f) + (1.f - (float)P.X) * 0.25f;
-	float Rg = (float)P.specificGasConstant;
-	float temperature = pre / (mu_inv * Rg * den);
-	if (temperature < (float)P.tfloor) pre = mu_inv * Rg * den * (float)P.tfloor;
+	if (pre < P.pfloor) pre = P.pfloor;
+	float mu_inv = P.X * (hii + 1.f) + (1.f - P.X) * 0.25f;
+	float temperature = pre / (mu_inv * P.Rg * den);
+	if (temperature < P.tfloor) pre = mu_inv * P.Rg * den * P.tfloor;
 	u[DEN] = den;
-	u[PRE] = pre / ((float)P.gamma - 1.f) + ke;
+	u[PRE] = pre / (P.gamma - 1.f) + ke;
 	u[HII] = hii * den;
 	u[ADV] = adv * den;
 #pragma unroll
@@ -254,33 +260,37 @@ __device__ __forceinline__ void hllc_n(const Prim& L, const Prim& R, const float
 }
 
 // Rotated HLLC-HLL flux through a face with normal e_dim (Riemann.cpp:181-244).
+// The branch tests use the exact components of the velocity jump dv along
+// and across the face normal (the reference tests n1 x d == 0 and
+// n2 x d == 0 exactly), and n2 is built from them without cancellation:
+//   n1 = sign(dv_par) dv / |dv|,  |n1 . d| = |dv_par| / |dv| = cos,
+//   n2 = (d |dv|^2 - dv_par dv) / (|dv| |dv_perp|),  n2 . d = |dv_perp| / |dv| = sin.
 // No array is indexed with the run-time dim, so everything stays in registers.
 __device__ __forceinline__ void riemann32(int kind, const Prim& L, const Prim& R, int dim, float gamma, float* F) {
 	const float g1inv = 1.f / (gamma - 1.f);
 	const float d[3] = {dim == 0 ? 1.f : 0.f, dim == 1 ? 1.f : 0.f, dim == 2 ? 1.f : 0.f};
 	if (kind == RS_HLLC) { hllc_n(L, R, d, gamma, g1inv, F); return; }
 	if (kind == RS_HLL) { hll_n(L, R, d, gamma, g1inv, F); return; }
-	float n1[3] = {R.v[0] - L.v[0], R.v[1] - L.v[1], R.v[2] - L.v[2]};
-	float c = n1[0] * d[0] + n1[1] * d[1] + n1[2] * d[2];
-	float sgn = c < 0 ? -1.f : 1.f;  // orient n1 . d >= 0
-	float nn = n1[0] * n1[0] + n1[1] * n1[1] + n1[2] * n1[2];
-	if (nn < 1.0e-12f) { hllc_n(L, R, d, gamma, g1inv, F); return; }  // |dv| < 1e-6
-	float inv = sgn * rsqrtf(nn);
-	n1[0] *= inv; n1[1] *= inv; n1[2] *= inv;
-	c = n1[0] * d[0] + n1[1] * d[1] + n1[2] * d[2];
-	// n2 = (n1 x d) x n1 = d - (n1 . d) n1, already oriented with n2 . d >= 0
-	float n2[3] = {d[0] - c * n1[0], d[1] - c * n1[1], d[2] - c * n1[2]};
-	float n2n = n2[0] * n2[0] + n2[1] * n2[1] + n2[2] * n2[2];
-	if (n2n <= 1.0e-14f) { hll_n(L, R, d, gamma, g1inv, F); return; }   // n1 parallel to d
-	if (c <= 1.0e-7f) { hllc_n(L, R, d, gamma, g1inv, F); return; }     // n1 normal to d: n2 = d
-	float inv2 = rsqrtf(n2n);
-	n2[0] *= inv2; n2[1] *= inv2; n2[2] *= inv2;
+	const float dv[3] = {R.v[0] - L.v[0], R.v[1] - L.v[1], R.v[2] - L.v[2]};
+	const float par = dv[0] * d[0] + dv[1] * d[1] + dv[2] * d[2];  // exact: one term is non-zero
+	const float perp[3] = {dv[0] - par * d[0], dv[1] - par * d[1], dv[2] - par * d[2]};  // exact
+	const float pp = perp[0] * perp[0] + perp[1] * perp[1] + perp[2] * perp[2];
+	const float rr = par * par + pp;
+	if (rr < 1.0e-12f) { hllc_n(L, R, d, gamma, g1inv, F); return; }  // |dv| < 1e-6
+	if (pp == 0.f) { hll_n(L, R, d, gamma, g1inv, F); return; }        // dv parallel to d
+	if (par == 0.f) { hllc_n(L, R, d, gamma, g1inv, F); return; }     // dv normal to d
+	const float r = sqrtf(rr), s = sqrtf(pp);
+	const float inv_r = 1.f / r;
+	const float sg = par < 0 ? -1.f : 1.f;
+	const float n1[3] = {sg * dv[0] * inv_r, sg * dv[1] * inv_r, sg * dv[2] * inv_r};
+	const float cosv = fabsf(par) * inv_r, sinv = s * inv_r;
+	const float k2 = par * inv_r / s;
+	const float n2[3] = {sinv * d[0] - k2 * perp[0], sinv * d[1] - k2 * perp[1], sinv * d[2] - k2 * perp[2]};
 	float F1[7], F2[7];
 	hll_n(L, R, n1, gamma, g1inv, F1);
 	hllc_n(L, R, n2, gamma, g1inv, F2);
-	float w2 = n2[0] * d[0] + n2[1] * d[1] + n2[2] * d[2];
 #pragma unroll
-	for (int i = 0; i < 7; ++i) F[i] = c * F1[i] + w2 * F2[i];
+	for (int i = 0; i < 7; ++i) F[i] = cosv * F1[i] + sinv * F2[i];
 }
 
 struct SmemQ {
@@ -319,8 +329,8 @@ __device__ __forceinline__ void apply_flip(Prim& q, int dim, int cond, int side)
 
 // Loads plane z (global index, may be a ghost plane) of the CTA's x/y box into ring slot.
 template <int STAGE>
-__device__ __forceinline__ void load_plane(const Params& P, const float* __restrict__ U, SmemQ& s, int slot, int x0, int y0,
-                                           int z) {
+__device__ __forceinline__ void load_plane(const Params& P, const Scaled& SP, const float* __restrict__ U, SmemQ& s,
+                                           int slot, int x0, int y0, int z) {
 	int zc, zside;
 	int zs = P.nd > 2 ? bc_src(P, 2, z, P.nz, zc, zside) : 0;
 	if (P.nd <= 2) zc = -1;
@@ -340,7 +350,7 @@ __device__ __forceinline__ void load_plane(const Params& P, const float* __restr
 #pragma unroll
 		for (int f = 0; f < 7; ++f) u[f] = __ldg(&U[f * N + id]);
 		Prim q = prim_from_cons(u, (float)P.gamma, P.nd);
-		if (STAGE == 1) fix_prim(P, q, u[DEN]);
+		if (STAGE == 1) fix_prim(SP, q, u[DEN]);
 		apply_flip(q, 0, xc, xside);
 		if (P.nd > 1) apply_flip(q, 1, yc, yside);
 		if (P.nd > 2) apply_flip(q, 2, zc, zside);
@@ -395,8 +405,8 @@ __device__ __forceinline__ void face_flux(int order, int lim_rt, int rs_rt, cons
 // LIM / RS: limiter and Riemann solver fixed at compile time (-1: chosen at run time).
 template <int STAGE, int LIM, int RS>
 __global__ void __launch_bounds__(BX* BY, 2)
-    k_hydro_stage_fp32(Params P, State S, const float* __restrict__ Uq, const float* __restrict__ Ubase,
-                       float* __restrict__ Uout, int zchunk) {
+    k_hydro_stage_fp32(Params P, State S, const float* __restrict__ Uq, const float* Ubase,
+                       float* Uout, int zchunk) {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	SmemQ& s = *reinterpret_cast<SmemQ*>(smem_raw);
 	float* Fx = reinterpret_cast<float*>(smem_raw + sizeof(SmemQ));   // [7][BY][BX+1]
@@ -408,8 +418,11 @@ __global__ void __launch_bounds__(BX* BY, 2)
 	const int nd = P.nd;
 	const int z1 = nd > 2 ? min(z0 + zchunk, P.nz) : 1;
 	const float gamma = (float)P.gamma;
-	const double dt = (STAGE == 1 ? 0.5 : 1.0) * S.scal[0];
+	const Scaled SP(P);
+	// scaled time: t' = t v0 (lengths stay in code units)
+	const double dt = (STAGE == 1 ? 0.5 : 1.0) * S.scal[0] * P.f32_v0;
 	const float dtf = (float)dt;
+	const float gscale = (float)(1.0 / P.f32_p0);
 	const long long N = P.N;
 	const int gx = x0 + tx, gy = y0 + ty;
 	const bool active = gx < P.nx && gy < P.ny;
@@ -436,9 +449,9 @@ __global__ void __launch_bounds__(BX* BY, 2)
 
 	auto slot_of = [](int z) { return ((z % NPLANE) + NPLANE) % NPLANE; };
 	if (nd > 2) {
-		for (int z = z0 - 2; z <= z0 + 1; ++z) load_plane<STAGE>(P, Uq, s, slot_of(z), x0, y0, z);
+		for (int z = z0 - 2; z <= z0 + 1; ++z) load_plane<STAGE>(P, SP, Uq, s, slot_of(z), x0, y0, z);
 	} else {
-		load_plane<STAGE>(P, Uq, s, 0, x0, y0, 0);
+		load_plane<STAGE>(P, SP, Uq, s, 0, x0, y0, 0);
 	}
 	__syncthreads();
 	if (nd > 2) {
@@ -455,7 +468,7 @@ __global__ void __launch_bounds__(BX* BY, 2)
 		const int sc = nd > 2 ? slot_of(z) : 0;
 		const int zb = (z - z0) & 1;  // Fz buffer holding the face z - 1/2
 		if (nd > 2) {
-			load_plane<STAGE>(P, Uq, s, slot_of(z + 2), x0, y0, z + 2);
+			load_plane<STAGE>(P, SP, Uq, s, slot_of(z + 2), x0, y0, z + 2);
 			__syncthreads();
 		}
 		for (int f = threadIdx.x; f < nfx + nfy + nfz; f += blockDim.x) {
@@ -519,7 +532,7 @@ __global__ void __launch_bounds__(BX* BY, 2)
 			Prim qc = get(s, sc, ty + HALO, tx + HALO);
 			if (S.grav) {
 				for (int k = 0; k < 3; ++k) {
-					float g = (float)S.grav[(long long)k * N + id];
+					float g = (float)S.grav[(long long)k * N + id] * gscale;
 					udot[VEL + k] += g;
 					udot[PRE] += qc.v[k] * g;
 				}
@@ -534,9 +547,9 @@ __global__ void __launch_bounds__(BX* BY, 2)
 				double cxc[3];
 				cell_xc(P, cijk, cxc);
 				if (is_wind(P, id, cijk, cxc)) {
-					float mdot = (float)P.mdot;
+					float mdot = (float)(P.mdot / (P.f32_rho0 * P.f32_v0));
 					udot[DEN] += mdot;
-					udot[PRE] += (float)P.edot;
+					udot[PRE] += (float)(P.edot / (P.f32_p0 * P.f32_v0));
 					udot[HII] += (ub[HII] / ub[DEN]) * mdot;
 					udot[ADV] += mdot;
 				}
@@ -544,19 +557,20 @@ __global__ void __launch_bounds__(BX* BY, 2)
 			float u[7];
 #pragma unroll
 			for (int i = 0; i < 7; ++i) u[i] = ub[i] + dtf * udot[i];
-			bad |= !fix_cons(P, u);
+			bad |= !fix_cons(SP, u);
 #pragma unroll
 			for (int i = 0; i < 7; ++i) Uout[i * N + id] = u[i];
 			if (STAGE == 2) {
 				// the next step's CFL limit from Q(U1) with floors (Torch::fullStep:
 				// globalQfromU + fixPrimitives, then Hydrodynamics::calculateTimeStep)
 				Prim q = prim_from_cons(u, gamma, nd);
-				fix_prim(P, q, u[DEN]);
+				fix_prim(SP, q, u[DEN]);
+				// velocities are in units of v0: inv_t = (|v| + c) v0 / dx
 				double ss = sqrt(P.gamma * (double)q.p / (double)q.d);
 				double inv_t = 0;
 #pragma unroll
 				for (int k = 0; k < 3; ++k)
-					if (k < nd) inv_t += (fabs((double)q.v[k]) + ss) / P.dx[k];
+					if (k < nd) inv_t += (fabs((double)q.v[k]) + ss) * P.f32_v0 / P.dx[k];
 				if (inv_t == 0) inv_t = 1.0 / P.dt_max;
 				tmin = dmin_(tmin, 0.5 / inv_t);
 			}
@@ -601,14 +615,20 @@ void launch_hydro_stage_fp32(int stage, const Params& P, const State& S, const f
 	}
 }
 
-// FP64 <-> FP32 state conversion (entry to / exit from the FP32 form).
-__global__ void k_f64_to_f32(const double* __restrict__ a, float* __restrict__ b, long long n) {
-	long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-	if (i < n) b[i] = (float)a[i];
+// FP64 <-> FP32 state conversion (entry to / exit from the FP32 form), with
+// the per-field reference values of the scaled units.
+__device__ __forceinline__ double field_scale(const Params& P, int f) {
+	if (f == PRE) return P.f32_p0;
+	if (f >= VEL) return P.f32_rho0 * P.f32_v0;
+	return P.f32_rho0;
 }
-__global__ void k_f32_to_f64(const float* __restrict__ a, double* __restrict__ b, long long n) {
+__global__ void k_f64_to_f32(Params P, const double* __restrict__ a, float* __restrict__ b) {
 	long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-	if (i < n) b[i] = (double)a[i];
+	if (i < 7 * P.N) b[i] = (float)(a[i] / field_scale(P, (int)(i / P.N)));
+}
+__global__ void k_f32_to_f64(Params P, const float* __restrict__ a, double* __restrict__ b) {
+	long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (i < 7 * P.N) b[i] = (double)a[i] * field_scale(P, (int)(i / P.N));
 }
 
 }  // namespace trg

@@ -500,6 +500,15 @@ std::string host_setup(const trg_params& p, const double* den, const double* pre
 		out.sweep_all[pa[s]++] = (int)id;
 		if (!wind[id]) out.sweep_nonwind[pn[s]++] = (int)id;
 	}
+	// reference values of the FP32 form: medians of the initial density and pressure
+	{
+		std::vector<double> d(Q + DEN * N, Q + DEN * N + N), pr(Q + PRE * N, Q + PRE * N + N);
+		std::nth_element(d.begin(), d.begin() + N / 2, d.end());
+		std::nth_element(pr.begin(), pr.begin() + N / 2, pr.end());
+		P.f32_rho0 = d[N / 2] > 0 ? d[N / 2] : 1.0;
+		P.f32_p0 = pr[N / 2] > 0 ? pr[N / 2] : 1.0;
+		P.f32_v0 = std::sqrt(P.f32_p0 / P.f32_rho0);
+	}
 	out.nactive = 0;
 	out.active[out.nactive++] = 0;                      // HYDRO
 	if (p.cooling_on) out.active[out.nactive++] = 2;    // THERMO

@@ -25,6 +25,6 @@ __global__ void k_dt_reset(Params P, State S);
 void launch_hydro_stage_fp32(int stage, const Params& P, const State& S, const float* Uq, const float* Ubase,
                              float* Uout, int zchunk, cudaStream_t stream);
 size_t hydro_stage_fp32_smem();
-__global__ void k_f64_to_f32(const double* a, float* b, long long n);
-__global__ void k_f32_to_f64(const float* a, double* b, long long n);
+__global__ void k_f64_to_f32(Params P, const double* a, float* b);
+__global__ void k_f32_to_f64(Params P, const float* a, double* b);
 }  // namespace trg

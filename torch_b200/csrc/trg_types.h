@@ -54,6 +54,10 @@ struct Params {
 	// thermodynamics constants (Thermodynamics::initialise, Thermodynamics.cpp:24-57)
 	double z0, T1, T2, T3, T4, imlc, nmlc, ciec_minT, ciec, cxhi_damp, n0, nmc;
 	double fuvh_a, fuvh_b, fuvh_c, irh_a, irh_b, crh;
+	// FP32 form: the hydro state is stored divided by these reference values
+	// (density rho0, pressure / energy density p0, velocity v0 = sqrt(p0/rho0)),
+	// so that FP32 holds it far from its range limits whatever the code units.
+	double f32_rho0, f32_p0, f32_v0;
 };
 
 // Device pointers of one context (FP64 state).
