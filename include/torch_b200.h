@@ -136,6 +136,23 @@ int trg_profile_read(trg_ctx* c, const char* name, double* total_ms, long long* 
 const char* trg_last_error(const trg_ctx* c);
 void trg_destroy(trg_ctx* c);
 
+/* No counterpart in the reference.  One FP32 RK2 hydro step - the two fused
+ * stage kernels of the FP32 form - from U_in to U_out, both caller-owned
+ * device arrays of [7][N] doubles in code units (the layout of trg_get_state;
+ * U_in == U_out is allowed), for time step dt, on `stream` (a cudaStream_t,
+ * NULL for the default stream), using the parameters of context c.  It
+ * allocates no device memory: for callers that may not allocate once they run
+ * (their device memory is reserved up front by their own allocator, or
+ * cudaMalloc's implicit synchronisation is not allowed on their stepping
+ * path).  Its intermediate state lives in a static device array of at most
+ * TRG_NOALLOC_MAX_CELLS cells (about 14 MiB, held by every GPU that loads the
+ * library until exit); larger grids are rejected with TRG_ERR_ARG.  All calls
+ * share that array: calls that overlap on the GPU race.  The first call on a
+ * device looks the array's address up, so make it before any stream capture.
+ * The call waits for its stream and returns the step's error status. */
+#define TRG_NOALLOC_MAX_CELLS 262144
+int trg_hydro_step_fp32_noalloc(trg_ctx* c, const double* U_in, double* U_out, double dt, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -95,6 +95,7 @@ _SIGNATURES = [
     ("trg_stream", C.c_void_p, [C.c_void_p]),
     ("trg_profile_enable", C.c_int, [C.c_void_p, C.c_int]),
     ("trg_profile_read", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
+    ("trg_hydro_step_fp32_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
 ]
 
 

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/torch_b200.h"
+#include "ctx_access.h"
 #include "setup.h"
 #include "trg_kernels.h"
 
@@ -286,6 +287,22 @@ int ensure_dt_hist(trg_ctx* c, long long needed) {
 
 }  // namespace
 
+namespace trg {
+const Params& ctx_params(const trg_ctx* c) { return c->P; }
+State ctx_state(const trg_ctx* c) { return c->S; }
+int ctx_device(const trg_ctx* c) { return c->raw.device; }
+int ctx_fp32_zchunk(const trg_ctx* c) {
+	int sms = 148;
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->raw.device);
+	long long tiles = (long long)((c->P.nx + 31) / 32) * ((c->P.ny + 7) / 8);
+	long long nchunks = (4LL * 2 * sms + tiles - 1) / tiles;
+	if (nchunks < 1) nchunks = 1;
+	int zc = (int)((c->P.nz + nchunks - 1) / nchunks);
+	return zc < 16 ? 16 : zc;
+}
+int ctx_fail(trg_ctx* c, int code, const std::string& msg) { return set_error(c, code, msg); }
+}  // namespace trg
+
 extern "C" {
 
 int trg_create(const trg_params* p, const double* den, const double* pre, const double* hii, const double* v0,
@@ -365,17 +382,8 @@ int trg_create(const trg_params* p, const double* den, const double* pre, const 
 		if (c->hs.nactive != 1 || c->P.nd < 2)
 			return set_error(c, TRG_ERR_ARG, "the FP32 form runs hydro-only steps on 2-D and 3-D grids");
 		c->fp32 = true;
-		{
-			// z chunk per CTA: aim for about four waves of two 256-thread CTAs per SM
-			int dev_sms = 148;
-			cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, p->device);
-			long long tiles = (long long)((c->P.nx + 31) / 32) * ((c->P.ny + 7) / 8);
-			long long want = 4LL * 2 * dev_sms;
-			long long nchunks = (want + tiles - 1) / tiles;
-			if (nchunks < 1) nchunks = 1;
-			int zc = (int)((c->P.nz + nchunks - 1) / nchunks);
-			c->zchunk = zc < 16 ? 16 : zc;
-		}
+		// z chunk per CTA: about four waves of two 256-thread CTAs per SM
+		c->zchunk = ctx_fp32_zchunk(c);
 		if ((rc = dalloc(c, &c->U32, 7 * N)) || (rc = dalloc(c, &c->U32s, 7 * N))) return rc;
 		LAUNCH(k_f64_to_f32, 7 * N, 256, c->P, S.U, c->U32);
 		CUDA_TRY(cudaMemsetAsync(c->U32s, 0, 7 * N * sizeof(float), st));
