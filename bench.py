@@ -253,8 +253,9 @@ def time_form(args, precision, tp, ic, local, pg, profile_names, stream_mod):
 
 
 PROFILE_NAMES = ("k_hydro_stage_fp32", "k_faces_fp64", "k_hydro_update_fp64", "k_q_from_u", "k_dt_reduce",
-                 "k_dt_finalize", "k_dt_reset", "k_time_advance", "k_rad_shell", "k_colden_shell", "k_thermo",
-                 "k_rad_heating", "k_rad_update", "k_rad_wind")
+                 "k_dt_finalize", "k_dt_reset", "k_time_advance", "graph_rad_sweep", "graph_colden_sweep",
+                 "k_rad_shell", "k_colden_shell", "k_thermo", "k_rad_heating", "k_rad_update", "k_rad_wind",
+                 "k_rad_no_star")
 
 
 def run_ours(args, world, rank, local, pg):

@@ -82,3 +82,19 @@ def test_fp32_non_multiple_tile_sizes():
     tp, ic = workloads.sedov(n=37)
     ed, ep, eE, a, b = errors(tp, ic, 15)
     assert ed <= 1e-4 and ep <= 1e-4
+
+
+def test_fp32_form_radiation_hydro_hii_region():
+    """Radiation + cooling on: hydro sub-steps through the FP32 kernel, the
+    rest in FP64.  Density and pressure against the FP64 form after 20 steps."""
+    tp, ic = workloads.hii_region(n=24, seed=9)
+    ed, ep, eE, a, b = errors(tp, ic, 20)
+    print(f"hii24 rad-hydro 20 steps: den {ed:.2e} pre {ep:.2e}")
+    assert ed <= 1e-4 and ep <= 1e-4
+
+
+def test_fp32_form_radiation_hydro_config1():
+    tp, ic = workloads.blister()
+    ed, ep, eE, a, b = errors(tp, ic, 30)
+    print(f"config1 rad-hydro 30 steps: den {ed:.2e} pre {ep:.2e}")
+    assert ed <= 1e-4 and ep <= 1e-4

@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/torch_b200.h"
@@ -33,8 +34,16 @@ struct trg_ctx {
 	int* d_sweep_all = nullptr;
 	int* d_sweep_nonwind = nullptr;
 	int* d_wind = nullptr;
-	// FP32 form: conserved state U0/U1 and the RK2 intermediate U*
+	// FP32 form: conserved state U0/U1 and the RK2 intermediate U* (hydro-only runs);
+	// with radiation/cooling (`mixed`) the state stays FP64 and the hydro
+	// sub-steps run through the FP32 kernel
 	bool fp32 = false;
+	bool mixed = false;
+	// CUDA graphs of the shell sweeps (all shells of one sweep, launched as one)
+	cudaGraphExec_t g_colden = nullptr;
+	cudaGraphExec_t g_rad[2] = {nullptr, nullptr};
+	long long g_colden_nodes = 0, g_rad_nodes[2] = {0, 0};
+	bool use_graphs = true;
 	float* U32 = nullptr;
 	float* U32s = nullptr;
 	int zchunk = 64;
@@ -121,12 +130,49 @@ void profile_collect(trg_ctx* c) {
 
 void q_from_u(trg_ctx* c, const double* Usrc, int fix) { LAUNCH(k_q_from_u_fp64, c->P.N, 256, c->P, c->S, Usrc, fix); }
 
-void colden_sweep(trg_ctx* c) {
+void colden_sweep_direct(trg_ctx* c) {
 	const auto& off = c->hs.off_all;
 	for (size_t s = 0; s + 1 < off.size(); ++s) {
 		int count = (int)(off[s + 1] - off[s]);
 		LAUNCH(k_colden_shell_fp64, count, 128, c->P, c->S, c->d_sweep_all + off[s], count);
 	}
+}
+
+// Captures `body` (kernel launches on c->stream) into an executable graph.
+template <typename F>
+cudaGraphExec_t capture_graph(trg_ctx* c, F body, long long& nodes) {
+	bool prof = c->profiling;
+	c->profiling = false;
+	long long before = c->launches;
+	cudaGraph_t g = nullptr;
+	cudaGraphExec_t ge = nullptr;
+	if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+		body();
+		if (cudaStreamEndCapture(c->stream, &g) == cudaSuccess && g) {
+			if (cudaGraphInstantiate(&ge, g, 0) != cudaSuccess) ge = nullptr;
+			cudaGraphDestroy(g);
+		}
+	}
+	nodes = c->launches - before;
+	c->launches = before;
+	c->profiling = prof;
+	cudaGetLastError();
+	return ge;
+}
+
+void launch_graph(trg_ctx* c, cudaGraphExec_t ge, long long nodes, const char* name) {
+	cudaEvent_t ea = nullptr, eb = nullptr;
+	if (c->profiling) { ea = pool_event(c); eb = pool_event(c); cudaEventRecord(ea, c->stream); }
+	cudaGraphLaunch(ge, c->stream);
+	if (c->profiling) { cudaEventRecord(eb, c->stream); c->recs.push_back({name, ea, eb}); }
+	c->launches += nodes;
+}
+
+void colden_sweep(trg_ctx* c) {
+	if (c->use_graphs && !c->g_colden)
+		c->g_colden = capture_graph(c, [&] { colden_sweep_direct(c); }, c->g_colden_nodes);
+	if (c->use_graphs && c->g_colden) launch_graph(c, c->g_colden, c->g_colden_nodes, "graph_colden_sweep");
+	else colden_sweep_direct(c);
 }
 
 void thermo_pre(trg_ctx* c) {
@@ -146,8 +192,27 @@ void hydro_fluxes(trg_ctx* c) {
 	for (int d = 0; d < c->P.nd; ++d) LAUNCH(k_faces_fp64, c->S.nfaces[d], 128, c->P, c->S, d);
 }
 
+void rad_sweep_direct(trg_ctx* c, double h) {
+	int nw = (int)c->hs.wind_cells.size();
+	LAUNCH(k_rad_wind_reset, nw, 128, c->P, c->S, c->d_wind, nw);
+	const auto& off = c->hs.off_nonwind;
+	for (size_t s = 0; s + 1 < off.size(); ++s) {
+		int count = (int)(off[s + 1] - off[s]);
+		LAUNCH(k_rad_shell_fp64, count, 128, c->P, c->S, c->d_sweep_nonwind + off[s], count, h,
+		       (const double*)nullptr);
+	}
+}
+
 void rad_integrate(trg_ctx* c, double h) {
 	// Radiation::transferRadiation (Radiation.cpp:569-651)
+	if (c->P.star_on && (h == 0.5 || h == 1.0) && c->use_graphs) {
+		int gi = h == 0.5 ? 0 : 1;
+		if (!c->g_rad[gi]) c->g_rad[gi] = capture_graph(c, [&] { rad_sweep_direct(c, h); }, c->g_rad_nodes[gi]);
+		if (c->g_rad[gi]) {
+			launch_graph(c, c->g_rad[gi], c->g_rad_nodes[gi], "graph_rad_sweep");
+			return;
+		}
+	}
 	if (c->P.star_on) {
 		int nw = (int)c->hs.wind_cells.size();
 		LAUNCH(k_rad_wind_reset, nw, 128, c->P, c->S, c->d_wind, nw);
@@ -170,6 +235,16 @@ void sub_step(trg_ctx* c, double h, bool hasCalculatedHeatFlux, int comp) {
 	}
 	switch (comp) {
 	case COMP_HYDRO:
+		if (c->mixed) {
+			// FP32 hydro pass on the FP64 state, into U1, then swap
+			cudaEvent_t ea = nullptr, eb = nullptr;
+			if (c->profiling) { ea = pool_event(c); eb = pool_event(c); cudaEventRecord(ea, c->stream); }
+			launch_hydro_substep_fp32(c->P, c->S, c->S.U, c->S.U1, h, c->zchunk, c->stream);
+			if (c->profiling) { cudaEventRecord(eb, c->stream); c->recs.push_back({"k_hydro_stage_fp32", ea, eb}); }
+			c->launches++;
+			std::swap(c->S.U, c->S.U1);
+			break;
+		}
 		hydro_fluxes(c);
 		LAUNCH(k_hydro_update_fp64, c->P.N, 256, c->P, c->S, h, (const double*)c->S.U, c->S.U, 0);
 		break;
@@ -378,9 +453,12 @@ int trg_create(const trg_params* p, const double* den, const double* pre, const 
 		CUDA_TRY(cudaMemcpyAsync(c->d_wind, c->hs.wind_cells.data(), c->hs.wind_cells.size() * sizeof(int),
 		                         cudaMemcpyHostToDevice, st));
 	if ((rc = ensure_dt_hist(c, 1024))) return rc;
-	if (p->precision == TRG_PRECISION_FP32) {
-		if (c->hs.nactive != 1 || c->P.nd < 2)
-			return set_error(c, TRG_ERR_ARG, "the FP32 form runs hydro-only steps on 2-D and 3-D grids");
+	if (p->precision == TRG_PRECISION_FP32 && c->hs.nactive > 1) {
+		if (c->P.nd < 2) return set_error(c, TRG_ERR_ARG, "the FP32 form needs a 2-D or 3-D grid");
+		c->mixed = true;
+		c->zchunk = ctx_fp32_zchunk(c);
+	} else if (p->precision == TRG_PRECISION_FP32) {
+		if (c->P.nd < 2) return set_error(c, TRG_ERR_ARG, "the FP32 form needs a 2-D or 3-D grid");
 		c->fp32 = true;
 		// z chunk per CTA: about four waves of two 256-thread CTAs per SM
 		c->zchunk = ctx_fp32_zchunk(c);
@@ -460,7 +538,7 @@ int trg_profile_read(trg_ctx* c, const char* name, double* total_ms, long long* 
 
 int trg_component(trg_ctx* c, int comp, int phase, double dt, double* out) {
 	if (!c) return TRG_ERR_ARG;
-	if (c->fp32) return set_error(c, TRG_ERR_ARG, "per-component phases are provided by the FP64 form");
+	if (c->fp32 || c->mixed) return set_error(c, TRG_ERR_ARG, "per-component phases are provided by the FP64 form");
 	// The phase kernels read dt from the device scalar: stage the caller's dt.
 	CUDA_TRY(cudaMemcpyAsync(c->S.scal, &dt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
 	switch (phase) {
@@ -558,6 +636,9 @@ void trg_destroy(trg_ctx* c) {
 	if (c->stream) cudaStreamSynchronize(c->stream);
 	profile_collect(c);
 	for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
+	if (c->g_colden) cudaGraphExecDestroy(c->g_colden);
+	for (auto& g : c->g_rad)
+		if (g) cudaGraphExecDestroy(g);
 	for (void* p : c->allocs) cudaFree(p);
 	if (c->stream) cudaStreamDestroy(c->stream);
 	delete c;

@@ -51,6 +51,28 @@ struct Scaled {
 __device__ __forceinline__ float fminf_(float a, float b) { return (b < a) ? b : a; }
 __device__ __forceinline__ float fmaxf_(float a, float b) { return (a < b) ? b : a; }
 
+// Conserved-state storage of the FP32 kernels: float arrays hold the scaled
+// units directly; double arrays (the operator split's FP64 state) hold code
+// units and are scaled on load and unscaled on store.
+struct StoreScale {
+	double s[3], is[3];  // density-like, pressure / energy, momentum
+	__host__ __device__ explicit StoreScale(const Params& P) {
+		s[0] = P.f32_rho0;
+		s[1] = P.f32_p0;
+		s[2] = P.f32_rho0 * P.f32_v0;
+		for (int i = 0; i < 3; ++i) is[i] = 1.0 / s[i];
+	}
+	__device__ __forceinline__ int cls(int f) const { return f == PRE ? 1 : (f >= VEL ? 2 : 0); }
+};
+__device__ __forceinline__ float load_u(const float* U, long long idx, const StoreScale&, int) { return __ldg(&U[idx]); }
+__device__ __forceinline__ float load_u(const double* U, long long idx, const StoreScale& sc, int f) {
+	return (float)(__ldg(&U[idx]) * sc.is[sc.cls(f)]);
+}
+__device__ __forceinline__ void store_u(float* U, long long idx, float v, const StoreScale&, int) { U[idx] = v; }
+__device__ __forceinline__ void store_u(double* U, long long idx, float v, const StoreScale& sc, int f) {
+	U[idx] = (double)v * sc.s[sc.cls(f)];
+}
+
 // error-free transformations
 __device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
 	s = a + b;
@@ -328,9 +350,9 @@ __device__ __forceinline__ void apply_flip(Prim& q, int dim, int cond, int side)
 }
 
 // Loads plane z (global index, may be a ghost plane) of the CTA's x/y box into ring slot.
-template <int STAGE>
-__device__ __forceinline__ void load_plane(const Params& P, const Scaled& SP, const float* __restrict__ U, SmemQ& s,
-                                           int slot, int x0, int y0, int z) {
+template <int STAGE, typename TS>
+__device__ __forceinline__ void load_plane(const Params& P, const Scaled& SP, const StoreScale& SC,
+                                           const TS* __restrict__ U, SmemQ& s, int slot, int x0, int y0, int z) {
 	int zc, zside;
 	int zs = P.nd > 2 ? bc_src(P, 2, z, P.nz, zc, zside) : 0;
 	if (P.nd <= 2) zc = -1;
@@ -348,7 +370,7 @@ __device__ __forceinline__ void load_plane(const Params& P, const Scaled& SP, co
 		long long id = xs + (long long)P.nx * (ys + (long long)P.ny * zs);
 		float u[7];
 #pragma unroll
-		for (int f = 0; f < 7; ++f) u[f] = __ldg(&U[f * N + id]);
+		for (int f = 0; f < 7; ++f) u[f] = load_u(U, f * N + id, SC, f);
 		Prim q = prim_from_cons(u, (float)P.gamma, P.nd);
 		if (STAGE == 1) fix_prim(SP, q, u[DEN]);
 		apply_flip(q, 0, xc, xside);
@@ -398,15 +420,17 @@ __device__ __forceinline__ void face_flux(int order, int lim_rt, int rs_rt, cons
 	riemann32(RS >= 0 ? RS : rs_rt, L, R, dim, gamma, F);
 }
 
-// One RK2 stage (STAGE 1: predictor with floors on Q, h = 1/2; STAGE 2:
-// corrector on Q(U*), h = 1, plus the next step's CFL minimum).
-// Ubase: the state the Euler update starts from (U0 in both stages);
-// Uq: the state the primitives come from (U0, then U*); Uout: result.
+// One Euler stage U_out = fix(U_base + h dt L(Q(U_q))).
+// STAGE 1: Q with floors (fixPrimitives) - the RK2 predictor (h = 1/2) and the
+//          hydro sub-step of the operator split (h = 1/2 or 1);
+// STAGE 2: Q(U*) without floors, plus the next step's CFL minimum - the RK2
+//          corrector (h = 1).
+// TS: storage type (float: scaled units; double: code units).
 // LIM / RS: limiter and Riemann solver fixed at compile time (-1: chosen at run time).
-template <int STAGE, int LIM, int RS>
+template <int STAGE, typename TS, int LIM, int RS>
 __global__ void __launch_bounds__(BX* BY, 2)
-    k_hydro_stage_fp32(Params P, State S, const float* __restrict__ Uq, const float* Ubase,
-                       float* Uout, int zchunk) {
+    k_hydro_stage_fp32(Params P, State S, const TS* __restrict__ Uq, const TS* Ubase, TS* Uout, double hfac,
+                       int zchunk) {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	SmemQ& s = *reinterpret_cast<SmemQ*>(smem_raw);
 	float* Fx = reinterpret_cast<float*>(smem_raw + sizeof(SmemQ));   // [7][BY][BX+1]
@@ -420,7 +444,8 @@ __global__ void __launch_bounds__(BX* BY, 2)
 	const float gamma = (float)P.gamma;
 	const Scaled SP(P);
 	// scaled time: t' = t v0 (lengths stay in code units)
-	const double dt = (STAGE == 1 ? 0.5 : 1.0) * S.scal[0] * P.f32_v0;
+	const StoreScale SC(P);
+	const double dt = hfac * S.scal[0] * P.f32_v0;
 	const float dtf = (float)dt;
 	const float gscale = (float)(1.0 / P.f32_p0);
 	const long long N = P.N;
@@ -449,9 +474,9 @@ __global__ void __launch_bounds__(BX* BY, 2)
 
 	auto slot_of = [](int z) { return ((z % NPLANE) + NPLANE) % NPLANE; };
 	if (nd > 2) {
-		for (int z = z0 - 2; z <= z0 + 1; ++z) load_plane<STAGE>(P, SP, Uq, s, slot_of(z), x0, y0, z);
+		for (int z = z0 - 2; z <= z0 + 1; ++z) load_plane<STAGE>(P, SP, SC, Uq, s, slot_of(z), x0, y0, z);
 	} else {
-		load_plane<STAGE>(P, SP, Uq, s, 0, x0, y0, 0);
+		load_plane<STAGE>(P, SP, SC, Uq, s, 0, x0, y0, 0);
 	}
 	__syncthreads();
 	if (nd > 2) {
@@ -468,7 +493,7 @@ __global__ void __launch_bounds__(BX* BY, 2)
 		const int sc = nd > 2 ? slot_of(z) : 0;
 		const int zb = (z - z0) & 1;  // Fz buffer holding the face z - 1/2
 		if (nd > 2) {
-			load_plane<STAGE>(P, SP, Uq, s, slot_of(z + 2), x0, y0, z + 2);
+			load_plane<STAGE>(P, SP, SC, Uq, s, slot_of(z + 2), x0, y0, z + 2);
 			__syncthreads();
 		}
 		for (int f = threadIdx.x; f < nfx + nfy + nfz; f += blockDim.x) {
@@ -541,7 +566,7 @@ __global__ void __launch_bounds__(BX* BY, 2)
 			else if (P.geometry == G_SPH) udot[VEL + 0] += qc.p * rgeo;
 			float ub[7];
 #pragma unroll
-			for (int i = 0; i < 7; ++i) ub[i] = Ubase[i * N + id];
+			for (int i = 0; i < 7; ++i) ub[i] = load_u(Ubase, i * N + id, SC, i);
 			if (P.star_on && P.mdot != 0) {
 				int cijk[3] = {gx, gy, z};
 				double cxc[3];
@@ -559,7 +584,7 @@ __global__ void __launch_bounds__(BX* BY, 2)
 			for (int i = 0; i < 7; ++i) u[i] = ub[i] + dtf * udot[i];
 			bad |= !fix_cons(SP, u);
 #pragma unroll
-			for (int i = 0; i < 7; ++i) Uout[i * N + id] = u[i];
+			for (int i = 0; i < 7; ++i) store_u(Uout, i * N + id, u[i], SC, i);
 			if (STAGE == 2) {
 				// the next step's CFL limit from Q(U1) with floors (Torch::fullStep:
 				// globalQfromU + fixPrimitives, then Hydrodynamics::calculateTimeStep)
@@ -591,28 +616,38 @@ size_t hydro_stage_fp32_smem() {
 	return sizeof(SmemQ) + sizeof(float) * 7 * (BY * (BX + 1) + (BY + 1) * BX + 2 * BX * BY);
 }
 
-template <int STAGE, int LIM, int RS>
-static void launch_one(const Params& P, const State& S, const float* Uq, const float* Ubase, float* Uout, int zchunk,
-                       cudaStream_t stream) {
+template <int STAGE, typename TS, int LIM, int RS>
+static void launch_one(const Params& P, const State& S, const TS* Uq, const TS* Ubase, TS* Uout, double hfac,
+                       int zchunk, cudaStream_t stream) {
 	size_t smem = hydro_stage_fp32_smem();
 	int zc = P.nd > 2 ? zchunk : 1;
 	dim3 grid((P.nx + BX - 1) / BX, (P.ny + BY - 1) / BY, P.nd > 2 ? (P.nz + zc - 1) / zc : 1);
-	cudaFuncSetAttribute(k_hydro_stage_fp32<STAGE, LIM, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-	k_hydro_stage_fp32<STAGE, LIM, RS><<<grid, BX * BY, smem, stream>>>(P, S, Uq, Ubase, Uout, zc);
+	cudaFuncSetAttribute(k_hydro_stage_fp32<STAGE, TS, LIM, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                     (int)smem);
+	k_hydro_stage_fp32<STAGE, TS, LIM, RS><<<grid, BX * BY, smem, stream>>>(P, S, Uq, Ubase, Uout, hfac, zc);
 }
 
+// the reference's configured and default pair (albada, RotatedHLLC) is compiled
+// with both fixed; any other pair takes the run-time switches
 void launch_hydro_stage_fp32(int stage, const Params& P, const State& S, const float* Uq, const float* Ubase,
                              float* Uout, int zchunk, cudaStream_t stream) {
-	// the reference's configured and default pair (albada, RotatedHLLC) is compiled
-	// with both fixed; any other pair takes the run-time switches
 	bool fast = P.limiter == 6 && P.riemann == RS_ROTATED;
 	if (stage == 1) {
-		if (fast) launch_one<1, 6, RS_ROTATED>(P, S, Uq, Ubase, Uout, zchunk, stream);
-		else launch_one<1, -1, -1>(P, S, Uq, Ubase, Uout, zchunk, stream);
+		if (fast) launch_one<1, float, 6, RS_ROTATED>(P, S, Uq, Ubase, Uout, 0.5, zchunk, stream);
+		else launch_one<1, float, -1, -1>(P, S, Uq, Ubase, Uout, 0.5, zchunk, stream);
 	} else {
-		if (fast) launch_one<2, 6, RS_ROTATED>(P, S, Uq, Ubase, Uout, zchunk, stream);
-		else launch_one<2, -1, -1>(P, S, Uq, Ubase, Uout, zchunk, stream);
+		if (fast) launch_one<2, float, 6, RS_ROTATED>(P, S, Uq, Ubase, Uout, 1.0, zchunk, stream);
+		else launch_one<2, float, -1, -1>(P, S, Uq, Ubase, Uout, 1.0, zchunk, stream);
 	}
+}
+
+// Hydro sub-step of the operator split in the FP32 form, on the FP64 state:
+// Uout = fix(U + h dt L(fixPrimitives(Q(U)))).
+void launch_hydro_substep_fp32(const Params& P, const State& S, const double* U, double* Uout, double h, int zchunk,
+                               cudaStream_t stream) {
+	bool fast = P.limiter == 6 && P.riemann == RS_ROTATED;
+	if (fast) launch_one<1, double, 6, RS_ROTATED>(P, S, U, U, Uout, h, zchunk, stream);
+	else launch_one<1, double, -1, -1>(P, S, U, U, Uout, h, zchunk, stream);
 }
 
 // FP64 <-> FP32 state conversion (entry to / exit from the FP32 form), with

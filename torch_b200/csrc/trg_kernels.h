@@ -25,6 +25,8 @@ __global__ void k_dt_reset(Params P, State S);
 void launch_hydro_stage_fp32(int stage, const Params& P, const State& S, const float* Uq, const float* Ubase,
                              float* Uout, int zchunk, cudaStream_t stream);
 size_t hydro_stage_fp32_smem();
+void launch_hydro_substep_fp32(const Params& P, const State& S, const double* U, double* Uout, double h, int zchunk,
+                               cudaStream_t stream);
 __global__ void k_f64_to_f32(Params P, const double* a, float* b);
 __global__ void k_f32_to_f64(Params P, const float* a, double* b);
 }  // namespace trg
