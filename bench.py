@@ -1,14 +1,20 @@
 """Benchmark of the TORCH full step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload sedov|hii] [--n 256] [--precision fp32|fp64]
+                    [--workload hii|sedov] [--n 256] [--precision both|fp32|fp64]
 
-Default workload: the 256^3 hydro-only Sedov blast (rho = 1e-20 g/cm^3,
-P = 1e-12 dyn/cm^2, 1e51 erg in a 3-cell sphere, outflow boundaries,
-albada-limited piecewise-linear reconstruction, rotated HLLC, RK2).  A step is
-one Torch::fullStep over the whole grid; the metric is cell updates per
-second (cells x full steps / time).  Inputs (7 x 256^3 cells) are far larger
-than the 126 MB L2, so no flush is needed between steps.
+Default workload: the 256^3 HII-region expansion (side 2 pc, star at the
+centre with Q = 1e49 photons/s, lognormal density with mean 1e3 cm^-3,
+sigma_ln 0.5 and a k^-11/3 spectrum from seed 12345, T = 100 K, radiation
+and cooling on).  A step is one Torch::fullStep over the whole grid (hydro,
+radiative transfer, heating/cooling, the time-step reduction); the metric is
+cell updates per second (cells x full steps / time).  The head number is the
+FP32 form (FP32 hydro, FP64 ionisation solve and reductions); the plain FP64
+form is timed beside it on the same input (`plain_fp64`) and the FP32 form's
+density and pressure error against it after the same steps is reported
+(`error_vs_fp64`).  `--workload sedov` is the 256^3 hydro-only Sedov blast.
+Inputs (7 x 256^3 cells) are far larger than the 126 MB L2, so no flush is
+needed between steps.
 
 One JSON line on rank 0.  Under torchrun (N > 1) every rank advances its own
 replica of the workload on its own GPU (the step does not shard in this
@@ -35,7 +41,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "cell-updates/s/GPU full step 256^3"
+METRIC = "cell-updates/s/GPU full step 256\u00b3: learned+FP32 vs plain FP64, at stated error"
 UNIT = "cell-updates/s"
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
@@ -77,7 +83,7 @@ class ClockSampler:
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,utilization.gpu")
 
     def __init__(self, device):
         self.device = device
@@ -104,22 +110,29 @@ class ClockSampler:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
-        sm, smax, reasons = [], None, set()
+        # only samples taken while the GPU was busy (utilization >= 50 %) count as
+        # "under load"; the sampler runs from before the first timed step to after the last
+        sm, smax, reasons, idle = [], None, set(), 0
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.lines:
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
+                util = float(parts[9])
+                clk = float(parts[1])
                 smax = float(parts[2])
             except ValueError:
                 continue
+            if util < 50:
+                idle += 1
+                continue
+            sm.append(clk)
             for nm, v in zip(names, parts[5:9]):
                 if v.lower() in ("active", "1", "yes"):
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "idle_samples_dropped": idle}
 
 
 def dist_setup():
@@ -258,6 +271,28 @@ PROFILE_NAMES = ("k_hydro_stage_fp32", "k_faces_fp64", "k_hydro_update_fp64", "k
                  "k_rad_no_star")
 
 
+def _conserved(sim):
+    import torch_b200
+    U = np.empty((7, sim.N), dtype=np.float64)
+    rc = sim.lib.trg_get_state(sim.ctx, U.ctypes.data_as(torch_b200.C.c_void_p), None, None, None, None)
+    if rc:
+        raise RuntimeError(f"trg_get_state failed: {rc}")
+    return U
+
+
+def form_error(sim_a, sim_b, gamma, nd):
+    """Relative L1 (sum |a-b| / sum |b|) of density and pressure between two forms."""
+    Ua, Ub = _conserved(sim_a), _conserved(sim_b)
+
+    def pressure(U):
+        ke = sum(U[4 + i] ** 2 for i in range(nd)) / (2.0 * U[0])
+        return (U[1] - ke) * (gamma - 1.0)
+
+    def rel(a, b):
+        return float(np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300))
+    return {"den_rel_l1": rel(Ua[0], Ub[0]), "pre_rel_l1": rel(pressure(Ua), pressure(Ub))}
+
+
 def run_ours(args, world, rank, local, pg):
     import torch
     import torch_b200
@@ -280,6 +315,12 @@ def run_ours(args, world, rank, local, pg):
     ms_max, launches, prof = results[head]
     value = N * args.steps * world / (ms_max / 1e3)
     sim = sims[head]
+    error = None
+    if "fp64" in sims and head != "fp64":
+        # both forms advanced W + K steps from the same initial state
+        error = form_error(sims[head], sims["fp64"], tp.heatCapacityRatio, int(ic.nd))
+        error["steps"] = args.warmup + args.steps
+        error["against"] = "plain FP64 form on the GPU (bit-exact twin of the FP64 oracle)"
     for form, s in sims.items():
         if form != head:
             s.close()
@@ -358,7 +399,7 @@ def run_ours(args, world, rank, local, pg):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if head == "fp32" else "f64",
             "data": "synthetic", "config": workload_config(args.workload, args.n, head, world),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": clk, "kernels": kernel_share,
+            "clocks": clk, "kernels": kernel_share, "error_vs_fp64": error,
         }
         line.update(other)
         print(json.dumps(line), flush=True)
@@ -368,10 +409,10 @@ def run_ours(args, world, rank, local, pg):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["sedov", "hii"], default="sedov")
+    ap.add_argument("--workload", choices=["hii", "sedov"], default="hii")
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--precision", choices=["both", "fp32", "fp64"], default="both")
     ap.add_argument("--e2e-steps", type=int, default=3)

@@ -133,6 +133,29 @@ int trg_enqueue_steps(trg_ctx* c, int nsteps, double dt_next_checkpoint);
 void* trg_stream(const trg_ctx* c);
 int trg_profile_enable(trg_ctx* c, int on);
 int trg_profile_read(trg_ctx* c, const char* name, double* total_ms, long long* launches);
+
+/* Solver counters (no counterpart in the reference, which counts nothing):
+ * when enabled, the implicit ionisation solve (Radiation::update_HIIfrac,
+ * src/Radiation/Radiation.cpp:375-478) and the thermal subcycles
+ * (Thermodynamics::integrate, src/Thermodynamics/Thermodynamics.cpp:266-337)
+ * accumulate the TRG_STAT_* counters below.  trg_stats copies TRG_NSTATS
+ * values out (after synchronising) and zeroes them when reset != 0. */
+#define TRG_NSTATS 24
+enum {
+	TRG_STAT_PICARD_CELLS = 0, /* cells that ran the Picard solve */
+	TRG_STAT_PICARD_ITERS = 1, /* Picard iterations, summed over cells */
+	TRG_STAT_PICARD_MAX = 2,   /* most iterations in one cell */
+	TRG_STAT_PICARD_HIST = 3,  /* 8 bins: 1, 2, 3-4, 5-8, 9-16, 17-64, 65-1024, >1024 iterations */
+	TRG_STAT_LEARNED_CELLS = 11,    /* cells that started from the learned iterate */
+	TRG_STAT_LEARNED_ACCEPTED = 12, /* ... and converged within the first iteration */
+	TRG_STAT_LEARNED_ITERS = 13,    /* Picard iterations of the learned-start cells, fallbacks included */
+	TRG_STAT_THERMO_CELLS = 14,     /* cells that subcycled */
+	TRG_STAT_THERMO_SUBCYCLES = 15, /* subcycles, summed over cells */
+	TRG_STAT_THERMO_MAX = 16,       /* most subcycles in one cell */
+	TRG_STAT_SWEEPS = 17            /* radiation sweeps counted */
+};
+int trg_stats_enable(trg_ctx* c, int on);
+int trg_stats(trg_ctx* c, unsigned long long* out, int reset);
 const char* trg_last_error(const trg_ctx* c);
 void trg_destroy(trg_ctx* c);
 

@@ -95,6 +95,8 @@ _SIGNATURES = [
     ("trg_stream", C.c_void_p, [C.c_void_p]),
     ("trg_profile_enable", C.c_int, [C.c_void_p, C.c_int]),
     ("trg_profile_read", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
+    ("trg_stats_enable", C.c_int, [C.c_void_p, C.c_int]),
+    ("trg_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong), C.c_int]),
     ("trg_hydro_step_fp32_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
 ]
 
@@ -114,6 +116,10 @@ def load_library():
             fn.argtypes = args
         _lib = lib
     return _lib
+
+
+NSTATS = 24
+PICARD_BINS = ("1", "2", "3-4", "5-8", "9-16", "17-64", "65-1024", ">1024")
 
 
 def make_params(tp: TorchParameters, side_length: float, ncells, precision: int = PRECISION_FP64,
@@ -231,6 +237,19 @@ class Torch:
         n = C.c_longlong(0)
         self._check(self.lib.trg_profile_read(self.ctx, name.encode(), C.byref(ms), C.byref(n)))
         return ms.value, n.value
+
+    def stats_enable(self, on: bool):
+        self._check(self.lib.trg_stats_enable(self.ctx, int(on)))
+
+    def stats(self, reset: bool = False) -> dict:
+        """Solver counters (TRG_STAT_* of the C header) as a dict."""
+        buf = (C.c_ulonglong * NSTATS)()
+        self._check(self.lib.trg_stats(self.ctx, buf, int(reset)))
+        v = list(buf)
+        return {"picard_cells": v[0], "picard_iters": v[1], "picard_max": v[2],
+                "picard_hist": dict(zip(PICARD_BINS, v[3:11])),
+                "learned_cells": v[11], "learned_accepted": v[12], "learned_iters": v[13],
+                "thermo_cells": v[14], "thermo_subcycles": v[15], "thermo_max": v[16], "sweeps": v[17]}
 
     def component(self, comp: int, phase: int, dt: float = 0.0) -> float:
         out = C.c_double(0)

@@ -39,6 +39,8 @@ struct trg_ctx {
 	// sub-steps run through the FP32 kernel
 	bool fp32 = false;
 	bool mixed = false;
+	// FP32 form (either kind): the FP64 kernels come from the fast build
+	bool fastk = false;
 	// CUDA graphs of the shell sweeps (all shells of one sweep, launched as one)
 	cudaGraphExec_t g_colden = nullptr;
 	cudaGraphExec_t g_rad[2] = {nullptr, nullptr};
@@ -115,6 +117,9 @@ void profile_collect(trg_ctx* c) {
 	c->recs.clear();
 }
 
+// the exact or the fast build of a kernels_fp64.cu kernel, by the context's form
+#define KF(name) (c->fastk ? trg::fast::name : trg::exact::name)
+
 #define LAUNCH(kernel, n, block, ...)                                                        \
 	do {                                                                                     \
 		if ((n) > 0) {                                                                       \
@@ -128,13 +133,13 @@ void profile_collect(trg_ctx* c) {
 		}                                                                                    \
 	} while (0)
 
-void q_from_u(trg_ctx* c, const double* Usrc, int fix) { LAUNCH(k_q_from_u_fp64, c->P.N, 256, c->P, c->S, Usrc, fix); }
+void q_from_u(trg_ctx* c, const double* Usrc, int fix) { LAUNCH(KF(k_q_from_u_fp64), c->P.N, 256, c->P, c->S, Usrc, fix); }
 
 void colden_sweep_direct(trg_ctx* c) {
 	const auto& off = c->hs.off_all;
 	for (size_t s = 0; s + 1 < off.size(); ++s) {
 		int count = (int)(off[s + 1] - off[s]);
-		LAUNCH(k_colden_shell_fp64, count, 128, c->P, c->S, c->d_sweep_all + off[s], count);
+		LAUNCH(KF(k_colden_shell_fp64), count, 128, c->P, c->S, c->d_sweep_all + off[s], count);
 	}
 }
 
@@ -178,10 +183,10 @@ void colden_sweep(trg_ctx* c) {
 void thermo_pre(trg_ctx* c) {
 	// Thermodynamics::preTimeStepCalculations: column densities, then rates.
 	if (c->P.star_on) colden_sweep(c);
-	LAUNCH(k_thermo_rates_fp64, c->P.N, 256, c->P, c->S);
+	LAUNCH(KF(k_thermo_rates_fp64), c->P.N, 256, c->P, c->S);
 }
 
-void rad_pre(trg_ctx* c) { LAUNCH(k_rad_heating_fp64, c->P.N, 256, c->P, c->S); }
+void rad_pre(trg_ctx* c) { LAUNCH(KF(k_rad_heating_fp64), c->P.N, 256, c->P, c->S); }
 
 void comp_pre(trg_ctx* c, int comp) {
 	if (comp == COMP_RAD) rad_pre(c);
@@ -189,16 +194,16 @@ void comp_pre(trg_ctx* c, int comp) {
 }
 
 void hydro_fluxes(trg_ctx* c) {
-	for (int d = 0; d < c->P.nd; ++d) LAUNCH(k_faces_fp64, c->S.nfaces[d], 128, c->P, c->S, d);
+	for (int d = 0; d < c->P.nd; ++d) LAUNCH(KF(k_faces_fp64), c->S.nfaces[d], 128, c->P, c->S, d);
 }
 
 void rad_sweep_direct(trg_ctx* c, double h) {
 	int nw = (int)c->hs.wind_cells.size();
-	LAUNCH(k_rad_wind_reset, nw, 128, c->P, c->S, c->d_wind, nw);
+	LAUNCH(KF(k_rad_wind_reset), nw, 128, c->P, c->S, c->d_wind, nw);
 	const auto& off = c->hs.off_nonwind;
 	for (size_t s = 0; s + 1 < off.size(); ++s) {
 		int count = (int)(off[s + 1] - off[s]);
-		LAUNCH(k_rad_shell_fp64, count, 128, c->P, c->S, c->d_sweep_nonwind + off[s], count, h,
+		LAUNCH(KF(k_rad_shell_fp64), count, 128, c->P, c->S, c->d_sweep_nonwind + off[s], count, h,
 		       (const double*)nullptr);
 	}
 }
@@ -215,15 +220,15 @@ void rad_integrate(trg_ctx* c, double h) {
 	}
 	if (c->P.star_on) {
 		int nw = (int)c->hs.wind_cells.size();
-		LAUNCH(k_rad_wind_reset, nw, 128, c->P, c->S, c->d_wind, nw);
+		LAUNCH(KF(k_rad_wind_reset), nw, 128, c->P, c->S, c->d_wind, nw);
 		const auto& off = c->hs.off_nonwind;
 		for (size_t s = 0; s + 1 < off.size(); ++s) {
 			int count = (int)(off[s + 1] - off[s]);
-			LAUNCH(k_rad_shell_fp64, count, 128, c->P, c->S, c->d_sweep_nonwind + off[s], count, h,
+			LAUNCH(KF(k_rad_shell_fp64), count, 128, c->P, c->S, c->d_sweep_nonwind + off[s], count, h,
 			       (const double*)nullptr);
 		}
 	} else {
-		LAUNCH(k_rad_no_star_fp64, c->P.N, 256, c->P, c->S, h);
+		LAUNCH(KF(k_rad_no_star_fp64), c->P.N, 256, c->P, c->S, h);
 	}
 }
 
@@ -246,15 +251,15 @@ void sub_step(trg_ctx* c, double h, bool hasCalculatedHeatFlux, int comp) {
 			break;
 		}
 		hydro_fluxes(c);
-		LAUNCH(k_hydro_update_fp64, c->P.N, 256, c->P, c->S, h, (const double*)c->S.U, c->S.U, 0);
+		LAUNCH(KF(k_hydro_update_fp64), c->P.N, 256, c->P, c->S, h, (const double*)c->S.U, c->S.U, 0);
 		break;
 	case COMP_RAD:
 		rad_integrate(c, h);
-		LAUNCH(k_rad_update_fp64, c->P.N, 256, c->P, c->S, h, 0);
+		LAUNCH(KF(k_rad_update_fp64), c->P.N, 256, c->P, c->S, h, 0);
 		break;
 	default:
-		LAUNCH(k_thermo_integrate_fp64, c->P.N, 256, c->P, c->S, h);
-		LAUNCH(k_thermo_update_fp64, c->P.N, 256, c->P, c->S, h, 0);
+		LAUNCH(KF(k_thermo_integrate_fp64), c->P.N, 256, c->P, c->S, h);
+		LAUNCH(KF(k_thermo_update_fp64), c->P.N, 256, c->P, c->S, h, 0);
 		break;
 	}
 }
@@ -263,17 +268,17 @@ void hydro_step(trg_ctx* c) {
 	// Torch::hydroStep (hasCalculatedHeatFlux = true), Torch.cpp:366-387: the
 	// saved state W is the untouched U; the predictor writes U1.
 	hydro_fluxes(c);
-	LAUNCH(k_hydro_update_fp64, c->P.N, 256, c->P, c->S, 0.5, (const double*)c->S.U, c->S.U1, 0);
+	LAUNCH(KF(k_hydro_update_fp64), c->P.N, 256, c->P, c->S, 0.5, (const double*)c->S.U, c->S.U1, 0);
 	q_from_u(c, c->S.U1, 0);
 	hydro_fluxes(c);
-	LAUNCH(k_hydro_update_fp64, c->P.N, 256, c->P, c->S, 1.0, (const double*)c->S.U, c->S.U, 0);
+	LAUNCH(KF(k_hydro_update_fp64), c->P.N, 256, c->P, c->S, 1.0, (const double*)c->S.U, c->S.U, 0);
 }
 
 void time_step(trg_ctx* c, double dt_next) {
 	// Torch::calculateTimeStep and the min with dt_next_checkpoint (Torch.cpp:304-339, :394)
 	int step = c->steps < c->dt_hist_cap ? (int)c->steps : -1;
 	if (c->first_time) {
-		LAUNCH(k_dt_finalize, 1, 1, c->P, c->S, dt_next, 1, step);
+		LAUNCH(KF(k_dt_finalize), 1, 1, c->P, c->S, dt_next, 1, step);
 		c->first_time = 0;
 		return;
 	}
@@ -282,9 +287,9 @@ void time_step(trg_ctx* c, double dt_next) {
 		first_cell = c->hs.first_nonwind_cell;
 		c->rad_once_pending = 0;
 	}
-	LAUNCH(k_dt_reset, 1, 1, c->P, c->S);
-	LAUNCH(k_dt_reduce_fp64, c->P.N, 256, c->P, c->S, first_cell);
-	LAUNCH(k_dt_finalize, 1, 1, c->P, c->S, dt_next, 0, step);
+	LAUNCH(KF(k_dt_reset), 1, 1, c->P, c->S);
+	LAUNCH(KF(k_dt_reduce_fp64), c->P.N, 256, c->P, c->S, first_cell);
+	LAUNCH(KF(k_dt_finalize), 1, 1, c->P, c->S, dt_next, 0, step);
 }
 
 void enqueue_full_step_fp32(trg_ctx* c, double dt_next) {
@@ -292,9 +297,9 @@ void enqueue_full_step_fp32(trg_ctx* c, double dt_next) {
 	// the previous corrector reduced (FP64), the two RK2 stages are one fused
 	// kernel each.
 	int step = c->steps < c->dt_hist_cap ? (int)c->steps : -1;
-	LAUNCH(k_dt_finalize, 1, 1, c->P, c->S, dt_next, c->first_time, step);
+	LAUNCH(KF(k_dt_finalize), 1, 1, c->P, c->S, dt_next, c->first_time, step);
 	c->first_time = 0;
-	LAUNCH(k_dt_reset, 1, 1, c->P, c->S);
+	LAUNCH(KF(k_dt_reset), 1, 1, c->P, c->S);
 	auto stage = [&](int st, const float* Uq, const float* Ub, float* Uo) {
 		cudaEvent_t ea = nullptr, eb = nullptr;
 		if (c->profiling) { ea = pool_event(c); eb = pool_event(c); cudaEventRecord(ea, c->stream); }
@@ -304,7 +309,7 @@ void enqueue_full_step_fp32(trg_ctx* c, double dt_next) {
 	};
 	stage(1, c->U32, c->U32, c->U32s);
 	stage(2, c->U32s, c->U32, c->U32);
-	LAUNCH(k_time_advance, 1, 1, c->S);
+	LAUNCH(KF(k_time_advance), 1, 1, c->S);
 	c->steps++;
 }
 
@@ -329,7 +334,7 @@ void enqueue_full_step(trg_ctx* c, double dt_next) {
 		}
 		for (int i = ncomps - 2; i >= 0; --i) sub_step(c, 0.5, false, c->hs.active[(i + c->stepCounter) % ncomps]);
 	}
-	LAUNCH(k_time_advance, 1, 1, c->S);
+	LAUNCH(KF(k_time_advance), 1, 1, c->S);
 	c->steps++;
 }
 
@@ -415,6 +420,7 @@ int trg_create(const trg_params* p, const double* den, const double* pre, const 
 	rc |= dalloc(c, &S.ds, N);
 	rc |= dalloc(c, &S.shellVol, N);
 	rc |= dalloc(c, &S.err, 1);
+	rc |= dalloc(c, &S.stats, TRG_NSTATS);
 	rc |= dalloc(c, &S.scal, 8);
 	if (c->hs.has_grav) rc |= dalloc(c, &S.grav, 3 * N);
 	for (int d = 0; d < 3; ++d) {
@@ -441,6 +447,7 @@ int trg_create(const trg_params* p, const double* den, const double* pre, const 
 	CUDA_TRY(cudaMemsetAsync(S.UDOT, 0, 7 * N * sizeof(double), st));
 	CUDA_TRY(cudaMemsetAsync(S.U1, 0, 7 * N * sizeof(double), st));
 	CUDA_TRY(cudaMemsetAsync(S.err, 0, sizeof(unsigned), st));
+	CUDA_TRY(cudaMemsetAsync(S.stats, 0, TRG_NSTATS * sizeof(unsigned long long), st));
 	CUDA_TRY(cudaMemsetAsync(S.scal, 0, 8 * sizeof(double), st));
 	CUDA_TRY(cudaMemcpyAsync(c->d_tables, &c->hs.tables, sizeof(Tables), cudaMemcpyHostToDevice, st));
 	if (!c->hs.sweep_all.empty())
@@ -456,10 +463,12 @@ int trg_create(const trg_params* p, const double* den, const double* pre, const 
 	if (p->precision == TRG_PRECISION_FP32 && c->hs.nactive > 1) {
 		if (c->P.nd < 2) return set_error(c, TRG_ERR_ARG, "the FP32 form needs a 2-D or 3-D grid");
 		c->mixed = true;
+		c->fastk = true;
 		c->zchunk = ctx_fp32_zchunk(c);
 	} else if (p->precision == TRG_PRECISION_FP32) {
 		if (c->P.nd < 2) return set_error(c, TRG_ERR_ARG, "the FP32 form needs a 2-D or 3-D grid");
 		c->fp32 = true;
+		c->fastk = true;
 		// z chunk per CTA: about four waves of two 256-thread CTAs per SM
 		c->zchunk = ctx_fp32_zchunk(c);
 		if ((rc = dalloc(c, &c->U32, 7 * N)) || (rc = dalloc(c, &c->U32s, 7 * N))) return rc;
@@ -547,13 +556,13 @@ int trg_component(trg_ctx* c, int comp, int phase, double dt, double* out) {
 		else if (comp == TRG_COMP_RAD) rad_pre(c);
 		break;
 	case TRG_PHASE_DT: {
-		LAUNCH(k_dt_reset, 1, 1, c->P, c->S);
+		LAUNCH(KF(k_dt_reset), 1, 1, c->P, c->S);
 		long long first_cell = -1;
 		if (comp == TRG_COMP_RAD && c->P.radiation_on && c->P.star_on && c->P.K1 != 0.0 && c->rad_once_pending) {
 			first_cell = c->hs.first_nonwind_cell;
 			c->rad_once_pending = 0;
 		}
-		LAUNCH(k_dt_reduce_fp64, c->P.N, 256, c->P, c->S, first_cell);
+		LAUNCH(KF(k_dt_reduce_fp64), c->P.N, 256, c->P, c->S, first_cell);
 		double mins[3];
 		CUDA_TRY(cudaMemcpyAsync(mins, c->S.scal + 2, sizeof(mins), cudaMemcpyDeviceToHost, c->stream));
 		CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -567,19 +576,19 @@ int trg_component(trg_ctx* c, int comp, int phase, double dt, double* out) {
 	case TRG_PHASE_INTEGRATE:
 		if (comp == TRG_COMP_HYDRO) hydro_fluxes(c);
 		else if (comp == TRG_COMP_RAD) rad_integrate(c, 1.0);
-		else if (comp == TRG_COMP_THERMO) LAUNCH(k_thermo_integrate_fp64, c->P.N, 256, c->P, c->S, 1.0);
+		else if (comp == TRG_COMP_THERMO) LAUNCH(KF(k_thermo_integrate_fp64), c->P.N, 256, c->P, c->S, 1.0);
 		break;
 	case TRG_PHASE_SOURCES:
 		if (comp == TRG_COMP_HYDRO)
-			LAUNCH(k_hydro_update_fp64, c->P.N, 256, c->P, c->S, 1.0, (const double*)c->S.U, c->S.U, 1);
-		else if (comp == TRG_COMP_RAD) LAUNCH(k_rad_update_fp64, c->P.N, 256, c->P, c->S, 1.0, 1);
-		else if (comp == TRG_COMP_THERMO) LAUNCH(k_thermo_update_fp64, c->P.N, 256, c->P, c->S, 1.0, 1);
+			LAUNCH(KF(k_hydro_update_fp64), c->P.N, 256, c->P, c->S, 1.0, (const double*)c->S.U, c->S.U, 1);
+		else if (comp == TRG_COMP_RAD) LAUNCH(KF(k_rad_update_fp64), c->P.N, 256, c->P, c->S, 1.0, 1);
+		else if (comp == TRG_COMP_THERMO) LAUNCH(KF(k_thermo_update_fp64), c->P.N, 256, c->P, c->S, 1.0, 1);
 		break;
 	case TRG_PHASE_Q_FROM_U:
 		q_from_u(c, c->S.U, 1);
 		break;
 	case TRG_PHASE_ADVANCE:
-		LAUNCH(k_advance_fp64, c->P.N, 256, c->P, c->S, dt);
+		LAUNCH(KF(k_advance_fp64), c->P.N, 256, c->P, c->S, dt);
 		break;
 	default:
 		return set_error(c, TRG_ERR_ARG, "unknown phase");
@@ -628,6 +637,36 @@ double trg_time(const trg_ctx* c) {
 
 double trg_dt_max(const trg_ctx* c) { return c ? c->hs.dt_max : 0; }
 long trg_ncells(const trg_ctx* c) { return c ? (long)c->P.N : 0; }
+static void drop_graphs(trg_ctx* c) {
+	// the sweep graphs hold the kernel arguments (Params, State) by value
+	if (c->g_colden) cudaGraphExecDestroy(c->g_colden);
+	c->g_colden = nullptr;
+	for (auto& g : c->g_rad) {
+		if (g) cudaGraphExecDestroy(g);
+		g = nullptr;
+	}
+}
+
+int trg_stats_enable(trg_ctx* c, int on) {
+	if (!c) return TRG_ERR_ARG;
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	if ((c->P.stats_on != 0) != (on != 0)) drop_graphs(c);
+	c->P.stats_on = on ? 1 : 0;
+	return TRG_OK;
+}
+
+int trg_stats(trg_ctx* c, unsigned long long* out, int reset) {
+	if (!c || !out) return TRG_ERR_ARG;
+	CUDA_TRY(cudaMemcpyAsync(out, c->S.stats, TRG_NSTATS * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+	                         c->stream));
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	if (reset) {
+		CUDA_TRY(cudaMemsetAsync(c->S.stats, 0, TRG_NSTATS * sizeof(unsigned long long), c->stream));
+		CUDA_TRY(cudaStreamSynchronize(c->stream));
+	}
+	return TRG_OK;
+}
+
 long long trg_kernel_launches(const trg_ctx* c) { return c ? c->launches : 0; }
 const char* trg_last_error(const trg_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
@@ -636,9 +675,7 @@ void trg_destroy(trg_ctx* c) {
 	if (c->stream) cudaStreamSynchronize(c->stream);
 	profile_collect(c);
 	for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
-	if (c->g_colden) cudaGraphExecDestroy(c->g_colden);
-	for (auto& g : c->g_rad)
-		if (g) cudaGraphExecDestroy(g);
+	drop_graphs(c);
 	for (void* p : c->allocs) cudaFree(p);
 	if (c->stream) cudaStreamDestroy(c->stream);
 	delete c;

@@ -1,9 +1,13 @@
-// FP64 kernels of the operator-split step (the plain-FP64 form).
+// FP64 kernels of the operator-split step.
 //
-// Compiled with --fmad=false: every kernel reproduces the reference's FP64
-// arithmetic in the reference's operation order.  exp/log/log10/pow come from
-// trg_math.h (IEEE +-*/ only), which the CPU oracle can share, so that the
-// GPU and CPU runs agree to the last bit.
+// This file is compiled twice.  The exact build (namespace trg::exact, the
+// plain-FP64 form) uses --fmad=false: every kernel reproduces the reference's
+// FP64 arithmetic in the reference's operation order, and exp/log/log10/pow
+// come from trg_math.h (IEEE +-*/ only), which the CPU oracle can share, so
+// that the GPU and CPU runs agree to the last bit.  The fast build
+// (trg::fast, -DTRG_FAST_MATH, FMA contraction on) serves the FP32 form, whose
+// radiation, cooling and time-step kernels stay FP64 but need not round like
+// the reference.
 //
 // Layout: SoA, field-major, interior cells only, flat index i + nx*(j + ny*k).
 // Ghost cells are not stored: boundary conditions are applied while loading
@@ -11,7 +15,11 @@
 #include "trg_device.cuh"
 #include "trg_kernels.h"
 
+#ifndef TRG_KNS
+#define TRG_KNS exact
+#endif
 namespace trg {
+namespace TRG_KNS {
 
 // ------------------------------------------------------------------ limiters
 __device__ __forceinline__ double minmod(double a, double b) { return (a * b > 0) ? (fabs(a) < fabs(b) ? a : b) : 0; }
@@ -69,7 +77,8 @@ __device__ void hllc(double* F, const double* Ql, const double* Qr, double a_l2,
 		FfromQ(F_lr, Qlr, gamma, nd, dim);
 		double A_lr = Qlr[DEN] * (S_lr - Qlr[VEL + dim]) / (S_lr - S_c);
 		U_c[DEN] = A_lr;
-		for (int id = 0; id < nd; ++id) U_c[VEL + id] = A_lr * Qlr[VEL + id];
+		#pragma unroll
+		for (int id = 0; id < 3; ++id) if (id < nd) U_c[VEL + id] = A_lr * Qlr[VEL + id];
 		U_c[VEL + dim] = A_lr * S_c;
 		U_c[PRE] = A_lr * ((U_lr[PRE] / Qlr[DEN]) +
 		                   (S_c - Qlr[VEL + dim]) * (S_c + Qlr[PRE] / (Qlr[DEN] * (S_lr - Qlr[VEL + dim]))));
@@ -310,7 +319,8 @@ __device__ __forceinline__ void hydro_udot(const Params& P, const State& S, long
 	double vol = cell_volume(P, xc[0]);
 #pragma unroll
 	for (int i = 0; i < NU; ++i) udot[i] = 0;
-	for (int dim = 0; dim < P.nd; ++dim) {
+	#pragma unroll
+	for (int dim = 0; dim < 3; ++dim) if (dim < P.nd) {
 		long long fl, fr;
 		face_ids(P, ijk, dim, fl, fr);
 		double al = face_area(P, xc, dim, 0), ar = face_area(P, xc, dim, 1);
@@ -408,8 +418,8 @@ __global__ void __launch_bounds__(256) k_advance_fp64(Params P, State S, double 
 // Radiation.cpp:243-251.
 __device__ __forceinline__ double photoionisation_rate(double nHI, double T, double delT, double shellVol, double photonRate) {
 	if (nHI == 0 || shellVol == 0) return 0.0;
-	double emT = trg_exp(-T);
-	double emdT = trg_exp(-delT);
+	double emT = d_exp(-T);
+	double emdT = d_exp(-delT);
 	return photonRate * emT * (1.0 - emdT) / (nHI * shellVol);
 }
 
@@ -417,7 +427,7 @@ __device__ __forceinline__ double photoionisation_rate(double nHI, double T, dou
 __device__ __forceinline__ double collisional_ionisation_rate(const Params& P, double T) {
 	if (!P.collisions_on || T < 5.0e3) return 0.0;
 	double U = P.voronov_DE / T;
-	return P.voronov_A * (1. + P.voronov_P * sqrt(U)) * trg_exp(P.voronov_K * trg_log(U) - U) / (P.voronov_X + U);
+	return P.voronov_A * (1. + P.voronov_P * sqrt(U)) * d_exp(P.voronov_K * d_log(U) - U) / (P.voronov_X + U);
 }
 
 // Radiation::doric, Radiation.cpp:140-179.
@@ -433,7 +443,7 @@ __device__ __forceinline__ void doric(double dt, double& HII_avg, double& HII, d
 		if (1.0 - HII < epsilon) HII = 1.0 - epsilon;
 		HII_avg = HII;
 	} else {
-		double e = trg_exp(-dt * inv_ti);
+		double e = d_exp(-dt * inv_ti);
 		HII = xeq + (HII_old - xeq) * e;
 		HII = smax(smin(HII, 1.0), 0.0);
 		if (1.0 - HII < epsilon) HII = 1.0 - epsilon;
@@ -443,45 +453,55 @@ __device__ __forceinline__ void doric(double dt, double& HII_avg, double& HII, d
 	}
 }
 
+__device__ __forceinline__ double pick3(double a0, double a1, double a2, int k) { return k == 0 ? a0 : (k == 1 ? a1 : a2); }
+
 // C2-Ray upwind neighbours and weights (Grid::calculateNearestNeighbours,
 // Grid.cpp:922-952) computed on the fly.  A neighbour outside the interior
 // (a ghost cell or none in the reference) contributes zero optical depth and
 // is returned as -1.
+// The rotated frame (irot) is resolved with selects rather than indexed
+// arrays, so that everything stays in registers.
 __device__ __forceinline__ void neighbours(const Params& P, const int* ijk, const double* xc, long long* nb, double* w) {
 	int plane = 0;
 	double dmax = 0;
-	for (int i = 0; i < P.nd; ++i) {
-		double dd = fabs(xc[i] - P.sxc[i]);
-		if (dd > dmax) { dmax = dd; plane = i; }
-	}
-	int irot[3] = {(plane + 1) % 3, (plane + 2) % 3, plane % 3};
-	double d[3];
-	int s[3], LR[3];
-	for (int i = 0; i < 3; i++) {
-		d[i] = xc[irot[i]] - P.sxc[irot[i]];
-		s[i] = d[i] < -1.0 / 10.0 ? -1 : 1;
-		LR[i] = fabs(d[i]) < 1.0 / 10.0 ? 0 : s[i];
-	}
-	const int off[4][3] = {{0, 0, -LR[2]}, {0, -LR[1], -LR[2]}, {-LR[0], 0, -LR[2]}, {-LR[0], -LR[1], -LR[2]}};
+#pragma unroll
+	for (int i = 0; i < 3; ++i)
+		if (i < P.nd) {
+			double dd = fabs(xc[i] - P.sxc[i]);
+			if (dd > dmax) { dmax = dd; plane = i; }
+		}
+	// irot = {(plane + 1) % 3, (plane + 2) % 3, plane}
+	const int r0 = plane == 2 ? 0 : plane + 1, r1 = plane == 0 ? 2 : plane - 1, r2 = plane;
+	const double x0 = pick3(xc[0], xc[1], xc[2], r0), x1 = pick3(xc[0], xc[1], xc[2], r1);
+	const double d0 = x0 - pick3(P.sxc[0], P.sxc[1], P.sxc[2], r0);
+	const double d1 = x1 - pick3(P.sxc[0], P.sxc[1], P.sxc[2], r1);
+	const double d2 = pick3(xc[0], xc[1], xc[2], r2) - pick3(P.sxc[0], P.sxc[1], P.sxc[2], r2);
+	const int s0 = d0 < -1.0 / 10.0 ? -1 : 1, s1 = d1 < -1.0 / 10.0 ? -1 : 1, s2 = d2 < -1.0 / 10.0 ? -1 : 1;
+	const int L0 = fabs(d0) < 1.0 / 10.0 ? 0 : s0, L1 = fabs(d1) < 1.0 / 10.0 ? 0 : s1, L2 = fabs(d2) < 1.0 / 10.0 ? 0 : s2;
+	// offsets in the rotated frame: n = 0: (0, 0, -L2), 1: (0, -L1, -L2), 2: (-L0, 0, -L2), 3: (-L0, -L1, -L2)
+#pragma unroll
 	for (int n = 0; n < 4; ++n) {
-		int t[3] = {ijk[0], ijk[1], ijk[2]};
-		for (int r = 0; r < 3; ++r) t[irot[r]] += off[n][r];
-		bool in = t[0] >= 0 && t[0] < P.nx && t[1] >= 0 && t[1] < P.ny && t[2] >= 0 && t[2] < P.nz;
-		nb[n] = in ? flat_id(P, t[0], t[1], t[2]) : -1;
+		const int o0 = (n & 2) ? -L0 : 0, o1 = (n & 1) ? -L1 : 0, o2 = -L2;
+		const int ti = ijk[0] + (r0 == 0 ? o0 : 0) + (r1 == 0 ? o1 : 0) + (r2 == 0 ? o2 : 0);
+		const int tj = ijk[1] + (r0 == 1 ? o0 : 0) + (r1 == 1 ? o1 : 0) + (r2 == 1 ? o2 : 0);
+		const int tk = ijk[2] + (r0 == 2 ? o0 : 0) + (r1 == 2 ? o1 : 0) + (r2 == 2 ? o2 : 0);
+		bool in = ti >= 0 && ti < P.nx && tj >= 0 && tj < P.ny && tk >= 0 && tk < P.nz;
+		nb[n] = in ? flat_id(P, ti, tj, tk) : -1;
 	}
-	double ic0 = (int)xc[irot[0]] - 0.5 * (s[2] * d[0] / d[2]);
-	double ic1 = (int)xc[irot[1]] - 0.5 * (s[2] * d[1] / d[2]);
-	double delta0 = fabs(2.0 * ic0 - 2.0 * (int)xc[irot[0]] + s[0]);
-	double delta1 = fabs(2.0 * ic1 - 2.0 * (int)xc[irot[1]] + s[1]);
-	w[0] = (fabs(d[2]) > 0.9) ? delta0 * delta1 : 0;
-	w[1] = ((fabs(d[1]) > 0.9) && (fabs(d[2]) > 0.9)) ? delta0 * (1.0 - delta1) : 0;
-	w[2] = ((fabs(d[0]) > 0.9) && (fabs(d[2]) > 0.9)) ? (1.0 - delta0) * delta1 : 0;
-	w[3] = ((fabs(d[0]) > 0.9) && (fabs(d[1]) > 0.9) && (fabs(d[2]) > 0.9)) ? (1.0 - delta0) * (1.0 - delta1) : 0;
+	double ic0 = (int)x0 - 0.5 * (s2 * d0 / d2);
+	double ic1 = (int)x1 - 0.5 * (s2 * d1 / d2);
+	double delta0 = fabs(2.0 * ic0 - 2.0 * (int)x0 + s0);
+	double delta1 = fabs(2.0 * ic1 - 2.0 * (int)x1 + s1);
+	w[0] = (fabs(d2) > 0.9) ? delta0 * delta1 : 0;
+	w[1] = ((fabs(d1) > 0.9) && (fabs(d2) > 0.9)) ? delta0 * (1.0 - delta1) : 0;
+	w[2] = ((fabs(d0) > 0.9) && (fabs(d2) > 0.9)) ? (1.0 - delta0) * delta1 : 0;
+	w[3] = ((fabs(d0) > 0.9) && (fabs(d1) > 0.9) && (fabs(d2) > 0.9)) ? (1.0 - delta0) * (1.0 - delta1) : 0;
 }
 
 __device__ __forceinline__ double dist2_cells(const Params& P, const double* xc) {
 	double d2 = 0;
-	for (int i = 0; i < P.nd; ++i) d2 += (xc[i] - P.sxc[i]) * (xc[i] - P.sxc[i]);
+	#pragma unroll
+	for (int i = 0; i < 3; ++i) if (i < P.nd) d2 += (xc[i] - P.sxc[i]) * (xc[i] - P.sxc[i]);
 	return d2;
 }
 
@@ -545,6 +565,7 @@ __global__ void __launch_bounds__(128) k_rad_shell_fp64(Params P, State S, const
 	bool star = (int)xc[0] == (int)P.sxc[0] && (int)xc[1] == (int)P.sxc[1] && (double)(int)xc[2] == P.sxc[2];
 	double q_den = FLD(S.Q, DEN, id), q_pre = FLD(S.Q, PRE, id), q_hii = FLD(S.Q, HII, id);
 	double ds = S.ds[id];
+	unsigned iters = 0;
 	if (star) {
 		FLD(S.R, R_HEAT, id) = 0;
 		FLD(S.Q, HII, id) = 1;
@@ -586,10 +607,12 @@ __global__ void __launch_bounds__(128) k_rad_shell_fp64(Params P, State S, const
 		FLD(S.R, R_HII_A, id) = HII_avg;
 		FLD(S.Q, HII, id) = x_new;
 		if (x_new > 0.001) FLD(S.Q, ADV, id) = 1;
+		iters = (unsigned)miter * 10006u + (unsigned)niter;
 	}
 	double nH = P.X * q_den / P.hydrogenMass;
 	FLD(S.R, R_DTAU, id) = (1.0 - FLD(S.Q, HII, id)) * nH * P.photoIonXsec * ds;
 	FLD(S.R, R_DTAU_A, id) = (1.0 - FLD(S.R, R_HII_A, id)) * nH * P.photoIonXsec * ds;
+	if (P.stats_on) stat_picard(S.stats, iters);
 }
 
 // Star off: Radiation::transferRadiation else-branch (Radiation.cpp:638-650), interior cells.
@@ -649,7 +672,8 @@ __global__ void __launch_bounds__(256) k_rad_update_fp64(Params P, State S, doub
 			double T_new = P.THI + (P.THII - P.THI) * q_hii;
 			double pre_new = P.specificGasConstant * mu_inv_new * q_den * T_new;
 			double ke = 0.0;
-			for (int dim = 0; dim < P.nd; ++dim) ke += 0.5 * u[VEL + dim] * u[VEL + dim] / u[DEN];
+			#pragma unroll
+			for (int dim = 0; dim < 3; ++dim) if (dim < P.nd) ke += 0.5 * u[VEL + dim] * u[VEL + dim] / u[DEN];
 			double E_new = pre_new / (P.gamma - 1.0) + ke;
 			udot[PRE] += (E_new - u[PRE]) / dt;
 		} else if (P.coupling == CP_NEQ) {
@@ -672,32 +696,32 @@ __global__ void __launch_bounds__(256) k_rad_update_fp64(Params P, State S, doub
 // ----------------------------------------------------------- thermodynamics
 // Henney et al. (2009) heating and cooling, Thermodynamics.cpp:113-211.
 __device__ __forceinline__ double th_imlc(const Params& P, double ne, double T) {
-	return P.imlc * P.z0 * ne * ne * trg_exp(-P.T1 / T - (P.T2 / T) * (P.T2 / T));
+	return P.imlc * P.z0 * ne * ne * d_exp(-P.T1 / T - (P.T2 / T) * (P.T2 / T));
 }
 __device__ __forceinline__ double th_nmlc(const Params& P, double ne, double nn, double T) {
-	return P.nmlc * P.z0 * ne * nn * trg_exp(-P.T3 / T - (P.T4 / T) * (P.T4 / T));
+	return P.nmlc * P.z0 * ne * nn * d_exp(-P.T3 / T - (P.T4 / T) * (P.T4 / T));
 }
 __device__ __forceinline__ double th_ciec(const Params& P, double ne, double T) {
 	if (T > P.ciec_minT) {
-		double cie_rate = P.ciec * ne * ne * P.z0 * trg_exp(-0.63 * trg_log(T)) * (1.0 - trg_exp(-trg_pow(1.0e-5 * T, 1.63)));
+		double cie_rate = P.ciec * ne * ne * P.z0 * d_exp(-0.63 * d_log(T)) * (1.0 - d_exp(-d_pow(1.0e-5 * T, 1.63)));
 		double smoothing = smin(1.0, (T - 5.0e4) / (2.0e4));
 		return cie_rate * smoothing;
 	}
 	return 0;
 }
 __device__ __forceinline__ double th_nmc(const Params& P, double nH, double x, double T) {
-	double T0 = 70.0 + 220.0 * trg_pow(nH / P.n0, 0.2);
-	return P.nmc * (1.0 - x) * (1.0 - x) * trg_pow(nH, 1.6) * sqrt(T) * trg_exp(-T0 / T);
+	double T0 = 70.0 + 220.0 * d_pow(nH / P.n0, 0.2);
+	return P.nmc * (1.0 - x) * (1.0 - x) * d_pow(nH, 1.6) * sqrt(T) * d_exp(-T0 / T);
 }
 __device__ __forceinline__ double th_cxhi(const Params& P, const State& S, double nH, double x, double T) {
-	double rate = spline_eval(S.tables->th_cxhi, trg_log10(T));
-	return x * (1.0 - x) * nH * nH * trg_exp((2.302585093 * rate) - ((T / P.cxhi_damp) * (T / P.cxhi_damp)));
+	double rate = spline_eval(S.tables->th_cxhi, d_log10(T));
+	return x * (1.0 - x) * nH * nH * d_exp((2.302585093 * rate) - ((T / P.cxhi_damp) * (T / P.cxhi_damp)));
 }
 __device__ __forceinline__ double th_fuvh(const Params& P, double nH, double Av, double F) {
-	return P.fuvh_a * nH * F * trg_exp(-1.9 * Av) / (P.fuvh_b + P.fuvh_c * F * trg_exp(-1.9 * Av) / nH);
+	return P.fuvh_a * nH * F * d_exp(-1.9 * Av) / (P.fuvh_b + P.fuvh_c * F * d_exp(-1.9 * Av) / nH);
 }
 __device__ __forceinline__ double th_irh(const Params& P, double nH, double Av, double F) {
-	return P.irh_a * nH * F * trg_exp(-0.05 * Av) * trg_exp(-2.0 * trg_log(1.0 + P.irh_b / nH));
+	return P.irh_a * nH * F * d_exp(-0.05 * Av) * d_exp(-2.0 * d_log(1.0 + P.irh_b / nH));
 }
 __device__ __forceinline__ double soft_landing(double rate, double T, double T_min) {
 	double result = rate;
@@ -767,7 +791,8 @@ __global__ void __launch_bounds__(256) k_thermo_rates_fp64(Params P, State S) {
 	double T = calc_temperature(P, x, q_pre, q_den);
 	double rsqrd = 0, F_FUV = 0;
 	if (P.star_on) {
-		for (int i = 0; i < P.nd; ++i) rsqrd += (xc[i] - P.sxc[i]) * (xc[i] - P.sxc[i]) * P.dx[i] * P.dx[i];
+		#pragma unroll
+		for (int i = 0; i < 3; ++i) if (i < P.nd) rsqrd += (xc[i] - P.sxc[i]) * (xc[i] - P.sxc[i]) * P.dx[i] * P.dx[i];
 		double Q_FUV = 0.5 * P.photonRate;
 		F_FUV = rsqrd != 0 ? Q_FUV / (1.2e7 * 4 * P.pi * rsqrd) : 0;
 	}
@@ -819,6 +844,11 @@ __global__ void __launch_bounds__(256) k_thermo_integrate_fp64(Params P, State S
 		double dtdti = dt / dti;
 		int nsteps = dtdti - (int)dtdti > 0 ? (int)(dtdti + 1.0) : (int)(dtdti + 0.5);
 		--nsteps;
+		if (P.stats_on) {
+			stat_add(S.stats, TRG_STAT_THERMO_CELLS, 1u);
+			stat_add(S.stats, TRG_STAT_THERMO_SUBCYCLES, (unsigned)nsteps);
+			stat_max(S.stats, TRG_STAT_THERMO_MAX, (unsigned)nsteps);
+		}
 		for (int i = 0; i < nsteps; ++i) {
 			double r = th_cooling(P, S, heat, ne, nn, nH, x, subT);
 			r = P.heating_amp * soft_landing(r, subT, Tmin);
@@ -891,7 +921,8 @@ __global__ void __launch_bounds__(256) k_dt_reduce_fp64(Params P, State S, long 
 		double q_den = FLD(S.Q, DEN, id), q_pre = FLD(S.Q, PRE, id), q_hii = FLD(S.Q, HII, id);
 		double inv_t = 0;
 		double ss = sqrt(P.gamma * q_pre / q_den);
-		for (int dim = 0; dim < P.nd; ++dim) inv_t += (fabs(FLD(S.Q, VEL + dim, id)) + ss) / P.dx[dim];
+		#pragma unroll
+		for (int dim = 0; dim < 3; ++dim) if (dim < P.nd) inv_t += (fabs(FLD(S.Q, VEL + dim, id)) + ss) / P.dx[dim];
 		if (inv_t == 0) inv_t = 1.0 / P.dt_max;
 		th = 0.5 / inv_t;
 		int ijk[3];
@@ -974,4 +1005,5 @@ __global__ void k_dt_reset(Params P, State S) {
 	slots[2] = big;
 }
 
+}  // namespace TRG_KNS
 }  // namespace trg

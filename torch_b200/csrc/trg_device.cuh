@@ -12,6 +12,23 @@
 
 #include "trg_math.h"
 #include "trg_types.h"
+#include "../../include/torch_b200.h"
+
+// Transcendentals of the radiation and cooling kernels.  The exact build
+// (FP64 form) uses the IEEE-only functions of trg_math.h, shared with the CPU
+// oracle; the fast build (FP32 form, compiled with TRG_FAST_MATH and FMA
+// contraction) uses CUDA's double-precision library.
+#ifdef TRG_FAST_MATH
+#define d_exp(x) exp(x)
+#define d_log(x) log(x)
+#define d_log10(x) log10(x)
+#define d_pow(x, y) pow(x, y)
+#else
+#define d_exp(x) trg_exp(x)
+#define d_log(x) trg_log(x)
+#define d_log10(x) trg_log10(x)
+#define d_pow(x, y) trg_pow(x, y)
+#endif
 
 namespace trg {
 
@@ -21,6 +38,15 @@ __device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b 
 __device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
 
 __device__ __forceinline__ void cell_ijk(const Params& P, long long id, int* ijk) {
+	if (P.N <= 0x7fffffffLL) {  // 32-bit division: a fraction of the cost of the 64-bit one
+		unsigned u = (unsigned)id, nx = (unsigned)P.nx, ny = (unsigned)P.ny;
+		unsigned q = u / nx;
+		ijk[0] = (int)(u - q * nx);
+		unsigned r = q / ny;
+		ijk[1] = (int)(q - r * ny);
+		ijk[2] = (int)r;
+		return;
+	}
 	ijk[0] = (int)(id % P.nx);
 	ijk[1] = (int)((id / P.nx) % P.ny);
 	ijk[2] = (int)(id / ((long long)P.nx * P.ny));
@@ -31,7 +57,8 @@ __device__ __forceinline__ long long flat_id(const Params& P, int i, int j, int 
 // Grid::buildCells (Grid.cpp:525-548): centre at index + 0.5 for dims < nd, 0 beyond.
 __device__ __forceinline__ void cell_xc(const Params& P, const int* ijk, double* xc) {
 	for (int i = 0; i < 3; ++i) xc[i] = (double)ijk[i];
-	for (int i = 0; i < P.nd; ++i) xc[i] += 0.5;
+	#pragma unroll
+	for (int i = 0; i < 3; ++i) if (i < P.nd) xc[i] += 0.5;
 }
 __device__ __forceinline__ int ncell(const Params& P, int d) { return d == 0 ? P.nx : (d == 1 ? P.ny : P.nz); }
 
@@ -41,7 +68,8 @@ __device__ __forceinline__ double cell_volume(const Params& P, double rc) {
 	double volume = 0, r1, r2;
 	if (P.geometry == G_CART) {
 		volume = 1.0;
-		for (int i = 0; i < P.nd; ++i) volume *= P.dx[i];
+		#pragma unroll
+		for (int i = 0; i < 3; ++i) if (i < P.nd) volume *= P.dx[i];
 	} else if (P.geometry == G_CYL) {
 		r2 = rc * P.dx[0] + 0.5 * P.dx[0];
 		r1 = rc * P.dx[0] - 0.5 * P.dx[0];
@@ -61,7 +89,8 @@ __device__ __forceinline__ double join_area(const Params& P, const double* xj, i
 	double area = 0, r1, r2;
 	if (P.geometry == G_CART) {
 		area = 1.0;
-		for (int i = 0; i < P.nd; ++i)
+		#pragma unroll
+		for (int i = 0; i < 3; ++i) if (i < P.nd)
 			if (i != dim) area *= P.dx[i];
 	} else if (P.geometry == G_CYL) {
 		if (dim == 0) {
@@ -91,7 +120,8 @@ __device__ __forceinline__ double face_area(const Params& P, const double* xc, i
 // Fluid::initialiseGrid wind test, Fluid.cpp:41-53.
 __device__ __forceinline__ bool is_wind(const Params& P, long long id, const int* ijk, const double* xc) {
 	double dist2 = 0;
-	for (int i = 0; i < P.nd; ++i)
+	#pragma unroll
+	for (int i = 0; i < 3; ++i) if (i < P.nd)
 		dist2 += ((int)xc[i] - P.star_pos[i]) * (xc[i] - P.star_pos[i]);
 	return dist2 <= (double)(P.wind_radius * P.wind_radius) || id == P.star_cell;
 }
@@ -101,7 +131,8 @@ __device__ __forceinline__ bool is_wind(const Params& P, long long id, const int
 __device__ __forceinline__ void UfromQ(double* u, const double* q, double gamma, int nd) {
 	double ke = 0;
 	u[DEN] = q[DEN];
-	for (int dim = 0; dim < nd; ++dim) {
+	#pragma unroll
+	for (int dim = 0; dim < 3; ++dim) if (dim < nd) {
 		u[VEL + dim] = q[VEL + dim] * q[DEN];
 		ke += 0.5 * q[DEN] * q[VEL + dim] * q[VEL + dim];
 	}
@@ -113,7 +144,8 @@ __device__ __forceinline__ void UfromQ(double* u, const double* q, double gamma,
 __device__ __forceinline__ void QfromU(double* q, const double* u, double gamma, int nd) {
 	q[DEN] = u[DEN];
 	double ke = 0;
-	for (int dim = 0; dim < nd; ++dim) {
+	#pragma unroll
+	for (int dim = 0; dim < 3; ++dim) if (dim < nd) {
 		q[VEL + dim] = u[VEL + dim] / u[DEN];
 		ke += 0.5 * u[VEL + dim] * u[VEL + dim] / u[DEN];
 	}
@@ -125,7 +157,8 @@ __device__ __forceinline__ void QfromU(double* q, const double* u, double gamma,
 __device__ __forceinline__ void FfromQ(double* f, const double* q, double gamma, int nd, int dim) {
 	f[DEN] = q[DEN] * q[VEL + dim];
 	double ke = 0;
-	for (int id = 0; id < nd; ++id) {
+	#pragma unroll
+	for (int id = 0; id < 3; ++id) if (id < nd) {
 		ke += q[VEL + id] * q[VEL + id];
 		int c = (dim + id) % nd;
 		f[VEL + c] = q[DEN] * q[VEL + c] * q[VEL + dim];
@@ -164,9 +197,11 @@ __device__ __forceinline__ bool fix_solution(const Params& P, double* u) {
 	double adv = smax(smin(u[ADV] / u[DEN], 1.0), 0.0);
 	double v[3] = {0, 0, 0};
 	double den = smax(u[DEN], P.dfloor);
-	for (int dim = 0; dim < P.nd; ++dim) v[dim] = u[VEL + dim] / u[DEN];
+	#pragma unroll
+	for (int dim = 0; dim < 3; ++dim) if (dim < P.nd) v[dim] = u[VEL + dim] / u[DEN];
 	double ke = 0.0;
-	for (int dim = 0; dim < P.nd; ++dim) ke += v[dim] * v[dim];
+	#pragma unroll
+	for (int dim = 0; dim < 3; ++dim) if (dim < P.nd) ke += v[dim] * v[dim];
 	ke *= 0.5 * u[DEN];
 	double pre = (u[PRE] - ke) * (P.gamma - 1.0);
 	ke *= den / u[DEN];
@@ -178,7 +213,8 @@ __device__ __forceinline__ bool fix_solution(const Params& P, double* u) {
 	u[PRE] = pre / (P.gamma - 1.0) + ke;
 	u[HII] = hii * den;
 	u[ADV] = adv * den;
-	for (int dim = 0; dim < P.nd; ++dim) u[VEL + dim] = den * v[dim];
+	#pragma unroll
+	for (int dim = 0; dim < 3; ++dim) if (dim < P.nd) u[VEL + dim] = den * v[dim];
 	if (u[DEN] == 0 || u[PRE] == 0) return false;
 	for (int f = 0; f < NU; ++f)
 		if (u[f] != u[f] || isinf(u[f])) return false;
@@ -207,9 +243,34 @@ __device__ __forceinline__ double spline_eval(const Spline& s, double x) {
 		else if (x < s.x[0]) return s.y[0] + s.min_slope * (x - s.x[0]);
 		return splint(s, x);
 	}
-	if (x > s.x[n - 1]) return s.y[n - 1] * trg_pow(x / s.x[n - 1], s.max_slope);
-	else if (x < s.x[0]) return s.y[0] * trg_pow(x / s.x[0], s.min_slope);
+	if (x > s.x[n - 1]) return s.y[n - 1] * d_pow(x / s.x[n - 1], s.max_slope);
+	else if (x < s.x[0]) return s.y[0] * d_pow(x / s.x[0], s.min_slope);
 	return splint(s, x);
+}
+
+// Diagnostic counters: one atomic per warp (the lanes that reach the call
+// together), so that enabling them costs little next to the solves they count.
+__device__ __forceinline__ void stat_add(unsigned long long* st, int idx, unsigned v) {
+	unsigned m = __activemask();
+	unsigned s = __reduce_add_sync(m, v);
+	if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && s) atomicAdd(st + idx, (unsigned long long)s);
+}
+__device__ __forceinline__ void stat_max(unsigned long long* st, int idx, unsigned v) {
+	unsigned m = __activemask();
+	unsigned s = __reduce_max_sync(m, v);
+	if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && s) atomicMax(st + idx, (unsigned long long)s);
+}
+// Picard iteration histogram bin: 1, 2, 3-4, 5-8, 9-16, 17-64, 65-1024, >1024
+__device__ __forceinline__ int iter_bin(unsigned it) {
+	return it <= 1 ? 0 : it <= 2 ? 1 : it <= 4 ? 2 : it <= 8 ? 3 : it <= 16 ? 4 : it <= 64 ? 5 : it <= 1024 ? 6 : 7;
+}
+__device__ __forceinline__ void stat_picard(unsigned long long* st, unsigned iters) {
+	stat_add(st, TRG_STAT_PICARD_CELLS, iters > 0);
+	stat_add(st, TRG_STAT_PICARD_ITERS, iters);
+	stat_max(st, TRG_STAT_PICARD_MAX, iters);
+	int b = iter_bin(iters);
+#pragma unroll
+	for (int k = 0; k < 8; ++k) stat_add(st, TRG_STAT_PICARD_HIST + k, iters > 0 && b == k);
 }
 
 }  // namespace trg

@@ -3,24 +3,34 @@
 #pragma once
 #include "trg_device.cuh"
 
+// kernels_fp64.cu, built twice: exact (plain-FP64 form, rounds like the
+// reference) and fast (FP32 form; FMA and CUDA libm)
+#define TRG_FP64_KERNELS \
+	__global__ void k_faces_fp64(Params P, State S, int dim); \
+	__global__ void k_hydro_update_fp64(Params P, State S, double h, const double* Ubase, double* Uout, int mode); \
+	__global__ void k_q_from_u_fp64(Params P, State S, const double* Usrc, int fix); \
+	__global__ void k_advance_fp64(Params P, State S, double dt); \
+	__global__ void k_rad_wind_reset(Params P, State S, const int* cells, int count); \
+	__global__ void k_rad_shell_fp64(Params P, State S, const int* cells, int count, double h, const double* hii_start); \
+	__global__ void k_rad_no_star_fp64(Params P, State S, double h); \
+	__global__ void k_rad_heating_fp64(Params P, State S); \
+	__global__ void k_rad_update_fp64(Params P, State S, double h, int mode); \
+	__global__ void k_colden_shell_fp64(Params P, State S, const int* cells, int count); \
+	__global__ void k_thermo_rates_fp64(Params P, State S); \
+	__global__ void k_thermo_integrate_fp64(Params P, State S, double h); \
+	__global__ void k_thermo_update_fp64(Params P, State S, double h, int mode); \
+	__global__ void k_dt_reduce_fp64(Params P, State S, long long first_cell); \
+	__global__ void k_dt_finalize(Params P, State S, double dt_next, int first_time, int step); \
+	__global__ void k_time_advance(State S); \
+	__global__ void k_dt_reset(Params P, State S);
+
 namespace trg {
-__global__ void k_faces_fp64(Params P, State S, int dim);
-__global__ void k_hydro_update_fp64(Params P, State S, double h, const double* Ubase, double* Uout, int mode);
-__global__ void k_q_from_u_fp64(Params P, State S, const double* Usrc, int fix);
-__global__ void k_advance_fp64(Params P, State S, double dt);
-__global__ void k_rad_wind_reset(Params P, State S, const int* cells, int count);
-__global__ void k_rad_shell_fp64(Params P, State S, const int* cells, int count, double h, const double* hii_start);
-__global__ void k_rad_no_star_fp64(Params P, State S, double h);
-__global__ void k_rad_heating_fp64(Params P, State S);
-__global__ void k_rad_update_fp64(Params P, State S, double h, int mode);
-__global__ void k_colden_shell_fp64(Params P, State S, const int* cells, int count);
-__global__ void k_thermo_rates_fp64(Params P, State S);
-__global__ void k_thermo_integrate_fp64(Params P, State S, double h);
-__global__ void k_thermo_update_fp64(Params P, State S, double h, int mode);
-__global__ void k_dt_reduce_fp64(Params P, State S, long long first_cell);
-__global__ void k_dt_finalize(Params P, State S, double dt_next, int first_time, int step);
-__global__ void k_time_advance(State S);
-__global__ void k_dt_reset(Params P, State S);
+namespace exact {
+TRG_FP64_KERNELS
+}
+namespace fast {
+TRG_FP64_KERNELS
+}
 // FP32 form of the hydro pass (kernels_fp32.cu)
 void launch_hydro_stage_fp32(int stage, const Params& P, const State& S, const float* Uq, const float* Ubase,
                              float* Uout, int zchunk, cudaStream_t stream);

@@ -58,6 +58,8 @@ struct Params {
 	// (density rho0, pressure / energy density p0, velocity v0 = sqrt(p0/rho0)),
 	// so that FP32 holds it far from its range limits whatever the code units.
 	double f32_rho0, f32_p0, f32_v0;
+	// diagnostic counters (State::stats) are updated only when this is set
+	int stats_on;
 };
 
 // Device pointers of one context (FP64 state).
@@ -79,6 +81,8 @@ struct State {
 	// scalars: [0] dt, [1] time, [2..4] per-component dt minima (as uint64 bits)
 	double* scal;
 	double* dt_hist;
+	// diagnostic counters, TRG_STAT_* indices of the C ABI header
+	unsigned long long* stats;
 };
 
 }  // namespace trg
