@@ -51,6 +51,7 @@ extern "C" {
 #define TRG_ERR_DT 5           /* invalid radiation time step */
 #define TRG_ERR_FLUX 6         /* Riemann solver produced a NaN HII flux */
 #define TRG_ERR_OOM 7          /* device allocation failed */
+#define TRG_ERR_TC 8           /* a tensor-core (tcgen05) wait expired */
 
 #define TRG_PRECISION_FP64 0   /* every kernel in FP64, reference operation order, no FMA */
 #define TRG_PRECISION_FP32 1   /* hydro in FP32 (compensated E - KE), FP64 for ionisation, dt, sums */
@@ -147,15 +148,68 @@ enum {
 	TRG_STAT_PICARD_MAX = 2,   /* most iterations in one cell */
 	TRG_STAT_PICARD_HIST = 3,  /* 8 bins: 1, 2, 3-4, 5-8, 9-16, 17-64, 65-1024, >1024 iterations */
 	TRG_STAT_LEARNED_CELLS = 11,    /* cells that started from the learned iterate */
-	TRG_STAT_LEARNED_ACCEPTED = 12, /* ... and converged within the first iteration */
-	TRG_STAT_LEARNED_ITERS = 13,    /* Picard iterations of the learned-start cells, fallbacks included */
+	TRG_STAT_LEARNED_ACCEPTED = 12, /* ... whose first iteration met the convergence test */
+	TRG_STAT_LEARNED_ITERS = 13,    /* Picard iterations of the learned-start cells */
 	TRG_STAT_THERMO_CELLS = 14,     /* cells that subcycled */
 	TRG_STAT_THERMO_SUBCYCLES = 15, /* subcycles, summed over cells */
 	TRG_STAT_THERMO_MAX = 16,       /* most subcycles in one cell */
-	TRG_STAT_SWEEPS = 17            /* radiation sweeps counted */
+	TRG_STAT_SWEEPS = 17,           /* radiation sweeps counted */
+	TRG_STAT_FRONT_CELLS = 18,      /* front cells (tau < 20, x_HII < 0.99): the learned start's domain */
+	TRG_STAT_FRONT_ITERS = 19       /* Picard iterations of the front cells */
 };
 int trg_stats_enable(trg_ctx* c, int on);
 int trg_stats(trg_ctx* c, unsigned long long* out, int reset);
+
+/* Learned starting iterate of the implicit ionisation solve (no counterpart
+ * in the reference, whose update_HIIfrac, src/Radiation/Radiation.cpp:375-478,
+ * always starts from the cell's current x_HII).
+ *
+ * Model: a 5 -> 64 -> 64 -> 3 perceptron with ReLU hidden layers, BF16
+ * weights and activations and FP32 accumulation on the tensor cores
+ * (tcgen05).  Inputs: log10 n_H, log10 T, x_HII, log10 of the optically thin
+ * photoionisation rate (photon rate e^-tau sigma ds / shell volume), log10 dt.
+ * Outputs: the change of logit10 from the start-of-step x_HII to the
+ * converged time-averaged fraction <x> and to the end-of-step x, and log2 of
+ * the plain solve's iteration count (logit10 p = log10(p / (1 - p)), p
+ * clipped to [1e-9, 1 - 1e-9]).  Parameters
+ * are a flat float vector of TRG_MLP_NPARAMS values: W1[5][64] b1[64]
+ * W2[64][64] b2[64] W3[64][3] b3[3], then the input mean[5] and 1/std[5] and
+ * the output mean[3] and 1/std[3] of the normalisation (x - mean) * scale.
+ *
+ * Training set records are 8 floats: the 5 inputs then the 3 targets, as the
+ * plain solve records them with trg_harvest.  trg_mlp_train sets the
+ * normalisation from the training set, then runs `epochs` passes of Adam
+ * (beta 0.9/0.999, eps 1e-8) over seeded shuffles in batches of `batch`, on
+ * the weighted squared error with per-output weights out_weight[3];
+ * loss_history[e] = mean weighted squared error of epoch e (may be null).
+ * trg_mlp_gradient returns the summed gradient and loss of one pass over the
+ * records without updating, for gradient checks.
+ *
+ * trg_learned_start(ctx, m) makes ctx's radiation sweeps start the Picard
+ * iteration of the front cells (tau < 20, x_HII < 0.99) that m predicts to
+ * need more than two plain iterations from m's predicted <x>: the prediction
+ * is accepted when the first iteration from it passes the solver's own
+ * convergence test (its residual is below the solver tolerance), else the
+ * plain iteration restarts from x_HII.  m = NULL restores the plain solve.  m must live on ctx's device; its parameters are
+ * copied, so later training does not change ctx until the next call.
+ * trg_harvest(ctx, capacity) makes the plain solve record front cells (at
+ * most `capacity` records; 0 stops and frees); trg_harvest_read copies up to
+ * `max` records out and returns how many were recorded in total. */
+#define TRG_MLP_NPARAMS 4755
+#define TRG_MLP_NTRAIN 4739
+typedef struct trg_mlp trg_mlp;
+int trg_mlp_create(const float* params, int device, trg_mlp** out);
+int trg_mlp_get_params(trg_mlp* m, float* params);
+int trg_mlp_set_params(trg_mlp* m, const float* params);
+int trg_mlp_forward(trg_mlp* m, const float* x, long n, float* y);
+int trg_mlp_gradient(trg_mlp* m, const float* records, long n, const float* out_weight, float* grad, double* loss);
+int trg_mlp_train(trg_mlp* m, const float* records, long n, int epochs, int batch, float lr, unsigned seed,
+                  const float* out_weight, float* loss_history);
+const char* trg_mlp_last_error(const trg_mlp* m);
+void trg_mlp_destroy(trg_mlp* m);
+int trg_learned_start(trg_ctx* c, const trg_mlp* m);
+int trg_harvest(trg_ctx* c, long capacity);
+long trg_harvest_read(trg_ctx* c, float* out, long max);
 const char* trg_last_error(const trg_ctx* c);
 void trg_destroy(trg_ctx* c);
 

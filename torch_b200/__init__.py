@@ -96,6 +96,19 @@ _SIGNATURES = [
     ("trg_profile_enable", C.c_int, [C.c_void_p, C.c_int]),
     ("trg_profile_read", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
     ("trg_stats_enable", C.c_int, [C.c_void_p, C.c_int]),
+    ("trg_mlp_create", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    ("trg_mlp_get_params", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("trg_mlp_set_params", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("trg_mlp_forward", C.c_int, [C.c_void_p, C.c_void_p, C.c_long, C.c_void_p]),
+    ("trg_mlp_gradient", C.c_int, [C.c_void_p, C.c_void_p, C.c_long, C.c_void_p, C.c_void_p,
+                                   C.POINTER(C.c_double)]),
+    ("trg_mlp_train", C.c_int, [C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_int, C.c_float, C.c_uint,
+                                C.c_void_p, C.c_void_p]),
+    ("trg_mlp_last_error", C.c_char_p, [C.c_void_p]),
+    ("trg_mlp_destroy", None, [C.c_void_p]),
+    ("trg_learned_start", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("trg_harvest", C.c_int, [C.c_void_p, C.c_long]),
+    ("trg_harvest_read", C.c_long, [C.c_void_p, C.c_void_p, C.c_long]),
     ("trg_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong), C.c_int]),
     ("trg_hydro_step_fp32_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
 ]
@@ -170,6 +183,89 @@ class State:
     dts: np.ndarray
 
 
+MLP_NPARAMS = 4755
+MLP_NTRAIN = 4739
+MLP_IN, MLP_HID, MLP_OUT = 5, 64, 3
+
+
+def mlp_init_params(seed: int = 0) -> np.ndarray:
+    """He-initialised parameter vector (biases zero, identity normalisation)."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(MLP_NPARAMS, dtype=np.float32)
+    o = 0
+    for fan_in, fan_out in ((MLP_IN, MLP_HID), (MLP_HID, MLP_HID), (MLP_HID, MLP_OUT)):
+        p[o:o + fan_in * fan_out] = rng.normal(0.0, np.sqrt(2.0 / fan_in), fan_in * fan_out)
+        o += fan_in * fan_out + fan_out
+    p[MLP_NTRAIN + 5:MLP_NTRAIN + 10] = 1.0   # input scale
+    p[MLP_NTRAIN + 13:MLP_NTRAIN + 16] = 1.0  # output scale
+    return p
+
+
+class Mlp:
+    """The learned starting iterate's network on one GPU (trg_mlp_*)."""
+
+    def __init__(self, params=None, device: int = 0, seed: int = 0):
+        self.lib = load_library()
+        p = np.ascontiguousarray(mlp_init_params(seed) if params is None else params, dtype=np.float32)
+        if p.size != MLP_NPARAMS:
+            raise ValueError(f"expected {MLP_NPARAMS} parameters")
+        h = C.c_void_p()
+        rc = self.lib.trg_mlp_create(p.ctypes.data_as(C.c_void_p), int(device), C.byref(h))
+        if rc != 0:
+            raise TrgError(rc, "trg_mlp_create failed")
+        self.handle = h.value
+
+    def _check(self, rc):
+        if rc != 0:
+            raise TrgError(rc, self.lib.trg_mlp_last_error(self.handle).decode())
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(MLP_NPARAMS, dtype=np.float32)
+        self._check(self.lib.trg_mlp_get_params(self.handle, p.ctypes.data_as(C.c_void_p)))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self._check(self.lib.trg_mlp_set_params(self.handle, p.ctypes.data_as(C.c_void_p)))
+
+    def forward(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, MLP_IN)
+        y = np.zeros((x.shape[0], MLP_OUT), dtype=np.float32)
+        self._check(self.lib.trg_mlp_forward(self.handle, x.ctypes.data_as(C.c_void_p), x.shape[0],
+                                             y.ctypes.data_as(C.c_void_p)))
+        return y
+
+    def gradient(self, records, out_weight=(1.0, 1.0, 1.0)):
+        r = np.ascontiguousarray(records, dtype=np.float32).reshape(-1, 8)
+        w = np.ascontiguousarray(out_weight, dtype=np.float32)
+        g = np.zeros(MLP_NTRAIN, dtype=np.float32)
+        loss = C.c_double(0)
+        self._check(self.lib.trg_mlp_gradient(self.handle, r.ctypes.data_as(C.c_void_p), r.shape[0],
+                                              w.ctypes.data_as(C.c_void_p), g.ctypes.data_as(C.c_void_p),
+                                              C.byref(loss)))
+        return g, loss.value
+
+    def train(self, records, epochs=10, batch=4096, lr=1e-3, seed=0, out_weight=(1.0, 0.25, 0.1)):
+        r = np.ascontiguousarray(records, dtype=np.float32).reshape(-1, 8)
+        w = np.ascontiguousarray(out_weight, dtype=np.float32)
+        hist = np.zeros(max(epochs, 1), dtype=np.float32)
+        self._check(self.lib.trg_mlp_train(self.handle, r.ctypes.data_as(C.c_void_p), r.shape[0], int(epochs),
+                                           int(batch), float(lr), int(seed), w.ctypes.data_as(C.c_void_p),
+                                           hist.ctypes.data_as(C.c_void_p)))
+        return hist[:epochs]
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.trg_mlp_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Torch:
     """One run on one GPU: ``Torch::initialise`` then ``full_step`` calls.
 
@@ -238,6 +334,27 @@ class Torch:
         self._check(self.lib.trg_profile_read(self.ctx, name.encode(), C.byref(ms), C.byref(n)))
         return ms.value, n.value
 
+    def learned_start(self, mlp):
+        """Start the front cells' ionisation solve from `mlp` (an Mlp), or plain with None."""
+        self._check(self.lib.trg_learned_start(self.ctx, mlp.handle if mlp is not None else None))
+
+    def harvest(self, capacity: int):
+        """Record up to `capacity` front-cell training records from the plain solve (0 stops)."""
+        self._check(self.lib.trg_harvest(self.ctx, int(capacity)))
+
+    def harvest_read(self, max_records: int = 1 << 26):
+        """(records [k x 8] float32, total recorded) of the current harvest."""
+        n = int(self.lib.trg_harvest_read(self.ctx, None, 0))
+        if n < 0:
+            raise TrgError(-n, "trg_harvest_read failed")
+        k = min(n, int(max_records))
+        out = np.zeros((k, 8), dtype=np.float32)
+        if k:
+            got = int(self.lib.trg_harvest_read(self.ctx, out.ctypes.data_as(C.c_void_p), k))
+            if got < 0:
+                raise TrgError(-got, "trg_harvest_read failed")
+        return out, n
+
     def stats_enable(self, on: bool):
         self._check(self.lib.trg_stats_enable(self.ctx, int(on)))
 
@@ -249,7 +366,8 @@ class Torch:
         return {"picard_cells": v[0], "picard_iters": v[1], "picard_max": v[2],
                 "picard_hist": dict(zip(PICARD_BINS, v[3:11])),
                 "learned_cells": v[11], "learned_accepted": v[12], "learned_iters": v[13],
-                "thermo_cells": v[14], "thermo_subcycles": v[15], "thermo_max": v[16], "sweeps": v[17]}
+                "thermo_cells": v[14], "thermo_subcycles": v[15], "thermo_max": v[16], "sweeps": v[17],
+                "front_cells": v[18], "front_iters": v[19]}
 
     def component(self, comp: int, phase: int, dt: float = 0.0) -> float:
         out = C.c_double(0)

@@ -17,6 +17,7 @@
 #include "ctx_access.h"
 #include "setup.h"
 #include "trg_kernels.h"
+#include "tc_mlp.cuh"
 
 using namespace trg;
 
@@ -48,6 +49,7 @@ struct trg_ctx {
 	bool use_graphs = true;
 	float* U32 = nullptr;
 	float* U32s = nullptr;
+	unsigned char* mlp_img = nullptr;
 	int zchunk = 64;
 	std::vector<void*> allocs;
 	int first_time = 1;
@@ -197,14 +199,28 @@ void hydro_fluxes(trg_ctx* c) {
 	for (int d = 0; d < c->P.nd; ++d) LAUNCH(KF(k_faces_fp64), c->S.nfaces[d], 128, c->P, c->S, d);
 }
 
+// One shell of the radiation sweep: the plain kernel, or with a network
+// loaded the learned-start kernel (its tensor-core tile needs dynamic shared
+// memory and 64 TMEM columns per CTA).
+void rad_shell_launch(trg_ctx* c, const int* cells, int count, double h) {
+	if (c->S.mlp_img) {
+		cudaEvent_t ea = nullptr, eb = nullptr;
+		if (c->profiling) { ea = pool_event(c); eb = pool_event(c); cudaEventRecord(ea, c->stream); }
+		KF(k_rad_shell_learned)<<<grid_for(count, 128), 128, mlp::INFER_SMEM, c->stream>>>(c->P, c->S, cells, count, h);
+		if (c->profiling) { cudaEventRecord(eb, c->stream); c->recs.push_back({"k_rad_shell_learned", ea, eb}); }
+		c->launches++;
+		return;
+	}
+	LAUNCH(KF(k_rad_shell_fp64), count, 128, c->P, c->S, cells, count, h);
+}
+
 void rad_sweep_direct(trg_ctx* c, double h) {
 	int nw = (int)c->hs.wind_cells.size();
 	LAUNCH(KF(k_rad_wind_reset), nw, 128, c->P, c->S, c->d_wind, nw);
 	const auto& off = c->hs.off_nonwind;
 	for (size_t s = 0; s + 1 < off.size(); ++s) {
 		int count = (int)(off[s + 1] - off[s]);
-		LAUNCH(KF(k_rad_shell_fp64), count, 128, c->P, c->S, c->d_sweep_nonwind + off[s], count, h,
-		       (const double*)nullptr);
+		rad_shell_launch(c, c->d_sweep_nonwind + off[s], count, h);
 	}
 }
 
@@ -224,8 +240,7 @@ void rad_integrate(trg_ctx* c, double h) {
 		const auto& off = c->hs.off_nonwind;
 		for (size_t s = 0; s + 1 < off.size(); ++s) {
 			int count = (int)(off[s + 1] - off[s]);
-			LAUNCH(KF(k_rad_shell_fp64), count, 128, c->P, c->S, c->d_sweep_nonwind + off[s], count, h,
-			       (const double*)nullptr);
+			rad_shell_launch(c, c->d_sweep_nonwind + off[s], count, h);
 		}
 	} else {
 		LAUNCH(KF(k_rad_no_star_fp64), c->P.N, 256, c->P, c->S, h);
@@ -349,6 +364,7 @@ int check_device_error(trg_ctx* c) {
 	if (e & ERRB_FLUX) return set_error(c, TRG_ERR_FLUX, "Riemann solver: HII flux is NaN");
 	if (e & ERRB_PICARD) return set_error(c, TRG_ERR_PICARD, "update_HIIfrac: implicit method not converging");
 	if (e & ERRB_DT) return set_error(c, TRG_ERR_DT, "Radiation::calculateTimeStep: invalid timestep");
+	if (e & ERRB_TC) return set_error(c, TRG_ERR_TC, "learned start: tensor-core wait expired");
 	return TRG_OK;
 }
 
@@ -667,6 +683,57 @@ int trg_stats(trg_ctx* c, unsigned long long* out, int reset) {
 	return TRG_OK;
 }
 
+int trg_learned_start(trg_ctx* c, const trg_mlp* m) {
+	if (!c) return TRG_ERR_ARG;
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	if (!m) {
+		c->S.mlp_img = nullptr;
+		drop_graphs(c);
+		return TRG_OK;
+	}
+	int dev = -1;
+	const unsigned char* src = mlp_device_image(m, &dev);
+	if (dev != c->raw.device) return set_error(c, TRG_ERR_ARG, "trg_learned_start: network on another device");
+	if (!c->mlp_img && dalloc(c, &c->mlp_img, mlp::IMG_INFER_BYTES)) return TRG_ERR_OOM;
+	CUDA_TRY(cudaMemcpy(c->mlp_img, src, mlp::IMG_INFER_BYTES, cudaMemcpyDeviceToDevice));
+	c->S.mlp_img = c->mlp_img;
+	drop_graphs(c);
+	return TRG_OK;
+}
+
+int trg_harvest(trg_ctx* c, long capacity) {
+	if (!c || capacity < 0) return TRG_ERR_ARG;
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	if (c->S.harvest) {
+		cudaFree(c->S.harvest);
+		cudaFree(c->S.harvest_n);
+	}
+	c->S.harvest = nullptr;
+	c->S.harvest_n = nullptr;
+	c->S.harvest_cap = 0;
+	if (capacity > 0) {
+		CUDA_TRY(cudaMalloc(&c->S.harvest, (size_t)capacity * 8 * sizeof(float)));
+		CUDA_TRY(cudaMalloc(&c->S.harvest_n, sizeof(unsigned long long)));
+		CUDA_TRY(cudaMemset(c->S.harvest_n, 0, sizeof(unsigned long long)));
+		c->S.harvest_cap = capacity;
+	}
+	drop_graphs(c);
+	return TRG_OK;
+}
+
+long trg_harvest_read(trg_ctx* c, float* out, long max) {
+	if (!c || !c->S.harvest) return 0;
+	if (cudaStreamSynchronize(c->stream) != cudaSuccess) return -TRG_ERR_CUDA;
+	unsigned long long n = 0;
+	if (cudaMemcpy(&n, c->S.harvest_n, sizeof(n), cudaMemcpyDeviceToHost) != cudaSuccess) return -TRG_ERR_CUDA;
+	long avail = (long)std::min<unsigned long long>(n, (unsigned long long)c->S.harvest_cap);
+	long k = std::min(avail, max);
+	if (out && k > 0 &&
+	    cudaMemcpy(out, c->S.harvest, (size_t)k * 8 * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+		return -TRG_ERR_CUDA;
+	return (long)n;
+}
+
 long long trg_kernel_launches(const trg_ctx* c) { return c ? c->launches : 0; }
 const char* trg_last_error(const trg_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
@@ -676,6 +743,8 @@ void trg_destroy(trg_ctx* c) {
 	profile_collect(c);
 	for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
 	drop_graphs(c);
+	if (c->S.harvest) cudaFree(c->S.harvest);
+	if (c->S.harvest_n) cudaFree(c->S.harvest_n);
 	for (void* p : c->allocs) cudaFree(p);
 	if (c->stream) cudaStreamDestroy(c->stream);
 	delete c;

@@ -14,6 +14,7 @@
 // (Grid::applyBCs, Grid.cpp:649-836, restated by map_ghost below).
 #include "trg_device.cuh"
 #include "trg_kernels.h"
+#include "tc_mlp.cuh"
 
 #ifndef TRG_KNS
 #define TRG_KNS exact
@@ -536,50 +537,115 @@ __global__ void k_rad_wind_reset(Params P, State S, const int* __restrict__ cell
 	FLD(S.R, R_HII_A, id) = 1;
 }
 
+// Learned starting iterate: cells whose solve may take more than one Picard
+// iteration (the ionisation front: optically thin enough to be reached,
+// not yet ionised) are the ones the network serves and the plain solver
+// records for its training set.
+__device__ __forceinline__ bool front_cell(double tau_avg, double q_hii) { return tau_avg < 20.0 && q_hii < 0.99; }
+
+// Network inputs of a cell (before its solve): log10 n_H, log10 T, x_HII,
+// log10 of the optically thin photoionisation rate photonRate e^-tau sigma
+// ds / shellVol, and log10 dt.
+__device__ __forceinline__ void learned_features(const Params& P, double n_H, double T, double q_hii, double tau_avg,
+                                                 double ds, double shellVol, double dt, float* f) {
+	f[0] = (float)log10(n_H);
+	f[1] = (float)log10(T);
+	f[2] = (float)q_hii;
+	f[3] = shellVol > 0 ? (float)(log10(P.photonRate * P.photoIonXsec * ds / shellVol) - 0.4342944819032518 * tau_avg)
+	                    : -30.0f;
+	f[4] = (float)log10(dt);
+}
+
+// log10(p / (1 - p)) with p clipped to [1e-9, 1 - 1e-9], and its inverse.
+__device__ __forceinline__ float logit10(double p) {
+	double q = fmin(fmax(p, 1e-9), 1.0 - 1e-9);
+	return (float)log10(q / (1.0 - q));
+}
+__device__ __forceinline__ double inv_logit10(float l) {
+	double v = fmin(fmax((double)l, -9.0), 9.0);
+	return 1.0 / (1.0 + exp10(-v));
+}
+
 // One shell of the causal sweep of Radiation::transferRadiation
 // (Radiation.cpp:600-612): tau interpolation, the implicit HII update
 // (update_HIIfrac, :375-478) and the new optical depths.  Every cell of a
 // shell reads only cells of inner shells, so a shell is fully parallel.
-__global__ void __launch_bounds__(128) k_rad_shell_fp64(Params P, State S, const int* __restrict__ cells, int count,
-                                                       double h, const double* __restrict__ hii_start) {
-	int t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t >= count) return;
-	long long id = cells[t];
-	int ijk[3];
-	double xc[3];
-	cell_ijk(P, id, ijk);
-	cell_xc(P, ijk, xc);
-	double dist2 = dist2_cells(P, xc);
-	if (dist2 > 0.95) {
-		long long nb[4];
-		double w[4];
-		neighbours(P, ijk, xc, nb, w);
-		FLD(S.R, R_TAU, id) = tau_sc(P, S, nb, w, R_TAU, R_DTAU);
-		FLD(S.R, R_TAU_A, id) = tau_sc(P, S, nb, w, R_TAU_A, R_DTAU_A);
-	} else {
-		FLD(S.R, R_TAU, id) = 0;
-		FLD(S.R, R_TAU_A, id) = 0;
-	}
+//
+// LEARNED: CTAs that hold a front cell run the tensor-core network on their
+// 128 cells (dynamic shared memory mlp::INFER_SMEM, TMEM 64 columns) and start
+// the front cells' Picard iteration from the predicted time-averaged
+// fraction.  The prediction is accepted when the first iteration from it
+// meets the solver's own convergence test (its residual is below the solver
+// tolerance); otherwise the cell restarts the plain iteration from x_HII, so
+// that a rejected prediction leaves the plain result unchanged.
+template <bool LEARNED>
+__device__ __forceinline__ void rad_shell(const Params& P, const State& S, const int* __restrict__ cells, int count,
+                                          double h) {
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	const bool valid = t < count;
+	if (!LEARNED && !valid) return;
+	const long long id = valid ? cells[t] : 0;
 	const double dt = h * S.scal[0];
-	// Radiation::isStar (Radiation.cpp:682-684): z compares an int with a double.
-	bool star = (int)xc[0] == (int)P.sxc[0] && (int)xc[1] == (int)P.sxc[1] && (double)(int)xc[2] == P.sxc[2];
-	double q_den = FLD(S.Q, DEN, id), q_pre = FLD(S.Q, PRE, id), q_hii = FLD(S.Q, HII, id);
-	double ds = S.ds[id];
+	bool star = false, front = false;
+	double q_den = 0, q_pre = 0, q_hii = 0, ds = 0, n_H = 0, T = 1, alphaB = 0, A_ci = 0, tau_avg = 0, shellVol = 0;
+	if (valid) {
+		int ijk[3];
+		double xc[3];
+		cell_ijk(P, id, ijk);
+		cell_xc(P, ijk, xc);
+		double dist2 = dist2_cells(P, xc);
+		if (dist2 > 0.95) {
+			long long nb[4];
+			double w[4];
+			neighbours(P, ijk, xc, nb, w);
+			FLD(S.R, R_TAU, id) = tau_sc(P, S, nb, w, R_TAU, R_DTAU);
+			FLD(S.R, R_TAU_A, id) = tau_sc(P, S, nb, w, R_TAU_A, R_DTAU_A);
+		} else {
+			FLD(S.R, R_TAU, id) = 0;
+			FLD(S.R, R_TAU_A, id) = 0;
+		}
+		// Radiation::isStar (Radiation.cpp:682-684): z compares an int with a double.
+		star = (int)xc[0] == (int)P.sxc[0] && (int)xc[1] == (int)P.sxc[1] && (double)(int)xc[2] == P.sxc[2];
+		q_den = FLD(S.Q, DEN, id);
+		q_pre = FLD(S.Q, PRE, id);
+		q_hii = FLD(S.Q, HII, id);
+		ds = S.ds[id];
+		if (!star) {
+			n_H = P.X * q_den / P.hydrogenMass;
+			T = calc_temperature(P, q_hii, q_pre, q_den);
+			alphaB = spline_eval(S.tables->rad_recomb, T);
+			A_ci = collisional_ionisation_rate(P, T);
+			tau_avg = FLD(S.R, R_TAU_A, id);
+			shellVol = S.shellVol[id];
+			front = front_cell(tau_avg, q_hii);
+		}
+	}
+	double start = q_hii;
+	bool learned = false, used_learned = false;
+	if (LEARNED) {
+		if (__syncthreads_or(front)) {
+			extern __shared__ __align__(128) unsigned char sm_mlp[];
+			float f[5] = {0, 0, 0, 0, 0}, y[3];
+			if (front) learned_features(P, n_H, T, q_hii, tau_avg, ds, shellVol, dt, f);
+			if (!mlp::infer_tile(sm_mlp, reinterpret_cast<const uint4*>(S.mlp_img), f, y)) {
+				if (threadIdx.x == 0) atomicOr(S.err, ERRB_TC);
+			} else if (front && y[2] > 1.0f) {
+				// predicted to need more than two plain iterations: start from the prediction
+				start = inv_logit10(logit10(q_hii) + y[0]);
+				learned = used_learned = true;
+			}
+		}
+		if (!valid) return;
+	}
 	unsigned iters = 0;
 	if (star) {
 		FLD(S.R, R_HEAT, id) = 0;
 		FLD(S.Q, HII, id) = 1;
 		FLD(S.R, R_HII_A, id) = 1;
 	} else {
-		double n_H = P.X * q_den / P.hydrogenMass;
 		double A_pi = 0;
 		double x_new = q_hii;
-		double HII_avg = hii_start ? hii_start[id] : x_new;
-		double T = calc_temperature(P, q_hii, q_pre, q_den);
-		double alphaB = spline_eval(S.tables->rad_recomb, T);
-		double A_ci = collisional_ionisation_rate(P, T);
-		double tau_avg = FLD(S.R, R_TAU_A, id);
-		double shellVol = S.shellVol[id];
+		double HII_avg = start;
 		double HII_avg_old;
 		int niter = 0, miter = 0;
 		bool converged = false;
@@ -594,6 +660,20 @@ __global__ void __launch_bounds__(128) k_rad_shell_fp64(Params P, State S, const
 			double nHII_Aci = HII_avg * n_H * A_ci;
 			doric(dt, HII_avg, x_new, A_pi, nHII_aB, nHII_Aci);
 			if ((fabs((HII_avg - HII_avg_old) / HII_avg) < 1.0e-3 || (HII_avg < 1.0e-5) || A_pi == 0)) converged = true;
+			if (learned) {
+				// the first iteration from the prediction is its residual test:
+				// accept, or restart the plain iteration from x_HII
+				learned = false;
+				if (P.stats_on) {
+					stat_add(S.stats, TRG_STAT_LEARNED_CELLS, 1u);
+					stat_add(S.stats, TRG_STAT_LEARNED_ACCEPTED, converged ? 1u : 0u);
+				}
+				if (converged) break;
+				iters = 1;
+				HII_avg = q_hii;
+				niter = 0;
+				continue;
+			}
 			if (niter > 10005) {
 				miter++;
 				niter = 0;
@@ -607,12 +687,37 @@ __global__ void __launch_bounds__(128) k_rad_shell_fp64(Params P, State S, const
 		FLD(S.R, R_HII_A, id) = HII_avg;
 		FLD(S.Q, HII, id) = x_new;
 		if (x_new > 0.001) FLD(S.Q, ADV, id) = 1;
-		iters = (unsigned)miter * 10006u + (unsigned)niter;
+		iters += (unsigned)miter * 10006u + (unsigned)niter;
+		if (LEARNED && P.stats_on && used_learned) stat_add(S.stats, TRG_STAT_LEARNED_ITERS, iters);
+		if (!LEARNED && front && S.harvest) {
+			// training record: 5 inputs, then the converged <x>, x and the iteration count
+			unsigned long long slot = atomicAdd(S.harvest_n, 1ull);
+			if (slot < (unsigned long long)S.harvest_cap) {
+				float* r = S.harvest + slot * 8;
+				learned_features(P, n_H, T, q_hii, tau_avg, ds, shellVol, dt, r);
+				r[5] = logit10(HII_avg) - logit10(q_hii);
+				r[6] = logit10(x_new) - logit10(q_hii);
+				r[7] = log2f((float)iters);
+			}
+		}
 	}
 	double nH = P.X * q_den / P.hydrogenMass;
 	FLD(S.R, R_DTAU, id) = (1.0 - FLD(S.Q, HII, id)) * nH * P.photoIonXsec * ds;
 	FLD(S.R, R_DTAU_A, id) = (1.0 - FLD(S.R, R_HII_A, id)) * nH * P.photoIonXsec * ds;
-	if (P.stats_on) stat_picard(S.stats, iters);
+	if (P.stats_on) {
+		stat_picard(S.stats, iters);
+		stat_add(S.stats, TRG_STAT_FRONT_CELLS, front ? 1u : 0u);
+		stat_add(S.stats, TRG_STAT_FRONT_ITERS, front ? iters : 0u);
+	}
+}
+
+__global__ void __launch_bounds__(128) k_rad_shell_fp64(Params P, State S, const int* __restrict__ cells, int count,
+                                                       double h) {
+	rad_shell<false>(P, S, cells, count, h);
+}
+__global__ void __launch_bounds__(128) k_rad_shell_learned(Params P, State S, const int* __restrict__ cells, int count,
+                                                          double h) {
+	rad_shell<true>(P, S, cells, count, h);
 }
 
 // Star off: Radiation::transferRadiation else-branch (Radiation.cpp:638-650), interior cells.

@@ -11,7 +11,8 @@
 	__global__ void k_q_from_u_fp64(Params P, State S, const double* Usrc, int fix); \
 	__global__ void k_advance_fp64(Params P, State S, double dt); \
 	__global__ void k_rad_wind_reset(Params P, State S, const int* cells, int count); \
-	__global__ void k_rad_shell_fp64(Params P, State S, const int* cells, int count, double h, const double* hii_start); \
+	__global__ void k_rad_shell_fp64(Params P, State S, const int* cells, int count, double h); \
+	__global__ void k_rad_shell_learned(Params P, State S, const int* cells, int count, double h); \
 	__global__ void k_rad_no_star_fp64(Params P, State S, double h); \
 	__global__ void k_rad_heating_fp64(Params P, State S); \
 	__global__ void k_rad_update_fp64(Params P, State S, double h, int mode); \
@@ -38,5 +39,9 @@ size_t hydro_stage_fp32_smem();
 void launch_hydro_substep_fp32(const Params& P, const State& S, const double* U, double* Uout, double h, int zchunk,
                                cudaStream_t stream);
 __global__ void k_f64_to_f32(Params P, const double* a, float* b);
+}  // namespace trg
+// network image of a trained model (mlp.cu) and the device it lives on
+const unsigned char* mlp_device_image(const trg_mlp* m, int* device);
+namespace trg {
 __global__ void k_f32_to_f64(Params P, const float* a, double* b);
 }  // namespace trg

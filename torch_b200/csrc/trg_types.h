@@ -15,7 +15,7 @@ enum { RS_HLLC = 0, RS_ROTATED = 1, RS_HLL = 2 };
 
 // Device error word bits (host maps them to TRG_ERR_*).
 enum : unsigned {
-	ERRB_NAN = 1u, ERRB_PICARD = 2u, ERRB_DT = 4u, ERRB_FLUX = 8u,
+	ERRB_NAN = 1u, ERRB_PICARD = 2u, ERRB_DT = 4u, ERRB_FLUX = 8u, ERRB_TC = 16u,
 };
 
 // Cubic spline table (SplineData, src/Integrators/SplineData.cpp) built on the host.
@@ -83,6 +83,12 @@ struct State {
 	double* dt_hist;
 	// diagnostic counters, TRG_STAT_* indices of the C ABI header
 	unsigned long long* stats;
+	// learned starting iterate: the network's inference image (null = plain solve)
+	const unsigned char* mlp_img;
+	// training-set recording by the plain solve: records of 8 floats
+	float* harvest;
+	long long harvest_cap;
+	unsigned long long* harvest_n;
 };
 
 }  // namespace trg
