@@ -240,6 +240,7 @@ def time_form(args, precision, tp, ic, local, pg, profile_names, stream_mod):
     import torch
     import torch_b200
     sim = torch_b200.Torch(tp, ic, precision=precision, device=local)
+    sim.tile = sim.autotune()
     dt_next = sim.dt_max
     stream = torch.cuda.ExternalStream(sim.stream_handle(), device=f"cuda:{local}")
     sim.run_steps(args.warmup)  # the first step is the reference's dt_max*1e-20 start step
@@ -293,6 +294,80 @@ def form_error(sim_a, sim_b, gamma, nd):
     return {"den_rel_l1": rel(Ua[0], Ub[0]), "pre_rel_l1": rel(pressure(Ua), pressure(Ub))}
 
 
+def run_batch(args, world, rank, local, pg):
+    """Independent 2-D cylindrical HII-region grids of uneven sizes, FP64,
+    advanced one launch per stage for all grids; beside it the same grids
+    stepped one by one (`unbatched`, on a bounded sample of grids)."""
+    import torch
+    import torch_b200
+    from torch_b200 import workloads
+
+    cases = workloads.blister_batch(G=args.grids, seed=2024 + rank)
+    grids = [torch_b200.Torch(tp, ic) for tp, ic in cases]
+    cells = sum(g.N for g in grids)
+    dt_next = min(g.dt_max for g in grids)
+    b = torch_b200.Batch(grids)
+    stream = torch.cuda.ExternalStream(b.stream_handle(), device=f"cuda:{local}")
+    b.run_steps(args.warmup, dt_next)
+    launches0 = b.kernel_launches()
+    b.profile(True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(pg)
+    torch.cuda.synchronize(local)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    b.enqueue_steps(args.steps, dt_next)
+    ev1.record(stream)
+    b.synchronize()
+    torch.cuda.synchronize(local)
+    barrier(pg)
+    clk = clocks.stop()
+    ms = max_over_ranks(pg, ev0.elapsed_time(ev1), local)
+    launches = b.kernel_launches() - launches0
+    prof = {}
+    for name in PROFILE_NAMES:
+        tt, cc = b.profile_read(name)
+        if cc:
+            prof[name] = {"ms": tt, "launches": cc}
+    b.profile(False)
+    b.close()
+    for g in grids:
+        g.close()
+    # the same kind of grids stepped one context at a time (first 16 grids)
+    sample = cases[:min(16, len(cases))]
+    singles = [torch_b200.Torch(tp, ic) for tp, ic in sample]
+    for s in singles:
+        s.run_steps(args.warmup, dt_next)
+    torch.cuda.synchronize(local)
+    t0 = time.perf_counter()
+    for s in singles:
+        s.run_steps(args.steps, dt_next)
+    torch.cuda.synchronize(local)
+    wall = time.perf_counter() - t0
+    ucells = sum(s.N for s in singles)
+    for s in singles:
+        s.close()
+    value = cells * args.steps * world / (ms / 1e3)
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s batched grids", "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"batch of {args.grids} 2-D cylindrical HII-region grids", "cells": cells,
+                       "precision": "fp64", "parallelism": f"replicas x{world}",
+                       "sizes": "nx U[64,256], ny U[64,320], Q log-U[1e47,1e49], alpha U[0,2], rc U[0.005,0.05] pc",
+                       "l2": "inputs larger than L2 (no flush)"},
+            "gpu_launches": int(launches), "launches_per_step": launches / max(1, args.steps), "clocks": clk,
+            "kernels": prof,
+            "unbatched": {"value": ucells * args.steps / wall, "grids": len(sample),
+                          "note": "the first grids stepped one context after another, host wall clock"},
+            "roofline": None, "cpu_baseline": None, "e2e": None,
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_ours(args, world, rank, local, pg):
     import torch
     import torch_b200
@@ -315,6 +390,7 @@ def run_ours(args, world, rank, local, pg):
     ms_max, launches, prof = results[head]
     value = N * args.steps * world / (ms_max / 1e3)
     sim = sims[head]
+    sim_tile = getattr(sim, "tile", None)
     error = None
     if "fp64" in sims and head != "fp64":
         # both forms advanced W + K steps from the same initial state
@@ -397,7 +473,9 @@ def run_ours(args, world, rank, local, pg):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if head == "fp32" else "f64",
-            "data": "synthetic", "config": workload_config(args.workload, args.n, head, world),
+            "data": "synthetic",
+            "config": dict(workload_config(args.workload, args.n, head, world),
+                           autotuned_tile_z=getattr(sim_tile, "__getitem__", lambda i: None)(0)),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk, "kernels": kernel_share, "error_vs_fp64": error,
         }
@@ -412,7 +490,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["hii", "sedov"], default="hii")
+    ap.add_argument("--workload", choices=["hii", "sedov", "batch"], default="hii")
+    ap.add_argument("--grids", type=int, default=256, help="grids of the batch workload")
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--precision", choices=["both", "fp32", "fp64"], default="both")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -425,6 +504,8 @@ def main():
     try:
         if args.impl == "reference":
             return run_reference_arm(args, rank)
+        if args.workload == "batch":
+            return run_batch(args, world, rank, local, pg)
         return run_ours(args, world, rank, local, pg)
     finally:
         if pg is not None:

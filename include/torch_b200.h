@@ -157,6 +157,14 @@ enum {
 	TRG_STAT_FRONT_CELLS = 18,      /* front cells (tau < 20, x_HII < 0.99): the learned start's domain */
 	TRG_STAT_FRONT_ITERS = 19       /* Picard iterations of the front cells */
 };
+/* Tile autotuner (no counterpart in the reference): for the FP32 form, times
+ * the fused hydro stage kernel on this grid for a range of CTA tile depths
+ * (z planes marched by one CTA) and keeps the fastest; the trials write only
+ * scratch and leave the state and time step untouched.  zchunk_out / ms_out
+ * (may be NULL) receive the choice and its time per launch; the FP64 form has
+ * nothing to tune (0). */
+int trg_autotune(trg_ctx* c, int* zchunk_out, double* ms_out);
+
 int trg_stats_enable(trg_ctx* c, int on);
 int trg_stats(trg_ctx* c, unsigned long long* out, int reset);
 
@@ -212,6 +220,30 @@ int trg_harvest(trg_ctx* c, long capacity);
 long trg_harvest_read(trg_ctx* c, float* out, long max);
 const char* trg_last_error(const trg_ctx* c);
 void trg_destroy(trg_ctx* c);
+
+/* Batches (no counterpart in the reference, which runs one grid per job):
+ * many independent grids advance together, one kernel launch per stage for
+ * all of them (one per shell for the radiation and column-density sweeps).
+ * trg_batch_create takes up to 512 contexts made by trg_create in the FP64
+ * form on one device, not yet stepped, with the same physics flags, solver
+ * and integrator components (sizes, geometry of the star, photon rate and
+ * initial state may differ), each of at most 4194304 cells.  While the batch
+ * exists the grids are stepped only through it; their states are read with
+ * trg_get_state after trg_batch_synchronize.  trg_batch_destroy hands the
+ * step count back to the grids, which stay owned by the caller.  Every grid
+ * takes its own time step (the step's minimum with dt_next_checkpoint). */
+typedef struct trg_batch trg_batch;
+int trg_batch_create(trg_ctx* const* grids, int ngrids, trg_batch** out);
+int trg_batch_run_steps(trg_batch* b, int nsteps, double dt_next_checkpoint);
+int trg_batch_enqueue_steps(trg_batch* b, int nsteps, double dt_next_checkpoint);
+int trg_batch_synchronize(trg_batch* b);
+void* trg_batch_stream(const trg_batch* b);
+long long trg_batch_kernel_launches(const trg_batch* b);
+long long trg_batch_cells(const trg_batch* b);
+int trg_batch_profile_enable(trg_batch* b, int on);
+int trg_batch_profile_read(trg_batch* b, const char* name, double* total_ms, long long* launches);
+const char* trg_batch_last_error(const trg_batch* b);
+void trg_batch_destroy(trg_batch* b);
 
 /* No counterpart in the reference.  One FP32 RK2 hydro step - the two fused
  * stage kernels of the FP32 form - from U_in to U_out, both caller-owned

@@ -103,3 +103,21 @@ def test_fp32_form_radiation_hydro_config1():
     ed, ep, eE, a, b = errors(tp, ic, 30)
     print(f"config1 rad-hydro 30 steps: den {ed:.2e} pre {ep:.2e}")
     assert ed <= 1e-4 and ep <= 1e-3
+
+
+def test_autotune_keeps_results_bitwise():
+    """The tile autotuner's trials touch only scratch, and the tile depth it
+    picks does not change any cell's arithmetic."""
+    tp, ic = workloads.sedov(n=40)
+    a = torch_b200.Torch(tp, ic, precision=torch_b200.PRECISION_FP32)
+    a.run_steps(3)
+    z, ms = a.autotune()
+    assert z >= 1 and ms > 0
+    a.run_steps(7)
+    sa = a.state()
+    a.close()
+    b = torch_b200.Torch(tp, ic, precision=torch_b200.PRECISION_FP32)
+    b.run_steps(10)
+    sb = b.state()
+    b.close()
+    assert np.array_equal(sa.U, sb.U)

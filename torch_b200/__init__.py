@@ -96,6 +96,7 @@ _SIGNATURES = [
     ("trg_profile_enable", C.c_int, [C.c_void_p, C.c_int]),
     ("trg_profile_read", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
     ("trg_stats_enable", C.c_int, [C.c_void_p, C.c_int]),
+    ("trg_autotune", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     ("trg_mlp_create", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     ("trg_mlp_get_params", C.c_int, [C.c_void_p, C.c_void_p]),
     ("trg_mlp_set_params", C.c_int, [C.c_void_p, C.c_void_p]),
@@ -107,6 +108,17 @@ _SIGNATURES = [
     ("trg_mlp_last_error", C.c_char_p, [C.c_void_p]),
     ("trg_mlp_destroy", None, [C.c_void_p]),
     ("trg_learned_start", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("trg_batch_create", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    ("trg_batch_run_steps", C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    ("trg_batch_enqueue_steps", C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    ("trg_batch_synchronize", C.c_int, [C.c_void_p]),
+    ("trg_batch_stream", C.c_void_p, [C.c_void_p]),
+    ("trg_batch_kernel_launches", C.c_longlong, [C.c_void_p]),
+    ("trg_batch_cells", C.c_longlong, [C.c_void_p]),
+    ("trg_batch_profile_enable", C.c_int, [C.c_void_p, C.c_int]),
+    ("trg_batch_profile_read", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
+    ("trg_batch_last_error", C.c_char_p, [C.c_void_p]),
+    ("trg_batch_destroy", None, [C.c_void_p]),
     ("trg_harvest", C.c_int, [C.c_void_p, C.c_long]),
     ("trg_harvest_read", C.c_long, [C.c_void_p, C.c_void_p, C.c_long]),
     ("trg_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong), C.c_int]),
@@ -355,6 +367,13 @@ class Torch:
                 raise TrgError(-got, "trg_harvest_read failed")
         return out, n
 
+    def autotune(self):
+        """Tile depth of the FP32 hydro kernel chosen by timing; (zchunk, ms per launch)."""
+        z = C.c_int(0)
+        ms = C.c_double(0)
+        self._check(self.lib.trg_autotune(self.ctx, C.byref(z), C.byref(ms)))
+        return z.value, ms.value
+
     def stats_enable(self, on: bool):
         self._check(self.lib.trg_stats_enable(self.ctx, int(on)))
 
@@ -400,6 +419,66 @@ class Torch:
 
     def __exit__(self, *exc):
         self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Independent grids advanced together, one launch per stage (trg_batch_*).
+
+    `grids` are fresh FP64 ``Torch`` runs with the same physics flags; they
+    are stepped only through the batch while it exists, and their states are
+    read with their own ``state()`` after ``synchronize()``.
+    """
+
+    def __init__(self, grids):
+        self.lib = load_library()
+        self.grids = list(grids)
+        arr = (C.c_void_p * len(self.grids))(*[g.ctx for g in self.grids])
+        h = C.c_void_p()
+        rc = self.lib.trg_batch_create(arr, len(self.grids), C.byref(h))
+        if rc != 0:
+            msgs = [g.lib.trg_last_error(g.ctx).decode() for g in self.grids]
+            raise TrgError(rc, next((m for m in msgs if m), "trg_batch_create failed"))
+        self.handle = h.value
+        self.cells = int(self.lib.trg_batch_cells(self.handle))
+
+    def _check(self, rc):
+        if rc != 0:
+            raise TrgError(rc, self.lib.trg_batch_last_error(self.handle).decode())
+
+    def run_steps(self, nsteps: int, dt_next_checkpoint: float):
+        self._check(self.lib.trg_batch_run_steps(self.handle, int(nsteps), float(dt_next_checkpoint)))
+
+    def enqueue_steps(self, nsteps: int, dt_next_checkpoint: float):
+        self._check(self.lib.trg_batch_enqueue_steps(self.handle, int(nsteps), float(dt_next_checkpoint)))
+
+    def synchronize(self):
+        self._check(self.lib.trg_batch_synchronize(self.handle))
+
+    def stream_handle(self) -> int:
+        return int(self.lib.trg_batch_stream(self.handle) or 0)
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.trg_batch_kernel_launches(self.handle))
+
+    def profile(self, on: bool):
+        self._check(self.lib.trg_batch_profile_enable(self.handle, int(on)))
+
+    def profile_read(self, name: str):
+        ms = C.c_double(0)
+        n = C.c_longlong(0)
+        self._check(self.lib.trg_batch_profile_read(self.handle, name.encode(), C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.trg_batch_destroy(self.handle)
+            self.handle = None
 
     def __del__(self):
         try:

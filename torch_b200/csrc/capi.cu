@@ -7,6 +7,7 @@
 // steps needs no host round trip.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -47,6 +48,9 @@ struct trg_ctx {
 	cudaGraphExec_t g_rad[2] = {nullptr, nullptr};
 	long long g_colden_nodes = 0, g_rad_nodes[2] = {0, 0};
 	bool use_graphs = true;
+	// per-grid scalar kernels (dt, time) run on this many threads: 1, or the
+	// number of grids of a batch
+	int nscalar = 1;
 	float* U32 = nullptr;
 	float* U32s = nullptr;
 	unsigned char* mlp_img = nullptr;
@@ -135,7 +139,10 @@ void profile_collect(trg_ctx* c) {
 		}                                                                                    \
 	} while (0)
 
-void q_from_u(trg_ctx* c, const double* Usrc, int fix) { LAUNCH(KF(k_q_from_u_fp64), c->P.N, 256, c->P, c->S, Usrc, fix); }
+// sel: 0 = S.U, 1 = S.U1
+#define LAUNCH_SCALAR(kernel, ...) LAUNCH(kernel, c->nscalar, c->nscalar > 1 ? 64 : 1, __VA_ARGS__)
+
+void q_from_u(trg_ctx* c, int sel, int fix) { LAUNCH(KF(k_q_from_u_fp64), c->P.N, 256, c->P, c->S, sel, fix); }
 
 void colden_sweep_direct(trg_ctx* c) {
 	const auto& off = c->hs.off_all;
@@ -250,7 +257,7 @@ void rad_integrate(trg_ctx* c, double h) {
 void sub_step(trg_ctx* c, double h, bool hasCalculatedHeatFlux, int comp) {
 	// Torch::subStep, Torch.cpp:352-364
 	if (!hasCalculatedHeatFlux) {
-		q_from_u(c, c->S.U, 1);
+		q_from_u(c, 0, 1);
 		comp_pre(c, comp);
 	}
 	switch (comp) {
@@ -266,7 +273,7 @@ void sub_step(trg_ctx* c, double h, bool hasCalculatedHeatFlux, int comp) {
 			break;
 		}
 		hydro_fluxes(c);
-		LAUNCH(KF(k_hydro_update_fp64), c->P.N, 256, c->P, c->S, h, (const double*)c->S.U, c->S.U, 0);
+		LAUNCH(KF(k_hydro_update_fp64), c->P.N, 256, c->P, c->S, h, 0, 0, 0);
 		break;
 	case COMP_RAD:
 		rad_integrate(c, h);
@@ -283,17 +290,17 @@ void hydro_step(trg_ctx* c) {
 	// Torch::hydroStep (hasCalculatedHeatFlux = true), Torch.cpp:366-387: the
 	// saved state W is the untouched U; the predictor writes U1.
 	hydro_fluxes(c);
-	LAUNCH(KF(k_hydro_update_fp64), c->P.N, 256, c->P, c->S, 0.5, (const double*)c->S.U, c->S.U1, 0);
-	q_from_u(c, c->S.U1, 0);
+	LAUNCH(KF(k_hydro_update_fp64), c->P.N, 256, c->P, c->S, 0.5, 0, 1, 0);
+	q_from_u(c, 1, 0);
 	hydro_fluxes(c);
-	LAUNCH(KF(k_hydro_update_fp64), c->P.N, 256, c->P, c->S, 1.0, (const double*)c->S.U, c->S.U, 0);
+	LAUNCH(KF(k_hydro_update_fp64), c->P.N, 256, c->P, c->S, 1.0, 0, 0, 0);
 }
 
 void time_step(trg_ctx* c, double dt_next) {
 	// Torch::calculateTimeStep and the min with dt_next_checkpoint (Torch.cpp:304-339, :394)
 	int step = c->steps < c->dt_hist_cap ? (int)c->steps : -1;
 	if (c->first_time) {
-		LAUNCH(KF(k_dt_finalize), 1, 1, c->P, c->S, dt_next, 1, step);
+		LAUNCH_SCALAR(KF(k_dt_finalize), c->P, c->S, dt_next, 1, step);
 		c->first_time = 0;
 		return;
 	}
@@ -302,9 +309,9 @@ void time_step(trg_ctx* c, double dt_next) {
 		first_cell = c->hs.first_nonwind_cell;
 		c->rad_once_pending = 0;
 	}
-	LAUNCH(KF(k_dt_reset), 1, 1, c->P, c->S);
+	LAUNCH_SCALAR(KF(k_dt_reset), c->P, c->S);
 	LAUNCH(KF(k_dt_reduce_fp64), c->P.N, 256, c->P, c->S, first_cell);
-	LAUNCH(KF(k_dt_finalize), 1, 1, c->P, c->S, dt_next, 0, step);
+	LAUNCH_SCALAR(KF(k_dt_finalize), c->P, c->S, dt_next, 0, step);
 }
 
 void enqueue_full_step_fp32(trg_ctx* c, double dt_next) {
@@ -312,9 +319,9 @@ void enqueue_full_step_fp32(trg_ctx* c, double dt_next) {
 	// the previous corrector reduced (FP64), the two RK2 stages are one fused
 	// kernel each.
 	int step = c->steps < c->dt_hist_cap ? (int)c->steps : -1;
-	LAUNCH(KF(k_dt_finalize), 1, 1, c->P, c->S, dt_next, c->first_time, step);
+	LAUNCH_SCALAR(KF(k_dt_finalize), c->P, c->S, dt_next, c->first_time, step);
 	c->first_time = 0;
-	LAUNCH(KF(k_dt_reset), 1, 1, c->P, c->S);
+	LAUNCH_SCALAR(KF(k_dt_reset), c->P, c->S);
 	auto stage = [&](int st, const float* Uq, const float* Ub, float* Uo) {
 		cudaEvent_t ea = nullptr, eb = nullptr;
 		if (c->profiling) { ea = pool_event(c); eb = pool_event(c); cudaEventRecord(ea, c->stream); }
@@ -324,7 +331,7 @@ void enqueue_full_step_fp32(trg_ctx* c, double dt_next) {
 	};
 	stage(1, c->U32, c->U32, c->U32s);
 	stage(2, c->U32s, c->U32, c->U32);
-	LAUNCH(KF(k_time_advance), 1, 1, c->S);
+	LAUNCH_SCALAR(KF(k_time_advance), c->P, c->S);
 	c->steps++;
 }
 
@@ -334,7 +341,7 @@ void enqueue_full_step(trg_ctx* c, double dt_next) {
 		return;
 	}
 	// Torch::fullStep, Torch.cpp:389-418
-	q_from_u(c, c->S.U, 1);
+	q_from_u(c, 0, 1);
 	if (c->P.cooling_on) thermo_pre(c);
 	if (c->P.radiation_on) rad_pre(c);
 	time_step(c, dt_next);
@@ -349,7 +356,7 @@ void enqueue_full_step(trg_ctx* c, double dt_next) {
 		}
 		for (int i = ncomps - 2; i >= 0; --i) sub_step(c, 0.5, false, c->hs.active[(i + c->stepCounter) % ncomps]);
 	}
-	LAUNCH(KF(k_time_advance), 1, 1, c->S);
+	LAUNCH_SCALAR(KF(k_time_advance), c->P, c->S);
 	c->steps++;
 }
 
@@ -493,7 +500,7 @@ int trg_create(const trg_params* p, const double* den, const double* pre, const 
 	}
 	// Torch::run prologue (Torch.cpp:245-264): Q from U with floors, and the
 	// column-density ray trace of fillHeatingArrays (Thermodynamics.cpp:420-421).
-	q_from_u(c, S.U, 1);
+	q_from_u(c, 0, 1);
 	if (c->P.star_on) colden_sweep(c);
 	// the host copies of the initial fields are no longer needed
 	std::vector<double>().swap(c->hs.U);
@@ -572,7 +579,7 @@ int trg_component(trg_ctx* c, int comp, int phase, double dt, double* out) {
 		else if (comp == TRG_COMP_RAD) rad_pre(c);
 		break;
 	case TRG_PHASE_DT: {
-		LAUNCH(KF(k_dt_reset), 1, 1, c->P, c->S);
+		LAUNCH_SCALAR(KF(k_dt_reset), c->P, c->S);
 		long long first_cell = -1;
 		if (comp == TRG_COMP_RAD && c->P.radiation_on && c->P.star_on && c->P.K1 != 0.0 && c->rad_once_pending) {
 			first_cell = c->hs.first_nonwind_cell;
@@ -596,12 +603,12 @@ int trg_component(trg_ctx* c, int comp, int phase, double dt, double* out) {
 		break;
 	case TRG_PHASE_SOURCES:
 		if (comp == TRG_COMP_HYDRO)
-			LAUNCH(KF(k_hydro_update_fp64), c->P.N, 256, c->P, c->S, 1.0, (const double*)c->S.U, c->S.U, 1);
+			LAUNCH(KF(k_hydro_update_fp64), c->P.N, 256, c->P, c->S, 1.0, 0, 0, 1);
 		else if (comp == TRG_COMP_RAD) LAUNCH(KF(k_rad_update_fp64), c->P.N, 256, c->P, c->S, 1.0, 1);
 		else if (comp == TRG_COMP_THERMO) LAUNCH(KF(k_thermo_update_fp64), c->P.N, 256, c->P, c->S, 1.0, 1);
 		break;
 	case TRG_PHASE_Q_FROM_U:
-		q_from_u(c, c->S.U, 1);
+		q_from_u(c, 0, 1);
 		break;
 	case TRG_PHASE_ADVANCE:
 		LAUNCH(KF(k_advance_fp64), c->P.N, 256, c->P, c->S, dt);
@@ -619,7 +626,7 @@ int trg_get_state(trg_ctx* c, double* U, double* Q, double* R, double* T, double
 	if (c->fp32) {
 		// expose the FP32 state as FP64 (Q = QfromU without floors)
 		LAUNCH(k_f32_to_f64, 7 * N, 256, c->P, c->U32, c->S.U);
-		q_from_u(c, c->S.U, 0);
+		q_from_u(c, 0, 0);
 	}
 	if (U) CUDA_TRY(cudaMemcpyAsync(U, c->S.U, 7 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
 	if (Q) CUDA_TRY(cudaMemcpyAsync(Q, c->S.Q, 7 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -734,6 +741,60 @@ long trg_harvest_read(trg_ctx* c, float* out, long max) {
 	return (long)n;
 }
 
+int trg_autotune(trg_ctx* c, int* zchunk_out, double* ms_out) {
+	if (!c) return TRG_ERR_ARG;
+	if (zchunk_out) *zchunk_out = 0;
+	if (ms_out) *ms_out = 0;
+	if (!(c->fp32 || c->mixed)) return TRG_OK;
+	// The timed launches only write scratch (U32s, or U1 of the mixed form),
+	// but they fold their CFL minimum into the time-step slots: save and
+	// restore those and the error word around the trials.
+	double scal[8];
+	unsigned err = 0;
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	CUDA_TRY(cudaMemcpy(scal, c->S.scal, sizeof(scal), cudaMemcpyDeviceToHost));
+	CUDA_TRY(cudaMemcpy(&err, c->S.err, sizeof(err), cudaMemcpyDeviceToHost));
+	std::vector<int> cand;
+	const int nz = c->P.nz;
+	for (int z : {4, 8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256})
+		if (z < nz) cand.push_back(z);
+	cand.push_back(nz);
+	cand.push_back(std::min(nz, ctx_fp32_zchunk(c)));
+	std::sort(cand.begin(), cand.end());
+	cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+	cudaEvent_t e0, e1;
+	CUDA_TRY(cudaEventCreate(&e0));
+	CUDA_TRY(cudaEventCreate(&e1));
+	auto trial = [&](int zc) {
+		if (c->fp32) launch_hydro_stage_fp32(1, c->P, c->S, c->U32, c->U32, c->U32s, zc, c->stream);
+		else launch_hydro_substep_fp32(c->P, c->S, c->S.U, c->S.U1, 0.5, zc, c->stream);
+	};
+	int best = c->zchunk;
+	float best_ms = 1e30f;
+	for (int zc : cand) {
+		trial(zc);
+		cudaEventRecord(e0, c->stream);
+		for (int r = 0; r < 3; ++r) trial(zc);
+		cudaEventRecord(e1, c->stream);
+		CUDA_TRY(cudaEventSynchronize(e1));
+		float ms = 0;
+		cudaEventElapsedTime(&ms, e0, e1);
+		if (ms < best_ms) {
+			best_ms = ms;
+			best = zc;
+		}
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	CUDA_TRY(cudaMemcpy(c->S.scal, scal, sizeof(scal), cudaMemcpyHostToDevice));
+	CUDA_TRY(cudaMemcpy(c->S.err, &err, sizeof(err), cudaMemcpyHostToDevice));
+	CUDA_TRY(cudaGetLastError());
+	c->zchunk = best;
+	if (zchunk_out) *zchunk_out = best;
+	if (ms_out) *ms_out = best_ms / 3.0;
+	return TRG_OK;
+}
+
 long long trg_kernel_launches(const trg_ctx* c) { return c ? c->launches : 0; }
 const char* trg_last_error(const trg_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
@@ -748,6 +809,211 @@ void trg_destroy(trg_ctx* c) {
 	for (void* p : c->allocs) cudaFree(p);
 	if (c->stream) cudaStreamDestroy(c->stream);
 	delete c;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ batches
+struct trg_batch {
+	int G = 0;
+	std::vector<trg_ctx*> grids;
+	trg_ctx* v = nullptr;  // the batch's own context: flags of grid 0, tables of all grids
+};
+
+namespace {
+
+template <typename T>
+int upload(trg_ctx* v, T** dst, const std::vector<T>& src) {
+	int rc = dalloc(v, dst, src.size() + 1);
+	if (rc) return rc;
+	if (!src.empty()) {
+		trg_ctx* c = v;
+		CUDA_TRY(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+	}
+	return TRG_OK;
+}
+
+long long round_up(long long n, long long m) { return (n + m - 1) / m * m; }
+
+// Concatenates shell `s` of every grid (lists `lists`, offsets `offs`) into
+// one batched sweep with (grid << BATCH_CELL_BITS) | cell entries.
+void concat_shells(const std::vector<trg_ctx*>& grids, bool nonwind, std::vector<int>& cells,
+                   std::vector<long long>& off) {
+	size_t nshell = 0;
+	for (auto* g : grids) nshell = std::max(nshell, (nonwind ? g->hs.off_nonwind : g->hs.off_all).size() - 1);
+	off.assign(1, 0);
+	for (size_t s = 0; s < nshell; ++s) {
+		for (size_t gi = 0; gi < grids.size(); ++gi) {
+			const auto& o = nonwind ? grids[gi]->hs.off_nonwind : grids[gi]->hs.off_all;
+			const auto& l = nonwind ? grids[gi]->hs.sweep_nonwind : grids[gi]->hs.sweep_all;
+			if (s + 1 >= o.size()) continue;
+			for (long long k = o[s]; k < o[s + 1]; ++k) cells.push_back(((int)gi << BATCH_CELL_BITS) | l[k]);
+		}
+		off.push_back((long long)cells.size());
+	}
+}
+
+bool same_flags(const trg_ctx* a, const trg_ctx* b) {
+	const Params &p = a->P, &q = b->P;
+	return p.nd == q.nd && p.geometry == q.geometry && p.order == q.order && p.riemann == q.riemann &&
+	       p.limiter == q.limiter && p.radiation_on == q.radiation_on && p.cooling_on == q.cooling_on &&
+	       p.star_on == q.star_on && p.collisions_on == q.collisions_on && p.coupling == q.coupling &&
+	       p.thermo_subcycling == q.thermo_subcycling && (p.K1 != 0.0) == (q.K1 != 0.0) &&
+	       a->hs.nactive == b->hs.nactive && a->hs.active[0] == b->hs.active[0] &&
+	       a->hs.active[1] == b->hs.active[1] && a->hs.active[2] == b->hs.active[2] && a->raw.device == b->raw.device;
+}
+
+}  // namespace
+
+extern "C" {
+
+int trg_batch_create(trg_ctx* const* grids, int G, trg_batch** out) {
+	if (!grids || !out || G < 1 || G > BATCH_MAX_GRIDS) return TRG_ERR_ARG;
+	*out = nullptr;
+	for (int g = 0; g < G; ++g) {
+		trg_ctx* c = grids[g];
+		if (!c) return TRG_ERR_ARG;
+		if (c->fp32 || c->mixed) return set_error(c, TRG_ERR_ARG, "trg_batch_create: batches run the FP64 form");
+		if (c->P.N > (long long)BATCH_CELL_MASK + 1)
+			return set_error(c, TRG_ERR_ARG, "trg_batch_create: a batched grid holds at most 4194304 cells");
+		if (c->steps != 0 || !c->first_time)
+			return set_error(c, TRG_ERR_ARG, "trg_batch_create: grids join a batch before their first step");
+		if (!same_flags(grids[0], c))
+			return set_error(c, TRG_ERR_ARG, "trg_batch_create: grids differ in physics flags, solver or device");
+		if (c->S.mlp_img || c->S.harvest)
+			return set_error(c, TRG_ERR_ARG, "trg_batch_create: no learned start or harvest in a batch");
+	}
+	trg_batch* b = new trg_batch();
+	b->G = G;
+	b->grids.assign(grids, grids + G);
+	trg_ctx* v = new trg_ctx();
+	b->v = v;
+	auto bail = [&](int rc) {
+		trg_batch_destroy(b);
+		return rc;
+	};
+	trg_ctx* c = v;  // for CUDA_TRY
+	v->raw = grids[0]->raw;
+	CUDA_TRY(cudaSetDevice(v->raw.device));
+	if (cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(TRG_ERR_CUDA);
+	v->P = grids[0]->P;
+	v->S = grids[0]->S;
+	v->hs.nactive = grids[0]->hs.nactive;
+	for (int i = 0; i < 3; ++i) v->hs.active[i] = grids[0]->hs.active[i];
+	v->nscalar = G;
+	v->fastk = false;
+	v->dt_hist_cap = 0;
+	// offsets of the padded cell and face ranges
+	std::vector<long long> cell_off(G + 1, 0), face_off[3], first_cell(G, -1);
+	for (int d = 0; d < 3; ++d) face_off[d].assign(G + 1, 0);
+	v->hs.first_nonwind_cell = -1;
+	for (int g = 0; g < G; ++g) {
+		cell_off[g + 1] = cell_off[g] + round_up(grids[g]->P.N, 256);
+		for (int d = 0; d < 3; ++d) face_off[d][g + 1] = face_off[d][g] + round_up(grids[g]->S.nfaces[d], 256);
+		first_cell[g] = grids[g]->hs.first_nonwind_cell;
+		if (first_cell[g] >= 0) v->hs.first_nonwind_cell = 0;
+	}
+	// per-grid copies; one error word and one counter block for the batch
+	if (dalloc(v, &v->S.err, 1) || dalloc(v, &v->S.stats, TRG_NSTATS)) return bail(TRG_ERR_OOM);
+	CUDA_TRY(cudaMemset(v->S.err, 0, sizeof(unsigned)));
+	CUDA_TRY(cudaMemset(v->S.stats, 0, TRG_NSTATS * sizeof(unsigned long long)));
+	std::vector<Params> Ps(G);
+	std::vector<State> Ss(G);
+	for (int g = 0; g < G; ++g) {
+		Ps[g] = grids[g]->P;
+		Ps[g].batch = nullptr;
+		Ps[g].stats_on = 0;
+		Ss[g] = grids[g]->S;
+		Ss[g].err = v->S.err;
+		Ss[g].stats = v->S.stats;
+	}
+	// batched sweeps and wind list
+	std::vector<int> wind;
+	for (int g = 0; g < G; ++g)
+		for (int w : grids[g]->hs.wind_cells) wind.push_back((g << BATCH_CELL_BITS) | w);
+	concat_shells(b->grids, false, v->hs.sweep_all, v->hs.off_all);
+	concat_shells(b->grids, true, v->hs.sweep_nonwind, v->hs.off_nonwind);
+	v->hs.wind_cells = wind;
+	Params* dP = nullptr;
+	State* dS = nullptr;
+	long long *dcell = nullptr, *dface[3] = {nullptr, nullptr, nullptr}, *dfirst = nullptr;
+	BatchTable* dtab = nullptr;
+	int rc = 0;
+	if ((rc = upload(v, &dP, Ps)) || (rc = upload(v, &dS, Ss)) || (rc = upload(v, &dcell, cell_off)) ||
+	    (rc = upload(v, &dface[0], face_off[0])) || (rc = upload(v, &dface[1], face_off[1])) ||
+	    (rc = upload(v, &dface[2], face_off[2])) || (rc = upload(v, &dfirst, first_cell)) ||
+	    (rc = upload(v, &v->d_sweep_all, v->hs.sweep_all)) ||
+	    (rc = upload(v, &v->d_sweep_nonwind, v->hs.sweep_nonwind)) || (rc = upload(v, &v->d_wind, wind)))
+		return bail(rc);
+	BatchTable tab;
+	tab.G = G;
+	tab.P = dP;
+	tab.S = dS;
+	tab.cell_off = dcell;
+	for (int d = 0; d < 3; ++d) tab.face_off[d] = dface[d];
+	tab.first_cell = dfirst;
+	if ((rc = upload(v, &dtab, std::vector<BatchTable>(1, tab)))) return bail(rc);
+	v->P.batch = dtab;
+	v->P.N = cell_off[G];
+	v->P.stats_on = 0;
+	for (int d = 0; d < 3; ++d) v->S.nfaces[d] = face_off[d][G];
+	v->S.mlp_img = nullptr;
+	v->S.harvest = nullptr;
+	v->S.harvest_n = nullptr;
+	v->S.dt_hist = nullptr;
+	*out = b;
+	return TRG_OK;
+}
+
+int trg_batch_enqueue_steps(trg_batch* b, int nsteps, double dt_next_checkpoint) {
+	if (!b || nsteps < 0) return TRG_ERR_ARG;
+	for (int s = 0; s < nsteps; ++s) enqueue_full_step(b->v, dt_next_checkpoint);
+	trg_ctx* c = b->v;
+	CUDA_TRY(cudaGetLastError());
+	return TRG_OK;
+}
+
+int trg_batch_run_steps(trg_batch* b, int nsteps, double dt_next_checkpoint) {
+	int rc = trg_batch_enqueue_steps(b, nsteps, dt_next_checkpoint);
+	if (rc) return rc;
+	return check_device_error(b->v);
+}
+
+int trg_batch_synchronize(trg_batch* b) {
+	if (!b) return TRG_ERR_ARG;
+	return check_device_error(b->v);
+}
+
+void* trg_batch_stream(const trg_batch* b) { return b ? (void*)b->v->stream : nullptr; }
+long long trg_batch_kernel_launches(const trg_batch* b) { return b ? b->v->launches : 0; }
+long long trg_batch_cells(const trg_batch* b) {
+	long long n = 0;
+	if (b)
+		for (auto* g : b->grids) n += g->P.N;
+	return n;
+}
+const char* trg_batch_last_error(const trg_batch* b) { return b ? b->v->err.c_str() : "null batch"; }
+
+int trg_batch_profile_enable(trg_batch* b, int on) { return b ? trg_profile_enable(b->v, on) : TRG_ERR_ARG; }
+int trg_batch_profile_read(trg_batch* b, const char* name, double* total_ms, long long* launches) {
+	return b ? trg_profile_read(b->v, name, total_ms, launches) : TRG_ERR_ARG;
+}
+
+void trg_batch_destroy(trg_batch* b) {
+	if (!b) return;
+	trg_ctx* v = b->v;
+	if (v) {
+		if (v->stream) cudaStreamSynchronize(v->stream);
+		// the grids continue on their own from where the batch left them
+		for (auto* g : b->grids) {
+			g->steps = v->steps;
+			g->first_time = v->first_time;
+			g->rad_once_pending = v->rad_once_pending;
+			g->stepCounter = v->stepCounter;
+		}
+		trg_destroy(v);
+	}
+	delete b;
 }
 
 }  // extern "C"

@@ -244,9 +244,21 @@ __device__ __forceinline__ void load_line(const Params& P, const double* __restr
 // Hydrodynamics::calcFluxes (Hydro.cpp:91-115) with the reconstruction of
 // Hydro.cpp:44-67: one thread per face along dim; face f lies between line
 // positions f-1 and f.
+__device__ __forceinline__ void b_faces_fp64(const Params& P, const State& S, long long t, int dim);
 __global__ void __launch_bounds__(128) k_faces_fp64(Params P, State S, int dim) {
-	long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (P.batch) {
+		const BatchTable& B = *P.batch;
+		const long long* off = B.face_off[dim];
+		const int g = batch_slot(off, B.G, blockIdx.x * (long long)blockDim.x);
+		const long long lt = blockIdx.x * (long long)blockDim.x + threadIdx.x - off[g];
+		if (lt < B.S[g].nfaces[dim]) b_faces_fp64(B.P[g], B.S[g], lt, dim);
+		return;
+	}
+	const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
 	if (t >= S.nfaces[dim]) return;
+	b_faces_fp64(P, S, t, dim);
+}
+__device__ __forceinline__ void b_faces_fp64(const Params& P, const State& S, long long t, int dim) {
 	int n = ncell(P, dim), f;
 	long long base, stride;
 	if (dim == 0) {
@@ -355,12 +367,13 @@ __device__ __forceinline__ void hydro_udot(const Params& P, const State& S, long
 }
 
 // Hydro update: UDOT from the face fluxes, then Fluid::advSolution (Fluid.cpp:80-87)
-// from Ubase and Fluid::fixSolution, written to Uout (may alias Ubase).
+// from Ubase and Fluid::fixSolution, written to Uout (may alias Ubase); the
+// selectors pick S.U (0) or S.U1 (1).
 // mode 1 accumulates UDOT into S.UDOT instead (component-phase interface).
-__global__ void __launch_bounds__(256) k_hydro_update_fp64(Params P, State S, double h, const double* Ubase, double* Uout,
-                                                          int mode) {
-	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-	if (id >= P.N) return;
+__device__ __forceinline__ void b_hydro_update_fp64(const Params& P, const State& S, long long id, double h, int sel_base,
+                                                    int sel_out, int mode) {
+	const double* Ubase = sel_base ? S.U1 : S.U;
+	double* Uout = sel_out ? S.U1 : S.U;
 	int ijk[3];
 	double xc[3], udot[7];
 	cell_ijk(P, id, ijk);
@@ -378,12 +391,24 @@ __global__ void __launch_bounds__(256) k_hydro_update_fp64(Params P, State S, do
 #pragma unroll
 	for (int i = 0; i < NU; ++i) FLD(Uout, i, id) = u[i];
 }
+__global__ void __launch_bounds__(256) k_hydro_update_fp64(Params P, State S, double h, int sel_base, int sel_out,
+                                                          int mode) {
+	if (P.batch) {
+		const BatchTable& B = *P.batch;
+		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
+		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
+		if (lid < B.P[g].N) b_hydro_update_fp64(B.P[g], B.S[g], lid, h, sel_base, sel_out, mode);
+		return;
+	}
+	const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	b_hydro_update_fp64(P, S, id, h, sel_base, sel_out, mode);
+}
 
 // Fluid::globalQfromU (+ fixPrimitives), Fluid.cpp:138-165, with the Q half of
 // Torch::checkValues (Torch.cpp:420-443).
-__global__ void __launch_bounds__(256) k_q_from_u_fp64(Params P, State S, const double* Usrc, int fix) {
-	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-	if (id >= P.N) return;
+__device__ __forceinline__ void b_q_from_u_fp64(const Params& P, const State& S, long long id, int sel_src, int fix) {
+	const double* Usrc = sel_src ? S.U1 : S.U;
 	double u[7], q[7];
 #pragma unroll
 	for (int i = 0; i < NU; ++i) { u[i] = FLD(Usrc, i, id); q[i] = FLD(S.Q, i, id); }
@@ -401,11 +426,22 @@ __global__ void __launch_bounds__(256) k_q_from_u_fp64(Params P, State S, const 
 	for (int i = 0; i < NU; ++i) FLD(S.Q, i, id) = q[i];
 	if (bad) atomicOr(S.err, ERRB_NAN);
 }
+__global__ void __launch_bounds__(256) k_q_from_u_fp64(Params P, State S, int sel_src, int fix) {
+	if (P.batch) {
+		const BatchTable& B = *P.batch;
+		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
+		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
+		if (lid < B.P[g].N) b_q_from_u_fp64(B.P[g], B.S[g], lid, sel_src, fix);
+		return;
+	}
+	const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	b_q_from_u_fp64(P, S, id, sel_src, fix);
+}
 
 // advSolution(dt) + fixSolution over the UDOT array (component-phase interface).
-__global__ void __launch_bounds__(256) k_advance_fp64(Params P, State S, double dt) {
-	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-	if (id >= P.N) return;
+__device__ __forceinline__ void b_advance_fp64(const Params& P, const State& S, long long id, double dt) {
+
 	double u[7];
 	for (int i = 0; i < NU; ++i) {
 		u[i] = FLD(S.U, i, id) + dt * FLD(S.UDOT, i, id);
@@ -413,6 +449,18 @@ __global__ void __launch_bounds__(256) k_advance_fp64(Params P, State S, double 
 	}
 	if (!fix_solution(P, u)) atomicOr(S.err, ERRB_NAN);
 	for (int i = 0; i < NU; ++i) FLD(S.U, i, id) = u[i];
+}
+__global__ void __launch_bounds__(256) k_advance_fp64(Params P, State S, double dt) {
+	if (P.batch) {
+		const BatchTable& B = *P.batch;
+		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
+		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
+		if (lid < B.P[g].N) b_advance_fp64(B.P[g], B.S[g], lid, dt);
+		return;
+	}
+	const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	b_advance_fp64(P, S, id, dt);
 }
 
 // ------------------------------------------------------------------ radiation
@@ -525,16 +573,23 @@ __device__ __forceinline__ double tau_sc(const Params& P, const State& S, const 
 }
 
 // Wind cells of Radiation::transferRadiation, Radiation.cpp:590-598.
-__global__ void k_rad_wind_reset(Params P, State S, const int* __restrict__ cells, int count) {
-	int t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t >= count) return;
-	long long id = cells[t];
+__device__ __forceinline__ void b_rad_wind_reset(const Params& P, const State& S, long long id) {
 	FLD(S.R, R_TAU, id) = 0;
 	FLD(S.R, R_TAU_A, id) = 0;
 	FLD(S.R, R_DTAU, id) = 0;
 	FLD(S.R, R_DTAU_A, id) = 0;
 	FLD(S.Q, HII, id) = 1;
 	FLD(S.R, R_HII_A, id) = 1;
+}
+__global__ void k_rad_wind_reset(Params P, State S, const int* __restrict__ cells, int count) {
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= count) return;
+	if (P.batch) {
+		const int e = cells[t];
+		b_rad_wind_reset(P.batch->P[e >> BATCH_CELL_BITS], P.batch->S[e >> BATCH_CELL_BITS], e & BATCH_CELL_MASK);
+		return;
+	}
+	b_rad_wind_reset(P, S, cells[t]);
 }
 
 // Learned starting iterate: cells whose solve may take more than one Picard
@@ -579,12 +634,9 @@ __device__ __forceinline__ double inv_logit10(float l) {
 // tolerance); otherwise the cell restarts the plain iteration from x_HII, so
 // that a rejected prediction leaves the plain result unchanged.
 template <bool LEARNED>
-__device__ __forceinline__ void rad_shell(const Params& P, const State& S, const int* __restrict__ cells, int count,
+__device__ __forceinline__ void rad_shell(const Params& P, const State& S, const long long id, const bool valid,
                                           double h) {
-	const int t = blockIdx.x * blockDim.x + threadIdx.x;
-	const bool valid = t < count;
 	if (!LEARNED && !valid) return;
-	const long long id = valid ? cells[t] : 0;
 	const double dt = h * S.scal[0];
 	bool star = false, front = false;
 	double q_den = 0, q_pre = 0, q_hii = 0, ds = 0, n_H = 0, T = 1, alphaB = 0, A_ci = 0, tau_avg = 0, shellVol = 0;
@@ -713,17 +765,27 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 
 __global__ void __launch_bounds__(128) k_rad_shell_fp64(Params P, State S, const int* __restrict__ cells, int count,
                                                        double h) {
-	rad_shell<false>(P, S, cells, count, h);
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= count) return;
+	if (P.batch) {
+		const int e = cells[t];
+		const int g = e >> BATCH_CELL_BITS;
+		rad_shell<false>(P.batch->P[g], P.batch->S[g], e & BATCH_CELL_MASK, true, h);
+		return;
+	}
+	rad_shell<false>(P, S, cells[t], true, h);
 }
+// Single grids only (the tensor-core tile needs all 128 threads of a CTA).
 __global__ void __launch_bounds__(128) k_rad_shell_learned(Params P, State S, const int* __restrict__ cells, int count,
                                                           double h) {
-	rad_shell<true>(P, S, cells, count, h);
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	const bool valid = t < count;
+	rad_shell<true>(P, S, valid ? cells[t] : 0, valid, h);
 }
 
 // Star off: Radiation::transferRadiation else-branch (Radiation.cpp:638-650), interior cells.
-__global__ void k_rad_no_star_fp64(Params P, State S, double h) {
-	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-	if (id >= P.N) return;
+__device__ __forceinline__ void b_rad_no_star_fp64(const Params& P, const State& S, long long id, double h) {
+
 	const double dt = h * S.scal[0];
 	double x_new = FLD(S.Q, HII, id), x_dummy = x_new;
 	double n_H = P.X * FLD(S.Q, DEN, id) / P.hydrogenMass;
@@ -733,11 +795,22 @@ __global__ void k_rad_no_star_fp64(Params P, State S, double h) {
 	doric(dt, x_new, x_dummy, 0, nHII_aB, nHII_Aci);
 	FLD(S.Q, HII, id) = x_new;
 }
+__global__ void k_rad_no_star_fp64(Params P, State S, double h) {
+	if (P.batch) {
+		const BatchTable& B = *P.batch;
+		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
+		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
+		if (lid < B.P[g].N) b_rad_no_star_fp64(B.P[g], B.S[g], lid, h);
+		return;
+	}
+	const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	b_rad_no_star_fp64(P, S, id, h);
+}
 
 // Radiation::preTimeStepCalculations (photoheating), Radiation.cpp:257-296, non-wind cells.
-__global__ void __launch_bounds__(256) k_rad_heating_fp64(Params P, State S) {
-	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-	if (id >= P.N) return;
+__device__ __forceinline__ void b_rad_heating_fp64(const Params& P, const State& S, long long id) {
+
 	int ijk[3];
 	double xc[3];
 	cell_ijk(P, id, ijk);
@@ -761,11 +834,22 @@ __global__ void __launch_bounds__(256) k_rad_heating_fp64(Params P, State S) {
 	FLD(S.R, R_HEAT, id) = softrate;
 	if (rate != rate) atomicOr(S.err, ERRB_NAN);
 }
+__global__ void __launch_bounds__(256) k_rad_heating_fp64(Params P, State S) {
+	if (P.batch) {
+		const BatchTable& B = *P.batch;
+		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
+		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
+		if (lid < B.P[g].N) b_rad_heating_fp64(B.P[g], B.S[g], lid);
+		return;
+	}
+	const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	b_rad_heating_fp64(P, S, id);
+}
 
 // Radiation::updateSourceTerms (Radiation.cpp:653-680) then advSolution + fixSolution.
-__global__ void __launch_bounds__(256) k_rad_update_fp64(Params P, State S, double h, int mode) {
-	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-	if (id >= P.N) return;
+__device__ __forceinline__ void b_rad_update_fp64(const Params& P, const State& S, long long id, double h, int mode) {
+
 	const double dt = h * S.scal[0];
 	double u[7], udot[7] = {0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
@@ -796,6 +880,18 @@ __global__ void __launch_bounds__(256) k_rad_update_fp64(Params P, State S, doub
 	if (!fix_solution(P, u)) atomicOr(S.err, ERRB_NAN);
 #pragma unroll
 	for (int i = 0; i < NU; ++i) FLD(S.U, i, id) = u[i];
+}
+__global__ void __launch_bounds__(256) k_rad_update_fp64(Params P, State S, double h, int mode) {
+	if (P.batch) {
+		const BatchTable& B = *P.batch;
+		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
+		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
+		if (lid < B.P[g].N) b_rad_update_fp64(B.P[g], B.S[g], lid, h, mode);
+		return;
+	}
+	const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	b_rad_update_fp64(P, S, id, h, mode);
 }
 
 // ----------------------------------------------------------- thermodynamics
@@ -848,10 +944,7 @@ __device__ __forceinline__ double th_cooling(const Params& P, const State& S, do
 }
 
 // One shell of Thermodynamics::rayTrace / updateColDen (Thermodynamics.cpp:339-417).
-__global__ void __launch_bounds__(128) k_colden_shell_fp64(Params P, State S, const int* __restrict__ cells, int count) {
-	int t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t >= count) return;
-	long long id = cells[t];
+__device__ __forceinline__ void b_colden_shell_fp64(const Params& P, const State& S, long long id) {
 	int ijk[3];
 	double xc[3];
 	cell_ijk(P, id, ijk);
@@ -875,11 +968,20 @@ __global__ void __launch_bounds__(128) k_colden_shell_fp64(Params P, State S, co
 	FLD(S.T, T_COL_DEN, id) = newcolden;
 	FLD(S.T, T_DCOL_DEN, id) = (FLD(S.Q, DEN, id) / P.hydrogenMass) * S.ds[id];
 }
+__global__ void __launch_bounds__(128) k_colden_shell_fp64(Params P, State S, const int* __restrict__ cells, int count) {
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= count) return;
+	if (P.batch) {
+		const int e = cells[t];
+		b_colden_shell_fp64(P.batch->P[e >> BATCH_CELL_BITS], P.batch->S[e >> BATCH_CELL_BITS], e & BATCH_CELL_MASK);
+		return;
+	}
+	b_colden_shell_fp64(P, S, cells[t]);
+}
 
 // Thermodynamics::preTimeStepCalculations rates, Thermodynamics.cpp:224-263, non-wind cells.
-__global__ void __launch_bounds__(256) k_thermo_rates_fp64(Params P, State S) {
-	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-	if (id >= P.N) return;
+__device__ __forceinline__ void b_thermo_rates_fp64(const Params& P, const State& S, long long id) {
+
 	int ijk[3];
 	double xc[3];
 	cell_ijk(P, id, ijk);
@@ -911,11 +1013,22 @@ __global__ void __launch_bounds__(256) k_thermo_rates_fp64(Params P, State S) {
 	rate = soft_landing(rate, T, S.Tmin[id]);
 	FLD(S.T, T_RATE, id) = P.heating_amp * rate;
 }
+__global__ void __launch_bounds__(256) k_thermo_rates_fp64(Params P, State S) {
+	if (P.batch) {
+		const BatchTable& B = *P.batch;
+		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
+		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
+		if (lid < B.P[g].N) b_thermo_rates_fp64(B.P[g], B.S[g], lid);
+		return;
+	}
+	const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	b_thermo_rates_fp64(P, S, id);
+}
 
 // Thermodynamics::integrate (pressure subcycling), Thermodynamics.cpp:266-337, non-wind cells.
-__global__ void __launch_bounds__(256) k_thermo_integrate_fp64(Params P, State S, double h) {
-	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-	if (id >= P.N || !P.thermo_subcycling) return;
+__device__ __forceinline__ void b_thermo_integrate_fp64(const Params& P, const State& S, long long id, double h) {
+	if (!P.thermo_subcycling) return;
 	int ijk[3];
 	double xc[3];
 	cell_ijk(P, id, ijk);
@@ -968,11 +1081,22 @@ __global__ void __launch_bounds__(256) k_thermo_integrate_fp64(Params P, State S
 	}
 	FLD(S.T, T_RATE, id) = (pressure - qpre) * dpre2rate;
 }
+__global__ void __launch_bounds__(256) k_thermo_integrate_fp64(Params P, State S, double h) {
+	if (P.batch) {
+		const BatchTable& B = *P.batch;
+		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
+		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
+		if (lid < B.P[g].N) b_thermo_integrate_fp64(B.P[g], B.S[g], lid, h);
+		return;
+	}
+	const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	b_thermo_integrate_fp64(P, S, id, h);
+}
 
 // Thermodynamics::updateSourceTerms (Thermodynamics.cpp:478-485) then advSolution + fixSolution.
-__global__ void __launch_bounds__(256) k_thermo_update_fp64(Params P, State S, double h, int mode) {
-	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-	if (id >= P.N) return;
+__device__ __forceinline__ void b_thermo_update_fp64(const Params& P, const State& S, long long id, double h, int mode) {
+
 	int ijk[3];
 	double xc[3];
 	cell_ijk(P, id, ijk);
@@ -994,6 +1118,18 @@ __global__ void __launch_bounds__(256) k_thermo_update_fp64(Params P, State S, d
 	if (!fix_solution(P, u)) atomicOr(S.err, ERRB_NAN);
 #pragma unroll
 	for (int i = 0; i < NU; ++i) FLD(S.U, i, id) = u[i];
+}
+__global__ void __launch_bounds__(256) k_thermo_update_fp64(Params P, State S, double h, int mode) {
+	if (P.batch) {
+		const BatchTable& B = *P.batch;
+		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
+		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
+		if (lid < B.P[g].N) b_thermo_update_fp64(B.P[g], B.S[g], lid, h, mode);
+		return;
+	}
+	const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	b_thermo_update_fp64(P, S, id, h, mode);
 }
 
 // ----------------------------------------------------------------- time step
@@ -1019,8 +1155,19 @@ __device__ __forceinline__ double block_min(double v) {
 // exact and order independent; they are combined with atomicMin on the bit
 // pattern.  first_cell: the first non-wind cell in causal order on the first
 // radiation call (the reference's static `once`), else -1.
+__device__ __forceinline__ void b_dt_reduce_fp64(const Params& P, const State& S, long long id, long long first_cell);
 __global__ void __launch_bounds__(256) k_dt_reduce_fp64(Params P, State S, long long first_cell) {
-	long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (P.batch) {
+		// grid ranges are padded to whole blocks: the block reduction stays within one grid
+		const BatchTable& B = *P.batch;
+		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
+		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
+		b_dt_reduce_fp64(B.P[g], B.S[g], lid, first_cell >= 0 ? B.first_cell[g] : -1);
+		return;
+	}
+	b_dt_reduce_fp64(P, S, blockIdx.x * (long long)blockDim.x + threadIdx.x, first_cell);
+}
+__device__ __forceinline__ void b_dt_reduce_fp64(const Params& P, const State& S, long long id, long long first_cell) {
 	double th = 1.0e308, tr = 1.0e308, tt = 1.0e308;
 	if (id < P.N) {
 		double q_den = FLD(S.Q, DEN, id), q_pre = FLD(S.Q, PRE, id), q_hii = FLD(S.Q, HII, id);
@@ -1084,7 +1231,16 @@ __global__ void __launch_bounds__(256) k_dt_reduce_fp64(Params P, State S, long 
 }
 
 // Torch::calculateTimeStep + the dt of Torch::fullStep (Torch.cpp:304-339, :394).
+__device__ __forceinline__ void b_dt_finalize(const Params& P, const State& S, double dt_next, int first_time, int step);
 __global__ void k_dt_finalize(Params P, State S, double dt_next, int first_time, int step) {
+	if (P.batch) {
+		const int g = blockIdx.x * blockDim.x + threadIdx.x;
+		if (g < P.batch->G) b_dt_finalize(P.batch->P[g], P.batch->S[g], dt_next, first_time, step);
+		return;
+	}
+	b_dt_finalize(P, S, dt_next, first_time, step);
+}
+__device__ __forceinline__ void b_dt_finalize(const Params& P, const State& S, double dt_next, int first_time, int step) {
 	double dt;
 	if (first_time) {
 		dt = P.dt_max * 1.0e-20;
@@ -1100,14 +1256,29 @@ __global__ void k_dt_finalize(Params P, State S, double dt_next, int first_time,
 	if (S.dt_hist && step >= 0) S.dt_hist[step] = dt;
 }
 
-__global__ void k_time_advance(State S) { S.scal[1] += S.scal[0]; }
+__global__ void k_time_advance(Params P, State S) {
+	if (P.batch) {
+		const int g = blockIdx.x * blockDim.x + threadIdx.x;
+		if (g < P.batch->G) P.batch->S[g].scal[1] += P.batch->S[g].scal[0];
+		return;
+	}
+	S.scal[1] += S.scal[0];
+}
 
-__global__ void k_dt_reset(Params P, State S) {
+__device__ __forceinline__ void b_dt_reset(const Params& P, const State& S) {
 	unsigned long long big = (unsigned long long)__double_as_longlong(P.dt_max);
 	unsigned long long* slots = reinterpret_cast<unsigned long long*>(S.scal + 2);
 	slots[0] = big;
 	slots[1] = big;
 	slots[2] = big;
+}
+__global__ void k_dt_reset(Params P, State S) {
+	if (P.batch) {
+		const int g = blockIdx.x * blockDim.x + threadIdx.x;
+		if (g < P.batch->G) b_dt_reset(P.batch->P[g], P.batch->S[g]);
+		return;
+	}
+	b_dt_reset(P, S);
 }
 
 }  // namespace TRG_KNS

@@ -273,4 +273,16 @@ __device__ __forceinline__ void stat_picard(unsigned long long* st, unsigned ite
 	for (int k = 0; k < 8; ++k) stat_add(st, TRG_STAT_PICARD_HIST + k, iters > 0 && b == k);
 }
 
+// Grid of a batched launch whose (padded) range holds position `pos`:
+// the last g with off[g] <= pos.
+__device__ __forceinline__ int batch_slot(const long long* off, int G, long long pos) {
+	int lo = 0, hi = G - 1;
+	while (lo < hi) {
+		int mid = (lo + hi + 1) >> 1;
+		if (off[mid] <= pos) lo = mid;
+		else hi = mid - 1;
+	}
+	return lo;
+}
+
 }  // namespace trg

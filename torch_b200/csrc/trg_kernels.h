@@ -7,8 +7,8 @@
 // reference) and fast (FP32 form; FMA and CUDA libm)
 #define TRG_FP64_KERNELS \
 	__global__ void k_faces_fp64(Params P, State S, int dim); \
-	__global__ void k_hydro_update_fp64(Params P, State S, double h, const double* Ubase, double* Uout, int mode); \
-	__global__ void k_q_from_u_fp64(Params P, State S, const double* Usrc, int fix); \
+	__global__ void k_hydro_update_fp64(Params P, State S, double h, int sel_base, int sel_out, int mode); \
+	__global__ void k_q_from_u_fp64(Params P, State S, int sel_src, int fix); \
 	__global__ void k_advance_fp64(Params P, State S, double dt); \
 	__global__ void k_rad_wind_reset(Params P, State S, const int* cells, int count); \
 	__global__ void k_rad_shell_fp64(Params P, State S, const int* cells, int count, double h); \
@@ -22,7 +22,7 @@
 	__global__ void k_thermo_update_fp64(Params P, State S, double h, int mode); \
 	__global__ void k_dt_reduce_fp64(Params P, State S, long long first_cell); \
 	__global__ void k_dt_finalize(Params P, State S, double dt_next, int first_time, int step); \
-	__global__ void k_time_advance(State S); \
+	__global__ void k_time_advance(Params P, State S); \
 	__global__ void k_dt_reset(Params P, State S);
 
 namespace trg {

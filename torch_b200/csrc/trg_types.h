@@ -31,6 +31,8 @@ struct Tables {
 
 // Code-unit parameters of one run (the reference's Constants, TorchParameters
 // after initialise(), Star, Thermodynamics constants).
+struct BatchTable;
+
 struct Params {
 	int nd, nx, ny, nz;
 	long long N;
@@ -60,6 +62,9 @@ struct Params {
 	double f32_rho0, f32_p0, f32_v0;
 	// diagnostic counters (State::stats) are updated only when this is set
 	int stats_on;
+	// batched launch over many grids (null for one grid): kernels take each
+	// grid's Params and State from this table
+	const BatchTable* batch;
 };
 
 // Device pointers of one context (FP64 state).
@@ -89,6 +94,23 @@ struct State {
 	float* harvest;
 	long long harvest_cap;
 	unsigned long long* harvest_n;
+};
+
+// Many independent grids advanced by one launch per stage.  Cell and face
+// ranges of the grids are laid end to end, each padded to a whole number of
+// 256-thread blocks, so that a block belongs to one grid (found by binary
+// search in the offsets); shell and wind lists hold (grid << BATCH_CELL_BITS) |
+// cell entries.
+constexpr int BATCH_CELL_BITS = 22;
+constexpr int BATCH_CELL_MASK = (1 << BATCH_CELL_BITS) - 1;
+constexpr int BATCH_MAX_GRIDS = 1 << (31 - BATCH_CELL_BITS);
+struct BatchTable {
+	int G;
+	const Params* P;             // per grid (their batch field is null)
+	const State* S;
+	const long long* cell_off;   // [G + 1]
+	const long long* face_off[3];  // [G + 1] per dimension
+	const long long* first_cell;   // [G] first non-wind cell in causal order
 };
 
 }  // namespace trg

@@ -11,6 +11,9 @@
 * ``hii_region``- 3-D HII-region expansion: lognormal density (mean 1e3 cm^-3,
                   sigma_ln 0.5, P(k) ~ k^-11/3, seeded), T = 100 K, star of
                   1e49 photons/s at the centre, radiation + cooling, wind off.
+* ``blister_batch`` - many independent 2-D cylindrical HII-region grids of
+                  uneven sizes (64-256 x 64-320), photon rates and cloud
+                  profiles, for batched stepping.
 
 Each returns ``(TorchParameters, InitialConditions)``.
 """
@@ -93,3 +96,29 @@ def hii_region(n=256, seed=12345, side=2 * PC2CM, photon_rate=1e49):
     tp = hii_region_parameters(n, side, photon_rate)
     g = setups.lognormal_cloud(n=n, side=side, seed=seed)
     return tp, make_initial_conditions(g["ncells"], g["dx"], g["den"], g["pre"], g["hii"], g["vel"])
+
+
+def blister_batch(G=256, seed=2024, nx_range=(64, 256), ny_range=(64, 320), q_range=(1e47, 1e49),
+                  alpha_range=(0.0, 2.0), rc_pc_range=(0.005, 0.05)):
+    """Independent 2-D cylindrical HII-region grids of uneven sizes: nx, ny
+    uniform in the ranges, photon rate log-uniform, cloud n(R) = n0 (1 +
+    R^2/rc^2)^-alpha with alpha and rc uniform (the shipped setup's profile,
+    nHI = 32000 cm^-3 at the star, star offset 0.35 pc, T = 300 K), the
+    shipped cell size (0.5 pc / 150), star on the axis at row 0.55 ny,
+    radiation and cooling on, wind off.  Returns a list of (params, initial
+    conditions)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(G):
+        nx = int(rng.integers(nx_range[0], nx_range[1] + 1))
+        ny = int(rng.integers(ny_range[0], ny_range[1] + 1))
+        q = float(10 ** rng.uniform(np.log10(q_range[0]), np.log10(q_range[1])))
+        alpha = float(rng.uniform(*alpha_range))
+        rc = float(rng.uniform(*rc_pc_range))
+        side = 0.5 * PC2CM * nx / 150
+        star_y = int(round(0.55 * ny))
+        tp = dataclasses.replace(blister_parameters((nx, ny, 1)), star_position=(0, star_y, 0), sideLength=side,
+                                 photonRate=q, windCellRadius=0, massLossRate=0.0)
+        g = setups.blister_profile(ncells=(nx, ny, 1), side=side, star_cell=(0, star_y), rc_pc=rc, alpha=alpha)
+        out.append((tp, make_initial_conditions((nx, ny, 1), g["dx"], g["den"], g["pre"], g["hii"], g["vel"])))
+    return out
