@@ -135,7 +135,9 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm), "idle_samples_dropped": idle}
 
 
-def dist_setup():
+def dist_setup(backend="nccl"):
+    """One process per GPU under torchrun (RANK/LOCAL_RANK/WORLD_SIZE/MASTER_*
+    from the environment); the ranks only synchronise and max-reduce times."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -143,9 +145,10 @@ def dist_setup():
     if world > 1:
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
+        if backend == "nccl":
+            torch.cuda.set_device(local)
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
         pg = dist
     return world, rank, local, pg
 
@@ -159,7 +162,8 @@ def max_over_ranks(pg, value, local):
     if pg is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    dev = f"cuda:{local}" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
@@ -235,7 +239,7 @@ def run_reference_arm(args, rank):
 
 
 # ----------------------------------------------------------------- GPU leg
-def time_form(args, precision, tp, ic, local, pg, profile_names, stream_mod):
+def time_form(args, precision, tp, ic, local, pg, profile_names):
     """Times K full steps of one precision form; returns (ms, launches, prof, sim)."""
     import torch
     import torch_b200
@@ -368,6 +372,57 @@ def run_batch(args, world, rank, local, pg):
     return 0
 
 
+def time_learned(args, sim32, N, world, local, pg):
+    """FP32 form with the learned starting iterate, after the plain FP32 timing:
+    six more FP32 steps record the plain solve's front cells, a network is
+    trained on them on the GPU, then K more FP32 steps are timed with it.
+    Solver counters of two further steps with and without the network follow
+    the timed region."""
+    import torch
+    import torch_b200
+    # training set: the plain solve's front cells over a few more FP32 steps
+    sim32.harvest(1 << 23)
+    sim32.run_steps(6)
+    recs, _ = sim32.harvest_read()
+    sim32.harvest(0)
+    t0 = time.perf_counter()
+    net = torch_b200.Mlp(device=local, seed=11)
+    hist = net.train(recs, epochs=30, batch=4096, lr=2e-3, seed=12)
+    torch.cuda.synchronize(local)
+    train_s = time.perf_counter() - t0
+    sim32.learned_start(net)
+    dt_next = sim32.dt_max
+    sim32.run_steps(1)  # captures the sweep graphs with the learned kernel
+    stream = torch.cuda.ExternalStream(sim32.stream_handle(), device=f"cuda:{local}")
+    barrier(pg)
+    torch.cuda.synchronize(local)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    sim32.enqueue_steps(args.steps, dt_next)
+    ev1.record(stream)
+    sim32.synchronize()
+    torch.cuda.synchronize(local)
+    barrier(pg)
+    ms = max_over_ranks(pg, ev0.elapsed_time(ev1), local)
+    sim32.stats_enable(True)
+    sim32.run_steps(2)
+    st = sim32.stats(reset=True)
+    sim32.learned_start(None)
+    sim32.run_steps(2)
+    st_plain = sim32.stats(reset=True)
+    sim32.stats_enable(False)
+    net.close()
+    return {"value": N * args.steps * world / (ms / 1e3), "ms_per_step": ms / args.steps,
+            "training": {"records": int(len(recs)), "epochs": 30, "seconds": train_s,
+                         "loss_first_last": [float(hist[0]), float(hist[-1])]},
+            "front_cells": st["front_cells"], "learned_cells": st["learned_cells"],
+            "accepted": st["learned_accepted"] / max(1, st["learned_cells"]),
+            "front_iters_per_cell": st["front_iters"] / max(1, st["front_cells"]),
+            "front_iters_per_cell_plain": st_plain["front_iters"] / max(1, st_plain["front_cells"]),
+            "picard_max": st["picard_max"], "picard_max_plain": st_plain["picard_max"],
+            "note": "counters from two steps after the timed region with the network, then two without it"}
+
+
 def run_ours(args, world, rank, local, pg):
     import torch
     import torch_b200
@@ -381,7 +436,7 @@ def run_ours(args, world, rank, local, pg):
     sims = {}
     for form in forms:
         prec = torch_b200.PRECISION_FP32 if form == "fp32" else torch_b200.PRECISION_FP64
-        ms, launches, prof, sim = time_form(args, prec, tp, ic, local, pg, PROFILE_NAMES, None)
+        ms, launches, prof, sim = time_form(args, prec, tp, ic, local, pg, PROFILE_NAMES)
         ms = max_over_ranks(pg, ms, local)
         results[form] = (ms, launches, prof)
         sims[form] = sim
@@ -397,17 +452,25 @@ def run_ours(args, world, rank, local, pg):
         error = form_error(sims[head], sims["fp64"], tp.heatCapacityRatio, int(ic.nd))
         error["steps"] = args.warmup + args.steps
         error["against"] = "plain FP64 form on the GPU (bit-exact twin of the FP64 oracle)"
+    learned = None
+    if args.learned and head == "fp32" and tp.radiation_on:
+        learned = time_learned(args, sims["fp32"], N, world, local, pg)
     for form, s in sims.items():
         if form != head:
             s.close()
 
     # roofline of the dominant hydro kernel
     peak, peak_kind = hbm_peak()
-    if head == "fp32":
+    if head == "fp32" and args.workload == "sedov":
         kname = "k_hydro_stage_fp32"
         # algorithmic bytes per cell per RK2 step in FP32: stage 1 reads U0 (28 B) and
         # writes U* (28 B); stage 2 reads U* and U0 and writes U1 (84 B): 140 B per two launches
         alg_per_launch = 140.0 * N / 2.0
+    elif head == "fp32":
+        kname = "k_hydro_stage_fp32"
+        # FP32 form of a radiation-hydro run: one launch per hydro sub-step on the
+        # FP64 state, reading U (7 x 8 B) and writing the new U (7 x 8 B)
+        alg_per_launch = 112.0 * N
     else:
         kname = "k_faces_fp64"
         # FP64 plain form, per face-flux launch (one per dimension, 2 stages):
@@ -477,7 +540,7 @@ def run_ours(args, world, rank, local, pg):
             "config": dict(workload_config(args.workload, args.n, head, world),
                            autotuned_tile_z=getattr(sim_tile, "__getitem__", lambda i: None)(0)),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": clk, "kernels": kernel_share, "error_vs_fp64": error,
+            "clocks": clk, "kernels": kernel_share, "error_vs_fp64": error, "learned_fp32": learned,
         }
         line.update(other)
         print(json.dumps(line), flush=True)
@@ -497,6 +560,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", dest="learned", action="store_false",
+                    help="skip the FP32 + learned-start measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

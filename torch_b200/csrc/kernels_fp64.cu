@@ -19,6 +19,13 @@
 #ifndef TRG_KNS
 #define TRG_KNS exact
 #endif
+// Batches run the plain-FP64 form only: the fast build leaves the batch
+// dispatch out, which keeps its kernels' instruction footprint small.
+#ifdef TRG_FAST_MATH
+#define TRG_BATCHED false
+#else
+#define TRG_BATCHED true
+#endif
 namespace trg {
 namespace TRG_KNS {
 
@@ -246,7 +253,7 @@ __device__ __forceinline__ void load_line(const Params& P, const double* __restr
 // positions f-1 and f.
 __device__ __forceinline__ void b_faces_fp64(const Params& P, const State& S, long long t, int dim);
 __global__ void __launch_bounds__(128) k_faces_fp64(Params P, State S, int dim) {
-	if (P.batch) {
+	if (TRG_BATCHED && P.batch) {
 		const BatchTable& B = *P.batch;
 		const long long* off = B.face_off[dim];
 		const int g = batch_slot(off, B.G, blockIdx.x * (long long)blockDim.x);
@@ -393,7 +400,7 @@ __device__ __forceinline__ void b_hydro_update_fp64(const Params& P, const State
 }
 __global__ void __launch_bounds__(256) k_hydro_update_fp64(Params P, State S, double h, int sel_base, int sel_out,
                                                           int mode) {
-	if (P.batch) {
+	if (TRG_BATCHED && P.batch) {
 		const BatchTable& B = *P.batch;
 		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
 		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
@@ -427,7 +434,7 @@ __device__ __forceinline__ void b_q_from_u_fp64(const Params& P, const State& S,
 	if (bad) atomicOr(S.err, ERRB_NAN);
 }
 __global__ void __launch_bounds__(256) k_q_from_u_fp64(Params P, State S, int sel_src, int fix) {
-	if (P.batch) {
+	if (TRG_BATCHED && P.batch) {
 		const BatchTable& B = *P.batch;
 		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
 		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
@@ -451,7 +458,7 @@ __device__ __forceinline__ void b_advance_fp64(const Params& P, const State& S, 
 	for (int i = 0; i < NU; ++i) FLD(S.U, i, id) = u[i];
 }
 __global__ void __launch_bounds__(256) k_advance_fp64(Params P, State S, double dt) {
-	if (P.batch) {
+	if (TRG_BATCHED && P.batch) {
 		const BatchTable& B = *P.batch;
 		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
 		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
@@ -584,7 +591,7 @@ __device__ __forceinline__ void b_rad_wind_reset(const Params& P, const State& S
 __global__ void k_rad_wind_reset(Params P, State S, const int* __restrict__ cells, int count) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= count) return;
-	if (P.batch) {
+	if (TRG_BATCHED && P.batch) {
 		const int e = cells[t];
 		b_rad_wind_reset(P.batch->P[e >> BATCH_CELL_BITS], P.batch->S[e >> BATCH_CELL_BITS], e & BATCH_CELL_MASK);
 		return;
@@ -767,7 +774,7 @@ __global__ void __launch_bounds__(128) k_rad_shell_fp64(Params P, State S, const
                                                        double h) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= count) return;
-	if (P.batch) {
+	if (TRG_BATCHED && P.batch) {
 		const int e = cells[t];
 		const int g = e >> BATCH_CELL_BITS;
 		rad_shell<false>(P.batch->P[g], P.batch->S[g], e & BATCH_CELL_MASK, true, h);
@@ -796,7 +803,7 @@ __device__ __forceinline__ void b_rad_no_star_fp64(const Params& P, const State&
 	FLD(S.Q, HII, id) = x_new;
 }
 __global__ void k_rad_no_star_fp64(Params P, State S, double h) {
-	if (P.batch) {
+	if (TRG_BATCHED && P.batch) {
 		const BatchTable& B = *P.batch;
 		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
 		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
@@ -835,7 +842,7 @@ __device__ __forceinline__ void b_rad_heating_fp64(const Params& P, const State&
 	if (rate != rate) atomicOr(S.err, ERRB_NAN);
 }
 __global__ void __launch_bounds__(256) k_rad_heating_fp64(Params P, State S) {
-	if (P.batch) {
+	if (TRG_BATCHED && P.batch) {
 		const BatchTable& B = *P.batch;
 		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
 		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
@@ -882,7 +889,7 @@ __device__ __forceinline__ void b_rad_update_fp64(const Params& P, const State& 
 	for (int i = 0; i < NU; ++i) FLD(S.U, i, id) = u[i];
 }
 __global__ void __launch_bounds__(256) k_rad_update_fp64(Params P, State S, double h, int mode) {
-	if (P.batch) {
+	if (TRG_BATCHED && P.batch) {
 		const BatchTable& B = *P.batch;
 		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
 		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
@@ -971,7 +978,7 @@ __device__ __forceinline__ void b_colden_shell_fp64(const Params& P, const State
 __global__ void __launch_bounds__(128) k_colden_shell_fp64(Params P, State S, const int* __restrict__ cells, int count) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= count) return;
-	if (P.batch) {
+	if (TRG_BATCHED && P.batch) {
 		const int e = cells[t];
 		b_colden_shell_fp64(P.batch->P[e >> BATCH_CELL_BITS], P.batch->S[e >> BATCH_CELL_BITS], e & BATCH_CELL_MASK);
 		return;
@@ -1014,7 +1021,7 @@ __device__ __forceinline__ void b_thermo_rates_fp64(const Params& P, const State
 	FLD(S.T, T_RATE, id) = P.heating_amp * rate;
 }
 __global__ void __launch_bounds__(256) k_thermo_rates_fp64(Params P, State S) {
-	if (P.batch) {
+	if (TRG_BATCHED && P.batch) {
 		const BatchTable& B = *P.batch;
 		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
 		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
@@ -1082,7 +1089,7 @@ __device__ __forceinline__ void b_thermo_integrate_fp64(const Params& P, const S
 	FLD(S.T, T_RATE, id) = (pressure - qpre) * dpre2rate;
 }
 __global__ void __launch_bounds__(256) k_thermo_integrate_fp64(Params P, State S, double h) {
-	if (P.batch) {
+	if (TRG_BATCHED && P.batch) {
 		const BatchTable& B = *P.batch;
 		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
 		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
@@ -1096,14 +1103,18 @@ __global__ void __launch_bounds__(256) k_thermo_integrate_fp64(Params P, State S
 
 // Thermodynamics::updateSourceTerms (Thermodynamics.cpp:478-485) then advSolution + fixSolution.
 __device__ __forceinline__ void b_thermo_update_fp64(const Params& P, const State& S, long long id, double h, int mode) {
-
+	// every load is issued before the first store, so that they overlap
+	double u[7];
+#pragma unroll
+	for (int i = 0; i < NU; ++i) u[i] = FLD(S.U, i, id);
+	const double rate = FLD(S.T, T_RATE, id);
 	int ijk[3];
 	double xc[3];
 	cell_ijk(P, id, ijk);
 	cell_xc(P, ijk, xc);
 	double udot_pre = 0;
 	if (!is_wind(P, id, ijk, xc)) {
-		udot_pre += FLD(S.T, T_RATE, id);
+		udot_pre += rate;
 		FLD(S.T, T_RATE, id) = 0;
 		FLD(S.T, T_HEAT, id) = 0;
 	}
@@ -1112,15 +1123,14 @@ __device__ __forceinline__ void b_thermo_update_fp64(const Params& P, const Stat
 		return;
 	}
 	const double dt = h * S.scal[0];
-	double u[7];
 #pragma unroll
-	for (int i = 0; i < NU; ++i) u[i] = FLD(S.U, i, id) + dt * (i == PRE ? udot_pre : 0.0);
+	for (int i = 0; i < NU; ++i) u[i] = u[i] + dt * (i == PRE ? udot_pre : 0.0);
 	if (!fix_solution(P, u)) atomicOr(S.err, ERRB_NAN);
 #pragma unroll
 	for (int i = 0; i < NU; ++i) FLD(S.U, i, id) = u[i];
 }
 __global__ void __launch_bounds__(256) k_thermo_update_fp64(Params P, State S, double h, int mode) {
-	if (P.batch) {
+	if (TRG_BATCHED && P.batch) {
 		const BatchTable& B = *P.batch;
 		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
 		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
@@ -1157,7 +1167,7 @@ __device__ __forceinline__ double block_min(double v) {
 // radiation call (the reference's static `once`), else -1.
 __device__ __forceinline__ void b_dt_reduce_fp64(const Params& P, const State& S, long long id, long long first_cell);
 __global__ void __launch_bounds__(256) k_dt_reduce_fp64(Params P, State S, long long first_cell) {
-	if (P.batch) {
+	if (TRG_BATCHED && P.batch) {
 		// grid ranges are padded to whole blocks: the block reduction stays within one grid
 		const BatchTable& B = *P.batch;
 		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
@@ -1233,7 +1243,7 @@ __device__ __forceinline__ void b_dt_reduce_fp64(const Params& P, const State& S
 // Torch::calculateTimeStep + the dt of Torch::fullStep (Torch.cpp:304-339, :394).
 __device__ __forceinline__ void b_dt_finalize(const Params& P, const State& S, double dt_next, int first_time, int step);
 __global__ void k_dt_finalize(Params P, State S, double dt_next, int first_time, int step) {
-	if (P.batch) {
+	if (TRG_BATCHED && P.batch) {
 		const int g = blockIdx.x * blockDim.x + threadIdx.x;
 		if (g < P.batch->G) b_dt_finalize(P.batch->P[g], P.batch->S[g], dt_next, first_time, step);
 		return;
@@ -1257,7 +1267,7 @@ __device__ __forceinline__ void b_dt_finalize(const Params& P, const State& S, d
 }
 
 __global__ void k_time_advance(Params P, State S) {
-	if (P.batch) {
+	if (TRG_BATCHED && P.batch) {
 		const int g = blockIdx.x * blockDim.x + threadIdx.x;
 		if (g < P.batch->G) P.batch->S[g].scal[1] += P.batch->S[g].scal[0];
 		return;
@@ -1273,7 +1283,7 @@ __device__ __forceinline__ void b_dt_reset(const Params& P, const State& S) {
 	slots[2] = big;
 }
 __global__ void k_dt_reset(Params P, State S) {
-	if (P.batch) {
+	if (TRG_BATCHED && P.batch) {
 		const int g = blockIdx.x * blockDim.x + threadIdx.x;
 		if (g < P.batch->G) b_dt_reset(P.batch->P[g], P.batch->S[g]);
 		return;

@@ -214,8 +214,8 @@ __device__ __forceinline__ bool infer_tile(unsigned char* sm, const uint4* __res
 	const float* Fs = reinterpret_cast<const float*>(W + IMG_F32);
 	bool ok = true;
 	uint32_t phase = 0;
-	float h[HID];
-	// layer 1 and layer 2: Z = A W, H = relu(Z + b) into the H tile
+	// layer 1 and layer 2: Z = A W, H = relu(Z + b) into the H tile, 16
+	// accumulator columns at a time (few live registers)
 #pragma unroll 1
 	for (int layer = 0; layer < 2; ++layer) {
 		if (t == 0) {
@@ -226,13 +226,16 @@ __device__ __forceinline__ bool infer_tile(unsigned char* sm, const uint4* __res
 		ok = mbar_wait(bar, phase) && ok;
 		phase ^= 1;
 		fence_after();
-#pragma unroll
-		for (int c = 0; c < HID / 16; ++c) tmem_ld16(tmem_row_addr(tm, 16 * c), h + 16 * c);
 		const float* b = Fs + (layer == 0 ? F_B1 : F_B2);
+#pragma unroll 1
+		for (int c = 0; c < HID / 16; ++c) {
+			float h[16];
+			tmem_ld16(tmem_row_addr(tm, 16 * c), h);
 #pragma unroll
-		for (int j = 0; j < HID; ++j) h[j] = fmaxf(h[j] + b[j], 0.0f);
-#pragma unroll
-		for (int c = 0; c < HID / 8; ++c) st_chunk(H, t, 8 * c, HID, h + 8 * c);
+			for (int j = 0; j < 16; ++j) h[j] = fmaxf(h[j] + b[16 * c + j], 0.0f);
+			st_chunk(H, t, 16 * c, HID, h);
+			st_chunk(H, t, 16 * c + 8, HID, h + 8);
+		}
 		sync_tc();
 	}
 	if (t == 0) {
