@@ -158,9 +158,11 @@ __device__ __forceinline__ bool fix_cons(const Scaled& P, float* u) {
 	return ok;
 }
 
-__device__ __forceinline__ float albada(float a, float b) {
+// `thr` is the reference's 1e-30 cut on a*b (code units) in the field's
+// scaled units: 1e-30 / s^2 for a field stored divided by s.
+__device__ __forceinline__ float albada(float a, float b, float thr) {
 	float ab = a * b;
-	return ab <= 1.0e-30f ? 0.f : ab * (a + b) / (a * a + b * b);
+	return ab <= thr ? 0.f : ab * (a + b) / (a * a + b * b);
 }
 __device__ __forceinline__ float minmod_(float a, float b) {
 	return (a * b > 0) ? (fabsf(a) < fabsf(b) ? a : b) : 0.f;
@@ -168,7 +170,7 @@ __device__ __forceinline__ float minmod_(float a, float b) {
 __device__ __forceinline__ float maxmod_(float a, float b) {
 	return (a * b > 0) ? (fabsf(a) > fabsf(b) ? a : b) : 0.f;
 }
-__device__ __forceinline__ float limiter32(int kind, float a, float b) {
+__device__ __forceinline__ float limiter32(int kind, float a, float b, float thr) {
 	switch (kind) {
 	case 0: return minmod_((a + b) * 0.5f, minmod_(2.f * a, 2.f * b));
 	case 1: return maxmod_(minmod_(b, 2.f * a), minmod_(2.f * b, a));
@@ -179,23 +181,27 @@ __device__ __forceinline__ float limiter32(int kind, float a, float b) {
 		float r = fabsf(a / b);
 		return (a + b * r) / (1.f + r);
 	}
-	case 5: return (a * b <= 1.0e-30f) ? 0.f : 1.5f * b * (a * a + a * b) / (a * a + a * b + b * b);
-	default: return albada(a, b);
+	case 5: return (a * b <= thr) ? 0.f : 1.5f * b * (a * a + a * b) / (a * a + a * b + b * b);
+	default: return albada(a, b, thr);
 	}
 }
 
 // Reconstructed face states: left = QR of cell c1 from (c0,c1,c2),
 // right = QL of cell c2 from (c1,c2,c3) (Hydro.cpp:44-50).
-__device__ __forceinline__ void reconstruct(int lim, const Prim& c0, const Prim& c1, const Prim& c2, const Prim& c3,
-                                            Prim& L, Prim& R) {
-#define REC(field)                                                                      \
+// Limiter cut-offs of the scaled fields (density, pressure, fractions, velocity).
+struct LimThr {
+	float d, p, x, v;
+};
+__device__ __forceinline__ void reconstruct(int lim, const LimThr& th, const Prim& c0, const Prim& c1, const Prim& c2,
+                                            const Prim& c3, Prim& L, Prim& R) {
+#define REC(field, thr)                                                                 \
 	{                                                                                   \
-		float sl = limiter32(lim, c1.field - c0.field, c2.field - c1.field);            \
-		float sr = limiter32(lim, c2.field - c1.field, c3.field - c2.field);            \
+		float sl = limiter32(lim, c1.field - c0.field, c2.field - c1.field, thr);       \
+		float sr = limiter32(lim, c2.field - c1.field, c3.field - c2.field, thr);       \
 		L.field = c1.field + 0.5f * sl;                                                 \
 		R.field = c2.field - 0.5f * sr;                                                 \
 	}
-	REC(d) REC(p) REC(x) REC(a) REC(v[0]) REC(v[1]) REC(v[2])
+	REC(d, th.d) REC(p, th.p) REC(x, th.x) REC(a, th.x) REC(v[0], th.v) REC(v[1], th.v) REC(v[2], th.v)
 #undef REC
 }
 
@@ -203,60 +209,70 @@ struct Flux {
 	float f[7];
 };
 
-// Physical flux and conserved state of a primitive state along unit normal n.
-__device__ __forceinline__ void flux_n(const Prim& q, const float* n, float g1inv, float& un, float* U, float* F) {
-	un = q.v[0] * n[0] + q.v[1] * n[1] + q.v[2] * n[2];
+// The normal-independent parts of a face's two states, computed once per
+// face and shared by the HLL and HLLC solves of the rotated solver:
+// conserved states and the normal-independent terms of the Einfeldt speeds
+// (characteristicWaveSpeeds, Riemann.cpp:27-42).
+struct FacePre {
+	float UL[7], UR[7];
+	float sl, sr, inv, c2, nu2;
+};
+__device__ __forceinline__ void cons_of(const Prim& q, float g1inv, float* U) {
 	float ke = 0.5f * q.d * (q.v[0] * q.v[0] + q.v[1] * q.v[1] + q.v[2] * q.v[2]);
-	float E = q.p * g1inv + ke;
-	float mflux = q.d * un;
 	U[DEN] = q.d;
-	U[PRE] = E;
+	U[PRE] = q.p * g1inv + ke;
 	U[HII] = q.d * q.x;
 	U[ADV] = q.d * q.a;
+	for (int k = 0; k < 3; ++k) U[VEL + k] = q.d * q.v[k];
+}
+__device__ __forceinline__ void face_pre(const Prim& L, const Prim& R, float gamma, float g1inv, FacePre& f) {
+	cons_of(L, g1inv, f.UL);
+	cons_of(R, g1inv, f.UR);
+	f.sl = sqrtf(L.d);
+	f.sr = sqrtf(R.d);
+	f.inv = 1.f / (f.sl + f.sr);
+	f.nu2 = 0.5f * f.sr * f.sl * f.inv * f.inv;
+	float aL2 = gamma * L.p / L.d, aR2 = gamma * R.p / R.d;
+	f.c2 = (f.sl * aL2 + f.sr * aR2) * f.inv;
+}
+// Physical flux of a state (conserved U) along unit normal n.
+__device__ __forceinline__ void flux_n(const Prim& q, const float* U, const float* n, float& un, float* F) {
+	un = q.v[0] * n[0] + q.v[1] * n[1] + q.v[2] * n[2];
+	float mflux = q.d * un;
 	F[DEN] = mflux;
-	F[PRE] = (E + q.p) * un;
+	F[PRE] = (U[PRE] + q.p) * un;
 	F[HII] = mflux * q.x;
 	F[ADV] = mflux * q.a;
-	for (int k = 0; k < 3; ++k) {
-		U[VEL + k] = q.d * q.v[k];
-		F[VEL + k] = mflux * q.v[k] + q.p * n[k];
-	}
+	for (int k = 0; k < 3; ++k) F[VEL + k] = mflux * q.v[k] + q.p * n[k];
 }
-
-// Einfeldt speeds along n (characteristicWaveSpeeds, Riemann.cpp:27-42).
-__device__ __forceinline__ void speeds_n(const Prim& L, const Prim& R, float unL, float unR, float gamma, float& SL,
-                                         float& SR) {
-	float sl = sqrtf(L.d), sr = sqrtf(R.d);
-	float inv = 1.f / (sl + sr);
-	float ut = (sl * unL + sr * unR) * inv;
-	float nu2 = 0.5f * sr * sl * inv * inv;
-	float aL2 = gamma * L.p / L.d, aR2 = gamma * R.p / R.d;
-	float d2 = (sl * aL2 + sr * aR2) * inv + nu2 * (unR - unL) * (unR - unL);
+__device__ __forceinline__ void speeds_n(const FacePre& f, float unL, float unR, float& SL, float& SR) {
+	float ut = (f.sl * unL + f.sr * unR) * f.inv;
+	float d2 = f.c2 + f.nu2 * (unR - unL) * (unR - unL);
 	float dd = sqrtf(d2);
 	SL = ut - dd;
 	SR = ut + dd;
 }
 
-__device__ __forceinline__ void hll_n(const Prim& L, const Prim& R, const float* n, float gamma, float g1inv, float* F) {
-	float UL[7], FL[7], UR[7], FR[7], unL, unR, SL, SR;
-	flux_n(L, n, g1inv, unL, UL, FL);
-	flux_n(R, n, g1inv, unR, UR, FR);
-	speeds_n(L, R, unL, unR, gamma, SL, SR);
+__device__ __forceinline__ void hll_n(const Prim& L, const Prim& R, const FacePre& f, const float* n, float* F) {
+	float FL[7], FR[7], unL, unR, SL, SR;
+	flux_n(L, f.UL, n, unL, FL);
+	flux_n(R, f.UR, n, unR, FR);
+	speeds_n(f, unL, unR, SL, SR);
 	if (SR <= 0) {
 		for (int i = 0; i < 7; ++i) F[i] = FR[i];
 	} else if (SL >= 0) {
 		for (int i = 0; i < 7; ++i) F[i] = FL[i];
 	} else {
 		float inv = 1.f / (SR - SL);
-		for (int i = 0; i < 7; ++i) F[i] = (SR * FL[i] - SL * FR[i] + SL * SR * (UR[i] - UL[i])) * inv;
+		for (int i = 0; i < 7; ++i) F[i] = (SR * FL[i] - SL * FR[i] + SL * SR * (f.UR[i] - f.UL[i])) * inv;
 	}
 }
 
-__device__ __forceinline__ void hllc_n(const Prim& L, const Prim& R, const float* n, float gamma, float g1inv, float* F) {
-	float UL[7], FL[7], UR[7], FR[7], unL, unR, SL, SR;
-	flux_n(L, n, g1inv, unL, UL, FL);
-	flux_n(R, n, g1inv, unR, UR, FR);
-	speeds_n(L, R, unL, unR, gamma, SL, SR);
+__device__ __forceinline__ void hllc_n(const Prim& L, const Prim& R, const FacePre& f, const float* n, float* F) {
+	float FL[7], FR[7], unL, unR, SL, SR;
+	flux_n(L, f.UL, n, unL, FL);
+	flux_n(R, f.UR, n, unR, FR);
+	speeds_n(f, unL, unR, SL, SR);
 	if (SL >= 0) {
 		for (int i = 0; i < 7; ++i) F[i] = FL[i];
 	} else if (SR <= 0) {
@@ -266,7 +282,7 @@ __device__ __forceinline__ void hllc_n(const Prim& L, const Prim& R, const float
 		float Sc = (R.p - L.p + mL * unL - mR * unR) / (mL - mR);
 		bool left = Sc >= 0;
 		const Prim& K = left ? L : R;
-		const float* UK = left ? UL : UR;
+		const float* UK = left ? f.UL : f.UR;
 		const float* FK = left ? FL : FR;
 		float SK = left ? SL : SR, unK = left ? unL : unR;
 		float mK = K.d * (SK - unK);
@@ -291,16 +307,18 @@ __device__ __forceinline__ void hllc_n(const Prim& L, const Prim& R, const float
 __device__ __forceinline__ void riemann32(int kind, const Prim& L, const Prim& R, int dim, float gamma, float* F) {
 	const float g1inv = 1.f / (gamma - 1.f);
 	const float d[3] = {dim == 0 ? 1.f : 0.f, dim == 1 ? 1.f : 0.f, dim == 2 ? 1.f : 0.f};
-	if (kind == RS_HLLC) { hllc_n(L, R, d, gamma, g1inv, F); return; }
-	if (kind == RS_HLL) { hll_n(L, R, d, gamma, g1inv, F); return; }
+	FacePre f;
+	face_pre(L, R, gamma, g1inv, f);
+	if (kind == RS_HLLC) { hllc_n(L, R, f, d, F); return; }
+	if (kind == RS_HLL) { hll_n(L, R, f, d, F); return; }
 	const float dv[3] = {R.v[0] - L.v[0], R.v[1] - L.v[1], R.v[2] - L.v[2]};
 	const float par = dv[0] * d[0] + dv[1] * d[1] + dv[2] * d[2];  // exact: one term is non-zero
 	const float perp[3] = {dv[0] - par * d[0], dv[1] - par * d[1], dv[2] - par * d[2]};  // exact
 	const float pp = perp[0] * perp[0] + perp[1] * perp[1] + perp[2] * perp[2];
 	const float rr = par * par + pp;
-	if (rr < 1.0e-12f) { hllc_n(L, R, d, gamma, g1inv, F); return; }  // |dv| < 1e-6
-	if (pp == 0.f) { hll_n(L, R, d, gamma, g1inv, F); return; }        // dv parallel to d
-	if (par == 0.f) { hllc_n(L, R, d, gamma, g1inv, F); return; }     // dv normal to d
+	if (rr < 1.0e-12f) { hllc_n(L, R, f, d, F); return; }  // |dv| < 1e-6
+	if (pp == 0.f) { hll_n(L, R, f, d, F); return; }        // dv parallel to d
+	if (par == 0.f) { hllc_n(L, R, f, d, F); return; }     // dv normal to d
 	const float r = sqrtf(rr), s = sqrtf(pp);
 	const float inv_r = 1.f / r;
 	const float sg = par < 0 ? -1.f : 1.f;
@@ -309,8 +327,8 @@ __device__ __forceinline__ void riemann32(int kind, const Prim& L, const Prim& R
 	const float k2 = par * inv_r / s;
 	const float n2[3] = {sinv * d[0] - k2 * perp[0], sinv * d[1] - k2 * perp[1], sinv * d[2] - k2 * perp[2]};
 	float F1[7], F2[7];
-	hll_n(L, R, n1, gamma, g1inv, F1);
-	hllc_n(L, R, n2, gamma, g1inv, F2);
+	hll_n(L, R, f, n1, F1);
+	hllc_n(L, R, f, n2, F2);
 #pragma unroll
 	for (int i = 0; i < 7; ++i) F[i] = cosv * F1[i] + sinv * F2[i];
 }
@@ -407,12 +425,13 @@ using namespace f32;
 // Reconstruction + Riemann solve for one face (the single call site of the
 // solver in the kernel keeps the instruction footprint small).
 template <int LIM, int RS>
-__device__ __forceinline__ void face_flux(int order, int lim_rt, int rs_rt, const Prim& c0, const Prim& c1, const Prim& c2,
+__device__ __forceinline__ void face_flux(int order, int lim_rt, int rs_rt, const LimThr& th, const Prim& c0, const Prim& c1,
+                                          const Prim& c2,
                                           const Prim& c3, int dim, float gamma, float* F) {
 	Prim L, R;
 	if (order == 1) {
 		const int lim = LIM >= 0 ? LIM : lim_rt;
-		reconstruct(lim, c0, c1, c2, c3, L, R);
+		reconstruct(lim, th, c0, c1, c2, c3, L, R);
 	} else {
 		L = c1;
 		R = c2;
@@ -452,6 +471,8 @@ __global__ void __launch_bounds__(BX* BY, 2)
 	const int gx = x0 + tx, gy = y0 + ty;
 	const bool active = gx < P.nx && gy < P.ny;
 	const int order = P.order, lim_rt = P.limiter, rs_rt = P.riemann;
+	const LimThr th{(float)(1.0e-30 / (P.f32_rho0 * P.f32_rho0)), (float)(1.0e-30 / (P.f32_p0 * P.f32_p0)), 1.0e-30f,
+	                (float)(1.0e-30 / (P.f32_v0 * P.f32_v0))};
 	// face counts of one plane (x faces, y faces, z faces at z + 1/2)
 	const int nfx = (BX + 1) * BY, nfy = nd > 1 ? BX * (BY + 1) : 0, nfz = nd > 2 ? BX * BY : 0;
 	double tmin = 1.0e308;
@@ -484,7 +505,7 @@ __global__ void __launch_bounds__(BX* BY, 2)
 		Prim c0 = get(s, slot_of(z0 - 2), ty + HALO, tx + HALO), c1 = get(s, slot_of(z0 - 1), ty + HALO, tx + HALO);
 		Prim c2 = get(s, slot_of(z0), ty + HALO, tx + HALO), c3 = get(s, slot_of(z0 + 1), ty + HALO, tx + HALO);
 		float F[7];
-		face_flux<LIM, RS>(order, lim_rt, rs_rt, c0, c1, c2, c3, 2, gamma, F);
+		face_flux<LIM, RS>(order, lim_rt, rs_rt, th, c0, c1, c2, c3, 2, gamma, F);
 #pragma unroll
 		for (int i = 0; i < 7; ++i) Fz[i * BX * BY + threadIdx.x] = F[i];
 	}
@@ -525,7 +546,7 @@ __global__ void __launch_bounds__(BX* BY, 2)
 				c2 = get(s, slot_of(z + 1), ly, lx); c3 = get(s, slot_of(z + 2), ly, lx);
 			}
 			float F[7];
-			face_flux<LIM, RS>(order, lim_rt, rs_rt, c0, c1, c2, c3, dim, gamma, F);
+			face_flux<LIM, RS>(order, lim_rt, rs_rt, th, c0, c1, c2, c3, dim, gamma, F);
 			if (dim == 0) {
 #pragma unroll
 				for (int i = 0; i < 7; ++i) Fx[(i * BY + b) * (BX + 1) + a] = F[i];
