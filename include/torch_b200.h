@@ -157,6 +157,29 @@ enum {
 	TRG_STAT_FRONT_CELLS = 18,      /* front cells (tau < 20, x_HII < 0.99): the learned start's domain */
 	TRG_STAT_FRONT_ITERS = 19       /* Picard iterations of the front cells */
 };
+/* Heating and cooling diagnostics (Thermodynamics::fillHeatingArrays,
+ * src/Integrators/Thermodynamics.cpp:419-461, as printed by
+ * DataPrinter::printHeating at every checkpoint of Torch::run): with
+ * trg_heating_enable(c, 1) the step keeps the terms it produces (EUV heating
+ * and recombination cooling of the radiation module, the total rate of the
+ * thermal sub-cycles); trg_heating then runs the column-density sweep and the
+ * remaining terms and copies the 11 fields [11][N] (code units, in the order
+ * IMLC NMLC RHII CEHI CIEC NMC EUVH FUVH IRH CRH TOT) to H. */
+#define TRG_NHEAT 11
+int trg_heating_enable(trg_ctx* c, int on);
+int trg_heating(trg_ctx* c, double* H);
+
+/* Checkpoint / restart (the reference restarts from its text snapshots,
+ * src/IO/DataReader.cpp:18-125, which hold the primitives only): the whole
+ * step state - U, Q, R (radiation), T (thermodynamics), T_min, the FP32
+ * state, time, time step and the split's counters - as one binary blob of
+ * trg_checkpoint_bytes(c) bytes.  trg_checkpoint_load restores it into a
+ * context created with the same parameters and grid; stepping on is
+ * bit-identical to the run that was saved. */
+long long trg_checkpoint_bytes(const trg_ctx* c);
+int trg_checkpoint_save(trg_ctx* c, void* buf, long long bytes);
+int trg_checkpoint_load(trg_ctx* c, const void* buf, long long bytes);
+
 /* Tile autotuner (no counterpart in the reference): for the FP32 form, times
  * the fused hydro stage kernel on this grid for a range of CTA tile depths
  * (z planes marched by one CTA) and keeps the fastest; the trials write only

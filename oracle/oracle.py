@@ -217,8 +217,9 @@ def read_trgs(path: str) -> State:
 
 
 def run_reference(params_path: str, ic_path: Optional[str], steps: int, workdir: str,
-                  setup_path: Optional[str] = None, timeout: float = 600) -> State:
-    """Runs the reference binary on a case in a fresh process and returns its final state."""
+                  setup_path: Optional[str] = None, timeout: float = 600, print2d: Optional[str] = None) -> State:
+    """Runs the reference binary on a case in a fresh process and returns its final state
+    (with `print2d`, the reference also writes its checkpoint files of that state there)."""
     binp = build_reference()
     if binp is None:
         raise FileNotFoundError("reference build unavailable (oracle/_ref/torch_ref)")
@@ -228,6 +229,8 @@ def run_reference(params_path: str, ic_path: Optional[str], steps: int, workdir:
         cmd.append(f"--ic={ic_path}")
     if setup_path:
         cmd.append(f"--setup={setup_path}")
+    if print2d:
+        cmd.append(f"--print2d={print2d}")
     r = subprocess.run(cmd, cwd=workdir, capture_output=True, text=True, timeout=timeout)
     if r.returncode != 0:
         raise RuntimeError(f"reference failed ({r.returncode}): {r.stderr[-2000:]}")

@@ -18,7 +18,9 @@
  *                                  step is offered dt_next_checkpoint = dt_max.
  *
  * Output: a binary state dump (format "TRGS", see write_state below) of the
- * interior cells in the reference's flat index order (x fastest).
+ * interior cells in the reference's flat index order (x fastest); with
+ * --print2d=DIR also the reference's own checkpoint files of the final state
+ * (DataPrinter::print2D and ::printHeating after fillHeatingArrays).
  *
  * Each invocation is one fresh process, because the reference keeps
  * function-local statics (Torch.cpp:305, Radiation.cpp:79, Radiation.cpp:300).
@@ -93,7 +95,7 @@ static void write_state(const std::string& path, Torch& torch, const std::vector
 }
 
 int main(int argc, char** argv) {
-	std::string params, setup, ic, out, out0;
+	std::string params, setup, ic, out, out0, print2d;
 	long steps = 0;
 	int print_params = 0;
 	for (int i = 1; i < argc; ++i) {
@@ -104,10 +106,11 @@ int main(int argc, char** argv) {
 		else if ((v = arg_value(argv[i], "--steps="))) steps = atol(v);
 		else if ((v = arg_value(argv[i], "--out="))) out = v;
 		else if ((v = arg_value(argv[i], "--out0="))) out0 = v;
+		else if ((v = arg_value(argv[i], "--print2d="))) print2d = v;
 		else if (strcmp(argv[i], "--print-params") == 0) print_params = 1;
 		else {
 			fprintf(stderr, "usage: torch_ref --params=P.lua [--setup=S.lua] [--ic=IC_000.txt] "
-			                "--steps=N --out=final.bin [--out0=initial.bin]\n");
+			                "--steps=N --out=final.bin [--out0=initial.bin] [--print2d=DIR]\n");
 			return 2;
 		}
 	}
@@ -173,6 +176,18 @@ int main(int argc, char** argv) {
 		}
 		if (!out.empty())
 			write_state(out, torch, dts);
+		if (!print2d.empty()) {
+			/* What Torch::run writes at a checkpoint (src/Torch/Torch.cpp:270-281):
+			 * fillHeatingArrays, then DataPrinter::printHeating and ::print2D,
+			 * here into <print2d>/heating_final.txt.gz and data2D_final.txt.gz. */
+			torch.thermodynamics.fillHeatingArrays(torch.fluid);
+			torch.inputOutput.dir2D = print2d;
+			torch.inputOutput.printing_on = true;
+			std::remove((print2d + "/heating_final.txt.gz").c_str());
+			std::remove((print2d + "/data2D_final.txt.gz").c_str());
+			torch.inputOutput.printHeating("final", torch.fluid.getGrid().currentTime, torch.fluid.getGrid());
+			torch.inputOutput.print2D("final", torch.fluid.getGrid().currentTime, torch.fluid.getGrid());
+		}
 	}
 	catch (std::exception& e) {
 		fprintf(stderr, "torch_ref: reference threw: %s\n", e.what());

@@ -5,9 +5,13 @@ container):  python tests/golden/make_golden.py
 
 For each case of tests/cases.py it writes <case>.npz holding the exact Lua
 parameter text and initial-condition text the reference read, the number of
-full steps, and the reference's final U, Q, R, T, T_min and dt history.
+full steps, and the reference's final U, Q, R, T, T_min and dt history.  For
+the cases of CHECKPOINT_CASES it also keeps the reference's own checkpoint
+files of the final state (DataPrinter::print2D and ::printHeating after
+fillHeatingArrays) as ckpt_<case>_data2D.txt.gz and ckpt_<case>_heating.txt.gz.
 """
 import os
+import shutil
 import sys
 import tempfile
 
@@ -24,6 +28,9 @@ import oracle  # noqa: E402
 from torch_b200 import config  # noqa: E402
 
 
+CHECKPOINT_CASES = ("blister_small", "hii3d_small")
+
+
 def make(name):
     with tempfile.TemporaryDirectory() as d:
         tp, ic, text, steps = cases.build(name, d)
@@ -31,7 +38,12 @@ def make(name):
         ppath = os.path.join(d, "params.lua")
         with open(ppath, "w") as f:
             f.write(params)
-        ref = oracle.run_reference(ppath, os.path.join(d, "ic_000.txt"), steps, d)
+        ref = oracle.run_reference(ppath, os.path.join(d, "ic_000.txt"), steps, d,
+                                   print2d=d if name in CHECKPOINT_CASES else None)
+        if name in CHECKPOINT_CASES:
+            for kind in ("data2D", "heating"):
+                shutil.copyfile(os.path.join(d, f"{kind}_final.txt.gz"),
+                                os.path.join(HERE, f"ckpt_{name}_{kind}.txt.gz"))
     out = os.path.join(HERE, f"{name}.npz")
     np.savez_compressed(out, params_lua=np.array(params), ic_text=np.array(text), steps=np.array(steps),
                         U=ref.U, Q=ref.Q, R=ref.R, T=ref.T, Tmin=ref.Tmin, dts=ref.dts, time=np.array(ref.time))

@@ -97,6 +97,11 @@ _SIGNATURES = [
     ("trg_profile_read", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
     ("trg_stats_enable", C.c_int, [C.c_void_p, C.c_int]),
     ("trg_autotune", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    ("trg_checkpoint_bytes", C.c_longlong, [C.c_void_p]),
+    ("trg_heating_enable", C.c_int, [C.c_void_p, C.c_int]),
+    ("trg_heating", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("trg_checkpoint_save", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
+    ("trg_checkpoint_load", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
     ("trg_mlp_create", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     ("trg_mlp_get_params", C.c_int, [C.c_void_p, C.c_void_p]),
     ("trg_mlp_set_params", C.c_int, [C.c_void_p, C.c_void_p]),
@@ -366,6 +371,27 @@ class Torch:
             if got < 0:
                 raise TrgError(-got, "trg_harvest_read failed")
         return out, n
+
+    def heating_enable(self, on: bool = True):
+        """Keep the heating/cooling terms during the step (for heating())."""
+        self._check(self.lib.trg_heating_enable(self.ctx, int(on)))
+
+    def heating(self) -> np.ndarray:
+        """Thermodynamics::fillHeatingArrays: the 11 terms [11, N] in code units."""
+        H = np.zeros((11, self.N), dtype=np.float64)
+        self._check(self.lib.trg_heating(self.ctx, H.ctypes.data_as(C.c_void_p)))
+        return H
+
+    def checkpoint(self) -> bytes:
+        """The whole step state as bytes (trg_checkpoint_save)."""
+        n = int(self.lib.trg_checkpoint_bytes(self.ctx))
+        buf = (C.c_char * n)()
+        self._check(self.lib.trg_checkpoint_save(self.ctx, buf, n))
+        return bytes(buf)
+
+    def restore(self, blob: bytes):
+        """Continues from a checkpoint of a run with the same parameters and grid."""
+        self._check(self.lib.trg_checkpoint_load(self.ctx, blob, len(blob)))
 
     def autotune(self):
         """Tile depth of the FP32 hydro kernel chosen by timing; (zchunk, ms per launch)."""

@@ -54,6 +54,7 @@ struct trg_ctx {
 	float* U32 = nullptr;
 	float* U32s = nullptr;
 	unsigned char* mlp_img = nullptr;
+	double* d_heat = nullptr;
 	int zchunk = 64;
 	std::vector<void*> allocs;
 	int first_time = 1;
@@ -644,6 +645,88 @@ int trg_set_conserved(trg_ctx* c, const double* U) {
 	return TRG_OK;
 }
 
+// ---------------------------------------------------------- checkpoints
+namespace {
+struct CkptHeader {
+	char magic[8];
+	int version, form;  // form: 0 FP64, 1 FP32 hydro-only, 2 FP32 with radiation/cooling
+	long long N;
+	int nx, ny, nz, nd;
+	long long steps;
+	int first_time, rad_once_pending, stepCounter, pad;
+	double scal[8];
+};
+int ckpt_form(const trg_ctx* c) { return c->fp32 ? 1 : (c->mixed ? 2 : 0); }
+}  // namespace
+
+long long trg_checkpoint_bytes(const trg_ctx* c) {
+	if (!c) return 0;
+	const long long N = c->P.N;
+	return (long long)sizeof(CkptHeader) + (7 + 7 + 6 + 4 + 1) * N * (long long)sizeof(double) +
+	       (c->fp32 ? 7 * N * (long long)sizeof(float) : 0);
+}
+
+int trg_checkpoint_save(trg_ctx* c, void* buf, long long bytes) {
+	if (!c || !buf || bytes < trg_checkpoint_bytes(c)) return TRG_ERR_ARG;
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	CkptHeader h{};
+	memcpy(h.magic, "TRGCKPT1", 8);
+	h.version = 1;
+	h.form = ckpt_form(c);
+	h.N = c->P.N;
+	h.nx = c->P.nx;
+	h.ny = c->P.ny;
+	h.nz = c->P.nz;
+	h.nd = c->P.nd;
+	h.steps = c->steps;
+	h.first_time = c->first_time;
+	h.rad_once_pending = c->rad_once_pending;
+	h.stepCounter = c->stepCounter;
+	CUDA_TRY(cudaMemcpy(h.scal, c->S.scal, sizeof(h.scal), cudaMemcpyDeviceToHost));
+	char* p = static_cast<char*>(buf);
+	memcpy(p, &h, sizeof(h));
+	p += sizeof(h);
+	const long long N = c->P.N;
+	const std::pair<const double*, long long> arrs[] = {
+	    {c->S.U, 7 * N}, {c->S.Q, 7 * N}, {c->S.R, 6 * N}, {c->S.T, 4 * N}, {c->S.Tmin, N}};
+	for (auto& a : arrs) {
+		CUDA_TRY(cudaMemcpy(p, a.first, a.second * sizeof(double), cudaMemcpyDeviceToHost));
+		p += a.second * sizeof(double);
+	}
+	if (c->fp32) CUDA_TRY(cudaMemcpy(p, c->U32, 7 * N * sizeof(float), cudaMemcpyDeviceToHost));
+	return TRG_OK;
+}
+
+int trg_checkpoint_load(trg_ctx* c, const void* buf, long long bytes) {
+	if (!c || !buf || bytes < (long long)sizeof(CkptHeader)) return TRG_ERR_ARG;
+	CkptHeader h;
+	memcpy(&h, buf, sizeof(h));
+	if (memcmp(h.magic, "TRGCKPT1", 8) != 0 || h.version != 1)
+		return set_error(c, TRG_ERR_ARG, "trg_checkpoint_load: not a checkpoint of this library");
+	if (h.form != ckpt_form(c) || h.N != c->P.N || h.nx != c->P.nx || h.ny != c->P.ny || h.nz != c->P.nz ||
+	    h.nd != c->P.nd || bytes < trg_checkpoint_bytes(c))
+		return set_error(c, TRG_ERR_ARG, "trg_checkpoint_load: the checkpoint is of another grid or form");
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	const char* p = static_cast<const char*>(buf) + sizeof(h);
+	const long long N = c->P.N;
+	const std::pair<double*, long long> arrs[] = {
+	    {c->S.U, 7 * N}, {c->S.Q, 7 * N}, {c->S.R, 6 * N}, {c->S.T, 4 * N}, {c->S.Tmin, N}};
+	for (auto& a : arrs) {
+		CUDA_TRY(cudaMemcpy(a.first, p, a.second * sizeof(double), cudaMemcpyHostToDevice));
+		p += a.second * sizeof(double);
+	}
+	if (c->fp32) CUDA_TRY(cudaMemcpy(c->U32, p, 7 * N * sizeof(float), cudaMemcpyHostToDevice));
+	CUDA_TRY(cudaMemcpy(c->S.scal, h.scal, sizeof(h.scal), cudaMemcpyHostToDevice));
+	CUDA_TRY(cudaMemset(c->S.UDOT, 0, 7 * N * sizeof(double)));
+	c->steps = h.steps;
+	c->first_time = h.first_time;
+	c->rad_once_pending = h.rad_once_pending;
+	c->stepCounter = h.stepCounter;
+	int rc = ensure_dt_hist(c, c->steps + 1);
+	if (rc) return rc;
+	return TRG_OK;
+}
+
 int trg_synchronize(trg_ctx* c) {
 	if (!c) return TRG_ERR_ARG;
 	CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -687,6 +770,33 @@ int trg_stats(trg_ctx* c, unsigned long long* out, int reset) {
 		CUDA_TRY(cudaMemsetAsync(c->S.stats, 0, TRG_NSTATS * sizeof(unsigned long long), c->stream));
 		CUDA_TRY(cudaStreamSynchronize(c->stream));
 	}
+	return TRG_OK;
+}
+
+int trg_heating_enable(trg_ctx* c, int on) {
+	if (!c) return TRG_ERR_ARG;
+	if (c->fp32) return set_error(c, TRG_ERR_ARG, "trg_heating_enable: hydro-only FP32 runs have no heating terms");
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	if (on && !c->S.H) {
+		if (!c->d_heat && dalloc(c, &c->d_heat, (size_t)NH * c->P.N)) return TRG_ERR_OOM;
+		CUDA_TRY(cudaMemset(c->d_heat, 0, (size_t)NH * c->P.N * sizeof(double)));
+		c->S.H = c->d_heat;
+	} else if (!on) {
+		c->S.H = nullptr;
+	}
+	drop_graphs(c);
+	return TRG_OK;
+}
+
+int trg_heating(trg_ctx* c, double* H) {
+	if (!c || !H) return TRG_ERR_ARG;
+	if (!c->S.H) return set_error(c, TRG_ERR_ARG, "trg_heating: call trg_heating_enable before stepping");
+	// Thermodynamics::fillHeatingArrays: rayTrace, then the per-cell terms
+	if (c->P.star_on) colden_sweep(c);
+	LAUNCH(KF(k_heating_arrays_fp64), c->P.N, 256, c->P, c->S);
+	int rc = check_device_error(c);
+	if (rc) return rc;
+	CUDA_TRY(cudaMemcpy(H, c->S.H, (size_t)NH * c->P.N * sizeof(double), cudaMemcpyDeviceToHost));
 	return TRG_OK;
 }
 

@@ -839,6 +839,11 @@ __device__ __forceinline__ void b_rad_heating_fp64(const Params& P, const State&
 	if (T < Tmin + 200 && rate < 0.0) softrate = smin(0.0, softrate * (T - Tmin) / 200.0);
 	softrate *= P.heating_amp;
 	FLD(S.R, R_HEAT, id) = softrate;
+	if (S.H) {
+		// Radiation.cpp:278-279 (0/0 when rate is 0, as in the reference)
+		FLD(S.H, H_EUVH, id) = photoion * (softrate / rate);
+		FLD(S.H, H_RHII, id) = -recombination * (softrate / rate);
+	}
 	if (rate != rate) atomicOr(S.err, ERRB_NAN);
 }
 __global__ void __launch_bounds__(256) k_rad_heating_fp64(Params P, State S) {
@@ -1042,6 +1047,8 @@ __device__ __forceinline__ void b_thermo_integrate_fp64(const Params& P, const S
 	cell_xc(P, ijk, xc);
 	if (is_wind(P, id, ijk, xc)) return;
 	if (FLD(S.Q, ADV, id) < P.thermo_hii_switch) {
+		if (S.H)
+			for (int i = 0; i < NH; ++i) FLD(S.H, i, id) = 0;
 		FLD(S.T, T_RATE, id) = 0;
 		return;
 	}
@@ -1087,6 +1094,7 @@ __device__ __forceinline__ void b_thermo_integrate_fp64(const Params& P, const S
 		}
 	}
 	FLD(S.T, T_RATE, id) = (pressure - qpre) * dpre2rate;
+	if (S.H) FLD(S.H, H_TOT, id) = FLD(S.T, T_RATE, id);  // Thermodynamics.cpp:335
 }
 __global__ void __launch_bounds__(256) k_thermo_integrate_fp64(Params P, State S, double h) {
 	if (TRG_BATCHED && P.batch) {
@@ -1140,6 +1148,46 @@ __global__ void __launch_bounds__(256) k_thermo_update_fp64(Params P, State S, d
 	const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
 	if (id >= P.N) return;
 	b_thermo_update_fp64(P, S, id, h, mode);
+}
+
+// Thermodynamics::fillHeatingArrays (Thermodynamics.cpp:419-461) after its
+// rayTrace (the column-density sweep, launched before), non-wind cells.
+// Single grids only.
+__global__ void __launch_bounds__(256) k_heating_arrays_fp64(Params P, State S) {
+	const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	int ijk[3];
+	double xc[3];
+	cell_ijk(P, id, ijk);
+	cell_xc(P, ijk, xc);
+	if (is_wind(P, id, ijk, xc)) return;
+	if (FLD(S.Q, ADV, id) < P.thermo_hii_switch) {
+		for (int i = 0; i < NH; ++i) FLD(S.H, i, id) = 0;
+		return;
+	}
+	double nH = P.X * FLD(S.Q, DEN, id) / P.hydrogenMass;
+	double x = FLD(S.Q, HII, id);
+	double ne = x * nH;
+	double nn = (1.0 - x) * nH;
+	double T = calc_temperature(P, x, FLD(S.Q, PRE, id), FLD(S.Q, DEN, id));
+	double rsqrd = 0, F_FUV = 0;
+	if (P.star_on) {
+#pragma unroll
+		for (int i = 0; i < 3; ++i)
+			if (i < P.nd) rsqrd += (xc[i] - P.sxc[i]) * (xc[i] - P.sxc[i]) * P.dx[i] * P.dx[i];
+		double Q_FUV = 0.5 * P.photonRate;
+		F_FUV = rsqrd != 0 ? Q_FUV / (1.2e7 * 4 * P.pi * rsqrd) : 0;
+	}
+	double Av_FUV = 1.086 * P.dustXsec * FLD(S.T, T_COL_DEN, id);
+	FLD(S.H, H_FUVH, id) = th_fuvh(P, nH, Av_FUV, F_FUV);
+	FLD(S.H, H_IRH, id) = th_irh(P, nH, Av_FUV, F_FUV);
+	FLD(S.H, H_CRH, id) = P.crh * nH;
+	FLD(S.H, H_IMLC, id) = -th_imlc(P, ne, T);
+	FLD(S.H, H_NMLC, id) = -th_nmlc(P, ne, nn, T);
+	FLD(S.H, H_CEHI, id) = -th_cxhi(P, S, nH, x, T);
+	FLD(S.H, H_CIEC, id) = -th_ciec(P, ne, T);
+	FLD(S.H, H_NMC, id) = -th_nmc(P, nH, x, T);
+	FLD(S.H, H_TOT, id) += FLD(S.H, H_RHII, id) + FLD(S.H, H_EUVH, id);
 }
 
 // ----------------------------------------------------------------- time step

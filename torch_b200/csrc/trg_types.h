@@ -8,6 +8,8 @@ namespace trg {
 enum { DEN = 0, PRE = 1, HII = 2, ADV = 3, VEL = 4, NU = 7 };
 enum { R_HII_A = 0, R_TAU, R_TAU_A, R_DTAU, R_DTAU_A, R_HEAT, NR };
 enum { T_COL_DEN = 0, T_DCOL_DEN, T_HEAT, T_RATE, NT };
+// heating / cooling diagnostics (HID, src/Torch/Common.hpp:32-34)
+enum { H_IMLC = 0, H_NMLC, H_RHII, H_CEHI, H_CIEC, H_NMC, H_EUVH, H_FUVH, H_IRH, H_CRH, H_TOT, NH };
 enum { G_CART = 0, G_CYL = 1, G_SPH = 2 };
 enum { BC_FREE = 0, BC_REFLECTING = 1, BC_OUTFLOW = 2, BC_INFLOW = 3, BC_PERIODIC = 4 };
 enum { CP_TTI = 0, CP_NEQ = 1, CP_OFF = 2 };
@@ -88,6 +90,9 @@ struct State {
 	double* dt_hist;
 	// diagnostic counters, TRG_STAT_* indices of the C ABI header
 	unsigned long long* stats;
+	// heating / cooling diagnostics [NH][N], kept up to date during the step
+	// when non-null (trg_heating_enable)
+	double* H;
 	// learned starting iterate: the network's inference image (null = plain solve)
 	const unsigned char* mlp_img;
 	// training-set recording by the plain solve: records of 8 floats
