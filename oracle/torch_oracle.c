@@ -1049,8 +1049,72 @@ static int update_hii_frac(orc_ctx* c, double dt, long id) {
 	return 0;
 }
 
+static int update_hii_frac2(orc_ctx* c, double dt, long id) {
+	/* Radiation::update_HIIfrac for the implicit2 and explicit schemes,
+	 * Radiation.cpp:375-478: implicit2 iterates with tau_avg = TAU; explicit
+	 * takes one doric step whose time-averaged result becomes Q[HII]. */
+	if (is_star(c, id)) {
+		FLD(c->R, R_HEAT, id) = 0;
+		FLD(c->Q, HII, id) = 1;
+		FLD(c->R, R_HII_A, id) = 1;
+		return 0;
+	}
+	if (c->p.rt_scheme == 1) {
+		double saved = FLD(c->R, R_TAU_A, id);
+		FLD(c->R, R_TAU_A, id) = FLD(c->R, R_TAU, id);  /* the iteration's tau_avg */
+		int e = update_hii_frac(c, dt, id);
+		FLD(c->R, R_TAU_A, id) = saved;
+		return e;
+	}
+	double n_H = c->X * FLD(c->Q, DEN, id) / c->hydrogenMass;
+	double x = FLD(c->Q, HII, id);
+	double x_avg = x;
+	double T = calc_temperature(c, FLD(c->Q, HII, id), FLD(c->Q, PRE, id), FLD(c->Q, DEN, id));
+	double alphaB = spline_eval(&c->rad_recomb, T);
+	double A_ci = collisional_ionisation_rate(c, T);
+	double tau = FLD(c->R, R_TAU, id), dtau = FLD(c->R, R_DTAU, id);
+	double nHI = (1.0 - x) * (c->X * FLD(c->Q, DEN, id) / c->hydrogenMass);
+	double A_pi = photoionisation_rate(nHI, tau, dtau, c->shellVol[id], c->photonRate);
+	double nHII_aB = x_avg * n_H * alphaB;
+	double nHII_Aci = x_avg * n_H * A_ci;
+	double x_dummy = x;
+	doric(dt, &x, &x_dummy, A_pi, nHII_aB, nHII_Aci);
+	FLD(c->Q, HII, id) = x;
+	if (x > 0.001) FLD(c->Q, ADV, id) = 1;
+	return 0;
+}
+
+static int transfer_radiation2(orc_ctx* c, double dt) {
+	/* Radiation::transferRadiation2, Radiation.cpp:508-567, with rayTrace,
+	 * :480-506 (single rank): the causal sweep only interpolates TAU and sets
+	 * the cell optical depths from the current fractions; the fractions are
+	 * then updated cell by cell, independently.  Star on (the caller's test). */
+	for (long w = 0; w < c->nwind; ++w) {
+		long id = c->wind[w];
+		FLD(c->R, R_TAU, id) = 0;
+		FLD(c->R, R_TAU_A, id) = 0;
+		FLD(c->R, R_DTAU, id) = 0;
+		FLD(c->R, R_DTAU_A, id) = 0;
+		FLD(c->Q, HII, id) = 1;
+		FLD(c->R, R_HII_A, id) = 1;
+	}
+	for (long k = 0; k < c->nnonwind; ++k) {
+		long id = c->nonwind[k];
+		update_tau_sc(c, 0, id, cell_dist2(c, id));
+		double nH = c->X * FLD(c->Q, DEN, id) / c->hydrogenMass;
+		FLD(c->R, R_DTAU, id) = (1.0 - FLD(c->Q, HII, id)) * nH * c->photoIonXsec * c->ds[id];
+		FLD(c->R, R_DTAU_A, id) = (1.0 - FLD(c->R, R_HII_A, id)) * nH * c->photoIonXsec * c->ds[id];
+	}
+	for (long k = 0; k < c->nnonwind; ++k) {
+		int e = update_hii_frac2(c, dt, c->nonwind[k]);
+		if (e) return e;
+	}
+	return 0;
+}
+
 static int transfer_radiation(orc_ctx* c, double dt) {
 	/* Radiation::transferRadiation, Radiation.cpp:569-651 (single rank) */
+	if (c->p.rt_scheme != 0 && c->p.star_on) return transfer_radiation2(c, dt);
 	if (c->p.star_on) {
 		for (long w = 0; w < c->nwind; ++w) {
 			long id = c->wind[w];
@@ -1515,8 +1579,6 @@ static int setup(orc_ctx* c, const double* den, const double* pre, const double*
                  const double* v0, const double* v1, const double* v2, const double* grav) {
 	orc_params* p = &c->p;
 	conv_t* cv = &c->cv;
-	if (p->rt_scheme != 0 && p->radiation_on)
-		return fail(c, ORC_ERR_PARAM, "only the implicit radiation scheme is supported");
 	/* Constants::initialise_DPT, Constants.cpp:27-50 */
 	conv_init(cv);
 	conv_set_dpt(cv, p->dscale, p->pscale, p->tscale);

@@ -40,7 +40,7 @@ typedef struct orc_params {
 	int limiter;                /* 0 monotonised_central, 1 superbee, 2 minmod, 3 maxmod, 4 leer, 5 ospre, 6 albada */
 	double K1, K2, K3, K4;
 	double photoion_xsec, alphaB, tau0, minX, THI, THII, mass_frac_h;
-	int rt_scheme;              /* 0 implicit (others unsupported) */
+	int rt_scheme;              /* 0 implicit, 1 implicit2, 2 explicit */
 	int collisions_on;
 	int coupling;               /* 0 tti, 1 neq, 2 off */
 	double heating_amp, thermo_hii_switch;

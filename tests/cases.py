@@ -75,6 +75,18 @@ def hii3d_offcentre():
     return tp, ic, 8
 
 
+def hii3d_implicit2():
+    """transferRadiation2 with the implicit2 scheme (Radiation.cpp:508-567)."""
+    tp, ic = workloads.hii_region(n=12, seed=6)
+    return dataclasses.replace(tp, rt_scheme="implicit2"), ic, 10
+
+
+def blister_explicit():
+    """transferRadiation2 with the explicit scheme, shipped 2-D setup at 30x40."""
+    tp, ic, steps = blister_small()
+    return dataclasses.replace(tp, rt_scheme="explicit"), ic, 20
+
+
 CASES = {
     "blister_small": blister_small,
     "sedov3d_small": sedov3d_small,
@@ -83,6 +95,8 @@ CASES = {
     "sedov3d_limiters": sedov3d_limiters,
     "hii3d_small": hii3d_small,
     "hii3d_offcentre": hii3d_offcentre,
+    "hii3d_implicit2": hii3d_implicit2,
+    "blister_explicit": blister_explicit,
 }
 
 

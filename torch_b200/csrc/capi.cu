@@ -46,6 +46,8 @@ struct trg_ctx {
 	// CUDA graphs of the shell sweeps (all shells of one sweep, launched as one)
 	cudaGraphExec_t g_colden = nullptr;
 	cudaGraphExec_t g_rad[2] = {nullptr, nullptr};
+	cudaGraphExec_t g_tau = nullptr;
+	long long g_tau_nodes = 0;
 	long long g_colden_nodes = 0, g_rad_nodes[2] = {0, 0};
 	bool use_graphs = true;
 	// per-grid scalar kernels (dt, time) run on this many threads: 1, or the
@@ -232,8 +234,33 @@ void rad_sweep_direct(trg_ctx* c, double h) {
 	}
 }
 
+// Radiation::transferRadiation2 (Radiation.cpp:508-567): the tau-only sweep
+// (one graph, like the other sweeps), then one launch over all non-wind cells.
+void tau_sweep_direct(trg_ctx* c) {
+	int nw = (int)c->hs.wind_cells.size();
+	LAUNCH(KF(k_rad_wind_reset), nw, 128, c->P, c->S, c->d_wind, nw);
+	const auto& off = c->hs.off_nonwind;
+	for (size_t s = 0; s + 1 < off.size(); ++s) {
+		int count = (int)(off[s + 1] - off[s]);
+		LAUNCH(KF(k_rad_tau_shell), count, 128, c->P, c->S, c->d_sweep_nonwind + off[s], count);
+	}
+}
+
+void rad_integrate2(trg_ctx* c, double h) {
+	if (c->use_graphs && !c->g_tau) c->g_tau = capture_graph(c, [&] { tau_sweep_direct(c); }, c->g_tau_nodes);
+	if (c->use_graphs && c->g_tau) launch_graph(c, c->g_tau, c->g_tau_nodes, "graph_tau_sweep");
+	else tau_sweep_direct(c);
+	int n = (int)c->hs.sweep_nonwind.size();
+	LAUNCH(KF(k_rad_solve2), n, 128, c->P, c->S, c->d_sweep_nonwind, n, h);
+}
+
 void rad_integrate(trg_ctx* c, double h) {
-	// Radiation::transferRadiation (Radiation.cpp:569-651)
+	// Radiation::integrate (Radiation.cpp:58-63): transferRadiation for the
+	// implicit scheme (:569-651), transferRadiation2 for the others
+	if (c->P.star_on && c->P.rt_scheme != 0) {
+		rad_integrate2(c, h);
+		return;
+	}
 	if (c->P.star_on && (h == 0.5 || h == 1.0) && c->use_graphs) {
 		int gi = h == 0.5 ? 0 : 1;
 		if (!c->g_rad[gi]) c->g_rad[gi] = capture_graph(c, [&] { rad_sweep_direct(c, h); }, c->g_rad_nodes[gi]);
@@ -747,6 +774,8 @@ static void drop_graphs(trg_ctx* c) {
 	// the sweep graphs hold the kernel arguments (Params, State) by value
 	if (c->g_colden) cudaGraphExecDestroy(c->g_colden);
 	c->g_colden = nullptr;
+	if (c->g_tau) cudaGraphExecDestroy(c->g_tau);
+	c->g_tau = nullptr;
 	for (auto& g : c->g_rad) {
 		if (g) cudaGraphExecDestroy(g);
 		g = nullptr;

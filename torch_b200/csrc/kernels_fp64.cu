@@ -790,6 +790,113 @@ __global__ void __launch_bounds__(128) k_rad_shell_learned(Params P, State S, co
 	rad_shell<true>(P, S, valid ? cells[t] : 0, valid, h);
 }
 
+// Radiation::transferRadiation2 (Radiation.cpp:508-567) for the implicit2 and
+// explicit schemes.  Its rayTrace (:480-506) is a causal sweep that only
+// interpolates TAU and sets DTAU / DTAU_A from the current fractions (one
+// shell per launch); the fractions are then updated by one launch over all
+// non-wind cells, which are independent of each other in these schemes.
+__device__ __forceinline__ void b_rad_tau_shell(const Params& P, const State& S, long long id) {
+	int ijk[3];
+	double xc[3];
+	cell_ijk(P, id, ijk);
+	cell_xc(P, ijk, xc);
+	double dist2 = dist2_cells(P, xc);
+	if (dist2 > 0.95) {
+		long long nb[4];
+		double w[4];
+		neighbours(P, ijk, xc, nb, w);
+		FLD(S.R, R_TAU, id) = tau_sc(P, S, nb, w, R_TAU, R_DTAU);
+	} else {
+		FLD(S.R, R_TAU, id) = 0;
+	}
+	double nH = P.X * FLD(S.Q, DEN, id) / P.hydrogenMass;
+	FLD(S.R, R_DTAU, id) = (1.0 - FLD(S.Q, HII, id)) * nH * P.photoIonXsec * S.ds[id];
+	FLD(S.R, R_DTAU_A, id) = (1.0 - FLD(S.R, R_HII_A, id)) * nH * P.photoIonXsec * S.ds[id];
+}
+__global__ void __launch_bounds__(128) k_rad_tau_shell(Params P, State S, const int* __restrict__ cells, int count) {
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= count) return;
+	if (TRG_BATCHED && P.batch) {
+		const int e = cells[t];
+		b_rad_tau_shell(P.batch->P[e >> BATCH_CELL_BITS], P.batch->S[e >> BATCH_CELL_BITS], e & BATCH_CELL_MASK);
+		return;
+	}
+	b_rad_tau_shell(P, S, cells[t]);
+}
+
+// Radiation::update_HIIfrac (Radiation.cpp:375-478) for implicit2 (Picard
+// iteration with tau_avg = TAU) and explicit (one doric step whose
+// time-averaged result becomes Q[HII]; HII_A is not written).
+__device__ __forceinline__ void b_rad_solve2(const Params& P, const State& S, long long id, double h) {
+	int ijk[3];
+	double xc[3];
+	cell_ijk(P, id, ijk);
+	cell_xc(P, ijk, xc);
+	const double dt = h * S.scal[0];
+	if ((int)xc[0] == (int)P.sxc[0] && (int)xc[1] == (int)P.sxc[1] && (double)(int)xc[2] == P.sxc[2]) {
+		FLD(S.R, R_HEAT, id) = 0;
+		FLD(S.Q, HII, id) = 1;
+		FLD(S.R, R_HII_A, id) = 1;
+		return;
+	}
+	const double q_den = FLD(S.Q, DEN, id), q_pre = FLD(S.Q, PRE, id), q_hii = FLD(S.Q, HII, id);
+	const double n_H = P.X * q_den / P.hydrogenMass;
+	const double T = calc_temperature(P, q_hii, q_pre, q_den);
+	const double alphaB = spline_eval(S.tables->rad_recomb, T);
+	const double A_ci = collisional_ionisation_rate(P, T);
+	const double ds = S.ds[id], shellVol = S.shellVol[id];
+	double x = q_hii;
+	if (P.rt_scheme == 1) {
+		double x_avg = x, x_avg_old, A_pi;
+		const double tau_avg = FLD(S.R, R_TAU, id);
+		int niter = 0, miter = 0;
+		bool converged = false;
+		while (!converged) {
+			niter++;
+			x_avg_old = x_avg;
+			x = q_hii;
+			double dtau_avg = (1.0 - x_avg) * n_H * P.photoIonXsec * ds;
+			double nHI = (1.0 - x_avg) * n_H;
+			A_pi = photoionisation_rate(nHI, tau_avg, dtau_avg, shellVol, P.photonRate);
+			double nHII_aB = x_avg * n_H * alphaB;
+			double nHII_Aci = x_avg * n_H * A_ci;
+			doric(dt, x_avg, x, A_pi, nHII_aB, nHII_Aci);
+			if ((fabs((x_avg - x_avg_old) / x_avg) < 1.0e-3 || (x_avg < 1.0e-5) || A_pi == 0)) converged = true;
+			if (niter > 10005) {
+				miter++;
+				niter = 0;
+				x_avg = 0.5 * (x_avg + x_avg_old);
+			}
+			if (miter > 5 || x != x) {
+				atomicOr(S.err, ERRB_PICARD);
+				break;
+			}
+		}
+		FLD(S.R, R_HII_A, id) = x_avg;
+	} else {
+		const double x_avg = x;
+		const double nHI = (1.0 - x) * (P.X * q_den / P.hydrogenMass);
+		const double A_pi = photoionisation_rate(nHI, FLD(S.R, R_TAU, id), FLD(S.R, R_DTAU, id), shellVol, P.photonRate);
+		const double nHII_aB = x_avg * n_H * alphaB;
+		const double nHII_Aci = x_avg * n_H * A_ci;
+		double x_dummy = x;
+		doric(dt, x, x_dummy, A_pi, nHII_aB, nHII_Aci);
+	}
+	FLD(S.Q, HII, id) = x;
+	if (x > 0.001) FLD(S.Q, ADV, id) = 1;
+}
+__global__ void __launch_bounds__(128) k_rad_solve2(Params P, State S, const int* __restrict__ cells, int count,
+                                                    double h) {
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= count) return;
+	if (TRG_BATCHED && P.batch) {
+		const int e = cells[t];
+		b_rad_solve2(P.batch->P[e >> BATCH_CELL_BITS], P.batch->S[e >> BATCH_CELL_BITS], e & BATCH_CELL_MASK, h);
+		return;
+	}
+	b_rad_solve2(P, S, cells[t], h);
+}
+
 // Star off: Radiation::transferRadiation else-branch (Radiation.cpp:638-650), interior cells.
 __device__ __forceinline__ void b_rad_no_star_fp64(const Params& P, const State& S, long long id, double h) {
 

@@ -231,7 +231,7 @@ std::string host_setup(const trg_params& p, const double* den, const double* pre
 	if ((p.nd < 3 && p.ncells[2] != 1) || (p.nd < 2 && p.ncells[1] != 1)) return "ncells beyond nd must be 1";
 	if (p.spatial_order != 0 && p.spatial_order != 1)
 		return "spatial_order must be 0 or 1 (Hydrodynamics::calcFluxes, Hydro.cpp:94-112)";
-	if (p.radiation_on && p.rt_scheme != 0) return "only the implicit radiation scheme is implemented";
+	if (p.rt_scheme < 0 || p.rt_scheme > 2) return "rt_scheme must be 0 (implicit), 1 (implicit2) or 2 (explicit)";
 	if (!den || !pre || !hii || !v0) return "den, pre, hii and v0 are required";
 	Converter cv;
 	cv.set_rho_pressure_time(p.dscale, p.pscale, p.tscale);
@@ -293,6 +293,7 @@ std::string host_setup(const trg_params& p, const double* den, const double* pre
 	P.star_on = p.star_on;
 	P.collisions_on = p.collisions_on;
 	P.coupling = p.coupling;
+	P.rt_scheme = p.rt_scheme;
 	P.thermo_subcycling = p.thermo_subcycling;
 	for (int i = 0; i < 3; ++i) P.star_pos[i] = p.star_pos[i];
 	P.wind_radius = p.star_on ? p.wind_cell_radius : 0;

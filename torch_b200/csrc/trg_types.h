@@ -50,6 +50,7 @@ struct Params {
 	double tau0, THI, THII, heating_amp, thermo_hii_switch;
 	double K1, K2, K3, K4;
 	int radiation_on, cooling_on, star_on, collisions_on, coupling, thermo_subcycling;
+	int rt_scheme;  // 0 implicit, 1 implicit2, 2 explicit (Radiation.cpp:48-53)
 	int star_pos[3];
 	int wind_radius;     // Star::windCellRadius when the star is on, else 0
 	long long star_cell; // flat index of the star cell or -1
