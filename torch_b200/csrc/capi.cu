@@ -43,6 +43,14 @@ struct trg_ctx {
 	bool mixed = false;
 	// FP32 form (either kind): the FP64 kernels come from the fast build
 	bool fastk = false;
+	// FP32 form with radiation/cooling: Q already holds the primitives of the
+	// current U (written by the FP32 hydro sub-step), so the next
+	// globalQfromU + fixPrimitives pass can be skipped
+	bool q_fresh = false;
+	// side stream: the radiation heating pass runs beside the column-density
+	// sweep at the start of a step (they touch disjoint fields)
+	cudaStream_t side = nullptr;
+	cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 	// CUDA graphs of the shell sweeps (all shells of one sweep, launched as one)
 	cudaGraphExec_t g_colden = nullptr;
 	cudaGraphExec_t g_rad[2] = {nullptr, nullptr};
@@ -285,7 +293,8 @@ void rad_integrate(trg_ctx* c, double h) {
 void sub_step(trg_ctx* c, double h, bool hasCalculatedHeatFlux, int comp) {
 	// Torch::subStep, Torch.cpp:352-364
 	if (!hasCalculatedHeatFlux) {
-		q_from_u(c, 0, 1);
+		if (!c->q_fresh) q_from_u(c, 0, 1);
+		c->q_fresh = false;
 		comp_pre(c, comp);
 	}
 	switch (comp) {
@@ -298,6 +307,7 @@ void sub_step(trg_ctx* c, double h, bool hasCalculatedHeatFlux, int comp) {
 			if (c->profiling) { cudaEventRecord(eb, c->stream); c->recs.push_back({"k_hydro_stage_fp32", ea, eb}); }
 			c->launches++;
 			std::swap(c->S.U, c->S.U1);
+			c->q_fresh = true;
 			break;
 		}
 		hydro_fluxes(c);
@@ -369,9 +379,24 @@ void enqueue_full_step(trg_ctx* c, double dt_next) {
 		return;
 	}
 	// Torch::fullStep, Torch.cpp:389-418
-	q_from_u(c, 0, 1);
-	if (c->P.cooling_on) thermo_pre(c);
-	if (c->P.radiation_on) rad_pre(c);
+	if (!c->q_fresh) q_from_u(c, 0, 1);
+	c->q_fresh = false;
+	if (c->P.cooling_on && c->P.radiation_on && c->P.star_on && c->side) {
+		// Radiation::preTimeStepCalculations (heating rates, reads Q, R) beside
+		// Thermodynamics::preTimeStepCalculations (column densities and rates,
+		// writes T): the sweep leaves most of the GPU idle
+		cudaEventRecord(c->ev_fork, c->stream);
+		cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+		std::swap(c->stream, c->side);
+		rad_pre(c);
+		std::swap(c->stream, c->side);
+		cudaEventRecord(c->ev_join, c->side);
+		thermo_pre(c);
+		cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+	} else {
+		if (c->P.cooling_on) thermo_pre(c);
+		if (c->P.radiation_on) rad_pre(c);
+	}
 	time_step(c, dt_next);
 	const int ncomps = c->hs.nactive;
 	if (ncomps == 1) {
@@ -458,6 +483,9 @@ int trg_create(const trg_params* p, const double* den, const double* pre, const 
 	const long long N = c->P.N;
 	CUDA_TRY(cudaSetDevice(p->device));
 	CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+	CUDA_TRY(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+	CUDA_TRY(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+	CUDA_TRY(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
 	State& S = c->S;
 	std::memset(&S, 0, sizeof(S));
 	int rc = 0;
@@ -597,6 +625,7 @@ int trg_profile_read(trg_ctx* c, const char* name, double* total_ms, long long* 
 }
 
 int trg_component(trg_ctx* c, int comp, int phase, double dt, double* out) {
+	if (c) c->q_fresh = false;
 	if (!c) return TRG_ERR_ARG;
 	if (c->fp32 || c->mixed) return set_error(c, TRG_ERR_ARG, "per-component phases are provided by the FP64 form");
 	// The phase kernels read dt from the device scalar: stage the caller's dt.
@@ -667,6 +696,7 @@ int trg_get_state(trg_ctx* c, double* U, double* Q, double* R, double* T, double
 
 int trg_set_conserved(trg_ctx* c, const double* U) {
 	if (!c || !U) return TRG_ERR_ARG;
+	c->q_fresh = false;
 	CUDA_TRY(cudaMemcpyAsync(c->S.U, U, 7 * c->P.N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
 	if (c->fp32) LAUNCH(k_f64_to_f32, 7 * c->P.N, 256, c->P, c->S.U, c->U32);
 	return TRG_OK;
@@ -680,7 +710,7 @@ struct CkptHeader {
 	long long N;
 	int nx, ny, nz, nd;
 	long long steps;
-	int first_time, rad_once_pending, stepCounter, pad;
+	int first_time, rad_once_pending, stepCounter, q_fresh;
 	double scal[8];
 };
 int ckpt_form(const trg_ctx* c) { return c->fp32 ? 1 : (c->mixed ? 2 : 0); }
@@ -709,6 +739,7 @@ int trg_checkpoint_save(trg_ctx* c, void* buf, long long bytes) {
 	h.first_time = c->first_time;
 	h.rad_once_pending = c->rad_once_pending;
 	h.stepCounter = c->stepCounter;
+	h.q_fresh = c->q_fresh ? 1 : 0;
 	CUDA_TRY(cudaMemcpy(h.scal, c->S.scal, sizeof(h.scal), cudaMemcpyDeviceToHost));
 	char* p = static_cast<char*>(buf);
 	memcpy(p, &h, sizeof(h));
@@ -745,6 +776,7 @@ int trg_checkpoint_load(trg_ctx* c, const void* buf, long long bytes) {
 	if (c->fp32) CUDA_TRY(cudaMemcpy(c->U32, p, 7 * N * sizeof(float), cudaMemcpyHostToDevice));
 	CUDA_TRY(cudaMemcpy(c->S.scal, h.scal, sizeof(h.scal), cudaMemcpyHostToDevice));
 	CUDA_TRY(cudaMemset(c->S.UDOT, 0, 7 * N * sizeof(double)));
+	c->q_fresh = h.q_fresh != 0;
 	c->steps = h.steps;
 	c->first_time = h.first_time;
 	c->rad_once_pending = h.rad_once_pending;
@@ -946,6 +978,10 @@ void trg_destroy(trg_ctx* c) {
 	if (c->S.harvest) cudaFree(c->S.harvest);
 	if (c->S.harvest_n) cudaFree(c->S.harvest_n);
 	for (void* p : c->allocs) cudaFree(p);
+	if (c->side) cudaStreamSynchronize(c->side);
+	if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+	if (c->ev_join) cudaEventDestroy(c->ev_join);
+	if (c->side) cudaStreamDestroy(c->side);
 	if (c->stream) cudaStreamDestroy(c->stream);
 	delete c;
 }

@@ -606,6 +606,20 @@ __global__ void __launch_bounds__(BX* BY, 2)
 			bad |= !fix_cons(SP, u);
 #pragma unroll
 			for (int i = 0; i < 7; ++i) store_u(Uout, i * N + id, u[i], SC, i);
+			if (sizeof(TS) == sizeof(double)) {
+				// hydro sub-step of a radiation-hydro run: also the FP64 primitives
+				// of the new state with floors (what globalQfromU + fixPrimitives
+				// of the next sub-step would compute), so that pass is skipped
+				Prim q = prim_from_cons(u, gamma, nd);
+				fix_prim(SP, q, u[DEN]);
+				FLD(S.Q, DEN, id) = (double)q.d * P.f32_rho0;
+				FLD(S.Q, PRE, id) = (double)q.p * P.f32_p0;
+				FLD(S.Q, HII, id) = (double)q.x;
+				FLD(S.Q, ADV, id) = (double)q.a;
+#pragma unroll
+				for (int k = 0; k < 3; ++k)
+					if (k < nd) FLD(S.Q, VEL + k, id) = (double)q.v[k] * P.f32_v0;
+			}
 			if (STAGE == 2) {
 				// the next step's CFL limit from Q(U1) with floors (Torch::fullStep:
 				// globalQfromU + fixPrimitives, then Hydrodynamics::calculateTimeStep)
