@@ -469,8 +469,8 @@ def run_ours(args, world, rank, local, pg):
     elif head == "fp32":
         kname = "k_hydro_stage_fp32"
         # FP32 form of a radiation-hydro run: one launch per hydro sub-step on the
-        # FP64 state, reading U (7 x 8 B) and writing the new U (7 x 8 B)
-        alg_per_launch = 112.0 * N
+        # FP64 state, reading U (7 x 8 B) and writing the new U and its Q (2 x 7 x 8 B)
+        alg_per_launch = 168.0 * N
     else:
         kname = "k_faces_fp64"
         # FP64 plain form, per face-flux launch (one per dimension, 2 stages):

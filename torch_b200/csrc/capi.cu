@@ -229,7 +229,8 @@ void rad_shell_launch(trg_ctx* c, const int* cells, int count, double h) {
 		c->launches++;
 		return;
 	}
-	LAUNCH(KF(k_rad_shell_fp64), count, 128, c->P, c->S, cells, count, h);
+	if (c->P.stats_on || c->S.harvest) LAUNCH(KF(k_rad_shell_diag), count, 128, c->P, c->S, cells, count, h);
+	else LAUNCH(KF(k_rad_shell_fp64), count, 128, c->P, c->S, cells, count, h);
 }
 
 void rad_sweep_direct(trg_ctx* c, double h) {
@@ -315,11 +316,14 @@ void sub_step(trg_ctx* c, double h, bool hasCalculatedHeatFlux, int comp) {
 		break;
 	case COMP_RAD:
 		rad_integrate(c, h);
-		LAUNCH(KF(k_rad_update_fp64), c->P.N, 256, c->P, c->S, h, 0);
+		// mode 2 (FP32 form): the update also leaves Q of the new state
+		LAUNCH(KF(k_rad_update_fp64), c->P.N, 256, c->P, c->S, h, c->mixed ? 2 : 0);
+		c->q_fresh = c->mixed;
 		break;
 	default:
 		LAUNCH(KF(k_thermo_integrate_fp64), c->P.N, 256, c->P, c->S, h);
-		LAUNCH(KF(k_thermo_update_fp64), c->P.N, 256, c->P, c->S, h, 0);
+		LAUNCH(KF(k_thermo_update_fp64), c->P.N, 256, c->P, c->S, h, c->mixed ? 2 : 0);
+		c->q_fresh = c->mixed;
 		break;
 	}
 }

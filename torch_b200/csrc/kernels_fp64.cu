@@ -414,6 +414,27 @@ __global__ void __launch_bounds__(256) k_hydro_update_fp64(Params P, State S, do
 
 // Fluid::globalQfromU (+ fixPrimitives), Fluid.cpp:138-165, with the Q half of
 // Torch::checkValues (Torch.cpp:420-443).
+// globalQfromU + fixPrimitives + checkValues of a cell whose new conserved
+// state u the caller has in registers (the FP32 form's updates finish with
+// it, so that the next sub-step's Q pass is skipped).  Q fields of velocity
+// components beyond nd are left as they are, as QfromU leaves them.
+__device__ __forceinline__ void store_fixed_q(const Params& P, const State& S, long long id, const double* u) {
+	double q[7] = {0, 0, 0, 0, 0, 0, 0};
+	QfromU(q, u, P.gamma, P.nd);
+	fix_primitives(P, q, u[DEN]);
+	bool bad = q[DEN] == 0 || q[PRE] == 0;
+#pragma unroll
+	for (int i = 0; i < NU; ++i) bad |= (u[i] != u[i]) || isinf(u[i]);
+	FLD(S.Q, DEN, id) = q[DEN];
+	FLD(S.Q, PRE, id) = q[PRE];
+	FLD(S.Q, HII, id) = q[HII];
+	FLD(S.Q, ADV, id) = q[ADV];
+#pragma unroll
+	for (int k = 0; k < 3; ++k)
+		if (k < P.nd) FLD(S.Q, VEL + k, id) = q[VEL + k];
+	if (bad) atomicOr(S.err, ERRB_NAN);
+}
+
 __device__ __forceinline__ void b_q_from_u_fp64(const Params& P, const State& S, long long id, int sel_src, int fix) {
 	const double* Usrc = sel_src ? S.U1 : S.U;
 	double u[7], q[7];
@@ -640,7 +661,9 @@ __device__ __forceinline__ double inv_logit10(float l) {
 // meets the solver's own convergence test (its residual is below the solver
 // tolerance); otherwise the cell restarts the plain iteration from x_HII, so
 // that a rejected prediction leaves the plain result unchanged.
-template <bool LEARNED>
+// DIAG: the counters and the training-set recording are compiled in (a
+// lean build without them keeps the sweep's instruction footprint small).
+template <bool LEARNED, bool DIAG>
 __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const long long id, const bool valid,
                                           double h) {
 	if (!LEARNED && !valid) return;
@@ -723,7 +746,7 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 				// the first iteration from the prediction is its residual test:
 				// accept, or restart the plain iteration from x_HII
 				learned = false;
-				if (P.stats_on) {
+				if (DIAG && P.stats_on) {
 					stat_add(S.stats, TRG_STAT_LEARNED_CELLS, 1u);
 					stat_add(S.stats, TRG_STAT_LEARNED_ACCEPTED, converged ? 1u : 0u);
 				}
@@ -747,8 +770,8 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 		FLD(S.Q, HII, id) = x_new;
 		if (x_new > 0.001) FLD(S.Q, ADV, id) = 1;
 		iters += (unsigned)miter * 10006u + (unsigned)niter;
-		if (LEARNED && P.stats_on && used_learned) stat_add(S.stats, TRG_STAT_LEARNED_ITERS, iters);
-		if (!LEARNED && front && S.harvest) {
+		if (LEARNED && DIAG && P.stats_on && used_learned) stat_add(S.stats, TRG_STAT_LEARNED_ITERS, iters);
+		if (!LEARNED && DIAG && front && S.harvest) {
 			// training record: 5 inputs, then the converged <x>, x and the iteration count
 			unsigned long long slot = atomicAdd(S.harvest_n, 1ull);
 			if (slot < (unsigned long long)S.harvest_cap) {
@@ -763,7 +786,7 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 	double nH = P.X * q_den / P.hydrogenMass;
 	FLD(S.R, R_DTAU, id) = (1.0 - FLD(S.Q, HII, id)) * nH * P.photoIonXsec * ds;
 	FLD(S.R, R_DTAU_A, id) = (1.0 - FLD(S.R, R_HII_A, id)) * nH * P.photoIonXsec * ds;
-	if (P.stats_on) {
+	if (DIAG && P.stats_on) {
 		stat_picard(S.stats, iters);
 		stat_add(S.stats, TRG_STAT_FRONT_CELLS, front ? 1u : 0u);
 		stat_add(S.stats, TRG_STAT_FRONT_ITERS, front ? iters : 0u);
@@ -777,17 +800,24 @@ __global__ void __launch_bounds__(128) k_rad_shell_fp64(Params P, State S, const
 	if (TRG_BATCHED && P.batch) {
 		const int e = cells[t];
 		const int g = e >> BATCH_CELL_BITS;
-		rad_shell<false>(P.batch->P[g], P.batch->S[g], e & BATCH_CELL_MASK, true, h);
+		rad_shell<false, false>(P.batch->P[g], P.batch->S[g], e & BATCH_CELL_MASK, true, h);
 		return;
 	}
-	rad_shell<false>(P, S, cells[t], true, h);
+	rad_shell<false, false>(P, S, cells[t], true, h);
+}
+// The same with the solver counters and training-set recording compiled in.
+__global__ void __launch_bounds__(128) k_rad_shell_diag(Params P, State S, const int* __restrict__ cells, int count,
+                                                       double h) {
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= count) return;
+	rad_shell<false, true>(P, S, cells[t], true, h);
 }
 // Single grids only (the tensor-core tile needs all 128 threads of a CTA).
 __global__ void __launch_bounds__(128) k_rad_shell_learned(Params P, State S, const int* __restrict__ cells, int count,
                                                           double h) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	const bool valid = t < count;
-	rad_shell<true>(P, S, valid ? cells[t] : 0, valid, h);
+	rad_shell<true, true>(P, S, valid ? cells[t] : 0, valid, h);
 }
 
 // Radiation::transferRadiation2 (Radiation.cpp:508-567) for the implicit2 and
@@ -999,6 +1029,7 @@ __device__ __forceinline__ void b_rad_update_fp64(const Params& P, const State& 
 	if (!fix_solution(P, u)) atomicOr(S.err, ERRB_NAN);
 #pragma unroll
 	for (int i = 0; i < NU; ++i) FLD(S.U, i, id) = u[i];
+	if (mode == 2) store_fixed_q(P, S, id, u);
 }
 __global__ void __launch_bounds__(256) k_rad_update_fp64(Params P, State S, double h, int mode) {
 	if (TRG_BATCHED && P.batch) {
@@ -1243,6 +1274,7 @@ __device__ __forceinline__ void b_thermo_update_fp64(const Params& P, const Stat
 	if (!fix_solution(P, u)) atomicOr(S.err, ERRB_NAN);
 #pragma unroll
 	for (int i = 0; i < NU; ++i) FLD(S.U, i, id) = u[i];
+	if (mode == 2) store_fixed_q(P, S, id, u);
 }
 __global__ void __launch_bounds__(256) k_thermo_update_fp64(Params P, State S, double h, int mode) {
 	if (TRG_BATCHED && P.batch) {

@@ -13,6 +13,7 @@
 	__global__ void k_rad_wind_reset(Params P, State S, const int* cells, int count); \
 	__global__ void k_rad_shell_fp64(Params P, State S, const int* cells, int count, double h); \
 	__global__ void k_rad_shell_learned(Params P, State S, const int* cells, int count, double h); \
+	__global__ void k_rad_shell_diag(Params P, State S, const int* cells, int count, double h); \
 	__global__ void k_rad_no_star_fp64(Params P, State S, double h); \
 	__global__ void k_rad_tau_shell(Params P, State S, const int* cells, int count); \
 	__global__ void k_rad_solve2(Params P, State S, const int* cells, int count, double h); \
