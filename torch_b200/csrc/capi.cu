@@ -47,6 +47,10 @@ struct trg_ctx {
 	// current U (written by the FP32 hydro sub-step), so the next
 	// globalQfromU + fixPrimitives pass can be skipped
 	bool q_fresh = false;
+	// the column densities of the thermodynamics depend on the density alone,
+	// which only hydro sub-steps change: a second sweep with no hydro sub-step
+	// since the last one would recompute the same values and is skipped
+	bool colden_valid = false;
 	// side stream: the radiation heating pass runs beside the column-density
 	// sweep at the start of a step (they touch disjoint fields)
 	cudaStream_t side = nullptr;
@@ -202,7 +206,10 @@ void colden_sweep(trg_ctx* c) {
 
 void thermo_pre(trg_ctx* c) {
 	// Thermodynamics::preTimeStepCalculations: column densities, then rates.
-	if (c->P.star_on) colden_sweep(c);
+	if (c->P.star_on && !c->colden_valid) {
+		colden_sweep(c);
+		c->colden_valid = true;
+	}
 	LAUNCH(KF(k_thermo_rates_fp64), c->P.N, 256, c->P, c->S);
 }
 
@@ -309,10 +316,12 @@ void sub_step(trg_ctx* c, double h, bool hasCalculatedHeatFlux, int comp) {
 			c->launches++;
 			std::swap(c->S.U, c->S.U1);
 			c->q_fresh = true;
+			c->colden_valid = false;
 			break;
 		}
 		hydro_fluxes(c);
 		LAUNCH(KF(k_hydro_update_fp64), c->P.N, 256, c->P, c->S, h, 0, 0, 0);
+		c->colden_valid = false;
 		break;
 	case COMP_RAD:
 		rad_integrate(c, h);
@@ -331,6 +340,7 @@ void sub_step(trg_ctx* c, double h, bool hasCalculatedHeatFlux, int comp) {
 void hydro_step(trg_ctx* c) {
 	// Torch::hydroStep (hasCalculatedHeatFlux = true), Torch.cpp:366-387: the
 	// saved state W is the untouched U; the predictor writes U1.
+	c->colden_valid = false;
 	hydro_fluxes(c);
 	LAUNCH(KF(k_hydro_update_fp64), c->P.N, 256, c->P, c->S, 0.5, 0, 1, 0);
 	q_from_u(c, 1, 0);
@@ -629,7 +639,7 @@ int trg_profile_read(trg_ctx* c, const char* name, double* total_ms, long long* 
 }
 
 int trg_component(trg_ctx* c, int comp, int phase, double dt, double* out) {
-	if (c) c->q_fresh = false;
+	if (c) c->q_fresh = c->colden_valid = false;
 	if (!c) return TRG_ERR_ARG;
 	if (c->fp32 || c->mixed) return set_error(c, TRG_ERR_ARG, "per-component phases are provided by the FP64 form");
 	// The phase kernels read dt from the device scalar: stage the caller's dt.
@@ -701,6 +711,7 @@ int trg_get_state(trg_ctx* c, double* U, double* Q, double* R, double* T, double
 int trg_set_conserved(trg_ctx* c, const double* U) {
 	if (!c || !U) return TRG_ERR_ARG;
 	c->q_fresh = false;
+	c->colden_valid = false;
 	CUDA_TRY(cudaMemcpyAsync(c->S.U, U, 7 * c->P.N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
 	if (c->fp32) LAUNCH(k_f64_to_f32, 7 * c->P.N, 256, c->P, c->S.U, c->U32);
 	return TRG_OK;
@@ -781,6 +792,7 @@ int trg_checkpoint_load(trg_ctx* c, const void* buf, long long bytes) {
 	CUDA_TRY(cudaMemcpy(c->S.scal, h.scal, sizeof(h.scal), cudaMemcpyHostToDevice));
 	CUDA_TRY(cudaMemset(c->S.UDOT, 0, 7 * N * sizeof(double)));
 	c->q_fresh = h.q_fresh != 0;
+	c->colden_valid = false;
 	c->steps = h.steps;
 	c->first_time = h.first_time;
 	c->rad_once_pending = h.rad_once_pending;
