@@ -155,8 +155,17 @@ enum {
 	TRG_STAT_THERMO_MAX = 16,       /* most subcycles in one cell */
 	TRG_STAT_SWEEPS = 17,           /* radiation sweeps counted */
 	TRG_STAT_FRONT_CELLS = 18,      /* front cells (tau < 20, x_HII < 0.99): the learned start's domain */
-	TRG_STAT_FRONT_ITERS = 19       /* Picard iterations of the front cells */
+	TRG_STAT_FRONT_ITERS = 19,      /* Picard iterations of the front cells */
+	TRG_STAT_FP64_CELLS = 20        /* FP32 form: hydro cell updates done in FP64 (pressure contrast) */
 };
+/* FP32 form with radiation or cooling (no counterpart in the reference): a
+ * hydro cell update is done in FP64 instead of FP32 where the pressures of
+ * its stencil (two cells either side along each axis) differ by more than
+ * the factor `contrast` (default 1e3; 0 turns the fallback off), i.e. around
+ * strong shocks, where FP32 flux differences keep too few digits.  The count
+ * of such updates is the TRG_STAT_FP64_CELLS counter. */
+int trg_fp32_contrast(trg_ctx* c, double contrast);
+
 /* Heating and cooling diagnostics (Thermodynamics::fillHeatingArrays,
  * src/Integrators/Thermodynamics.cpp:419-461, as printed by
  * DataPrinter::printHeating at every checkpoint of Torch::run): with

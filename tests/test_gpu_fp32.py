@@ -121,3 +121,26 @@ def test_autotune_keeps_results_bitwise():
     sb = b.state()
     b.close()
     assert np.array_equal(sa.U, sb.U)
+
+
+def test_fp64_fallback_for_high_pressure_contrast():
+    """HII region with radiation and cooling: the star's heating drives a blast
+    wave whose pressure jump FP32 cannot difference; the cells across it are
+    updated in FP64 (TRG_STAT_FP64_CELLS) and the pressure error against the
+    FP64 form stays at FP32 rounding level, not worse than without it."""
+    tp, ic = workloads.hii_region(n=48)
+    ref = run(tp, ic, 30, torch_b200.PRECISION_FP64)
+    g, nd = tp.heatCapacityRatio, ic.nd
+    errs = {}
+    for contrast in (0.0, 1.0e3):
+        t = torch_b200.Torch(tp, ic, precision=torch_b200.PRECISION_FP32)
+        t.fp32_contrast(contrast)
+        t.stats_enable(True)
+        t.run_steps(30)
+        st = t.stats()
+        s = t.state()
+        t.close()
+        errs[contrast] = common.rel_l1(pressure(s.U, g, nd), pressure(ref.U, g, nd))
+        print(f"contrast {contrast:g}: pre {errs[contrast]:.2e}, FP64 cell updates {st['fp64_cells']}")
+        assert (st["fp64_cells"] > 0) == (contrast > 0)
+    assert errs[1.0e3] <= 1e-6 and errs[1.0e3] <= errs[0.0]

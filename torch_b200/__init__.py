@@ -99,6 +99,7 @@ _SIGNATURES = [
     ("trg_autotune", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     ("trg_checkpoint_bytes", C.c_longlong, [C.c_void_p]),
     ("trg_heating_enable", C.c_int, [C.c_void_p, C.c_int]),
+    ("trg_fp32_contrast", C.c_int, [C.c_void_p, C.c_double]),
     ("trg_heating", C.c_int, [C.c_void_p, C.c_void_p]),
     ("trg_checkpoint_save", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
     ("trg_checkpoint_load", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
@@ -372,6 +373,10 @@ class Torch:
                 raise TrgError(-got, "trg_harvest_read failed")
         return out, n
 
+    def fp32_contrast(self, contrast: float):
+        """Pressure ratio above which the FP32 form updates a hydro cell in FP64 (0: off)."""
+        self._check(self.lib.trg_fp32_contrast(self.ctx, float(contrast)))
+
     def heating_enable(self, on: bool = True):
         """Keep the heating/cooling terms during the step (for heating())."""
         self._check(self.lib.trg_heating_enable(self.ctx, int(on)))
@@ -412,7 +417,7 @@ class Torch:
                 "picard_hist": dict(zip(PICARD_BINS, v[3:11])),
                 "learned_cells": v[11], "learned_accepted": v[12], "learned_iters": v[13],
                 "thermo_cells": v[14], "thermo_subcycles": v[15], "thermo_max": v[16], "sweeps": v[17],
-                "front_cells": v[18], "front_iters": v[19]}
+                "front_cells": v[18], "front_iters": v[19], "fp64_cells": v[20]}
 
     def component(self, comp: int, phase: int, dt: float = 0.0) -> float:
         out = C.c_double(0)

@@ -51,6 +51,9 @@ struct trg_ctx {
 	// which only hydro sub-steps change: a second sweep with no hydro sub-step
 	// since the last one would recompute the same values and is skipped
 	bool colden_valid = false;
+	// pressure ratio above which a hydro cell update of the FP32 form falls
+	// back to FP64 (0: never)
+	double fb_contrast = 1.0e3;
 	// side stream: the radiation heating pass runs beside the column-density
 	// sweep at the start of a step (they touch disjoint fields)
 	cudaStream_t side = nullptr;
@@ -310,10 +313,20 @@ void sub_step(trg_ctx* c, double h, bool hasCalculatedHeatFlux, int comp) {
 		if (c->mixed) {
 			// FP32 hydro pass on the FP64 state, into U1, then swap
 			cudaEvent_t ea = nullptr, eb = nullptr;
+			const bool fb = c->fb_contrast > 0 && c->S.fb_flag;
+			if (fb) {
+				// FP64 fallback, part 1: list the high-contrast cells and compute
+				// their faces in FP64 from this sub-step's primitives
+				cudaMemsetAsync(c->S.fb_count, 0, sizeof(unsigned), c->stream);
+				LAUNCH(KF(k_fb_flags), c->P.N, 256, c->P, c->S, c->fb_contrast);
+				LAUNCH(KF(k_fb_faces), 148LL * 8 * 128, 128, c->P, c->S);
+			}
 			if (c->profiling) { ea = pool_event(c); eb = pool_event(c); cudaEventRecord(ea, c->stream); }
 			launch_hydro_substep_fp32(c->P, c->S, c->S.U, c->S.U1, h, c->zchunk, c->stream);
 			if (c->profiling) { cudaEventRecord(eb, c->stream); c->recs.push_back({"k_hydro_stage_fp32", ea, eb}); }
 			c->launches++;
+			// part 2: their FP64 update overwrites the FP32 result
+			if (fb) LAUNCH(KF(k_fb_update), 148LL * 8 * 256, 256, c->P, c->S, h);
 			std::swap(c->S.U, c->S.U1);
 			c->q_fresh = true;
 			c->colden_valid = false;
@@ -558,6 +571,9 @@ int trg_create(const trg_params* p, const double* den, const double* pre, const 
 		c->mixed = true;
 		c->fastk = true;
 		c->zchunk = ctx_fp32_zchunk(c);
+		if ((rc = dalloc(c, &c->S.fb_flag, N)) || (rc = dalloc(c, &c->S.fb_list, N)) ||
+		    (rc = dalloc(c, &c->S.fb_count, 1)))
+			return rc;
 	} else if (p->precision == TRG_PRECISION_FP32) {
 		if (c->P.nd < 2) return set_error(c, TRG_ERR_ARG, "the FP32 form needs a 2-D or 3-D grid");
 		c->fp32 = true;
@@ -847,6 +863,12 @@ int trg_stats(trg_ctx* c, unsigned long long* out, int reset) {
 		CUDA_TRY(cudaMemsetAsync(c->S.stats, 0, TRG_NSTATS * sizeof(unsigned long long), c->stream));
 		CUDA_TRY(cudaStreamSynchronize(c->stream));
 	}
+	return TRG_OK;
+}
+
+int trg_fp32_contrast(trg_ctx* c, double contrast) {
+	if (!c || !(contrast >= 0)) return TRG_ERR_ARG;
+	c->fb_contrast = contrast;
 	return TRG_OK;
 }
 

@@ -606,10 +606,11 @@ __global__ void __launch_bounds__(BX* BY, 2)
 			bad |= !fix_cons(SP, u);
 #pragma unroll
 			for (int i = 0; i < 7; ++i) store_u(Uout, i * N + id, u[i], SC, i);
-			if (sizeof(TS) == sizeof(double)) {
+			if (sizeof(TS) == sizeof(double) && !(S.fb_flag && S.fb_flag[id])) {
 				// hydro sub-step of a radiation-hydro run: also the FP64 primitives
 				// of the new state with floors (what globalQfromU + fixPrimitives
-				// of the next sub-step would compute), so that pass is skipped
+				// of the next sub-step would compute), so that pass is skipped;
+				// cells of the FP64 fallback keep their old Q for its update
 				Prim q = prim_from_cons(u, gamma, nd);
 				fix_prim(SP, q, u[DEN]);
 				FLD(S.Q, DEN, id) = (double)q.d * P.f32_rho0;

@@ -373,6 +373,27 @@ __device__ __forceinline__ void hydro_udot(const Params& P, const State& S, long
 	}
 }
 
+// globalQfromU + fixPrimitives + checkValues of a cell whose new conserved
+// state u the caller has in registers (the FP32 form's updates finish with
+// it, so that the next sub-step's Q pass is skipped).  Q fields of velocity
+// components beyond nd are left as they are, as QfromU leaves them.
+__device__ __forceinline__ void store_fixed_q(const Params& P, const State& S, long long id, const double* u) {
+	double q[7] = {0, 0, 0, 0, 0, 0, 0};
+	QfromU(q, u, P.gamma, P.nd);
+	fix_primitives(P, q, u[DEN]);
+	bool bad = q[DEN] == 0 || q[PRE] == 0;
+#pragma unroll
+	for (int i = 0; i < NU; ++i) bad |= (u[i] != u[i]) || isinf(u[i]);
+	FLD(S.Q, DEN, id) = q[DEN];
+	FLD(S.Q, PRE, id) = q[PRE];
+	FLD(S.Q, HII, id) = q[HII];
+	FLD(S.Q, ADV, id) = q[ADV];
+#pragma unroll
+	for (int k = 0; k < 3; ++k)
+		if (k < P.nd) FLD(S.Q, VEL + k, id) = q[VEL + k];
+	if (bad) atomicOr(S.err, ERRB_NAN);
+}
+
 // Hydro update: UDOT from the face fluxes, then Fluid::advSolution (Fluid.cpp:80-87)
 // from Ubase and Fluid::fixSolution, written to Uout (may alias Ubase); the
 // selectors pick S.U (0) or S.U1 (1).
@@ -397,6 +418,7 @@ __device__ __forceinline__ void b_hydro_update_fp64(const Params& P, const State
 	if (!fix_solution(P, u)) atomicOr(S.err, ERRB_NAN);
 #pragma unroll
 	for (int i = 0; i < NU; ++i) FLD(Uout, i, id) = u[i];
+	if (mode == 2) store_fixed_q(P, S, id, u);
 }
 __global__ void __launch_bounds__(256) k_hydro_update_fp64(Params P, State S, double h, int sel_base, int sel_out,
                                                           int mode) {
@@ -414,27 +436,6 @@ __global__ void __launch_bounds__(256) k_hydro_update_fp64(Params P, State S, do
 
 // Fluid::globalQfromU (+ fixPrimitives), Fluid.cpp:138-165, with the Q half of
 // Torch::checkValues (Torch.cpp:420-443).
-// globalQfromU + fixPrimitives + checkValues of a cell whose new conserved
-// state u the caller has in registers (the FP32 form's updates finish with
-// it, so that the next sub-step's Q pass is skipped).  Q fields of velocity
-// components beyond nd are left as they are, as QfromU leaves them.
-__device__ __forceinline__ void store_fixed_q(const Params& P, const State& S, long long id, const double* u) {
-	double q[7] = {0, 0, 0, 0, 0, 0, 0};
-	QfromU(q, u, P.gamma, P.nd);
-	fix_primitives(P, q, u[DEN]);
-	bool bad = q[DEN] == 0 || q[PRE] == 0;
-#pragma unroll
-	for (int i = 0; i < NU; ++i) bad |= (u[i] != u[i]) || isinf(u[i]);
-	FLD(S.Q, DEN, id) = q[DEN];
-	FLD(S.Q, PRE, id) = q[PRE];
-	FLD(S.Q, HII, id) = q[HII];
-	FLD(S.Q, ADV, id) = q[ADV];
-#pragma unroll
-	for (int k = 0; k < 3; ++k)
-		if (k < P.nd) FLD(S.Q, VEL + k, id) = q[VEL + k];
-	if (bad) atomicOr(S.err, ERRB_NAN);
-}
-
 __device__ __forceinline__ void b_q_from_u_fp64(const Params& P, const State& S, long long id, int sel_src, int fix) {
 	const double* Usrc = sel_src ? S.U1 : S.U;
 	double u[7], q[7];
@@ -1476,6 +1477,74 @@ __global__ void k_dt_reset(Params P, State S) {
 		return;
 	}
 	b_dt_reset(P, S);
+}
+
+// ------------------------------------------- FP64 fallback of the FP32 form
+// A hydro sub-step of the FP32 form keeps FP64 arithmetic for the cells whose
+// stencil (two cells either side along each axis) spans a pressure ratio
+// above `contrast`: across such a jump (the blast wave the star drives into
+// the neutral gas) the FP32 flux differences keep too few digits.  The flag
+// pass lists those cells; their faces are computed in FP64 from the
+// sub-step's primitives before the FP32 pass overwrites Q, and their update
+// (FP64, with Q of the result) follows the FP32 pass, overwriting its values.
+__device__ __forceinline__ long long clamp_nb(const Params& P, const int* ijk, int dim, int off) {
+	int t[3] = {ijk[0], ijk[1], ijk[2]};
+	const int n = ncell(P, dim);
+	int v = (dim == 0 ? t[0] : dim == 1 ? t[1] : t[2]) + off;
+	v = v < 0 ? 0 : (v >= n ? n - 1 : v);
+	if (dim == 0) t[0] = v;
+	else if (dim == 1) t[1] = v;
+	else t[2] = v;
+	return flat_id(P, t[0], t[1], t[2]);
+}
+__global__ void __launch_bounds__(256) k_fb_flags(Params P, State S, double contrast) {
+	const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (id >= P.N) return;
+	int ijk[3];
+	cell_ijk(P, id, ijk);
+	double pmin = FLD(S.Q, PRE, id), pmax = pmin;
+#pragma unroll
+	for (int dim = 0; dim < 3; ++dim)
+		if (dim < P.nd) {
+#pragma unroll
+			for (int off = -2; off <= 2; ++off) {
+				if (off == 0) continue;
+				const double p = FLD(S.Q, PRE, clamp_nb(P, ijk, dim, off));
+				pmin = smin(pmin, p);
+				pmax = smax(pmax, p);
+			}
+		}
+	const bool f = pmax > contrast * pmin;
+	S.fb_flag[id] = f ? 1 : 0;
+	const unsigned m = __activemask();
+	const unsigned ballot = __ballot_sync(m, f);
+	if (!ballot) return;
+	const int leader = __ffs(ballot) - 1;
+	unsigned base = 0;
+	if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(S.fb_count, (unsigned)__popc(ballot));
+	base = __shfl_sync(m, base, leader);
+	if (f) S.fb_list[base + __popc(ballot & ((1u << (threadIdx.x & 31)) - 1))] = (int)id;
+	if (P.stats_on && (int)(threadIdx.x & 31) == leader) atomicAdd(S.stats + TRG_STAT_FP64_CELLS, (unsigned long long)__popc(ballot));
+}
+// FP64 face fluxes (into S.F) of every listed cell's faces.
+__global__ void __launch_bounds__(128) k_fb_faces(Params P, State S) {
+	const unsigned n = *S.fb_count;
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * 2 * P.nd;
+	     t += (long long)gridDim.x * blockDim.x) {
+		const long long id = S.fb_list[t / (2 * P.nd)];
+		const int k = (int)(t % (2 * P.nd)), dim = k >> 1;
+		int ijk[3];
+		cell_ijk(P, id, ijk);
+		long long fl, fr;
+		face_ids(P, ijk, dim, fl, fr);
+		b_faces_fp64(P, S, (k & 1) ? fr : fl, dim);
+	}
+}
+// FP64 update of every listed cell, U -> U1, with Q of the result.
+__global__ void __launch_bounds__(256) k_fb_update(Params P, State S, double h) {
+	const unsigned n = *S.fb_count;
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+		b_hydro_update_fp64(P, S, S.fb_list[t], h, 0, 1, 2);
 }
 
 }  // namespace TRG_KNS

@@ -24,6 +24,9 @@
 	__global__ void k_thermo_integrate_fp64(Params P, State S, double h); \
 	__global__ void k_thermo_update_fp64(Params P, State S, double h, int mode); \
 	__global__ void k_heating_arrays_fp64(Params P, State S); \
+	__global__ void k_fb_flags(Params P, State S, double contrast); \
+	__global__ void k_fb_faces(Params P, State S); \
+	__global__ void k_fb_update(Params P, State S, double h); \
 	__global__ void k_dt_reduce_fp64(Params P, State S, long long first_cell); \
 	__global__ void k_dt_finalize(Params P, State S, double dt_next, int first_time, int step); \
 	__global__ void k_time_advance(Params P, State S); \

@@ -96,6 +96,12 @@ struct State {
 	double* H;
 	// learned starting iterate: the network's inference image (null = plain solve)
 	const unsigned char* mlp_img;
+	// FP32 form, radiation-hydro runs: cells whose hydro stencil spans a
+	// pressure contrast FP32 cannot difference are updated in FP64 instead
+	// (flag per cell, compacted list and its length)
+	unsigned char* fb_flag;
+	int* fb_list;
+	unsigned* fb_count;
 	// training-set recording by the plain solve: records of 8 floats
 	float* harvest;
 	long long harvest_cap;
