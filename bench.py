@@ -1,7 +1,8 @@
 """Benchmark of the TORCH full step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload hii|sedov] [--n 256] [--precision both|fp32|fp64]
+                    [--workload hii|sedov|batch] [--n 256] [--precision both|fp32|fp64]
+    python bench.py --validate 1000 [--workload hii] [--n 256]   (accuracy, not timing)
 
 Default workload: the 256^3 HII-region expansion (side 2 pc, star at the
 centre with Q = 1e49 photons/s, lognormal density with mean 1e3 cm^-3,
@@ -27,6 +28,7 @@ workload.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -244,6 +246,8 @@ def time_form(args, precision, tp, ic, local, pg, profile_names):
     import torch
     import torch_b200
     sim = torch_b200.Torch(tp, ic, precision=precision, device=local)
+    if precision == torch_b200.PRECISION_FP32 and getattr(args, "fp32_contrast", None) is not None and tp.radiation_on:
+        sim.fp32_contrast(args.fp32_contrast)
     sim.tile = sim.autotune()
     dt_next = sim.dt_max
     stream = torch.cuda.ExternalStream(sim.stream_handle(), device=f"cuda:{local}")
@@ -423,6 +427,82 @@ def time_learned(args, sim32, N, world, local, pg):
             "note": "counters from two steps after the timed region with the network, then two without it"}
 
 
+def ifront_cells(hii, n):
+    """I-front distance (cells) from the central star along +x: the first cell
+    with HII < 0.5, linearly interpolated (the rule of the reference's
+    scripts/misc/calc_if.py:43-56)."""
+    x = hii.reshape(n, n, n)[n // 2, n // 2, n // 2:]
+    for i in range(1, len(x)):
+        if x[i] < 0.5:
+            return (i - 1) + (x[i - 1] - 0.5) / (x[i - 1] - x[i])
+    return float(len(x))
+
+
+def run_validate(args, rank, local):
+    """Accuracy of the FP32 form (and of the FP32 form with the learned start)
+    against the FP64 form after --validate steps of the workload: density and
+    pressure relative L1 and the I-front radius along +x."""
+    import torch_b200
+    if rank != 0:
+        return 0
+    tp, ic = build_workload(args.workload, args.n)
+    n, steps = args.n, args.validate
+    g, nd = tp.heatCapacityRatio, int(ic.nd)
+
+    def pressure(U):
+        return (U[1] - sum(U[4 + i] ** 2 for i in range(nd)) / (2.0 * U[0])) * (g - 1.0)
+
+    def rel(a, b):
+        return float(np.abs(a - b).sum() / np.abs(b).sum())
+
+    t0 = time.perf_counter()
+    ref = torch_b200.Torch(tp, ic, precision=torch_b200.PRECISION_FP64, device=local)
+    ref.run_steps(steps)
+    s_ref = ref.state()
+    ref.close()
+    out = {"metric": "FP32-form error against the FP64 form", "workload": f"{args.workload} {n}^3", "steps": steps,
+           "fp64_time_code": s_ref.time}
+    if tp.radiation_on:
+        out["ifront_fp64_cells"] = ifront_cells(s_ref.Q[2], n)
+    forms = [("fp64_perturbed", "perturbed"), ("fp32", None)]
+    if tp.radiation_on and args.learned:
+        forms.append(("fp32_learned", "learned"))
+    for name, extra in forms:
+        if extra == "perturbed":
+            # the problem's own sensitivity: the FP64 form from a density perturbed by 1e-7 (random, seeded)
+            rng = np.random.default_rng(7)
+            ic_p = dataclasses.replace(ic, den=ic.den * (1.0 + 1e-7 * rng.standard_normal(ic.den.shape)))
+            sim = torch_b200.Torch(tp, ic_p, precision=torch_b200.PRECISION_FP64, device=local)
+        else:
+            sim = torch_b200.Torch(tp, ic, precision=torch_b200.PRECISION_FP32, device=local)
+            if args.fp32_contrast is not None:
+                sim.fp32_contrast(args.fp32_contrast)
+        net = None
+        if extra == "learned":
+            # training set: the plain solve's front cells over the first 20 steps of a separate run
+            h = torch_b200.Torch(tp, ic, precision=torch_b200.PRECISION_FP32, device=local)
+            h.harvest(1 << 23)
+            h.run_steps(20)
+            recs, _ = h.harvest_read()
+            h.close()
+            net = torch_b200.Mlp(device=local, seed=11)
+            net.train(recs, epochs=30, batch=4096, lr=2e-3, seed=12)
+            sim.learned_start(net)
+        sim.run_steps(steps)
+        s = sim.state()
+        sim.close()
+        if net is not None:
+            net.close()
+        res = {"den_rel_l1": rel(s.U[0], s_ref.U[0]), "pre_rel_l1": rel(pressure(s.U), pressure(s_ref.U))}
+        if tp.radiation_on:
+            res["ifront_cells"] = ifront_cells(s.Q[2], n)
+            res["ifront_diff_cells"] = abs(res["ifront_cells"] - out["ifront_fp64_cells"])
+        out[name] = res
+    out["wall_s"] = time.perf_counter() - t0
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_ours(args, world, rank, local, pg):
     import torch
     import torch_b200
@@ -555,6 +635,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["hii", "sedov", "batch"], default="hii")
     ap.add_argument("--grids", type=int, default=256, help="grids of the batch workload")
+    ap.add_argument("--fp32-contrast", type=float, default=None,
+                    help="pressure ratio above which the FP32 form updates a hydro cell in FP64 (library default 1e3)")
+    ap.add_argument("--validate", type=int, default=0,
+                    help="instead of timing: error of the FP32 form against the FP64 form after this many steps")
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--precision", choices=["both", "fp32", "fp64"], default="both")
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -569,6 +653,8 @@ def main():
     try:
         if args.impl == "reference":
             return run_reference_arm(args, rank)
+        if args.validate:
+            return run_validate(args, rank, local)
         if args.workload == "batch":
             return run_batch(args, world, rank, local, pg)
         return run_ours(args, world, rank, local, pg)
