@@ -1,7 +1,7 @@
 """FP32 form of the hydro pass against the FP64 form (which is bit-exact with
 the CPU oracle): relative L1 error of density, pressure and energy.
 
-Bound: 1e-4 per field (the north-star FP32 bar), 1e-5 for the Sedov blast.
+Bound: 1e-4 per field (the bar set for the FP32 form), 1e-5 for the Sedov blast.
 """
 import numpy as np
 import pytest

@@ -2,7 +2,7 @@
 
 * Against the reference (golden fixtures written by the reference build) and
   the glibc oracle (bit-exact with the reference): relative L1 <= 1e-10 per
-  field (the north-star FP64 bar) up to 40 radiation-hydro steps; hydro-only
+  field (the bar set for the FP64 form) up to 40 radiation-hydro steps; hydro-only
   runs are bit-exact for 100 steps.
 * Against the portable-math oracle (same exp/log/log10/pow as the kernels,
   torch_b200/csrc/trg_math.h): bit-exact for 100 radiation-hydro steps.

@@ -114,7 +114,7 @@ def tolerance_probe_params(delta=4.342727686266e-4):
     """A network whose output is constant: every front cell is predicted slow
     and starts at odds (1 + 1e-3) times those of the plain start, one solver
     tolerance away.  The state change this causes is the scale against which
-    the learned start's change is judged."""
+    the learned start's change is compared."""
     p = np.zeros(torch_b200.MLP_NPARAMS, dtype=np.float32)
     n = torch_b200.MLP_NTRAIN
     p[n - 3:n] = (delta, 0.0, 2.0)
