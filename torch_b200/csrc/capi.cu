@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <utility>
@@ -24,6 +25,11 @@ using namespace trg;
 
 namespace {
 constexpr int COMP_HYDRO = 0, COMP_RAD = 1, COMP_THERMO = 2;
+}
+
+inline bool shell_overlap_default() {
+	const char* v = std::getenv("TRG_SHELL_OVERLAP");
+	return !(v && v[0] == '0');
 }
 
 struct trg_ctx {
@@ -65,6 +71,9 @@ struct trg_ctx {
 	long long g_tau_nodes = 0;
 	long long g_colden_nodes = 0, g_rad_nodes[2] = {0, 0};
 	bool use_graphs = true;
+	// shells after the first of a sweep start while the previous one runs
+	// (programmatic dependent launch); TRG_SHELL_OVERLAP=0 serialises them
+	bool shell_overlap = shell_overlap_default();
 	// per-grid scalar kernels (dt, time) run on this many threads: 1, or the
 	// number of grids of a batch
 	int nscalar = 1;
@@ -157,6 +166,36 @@ void profile_collect(trg_ctx* c) {
 		}                                                                                    \
 	} while (0)
 
+// A shell of a causal sweep.  Every shell after the first of a sweep is
+// launched with programmatic stream serialisation: its CTAs may start while
+// the previous shell runs and wait for it inside the kernel (sweep_wait).
+template <typename... KArgs, typename... Args>
+void launch_shell(trg_ctx* c, void (*kernel)(KArgs...), int n, int block, bool overlap, Args... args) {
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = dim3(grid_for(n, block));
+	cfg.blockDim = dim3(block);
+	cfg.dynamicSmemBytes = 0;
+	cfg.stream = c->stream;
+	cudaLaunchAttribute attr[1];
+	attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	attr[0].val.programmaticStreamSerializationAllowed = 1;
+	cfg.attrs = attr;
+	cfg.numAttrs = overlap && c->shell_overlap ? 1 : 0;
+	cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+#define LAUNCH_SHELL(kernel, n, block, overlap, ...)                                          \
+	do {                                                                                     \
+		if ((n) > 0) {                                                                       \
+			cudaEvent_t ea_ = nullptr, eb_ = nullptr;                                        \
+			if (c->profiling) { ea_ = pool_event(c); eb_ = pool_event(c);                    \
+			                    cudaEventRecord(ea_, c->stream); }                           \
+			launch_shell(c, kernel, (n), (block), (overlap), __VA_ARGS__);                   \
+			if (c->profiling) { cudaEventRecord(eb_, c->stream);                             \
+			                    c->recs.push_back({#kernel, ea_, eb_}); }                    \
+			c->launches++;                                                                   \
+		}                                                                                    \
+	} while (0)
+
 // sel: 0 = S.U, 1 = S.U1
 #define LAUNCH_SCALAR(kernel, ...) LAUNCH(kernel, c->nscalar, c->nscalar > 1 ? 64 : 1, __VA_ARGS__)
 
@@ -166,7 +205,7 @@ void colden_sweep_direct(trg_ctx* c) {
 	const auto& off = c->hs.off_all;
 	for (size_t s = 0; s + 1 < off.size(); ++s) {
 		int count = (int)(off[s + 1] - off[s]);
-		LAUNCH(KF(k_colden_shell_fp64), count, 128, c->P, c->S, c->d_sweep_all + off[s], count);
+		LAUNCH_SHELL(KF(k_colden_shell_fp64), count, 128, s > 0, c->P, c->S, c->d_sweep_all + off[s], count);
 	}
 }
 
@@ -230,7 +269,7 @@ void hydro_fluxes(trg_ctx* c) {
 // One shell of the radiation sweep: the plain kernel, or with a network
 // loaded the learned-start kernel (its tensor-core tile needs dynamic shared
 // memory and 64 TMEM columns per CTA).
-void rad_shell_launch(trg_ctx* c, const int* cells, int count, double h) {
+void rad_shell_launch(trg_ctx* c, const int* cells, int count, double h, bool overlap) {
 	if (c->S.mlp_img) {
 		cudaEvent_t ea = nullptr, eb = nullptr;
 		if (c->profiling) { ea = pool_event(c); eb = pool_event(c); cudaEventRecord(ea, c->stream); }
@@ -239,8 +278,8 @@ void rad_shell_launch(trg_ctx* c, const int* cells, int count, double h) {
 		c->launches++;
 		return;
 	}
-	if (c->P.stats_on || c->S.harvest) LAUNCH(KF(k_rad_shell_diag), count, 128, c->P, c->S, cells, count, h);
-	else LAUNCH(KF(k_rad_shell_fp64), count, 128, c->P, c->S, cells, count, h);
+	if (c->P.stats_on || c->S.harvest) LAUNCH_SHELL(KF(k_rad_shell_diag), count, 128, overlap, c->P, c->S, cells, count, h);
+	else LAUNCH_SHELL(KF(k_rad_shell_fp64), count, 128, overlap, c->P, c->S, cells, count, h);
 }
 
 void rad_sweep_direct(trg_ctx* c, double h) {
@@ -249,7 +288,7 @@ void rad_sweep_direct(trg_ctx* c, double h) {
 	const auto& off = c->hs.off_nonwind;
 	for (size_t s = 0; s + 1 < off.size(); ++s) {
 		int count = (int)(off[s + 1] - off[s]);
-		rad_shell_launch(c, c->d_sweep_nonwind + off[s], count, h);
+		rad_shell_launch(c, c->d_sweep_nonwind + off[s], count, h, s > 0);
 	}
 }
 
@@ -261,7 +300,7 @@ void tau_sweep_direct(trg_ctx* c) {
 	const auto& off = c->hs.off_nonwind;
 	for (size_t s = 0; s + 1 < off.size(); ++s) {
 		int count = (int)(off[s + 1] - off[s]);
-		LAUNCH(KF(k_rad_tau_shell), count, 128, c->P, c->S, c->d_sweep_nonwind + off[s], count);
+		LAUNCH_SHELL(KF(k_rad_tau_shell), count, 128, s > 0, c->P, c->S, c->d_sweep_nonwind + off[s], count);
 	}
 }
 
@@ -294,7 +333,7 @@ void rad_integrate(trg_ctx* c, double h) {
 		const auto& off = c->hs.off_nonwind;
 		for (size_t s = 0; s + 1 < off.size(); ++s) {
 			int count = (int)(off[s + 1] - off[s]);
-			rad_shell_launch(c, c->d_sweep_nonwind + off[s], count, h);
+			rad_shell_launch(c, c->d_sweep_nonwind + off[s], count, h, s > 0);
 		}
 	} else {
 		LAUNCH(KF(k_rad_no_star_fp64), c->P.N, 256, c->P, c->S, h);

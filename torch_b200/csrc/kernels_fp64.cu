@@ -583,13 +583,28 @@ __device__ __forceinline__ double dist2_cells(const Params& P, const double* xc)
 	return d2;
 }
 
-// Radiation::updateTauSC, Radiation.cpp:353-373.
+// Programmatic dependent launch.  The shells of a sweep after the first are
+// launched with programmatic stream serialisation, so that a shell's CTAs can
+// start while the previous shell still runs.  What a shell kernel does before
+// sweep_wait() reads only fields of its own cells that no shell of the sweep
+// writes (density, pressure, fractions, path lengths, volumes) and the rate
+// tables; sweep_wait() returns once the previous shell has completed and its
+// writes are visible (at once when the launch had no such dependency).  Each
+// shell lets the next one launch only after its own wait, so at most two
+// shells are resident at a time.
+__device__ __forceinline__ void sweep_wait() {
+	asm volatile("griddepcontrol.wait;" ::: "memory");
+	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Radiation::updateTauSC, Radiation.cpp:353-373.  Neighbour optical depths
+// written by the previous shell are read past L1.
 __device__ __forceinline__ double tau_sc(const Params& P, const State& S, const long long* nb, const double* w0, int rt, int rd) {
 	double tau[4] = {0, 0, 0, 0}, w[4];
 	for (int i = 0; i < 4; ++i) {
 		// A zero-weight neighbour contributes 0 * tau = 0 whatever its tau, and
 		// may belong to the shell being swept: it is not read.
-		if (nb[i] >= 0 && w0[i] != 0) tau[i] = FLD(S.R, rt, nb[i]) + FLD(S.R, rd, nb[i]);
+		if (nb[i] >= 0 && w0[i] != 0) tau[i] = __ldcg(&FLD(S.R, rt, nb[i])) + __ldcg(&FLD(S.R, rd, nb[i]));
 		w[i] = w0[i] / smax(P.tau0, tau[i]);
 	}
 	double sum_w = w[0] + w[1] + w[2] + w[3];
@@ -667,26 +682,19 @@ __device__ __forceinline__ double inv_logit10(float l) {
 template <bool LEARNED, bool DIAG>
 __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const long long id, const bool valid,
                                           double h) {
-	if (!LEARNED && !valid) return;
 	const double dt = h * S.scal[0];
-	bool star = false, front = false;
+	bool star = false, front = false, inner = false;
 	double q_den = 0, q_pre = 0, q_hii = 0, ds = 0, n_H = 0, T = 1, alphaB = 0, A_ci = 0, tau_avg = 0, shellVol = 0;
+	long long nb[4] = {-1, -1, -1, -1};
+	double w[4] = {0, 0, 0, 0};
 	if (valid) {
+		// everything that does not depend on the inner shells
 		int ijk[3];
 		double xc[3];
 		cell_ijk(P, id, ijk);
 		cell_xc(P, ijk, xc);
-		double dist2 = dist2_cells(P, xc);
-		if (dist2 > 0.95) {
-			long long nb[4];
-			double w[4];
-			neighbours(P, ijk, xc, nb, w);
-			FLD(S.R, R_TAU, id) = tau_sc(P, S, nb, w, R_TAU, R_DTAU);
-			FLD(S.R, R_TAU_A, id) = tau_sc(P, S, nb, w, R_TAU_A, R_DTAU_A);
-		} else {
-			FLD(S.R, R_TAU, id) = 0;
-			FLD(S.R, R_TAU_A, id) = 0;
-		}
+		inner = dist2_cells(P, xc) > 0.95;
+		if (inner) neighbours(P, ijk, xc, nb, w);
 		// Radiation::isStar (Radiation.cpp:682-684): z compares an int with a double.
 		star = (int)xc[0] == (int)P.sxc[0] && (int)xc[1] == (int)P.sxc[1] && (double)(int)xc[2] == P.sxc[2];
 		q_den = FLD(S.Q, DEN, id);
@@ -698,8 +706,18 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 			T = calc_temperature(P, q_hii, q_pre, q_den);
 			alphaB = spline_eval(S.tables->rad_recomb, T);
 			A_ci = collisional_ionisation_rate(P, T);
-			tau_avg = FLD(S.R, R_TAU_A, id);
 			shellVol = S.shellVol[id];
+		}
+	}
+	sweep_wait();
+	if (!LEARNED && !valid) return;
+	if (valid) {
+		const double tau = inner ? tau_sc(P, S, nb, w, R_TAU, R_DTAU) : 0.0;
+		const double tau_a = inner ? tau_sc(P, S, nb, w, R_TAU_A, R_DTAU_A) : 0.0;
+		FLD(S.R, R_TAU, id) = tau;
+		FLD(S.R, R_TAU_A, id) = tau_a;
+		if (!star) {
+			tau_avg = tau_a;
 			front = front_cell(tau_avg, q_hii);
 		}
 	}
@@ -721,6 +739,7 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 		if (!valid) return;
 	}
 	unsigned iters = 0;
+	double hii_new = 1, hii_a_new = 1;
 	if (star) {
 		FLD(S.R, R_HEAT, id) = 0;
 		FLD(S.Q, HII, id) = 1;
@@ -769,6 +788,8 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 		}
 		FLD(S.R, R_HII_A, id) = HII_avg;
 		FLD(S.Q, HII, id) = x_new;
+		hii_a_new = HII_avg;
+		hii_new = x_new;
 		if (x_new > 0.001) FLD(S.Q, ADV, id) = 1;
 		iters += (unsigned)miter * 10006u + (unsigned)niter;
 		if (LEARNED && DIAG && P.stats_on && used_learned) stat_add(S.stats, TRG_STAT_LEARNED_ITERS, iters);
@@ -785,8 +806,8 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 		}
 	}
 	double nH = P.X * q_den / P.hydrogenMass;
-	FLD(S.R, R_DTAU, id) = (1.0 - FLD(S.Q, HII, id)) * nH * P.photoIonXsec * ds;
-	FLD(S.R, R_DTAU_A, id) = (1.0 - FLD(S.R, R_HII_A, id)) * nH * P.photoIonXsec * ds;
+	FLD(S.R, R_DTAU, id) = (1.0 - hii_new) * nH * P.photoIonXsec * ds;
+	FLD(S.R, R_DTAU_A, id) = (1.0 - hii_a_new) * nH * P.photoIonXsec * ds;
 	if (DIAG && P.stats_on) {
 		stat_picard(S.stats, iters);
 		stat_add(S.stats, TRG_STAT_FRONT_CELLS, front ? 1u : 0u);
@@ -831,18 +852,17 @@ __device__ __forceinline__ void b_rad_tau_shell(const Params& P, const State& S,
 	double xc[3];
 	cell_ijk(P, id, ijk);
 	cell_xc(P, ijk, xc);
-	double dist2 = dist2_cells(P, xc);
-	if (dist2 > 0.95) {
-		long long nb[4];
-		double w[4];
-		neighbours(P, ijk, xc, nb, w);
-		FLD(S.R, R_TAU, id) = tau_sc(P, S, nb, w, R_TAU, R_DTAU);
-	} else {
-		FLD(S.R, R_TAU, id) = 0;
-	}
-	double nH = P.X * FLD(S.Q, DEN, id) / P.hydrogenMass;
-	FLD(S.R, R_DTAU, id) = (1.0 - FLD(S.Q, HII, id)) * nH * P.photoIonXsec * S.ds[id];
-	FLD(S.R, R_DTAU_A, id) = (1.0 - FLD(S.R, R_HII_A, id)) * nH * P.photoIonXsec * S.ds[id];
+	const bool inner = dist2_cells(P, xc) > 0.95;
+	long long nb[4];
+	double w[4];
+	if (inner) neighbours(P, ijk, xc, nb, w);
+	const double nH = P.X * FLD(S.Q, DEN, id) / P.hydrogenMass;
+	const double dtau = (1.0 - FLD(S.Q, HII, id)) * nH * P.photoIonXsec * S.ds[id];
+	const double dtau_a = (1.0 - FLD(S.R, R_HII_A, id)) * nH * P.photoIonXsec * S.ds[id];
+	sweep_wait();
+	FLD(S.R, R_TAU, id) = inner ? tau_sc(P, S, nb, w, R_TAU, R_DTAU) : 0.0;
+	FLD(S.R, R_DTAU, id) = dtau;
+	FLD(S.R, R_DTAU_A, id) = dtau_a;
 }
 __global__ void __launch_bounds__(128) k_rad_tau_shell(Params P, State S, const int* __restrict__ cells, int count) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1100,14 +1120,18 @@ __device__ __forceinline__ void b_colden_shell_fp64(const Params& P, const State
 	double xc[3];
 	cell_ijk(P, id, ijk);
 	cell_xc(P, ijk, xc);
-	double dist2 = dist2_cells(P, xc);
+	const bool inner = dist2_cells(P, xc) > 0.95 * 0.95;
+	long long nb[4];
+	double w0[4];
+	if (inner) neighbours(P, ijk, xc, nb, w0);
+	const double dcolden = (FLD(S.Q, DEN, id) / P.hydrogenMass) * S.ds[id];
+	sweep_wait();
 	double newcolden = 0.0;
-	if (dist2 > 0.95 * 0.95) {
-		long long nb[4];
-		double w0[4], colden[4] = {0, 0, 0, 0}, w[4];
-		neighbours(P, ijk, xc, nb, w0);
+	if (inner) {
+		double colden[4] = {0, 0, 0, 0}, w[4];
 		for (int i = 0; i < 4; ++i) {
-			if (nb[i] >= 0 && w0[i] != 0) colden[i] = FLD(S.T, T_COL_DEN, nb[i]) + FLD(S.T, T_DCOL_DEN, nb[i]);
+			if (nb[i] >= 0 && w0[i] != 0)
+				colden[i] = __ldcg(&FLD(S.T, T_COL_DEN, nb[i])) + __ldcg(&FLD(S.T, T_DCOL_DEN, nb[i]));
 			w[i] = colden[i] == 0 ? 0 : w0[i] / colden[i];
 		}
 		double sum_w = w[0] + w[1] + w[2] + w[3];
@@ -1117,7 +1141,7 @@ __device__ __forceinline__ void b_colden_shell_fp64(const Params& P, const State
 		}
 	}
 	FLD(S.T, T_COL_DEN, id) = newcolden;
-	FLD(S.T, T_DCOL_DEN, id) = (FLD(S.Q, DEN, id) / P.hydrogenMass) * S.ds[id];
+	FLD(S.T, T_DCOL_DEN, id) = dcolden;
 }
 __global__ void __launch_bounds__(128) k_colden_shell_fp64(Params P, State S, const int* __restrict__ cells, int count) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
