@@ -199,6 +199,31 @@ void launch_shell(trg_ctx* c, void (*kernel)(KArgs...), int n, int block, bool o
 // sel: 0 = S.U, 1 = S.U1
 #define LAUNCH_SCALAR(kernel, ...) LAUNCH(kernel, c->nscalar, c->nscalar > 1 ? 64 : 1, __VA_ARGS__)
 
+// R and T between the C ABI's field-after-field order (soa) and the device
+// layout (trg_types.h); U1, free between calls, stages the other side.
+__global__ void k_layout_rt(long long N, int nf, const double* __restrict__ src, double* __restrict__ dst,
+                            int to_device) {
+	const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (i >= nf * N) return;
+	const int f = (int)(i / N);
+	const long long id = i - f * N;
+	const long long d = nf == 6 ? r_index(N, f, id) : t_index(N, f, id);
+	if (to_device) dst[d] = src[i];
+	else dst[i] = src[d];
+}
+int upload_rt(trg_ctx* c, double* dev, const double* host, int nf) {
+	const long long N = c->P.N;
+	CUDA_TRY(cudaMemcpyAsync(c->S.U1, host, nf * N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+	k_layout_rt<<<grid_for(nf * N, 256), 256, 0, c->stream>>>(N, nf, c->S.U1, dev, 1);
+	return TRG_OK;
+}
+int download_rt(trg_ctx* c, double* host, const double* dev, int nf) {
+	const long long N = c->P.N;
+	k_layout_rt<<<grid_for(nf * N, 256), 256, 0, c->stream>>>(N, nf, dev, c->S.U1, 0);
+	CUDA_TRY(cudaMemcpyAsync(host, c->S.U1, nf * N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+	return TRG_OK;
+}
+
 void q_from_u(trg_ctx* c, int sel, int fix) { LAUNCH(KF(k_q_from_u_fp64), c->P.N, 256, c->P, c->S, sel, fix); }
 
 void colden_sweep_direct(trg_ctx* c) {
@@ -582,8 +607,7 @@ int trg_create(const trg_params* p, const double* den, const double* pre, const 
 	cudaStream_t st = c->stream;
 	CUDA_TRY(cudaMemcpyAsync(S.U, c->hs.U.data(), 7 * N * sizeof(double), cudaMemcpyHostToDevice, st));
 	CUDA_TRY(cudaMemcpyAsync(S.Q, c->hs.Q.data(), 7 * N * sizeof(double), cudaMemcpyHostToDevice, st));
-	CUDA_TRY(cudaMemcpyAsync(S.R, c->hs.R.data(), 6 * N * sizeof(double), cudaMemcpyHostToDevice, st));
-	CUDA_TRY(cudaMemcpyAsync(S.T, c->hs.T.data(), 4 * N * sizeof(double), cudaMemcpyHostToDevice, st));
+	if ((rc = upload_rt(c, S.R, c->hs.R.data(), 6)) || (rc = upload_rt(c, S.T, c->hs.T.data(), 4))) return rc;
 	CUDA_TRY(cudaMemcpyAsync(S.Tmin, c->hs.Tmin.data(), N * sizeof(double), cudaMemcpyHostToDevice, st));
 	CUDA_TRY(cudaMemcpyAsync(S.ds, c->hs.ds.data(), N * sizeof(double), cudaMemcpyHostToDevice, st));
 	CUDA_TRY(cudaMemcpyAsync(S.shellVol, c->hs.shellVol.data(), N * sizeof(double), cudaMemcpyHostToDevice, st));
@@ -756,8 +780,9 @@ int trg_get_state(trg_ctx* c, double* U, double* Q, double* R, double* T, double
 	}
 	if (U) CUDA_TRY(cudaMemcpyAsync(U, c->S.U, 7 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
 	if (Q) CUDA_TRY(cudaMemcpyAsync(Q, c->S.Q, 7 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
-	if (R) CUDA_TRY(cudaMemcpyAsync(R, c->S.R, 6 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
-	if (T) CUDA_TRY(cudaMemcpyAsync(T, c->S.T, 4 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
+	int rc = 0;
+	if (R && (rc = download_rt(c, R, c->S.R, 6))) return rc;
+	if (T && (rc = download_rt(c, T, c->S.T, 4))) return rc;
 	if (Tmin) CUDA_TRY(cudaMemcpyAsync(Tmin, c->S.Tmin, N * sizeof(double), cudaMemcpyDeviceToHost, st));
 	CUDA_TRY(cudaStreamSynchronize(st));
 	return TRG_OK;
@@ -776,6 +801,7 @@ int trg_set_conserved(trg_ctx* c, const double* U) {
 namespace {
 struct CkptHeader {
 	char magic[8];
+	// version 2: R and T in the grouped device layout (trg_types.h)
 	int version, form;  // form: 0 FP64, 1 FP32 hydro-only, 2 FP32 with radiation/cooling
 	long long N;
 	int nx, ny, nz, nd;
@@ -798,7 +824,7 @@ int trg_checkpoint_save(trg_ctx* c, void* buf, long long bytes) {
 	CUDA_TRY(cudaStreamSynchronize(c->stream));
 	CkptHeader h{};
 	memcpy(h.magic, "TRGCKPT1", 8);
-	h.version = 1;
+	h.version = 2;
 	h.form = ckpt_form(c);
 	h.N = c->P.N;
 	h.nx = c->P.nx;
@@ -829,7 +855,7 @@ int trg_checkpoint_load(trg_ctx* c, const void* buf, long long bytes) {
 	if (!c || !buf || bytes < (long long)sizeof(CkptHeader)) return TRG_ERR_ARG;
 	CkptHeader h;
 	memcpy(&h, buf, sizeof(h));
-	if (memcmp(h.magic, "TRGCKPT1", 8) != 0 || h.version != 1)
+	if (memcmp(h.magic, "TRGCKPT1", 8) != 0 || h.version != 2)
 		return set_error(c, TRG_ERR_ARG, "trg_checkpoint_load: not a checkpoint of this library");
 	if (h.form != ckpt_form(c) || h.N != c->P.N || h.nx != c->P.nx || h.ny != c->P.ny || h.nz != c->P.nz ||
 	    h.nd != c->P.nd || bytes < trg_checkpoint_bytes(c))

@@ -494,11 +494,16 @@ __global__ void __launch_bounds__(256) k_advance_fp64(Params P, State S, double 
 
 // ------------------------------------------------------------------ radiation
 // Radiation.cpp:243-251.
-__device__ __forceinline__ double photoionisation_rate(double nHI, double T, double delT, double shellVol, double photonRate) {
+// emT = exp(-T), passed in where T is fixed across calls.
+__device__ __forceinline__ double photoionisation_rate_e(double nHI, double emT, double delT, double shellVol,
+                                                         double photonRate) {
 	if (nHI == 0 || shellVol == 0) return 0.0;
-	double emT = d_exp(-T);
 	double emdT = d_exp(-delT);
 	return photonRate * emT * (1.0 - emdT) / (nHI * shellVol);
+}
+__device__ __forceinline__ double photoionisation_rate(double nHI, double T, double delT, double shellVol, double photonRate) {
+	if (nHI == 0 || shellVol == 0) return 0.0;
+	return photoionisation_rate_e(nHI, d_exp(-T), delT, shellVol, photonRate);
 }
 
 // Voronov (1997) fit, Radiation.cpp:231-237.
@@ -597,16 +602,11 @@ __device__ __forceinline__ void sweep_wait() {
 	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
-// Radiation::updateTauSC, Radiation.cpp:353-373.  Neighbour optical depths
-// written by the previous shell are read past L1.
-__device__ __forceinline__ double tau_sc(const Params& P, const State& S, const long long* nb, const double* w0, int rt, int rd) {
-	double tau[4] = {0, 0, 0, 0}, w[4];
-	for (int i = 0; i < 4; ++i) {
-		// A zero-weight neighbour contributes 0 * tau = 0 whatever its tau, and
-		// may belong to the shell being swept: it is not read.
-		if (nb[i] >= 0 && w0[i] != 0) tau[i] = __ldcg(&FLD(S.R, rt, nb[i])) + __ldcg(&FLD(S.R, rd, nb[i]));
-		w[i] = w0[i] / smax(P.tau0, tau[i]);
-	}
+// Radiation::updateTauSC, Radiation.cpp:353-373: the weighted interpolation of
+// the inner neighbours' optical depths tau[i] (zero where not read).
+__device__ __forceinline__ double tau_interp(const Params& P, const double* tau, const double* w0) {
+	double w[4];
+	for (int i = 0; i < 4; ++i) w[i] = w0[i] / smax(P.tau0, tau[i]);
 	double sum_w = w[0] + w[1] + w[2] + w[3];
 	double newtau = 0.0;
 	for (int i = 0; i < 4; ++i) {
@@ -615,15 +615,48 @@ __device__ __forceinline__ double tau_sc(const Params& P, const State& S, const 
 	}
 	return newtau;
 }
+// A zero-weight neighbour contributes 0 * tau = 0 whatever its tau, and may
+// belong to the shell being swept: it is not read.  Neighbour optical depths
+// written by the previous shell are read past L1, one 16-byte pair (TAU, DTAU
+// or TAU_A, DTAU_A) at a time.
+__device__ __forceinline__ bool nb_read(const long long* nb, const double* w0, int i) { return nb[i] >= 0 && w0[i] != 0; }
+// TAU (from TAU + DTAU of the neighbours)
+__device__ __forceinline__ double tau_sc(const Params& P, const State& S, const long long* nb, const double* w0) {
+	double tau[4] = {0, 0, 0, 0};
+	for (int i = 0; i < 4; ++i)
+		if (nb_read(nb, w0, i)) {
+			const double2 a = __ldcg(reinterpret_cast<const double2*>(S.R + nb[i] * 4));
+			tau[i] = a.x + a.y;
+		}
+	return tau_interp(P, tau, w0);
+}
+// TAU and TAU_A together (each neighbour's four optical depths share a sector)
+__device__ __forceinline__ void tau_sc2(const Params& P, const State& S, const long long* nb, const double* w0,
+                                        double& tau_out, double& tau_a_out) {
+	double tau[4] = {0, 0, 0, 0}, tau_a[4] = {0, 0, 0, 0};
+	for (int i = 0; i < 4; ++i)
+		if (nb_read(nb, w0, i)) {
+			const double2* q = reinterpret_cast<const double2*>(S.R + nb[i] * 4);
+			const double2 a = __ldcg(q), b = __ldcg(q + 1);
+			tau[i] = a.x + a.y;
+			tau_a[i] = b.x + b.y;
+		}
+	tau_out = tau_interp(P, tau, w0);
+	tau_a_out = tau_interp(P, tau_a, w0);
+}
+// All four optical depths of a cell in one store.
+__device__ __forceinline__ void store_taus(const State& S, long long id, double tau, double dtau, double tau_a,
+                                           double dtau_a) {
+	double2* q = reinterpret_cast<double2*>(S.R + id * 4);
+	q[0] = make_double2(tau, dtau);
+	q[1] = make_double2(tau_a, dtau_a);
+}
 
 // Wind cells of Radiation::transferRadiation, Radiation.cpp:590-598.
 __device__ __forceinline__ void b_rad_wind_reset(const Params& P, const State& S, long long id) {
-	FLD(S.R, R_TAU, id) = 0;
-	FLD(S.R, R_TAU_A, id) = 0;
-	FLD(S.R, R_DTAU, id) = 0;
-	FLD(S.R, R_DTAU_A, id) = 0;
+	store_taus(S, id, 0, 0, 0, 0);
 	FLD(S.Q, HII, id) = 1;
-	FLD(S.R, R_HII_A, id) = 1;
+	RFLD(S.R, R_HII_A, id) = 1;
 }
 __global__ void k_rad_wind_reset(Params P, State S, const int* __restrict__ cells, int count) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -634,6 +667,33 @@ __global__ void k_rad_wind_reset(Params P, State S, const int* __restrict__ cell
 		return;
 	}
 	b_rad_wind_reset(P, S, cells[t]);
+}
+
+// Radiation::preTimeStepCalculations for one non-wind cell (Radiation.cpp:257-296):
+// the heating rate from the current fractions and optical depths.
+__device__ __forceinline__ void rad_heating_cell(const Params& P, const State& S, long long id, double q_hii,
+                                                 double q_pre, double q_den) {
+	double Tmin = S.Tmin[id];
+	double n_H = (P.X * q_den / P.hydrogenMass);
+	double excessEnergy = P.photonEnergy - P.rydbergEnergy;
+	double T = calc_temperature(P, q_hii, q_pre, q_den);
+	double nHI = (1.0 - q_hii) * n_H;
+	double A_pi = photoionisation_rate(nHI, RFLD(S.R, R_TAU, id), RFLD(S.R, R_DTAU, id), S.shellVol[id], P.photonRate);
+	double photoion = n_H * (1.0 - q_hii) * A_pi * excessEnergy;
+	double rate_rc = spline_eval(S.tables->rad_cool, T);
+	double recombination = q_hii * q_hii * n_H * n_H * P.boltzmannConst * T * rate_rc;
+	double collisions = q_hii * (1.0 - q_hii) * n_H * n_H * collisional_ionisation_rate(P, T);
+	double rate = photoion - recombination - collisions;
+	double softrate = rate;
+	if (T < Tmin + 200 && rate < 0.0) softrate = smin(0.0, softrate * (T - Tmin) / 200.0);
+	softrate *= P.heating_amp;
+	RFLD(S.R, R_HEAT, id) = softrate;
+	if (S.H) {
+		// Radiation.cpp:278-279 (0/0 when rate is 0, as in the reference)
+		FLD(S.H, H_EUVH, id) = photoion * (softrate / rate);
+		FLD(S.H, H_RHII, id) = -recombination * (softrate / rate);
+	}
+	if (rate != rate) atomicOr(S.err, ERRB_NAN);
 }
 
 // Learned starting iterate: cells whose solve may take more than one Picard
@@ -711,11 +771,9 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 	}
 	sweep_wait();
 	if (!LEARNED && !valid) return;
+	double tau = 0, tau_a = 0;
 	if (valid) {
-		const double tau = inner ? tau_sc(P, S, nb, w, R_TAU, R_DTAU) : 0.0;
-		const double tau_a = inner ? tau_sc(P, S, nb, w, R_TAU_A, R_DTAU_A) : 0.0;
-		FLD(S.R, R_TAU, id) = tau;
-		FLD(S.R, R_TAU_A, id) = tau_a;
+		if (inner) tau_sc2(P, S, nb, w, tau, tau_a);
 		if (!star) {
 			tau_avg = tau_a;
 			front = front_cell(tau_avg, q_hii);
@@ -741,9 +799,9 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 	unsigned iters = 0;
 	double hii_new = 1, hii_a_new = 1;
 	if (star) {
-		FLD(S.R, R_HEAT, id) = 0;
+		RFLD(S.R, R_HEAT, id) = 0;
 		FLD(S.Q, HII, id) = 1;
-		FLD(S.R, R_HII_A, id) = 1;
+		RFLD(S.R, R_HII_A, id) = 1;
 	} else {
 		double A_pi = 0;
 		double x_new = q_hii;
@@ -751,13 +809,14 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 		double HII_avg_old;
 		int niter = 0, miter = 0;
 		bool converged = false;
+		const double em_tau = d_exp(-tau_avg);  // the same in every iteration
 		while (!converged) {
 			niter++;
 			HII_avg_old = HII_avg;
 			x_new = q_hii;
 			double dtau_avg = (1.0 - HII_avg) * n_H * P.photoIonXsec * ds;
 			double nHI = (1.0 - HII_avg) * n_H;
-			A_pi = photoionisation_rate(nHI, tau_avg, dtau_avg, shellVol, P.photonRate);
+			A_pi = photoionisation_rate_e(nHI, em_tau, dtau_avg, shellVol, P.photonRate);
 			double nHII_aB = HII_avg * n_H * alphaB;
 			double nHII_Aci = HII_avg * n_H * A_ci;
 			doric(dt, HII_avg, x_new, A_pi, nHII_aB, nHII_Aci);
@@ -786,7 +845,7 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 				break;
 			}
 		}
-		FLD(S.R, R_HII_A, id) = HII_avg;
+		RFLD(S.R, R_HII_A, id) = HII_avg;
 		FLD(S.Q, HII, id) = x_new;
 		hii_a_new = HII_avg;
 		hii_new = x_new;
@@ -806,8 +865,7 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 		}
 	}
 	double nH = P.X * q_den / P.hydrogenMass;
-	FLD(S.R, R_DTAU, id) = (1.0 - hii_new) * nH * P.photoIonXsec * ds;
-	FLD(S.R, R_DTAU_A, id) = (1.0 - hii_a_new) * nH * P.photoIonXsec * ds;
+	store_taus(S, id, tau, (1.0 - hii_new) * nH * P.photoIonXsec * ds, tau_a, (1.0 - hii_a_new) * nH * P.photoIonXsec * ds);
 	if (DIAG && P.stats_on) {
 		stat_picard(S.stats, iters);
 		stat_add(S.stats, TRG_STAT_FRONT_CELLS, front ? 1u : 0u);
@@ -858,11 +916,11 @@ __device__ __forceinline__ void b_rad_tau_shell(const Params& P, const State& S,
 	if (inner) neighbours(P, ijk, xc, nb, w);
 	const double nH = P.X * FLD(S.Q, DEN, id) / P.hydrogenMass;
 	const double dtau = (1.0 - FLD(S.Q, HII, id)) * nH * P.photoIonXsec * S.ds[id];
-	const double dtau_a = (1.0 - FLD(S.R, R_HII_A, id)) * nH * P.photoIonXsec * S.ds[id];
+	const double dtau_a = (1.0 - RFLD(S.R, R_HII_A, id)) * nH * P.photoIonXsec * S.ds[id];
 	sweep_wait();
-	FLD(S.R, R_TAU, id) = inner ? tau_sc(P, S, nb, w, R_TAU, R_DTAU) : 0.0;
-	FLD(S.R, R_DTAU, id) = dtau;
-	FLD(S.R, R_DTAU_A, id) = dtau_a;
+	RFLD(S.R, R_TAU, id) = inner ? tau_sc(P, S, nb, w) : 0.0;
+	RFLD(S.R, R_DTAU, id) = dtau;
+	RFLD(S.R, R_DTAU_A, id) = dtau_a;
 }
 __global__ void __launch_bounds__(128) k_rad_tau_shell(Params P, State S, const int* __restrict__ cells, int count) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -885,9 +943,9 @@ __device__ __forceinline__ void b_rad_solve2(const Params& P, const State& S, lo
 	cell_xc(P, ijk, xc);
 	const double dt = h * S.scal[0];
 	if ((int)xc[0] == (int)P.sxc[0] && (int)xc[1] == (int)P.sxc[1] && (double)(int)xc[2] == P.sxc[2]) {
-		FLD(S.R, R_HEAT, id) = 0;
+		RFLD(S.R, R_HEAT, id) = 0;
 		FLD(S.Q, HII, id) = 1;
-		FLD(S.R, R_HII_A, id) = 1;
+		RFLD(S.R, R_HII_A, id) = 1;
 		return;
 	}
 	const double q_den = FLD(S.Q, DEN, id), q_pre = FLD(S.Q, PRE, id), q_hii = FLD(S.Q, HII, id);
@@ -899,7 +957,7 @@ __device__ __forceinline__ void b_rad_solve2(const Params& P, const State& S, lo
 	double x = q_hii;
 	if (P.rt_scheme == 1) {
 		double x_avg = x, x_avg_old, A_pi;
-		const double tau_avg = FLD(S.R, R_TAU, id);
+		const double tau_avg = RFLD(S.R, R_TAU, id);
 		int niter = 0, miter = 0;
 		bool converged = false;
 		while (!converged) {
@@ -923,11 +981,11 @@ __device__ __forceinline__ void b_rad_solve2(const Params& P, const State& S, lo
 				break;
 			}
 		}
-		FLD(S.R, R_HII_A, id) = x_avg;
+		RFLD(S.R, R_HII_A, id) = x_avg;
 	} else {
 		const double x_avg = x;
 		const double nHI = (1.0 - x) * (P.X * q_den / P.hydrogenMass);
-		const double A_pi = photoionisation_rate(nHI, FLD(S.R, R_TAU, id), FLD(S.R, R_DTAU, id), shellVol, P.photonRate);
+		const double A_pi = photoionisation_rate(nHI, RFLD(S.R, R_TAU, id), RFLD(S.R, R_DTAU, id), shellVol, P.photonRate);
 		const double nHII_aB = x_avg * n_H * alphaB;
 		const double nHII_Aci = x_avg * n_H * A_ci;
 		double x_dummy = x;
@@ -975,34 +1033,12 @@ __global__ void k_rad_no_star_fp64(Params P, State S, double h) {
 
 // Radiation::preTimeStepCalculations (photoheating), Radiation.cpp:257-296, non-wind cells.
 __device__ __forceinline__ void b_rad_heating_fp64(const Params& P, const State& S, long long id) {
-
 	int ijk[3];
 	double xc[3];
 	cell_ijk(P, id, ijk);
 	cell_xc(P, ijk, xc);
 	if (is_wind(P, id, ijk, xc)) return;
-	double q_hii = FLD(S.Q, HII, id), q_pre = FLD(S.Q, PRE, id), q_den = FLD(S.Q, DEN, id);
-	double Tmin = S.Tmin[id];
-	double n_H = (P.X * q_den / P.hydrogenMass);
-	double excessEnergy = P.photonEnergy - P.rydbergEnergy;
-	double T = calc_temperature(P, q_hii, q_pre, q_den);
-	double nHI = (1.0 - q_hii) * n_H;
-	double A_pi = photoionisation_rate(nHI, FLD(S.R, R_TAU, id), FLD(S.R, R_DTAU, id), S.shellVol[id], P.photonRate);
-	double photoion = n_H * (1.0 - q_hii) * A_pi * excessEnergy;
-	double rate_rc = spline_eval(S.tables->rad_cool, T);
-	double recombination = q_hii * q_hii * n_H * n_H * P.boltzmannConst * T * rate_rc;
-	double collisions = q_hii * (1.0 - q_hii) * n_H * n_H * collisional_ionisation_rate(P, T);
-	double rate = photoion - recombination - collisions;
-	double softrate = rate;
-	if (T < Tmin + 200 && rate < 0.0) softrate = smin(0.0, softrate * (T - Tmin) / 200.0);
-	softrate *= P.heating_amp;
-	FLD(S.R, R_HEAT, id) = softrate;
-	if (S.H) {
-		// Radiation.cpp:278-279 (0/0 when rate is 0, as in the reference)
-		FLD(S.H, H_EUVH, id) = photoion * (softrate / rate);
-		FLD(S.H, H_RHII, id) = -recombination * (softrate / rate);
-	}
-	if (rate != rate) atomicOr(S.err, ERRB_NAN);
+	rad_heating_cell(P, S, id, FLD(S.Q, HII, id), FLD(S.Q, PRE, id), FLD(S.Q, DEN, id));
 }
 __global__ void __launch_bounds__(256) k_rad_heating_fp64(Params P, State S) {
 	if (TRG_BATCHED && P.batch) {
@@ -1036,7 +1072,7 @@ __device__ __forceinline__ void b_rad_update_fp64(const Params& P, const State& 
 			double E_new = pre_new / (P.gamma - 1.0) + ke;
 			udot[PRE] += (E_new - u[PRE]) / dt;
 		} else if (P.coupling == CP_NEQ) {
-			udot[PRE] += FLD(S.R, R_HEAT, id);
+			udot[PRE] += RFLD(S.R, R_HEAT, id);
 		}
 		udot[HII] += (q_hii * q_den - u[HII]) / dt;
 		udot[ADV] += (q_adv * q_den - u[ADV]) / dt;
@@ -1130,8 +1166,10 @@ __device__ __forceinline__ void b_colden_shell_fp64(const Params& P, const State
 	if (inner) {
 		double colden[4] = {0, 0, 0, 0}, w[4];
 		for (int i = 0; i < 4; ++i) {
-			if (nb[i] >= 0 && w0[i] != 0)
-				colden[i] = __ldcg(&FLD(S.T, T_COL_DEN, nb[i])) + __ldcg(&FLD(S.T, T_DCOL_DEN, nb[i]));
+			if (nb_read(nb, w0, i)) {
+				const double2 c = __ldcg(reinterpret_cast<const double2*>(S.T + nb[i] * 2));  // COL_DEN, DCOL_DEN
+				colden[i] = c.x + c.y;
+			}
 			w[i] = colden[i] == 0 ? 0 : w0[i] / colden[i];
 		}
 		double sum_w = w[0] + w[1] + w[2] + w[3];
@@ -1140,8 +1178,7 @@ __device__ __forceinline__ void b_colden_shell_fp64(const Params& P, const State
 			newcolden += w[i] * colden[i];
 		}
 	}
-	FLD(S.T, T_COL_DEN, id) = newcolden;
-	FLD(S.T, T_DCOL_DEN, id) = dcolden;
+	reinterpret_cast<double2*>(S.T + id * 2)[0] = make_double2(newcolden, dcolden);
 }
 __global__ void __launch_bounds__(128) k_colden_shell_fp64(Params P, State S, const int* __restrict__ cells, int count) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1163,7 +1200,7 @@ __device__ __forceinline__ void b_thermo_rates_fp64(const Params& P, const State
 	cell_xc(P, ijk, xc);
 	if (is_wind(P, id, ijk, xc)) return;
 	if (FLD(S.Q, ADV, id) < P.thermo_hii_switch) {
-		FLD(S.T, T_RATE, id) = 0;
+		TFLD(S.T, T_RATE, id) = 0;
 		return;
 	}
 	double q_den = FLD(S.Q, DEN, id), x = FLD(S.Q, HII, id), q_pre = FLD(S.Q, PRE, id);
@@ -1178,15 +1215,15 @@ __device__ __forceinline__ void b_thermo_rates_fp64(const Params& P, const State
 		double Q_FUV = 0.5 * P.photonRate;
 		F_FUV = rsqrd != 0 ? Q_FUV / (1.2e7 * 4 * P.pi * rsqrd) : 0;
 	}
-	double Av_FUV = 1.086 * P.dustXsec * FLD(S.T, T_COL_DEN, id);
+	double Av_FUV = 1.086 * P.dustXsec * TFLD(S.T, T_COL_DEN, id);
 	double rate = 0;
 	rate += th_fuvh(P, nH, Av_FUV, F_FUV);
 	rate += th_irh(P, nH, Av_FUV, F_FUV);
 	rate += P.crh * nH;
-	FLD(S.T, T_HEAT, id) = rate;
+	TFLD(S.T, T_HEAT, id) = rate;
 	rate = th_cooling(P, S, rate, ne, nn, nH, x, T);
 	rate = soft_landing(rate, T, S.Tmin[id]);
-	FLD(S.T, T_RATE, id) = P.heating_amp * rate;
+	TFLD(S.T, T_RATE, id) = P.heating_amp * rate;
 }
 __global__ void __launch_bounds__(256) k_thermo_rates_fp64(Params P, State S) {
 	if (TRG_BATCHED && P.batch) {
@@ -1212,13 +1249,13 @@ __device__ __forceinline__ void b_thermo_integrate_fp64(const Params& P, const S
 	if (FLD(S.Q, ADV, id) < P.thermo_hii_switch) {
 		if (S.H)
 			for (int i = 0; i < NH; ++i) FLD(S.H, i, id) = 0;
-		FLD(S.T, T_RATE, id) = 0;
+		TFLD(S.T, T_RATE, id) = 0;
 		return;
 	}
 	const double dt = h * S.scal[0];
 	double qden = FLD(S.Q, DEN, id), qpre = FLD(S.Q, PRE, id), x = FLD(S.Q, HII, id);
 	double Tmin = S.Tmin[id];
-	double rate0 = FLD(S.T, T_RATE, id), heat = FLD(S.T, T_HEAT, id);
+	double rate0 = TFLD(S.T, T_RATE, id), heat = TFLD(S.T, T_HEAT, id);
 	double nH = P.X * qden / P.hydrogenMass;
 	double ne = nH * (x);
 	double nn = nH * (1.0 - x);
@@ -1256,8 +1293,8 @@ __device__ __forceinline__ void b_thermo_integrate_fp64(const Params& P, const S
 			}
 		}
 	}
-	FLD(S.T, T_RATE, id) = (pressure - qpre) * dpre2rate;
-	if (S.H) FLD(S.H, H_TOT, id) = FLD(S.T, T_RATE, id);  // Thermodynamics.cpp:335
+	TFLD(S.T, T_RATE, id) = (pressure - qpre) * dpre2rate;
+	if (S.H) FLD(S.H, H_TOT, id) = TFLD(S.T, T_RATE, id);  // Thermodynamics.cpp:335
 }
 __global__ void __launch_bounds__(256) k_thermo_integrate_fp64(Params P, State S, double h) {
 	if (TRG_BATCHED && P.batch) {
@@ -1278,7 +1315,7 @@ __device__ __forceinline__ void b_thermo_update_fp64(const Params& P, const Stat
 	double u[7];
 #pragma unroll
 	for (int i = 0; i < NU; ++i) u[i] = FLD(S.U, i, id);
-	const double rate = FLD(S.T, T_RATE, id);
+	const double rate = TFLD(S.T, T_RATE, id);
 	int ijk[3];
 	double xc[3];
 	cell_ijk(P, id, ijk);
@@ -1286,8 +1323,8 @@ __device__ __forceinline__ void b_thermo_update_fp64(const Params& P, const Stat
 	double udot_pre = 0;
 	if (!is_wind(P, id, ijk, xc)) {
 		udot_pre += rate;
-		FLD(S.T, T_RATE, id) = 0;
-		FLD(S.T, T_HEAT, id) = 0;
+		TFLD(S.T, T_RATE, id) = 0;
+		TFLD(S.T, T_HEAT, id) = 0;
 	}
 	if (mode == 1) {
 		FLD(S.UDOT, PRE, id) += udot_pre;
@@ -1342,7 +1379,7 @@ __global__ void __launch_bounds__(256) k_heating_arrays_fp64(Params P, State S) 
 		double Q_FUV = 0.5 * P.photonRate;
 		F_FUV = rsqrd != 0 ? Q_FUV / (1.2e7 * 4 * P.pi * rsqrd) : 0;
 	}
-	double Av_FUV = 1.086 * P.dustXsec * FLD(S.T, T_COL_DEN, id);
+	double Av_FUV = 1.086 * P.dustXsec * TFLD(S.T, T_COL_DEN, id);
 	FLD(S.H, H_FUVH, id) = th_fuvh(P, nH, Av_FUV, F_FUV);
 	FLD(S.H, H_IRH, id) = th_irh(P, nH, Av_FUV, F_FUV);
 	FLD(S.H, H_CRH, id) = P.crh * nH;
@@ -1407,7 +1444,7 @@ __device__ __forceinline__ void b_dt_reduce_fp64(const Params& P, const State& S
 			double dt_max = P.dt_max;
 			double dtc = dt_max, dt1 = dt_max, dt2 = dt_max, dt3 = dt_max, dt4 = dt_max;
 			if (P.coupling == CP_NEQ) {
-				double heat = FLD(S.R, R_HEAT, id);
+				double heat = RFLD(S.R, R_HEAT, id);
 				if (heat != 0) dtc = fabs(FLD(S.U, PRE, id) / heat);
 			}
 			if (P.K1 != 0.0) {
@@ -1420,7 +1457,7 @@ __device__ __forceinline__ void b_dt_reduce_fp64(const Params& P, const State& S
 			if (P.K3 != 0.0 || P.K4 != 0.0) {
 				double nH = P.X * q_den / P.hydrogenMass;
 				double nHI = (1.0 - q_hii) * nH;
-				double A_pi = photoionisation_rate(nHI, FLD(S.R, R_TAU, id), FLD(S.R, R_DTAU, id), S.shellVol[id], P.photonRate);
+				double A_pi = photoionisation_rate(nHI, RFLD(S.R, R_TAU, id), RFLD(S.R, R_DTAU, id), S.shellVol[id], P.photonRate);
 				double Tq = calc_temperature(P, q_hii, q_pre, q_den);
 				double A_ci = collisional_ionisation_rate(P, Tq);
 				double A_rr = spline_eval(S.tables->rad_recomb, Tq);
@@ -1432,7 +1469,7 @@ __device__ __forceinline__ void b_dt_reduce_fp64(const Params& P, const State& S
 			if (tr == 0.0 || tr != tr || isinf(tr)) atomicOr(S.err, ERRB_DT);
 		}
 		if (P.cooling_on) {
-			double rate = FLD(S.T, T_RATE, id);
+			double rate = TFLD(S.T, T_RATE, id);
 			if (rate != 0) {
 				double frac = P.thermo_subcycling ? 1.0 : 0.1;
 				tt = fabs(frac * FLD(S.U, PRE, id) / rate);

@@ -33,6 +33,9 @@
 namespace trg {
 
 #define FLD(a, f, i) ((a)[(long long)(f) * P.N + (i)])
+// radiation and thermodynamics fields (layouts in trg_types.h)
+#define RFLD(a, f, i) ((a)[r_index(P.N, (f), (i))])
+#define TFLD(a, f, i) ((a)[t_index(P.N, (f), (i))])
 
 __device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
 __device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }

@@ -8,6 +8,25 @@ namespace trg {
 enum { DEN = 0, PRE = 1, HII = 2, ADV = 3, VEL = 4, NU = 7 };
 enum { R_HII_A = 0, R_TAU, R_TAU_A, R_DTAU, R_DTAU_A, R_HEAT, NR };
 enum { T_COL_DEN = 0, T_DCOL_DEN, T_HEAT, T_RATE, NT };
+
+// Device layout of the radiation fields R (6 N doubles): the optical depths
+// TAU, DTAU, TAU_A, DTAU_A of a cell side by side (one 32-byte sector, which
+// the causal sweep reads from each inner neighbour), then HII_A and HEAT as
+// plain arrays.  The thermodynamics fields T (4 N): COL_DEN, DCOL_DEN of a
+// cell side by side, then HEAT and RATE.  The C ABI exchanges both as field
+// after field ([6][N], [4][N]).
+#ifdef __CUDACC__
+#define TRG_HD __host__ __device__
+#else
+#define TRG_HD
+#endif
+TRG_HD inline constexpr int r_quad_slot(int f) { return f == R_TAU ? 0 : (f == R_DTAU ? 1 : (f == R_TAU_A ? 2 : 3)); }
+TRG_HD inline constexpr long long r_index(long long N, int f, long long id) {
+	return f == R_HII_A ? 4 * N + id : (f == R_HEAT ? 5 * N + id : id * 4 + r_quad_slot(f));
+}
+TRG_HD inline constexpr long long t_index(long long N, int f, long long id) {
+	return f <= T_DCOL_DEN ? id * 2 + f : (long long)f * N + id;
+}
 // heating / cooling diagnostics (HID, src/Torch/Common.hpp:32-34)
 enum { H_IMLC = 0, H_NMLC, H_RHII, H_CEHI, H_CIEC, H_NMC, H_EUVH, H_FUVH, H_IRH, H_CRH, H_TOT, NH };
 enum { G_CART = 0, G_CYL = 1, G_SPH = 2 };
