@@ -10,10 +10,15 @@
 // U0 and writes U1, and also reduces the next CFL time step (FP64, Hydro.cpp:77-89).
 //
 // Tiling: a CTA owns a 32 x 8 column of cells and marches along z, keeping the
-// primitives of five consecutive z-planes (the stencil of the z faces) in a
-// shared-memory ring; x/y halos of two cells are loaded with each plane.  Every
-// cell is read from HBM once per CTA (plus the 2-cell x/y halos, which other
-// CTAs share through L2), and every face flux is evaluated once.
+// primitives of three consecutive z-planes in a shared-memory ring; x/y halos
+// of two cells are loaded with each plane.  Every cell is read from HBM once
+// per CTA (plus the 2-cell x/y halos, which other CTAs share through L2), and
+// every face flux is evaluated once.  A thread owns one cell of the plane (a
+// warp owns one row): it computes the cell's limited slope once per direction
+// (a face takes the slopes of its two cells), its low x, low y and high z
+// faces, and its update.  x neighbours' slopes and fluxes move by warp
+// shuffle, y neighbours' through shared memory, and the z slope and z flux of
+// the column stay in registers from one plane to the next.
 //
 // The rotated solver is written in directional form: HLL with normal n1 and
 // HLLC with normal n2 are the reference's rotate / 1-D solve / rotate-back
@@ -33,7 +38,7 @@ namespace f32 {
 
 constexpr int BX = 32, BY = 8, HALO = 2;
 constexpr int SX = BX + 2 * HALO, SY = BY + 2 * HALO;
-constexpr int NPLANE = 5;
+constexpr int NPLANE = 3;
 
 struct Prim {
 	float d, p, x, a, v[3];
@@ -160,9 +165,13 @@ __device__ __forceinline__ bool fix_cons(const Scaled& P, float* u) {
 
 // `thr` is the reference's 1e-30 cut on a*b (code units) in the field's
 // scaled units: 1e-30 / s^2 for a field stored divided by s.
+// The slope arithmetic is written with explicit roundings (no contraction
+// left to the compiler), so that every call site computes a cell's slope and
+// face states identically: a face shared by two z chunks of the tiling gets
+// the same flux from both.
 __device__ __forceinline__ float albada(float a, float b, float thr) {
-	float ab = a * b;
-	return ab <= thr ? 0.f : ab * (a + b) / (a * a + b * b);
+	float ab = __fmul_rn(a, b);
+	return ab <= thr ? 0.f : __fmul_rn(ab, __fadd_rn(a, b)) / __fmaf_rn(a, a, __fmul_rn(b, b));
 }
 __device__ __forceinline__ float minmod_(float a, float b) {
 	return (a * b > 0) ? (fabsf(a) < fabsf(b) ? a : b) : 0.f;
@@ -179,30 +188,50 @@ __device__ __forceinline__ float limiter32(int kind, float a, float b, float thr
 	case 4: {
 		if (b == 0) return 0.f;
 		float r = fabsf(a / b);
-		return (a + b * r) / (1.f + r);
+		return __fmaf_rn(b, r, a) / __fadd_rn(1.f, r);
 	}
-	case 5: return (a * b <= thr) ? 0.f : 1.5f * b * (a * a + a * b) / (a * a + a * b + b * b);
+	case 5: {
+		const float ab = __fmul_rn(a, b), t = __fmaf_rn(a, a, ab);
+		return (ab <= thr) ? 0.f : __fmul_rn(__fmul_rn(1.5f, b), t) / __fmaf_rn(b, b, t);
+	}
 	default: return albada(a, b, thr);
 	}
 }
 
-// Reconstructed face states: left = QR of cell c1 from (c0,c1,c2),
-// right = QL of cell c2 from (c1,c2,c3) (Hydro.cpp:44-50).
 // Limiter cut-offs of the scaled fields (density, pressure, fractions, velocity).
 struct LimThr {
 	float d, p, x, v;
 };
-__device__ __forceinline__ void reconstruct(int lim, const LimThr& th, const Prim& c0, const Prim& c1, const Prim& c2,
-                                            const Prim& c3, Prim& L, Prim& R) {
-#define REC(field, thr)                                                                 \
-	{                                                                                   \
-		float sl = limiter32(lim, c1.field - c0.field, c2.field - c1.field, thr);       \
-		float sr = limiter32(lim, c2.field - c1.field, c3.field - c2.field, thr);       \
-		L.field = c1.field + 0.5f * sl;                                                 \
-		R.field = c2.field - 0.5f * sr;                                                 \
-	}
-	REC(d, th.d) REC(p, th.p) REC(x, th.x) REC(a, th.x) REC(v[0], th.v) REC(v[1], th.v) REC(v[2], th.v)
-#undef REC
+// Limited slope of a cell c between its neighbours cm and cp along one
+// direction, per field: limiter(c - cm, cp - c).  The reconstruction of
+// Hydro.cpp:44-50 gives a face between cells c1 and c2 the states
+// QR(c1) = c1 + slope(c1) / 2 and QL(c2) = c2 - slope(c2) / 2.
+__device__ __forceinline__ Prim slope_of(int lim, const LimThr& th, const Prim& cm, const Prim& c, const Prim& cp) {
+	Prim s;
+#define SLOPE(field, thr) s.field = limiter32(lim, c.field - cm.field, cp.field - c.field, thr);
+	SLOPE(d, th.d) SLOPE(p, th.p) SLOPE(x, th.x) SLOPE(a, th.x) SLOPE(v[0], th.v) SLOPE(v[1], th.v) SLOPE(v[2], th.v)
+#undef SLOPE
+	return s;
+}
+__device__ __forceinline__ Prim face_left(const Prim& c, const Prim& sl) {
+	Prim r;
+	r.d = __fmaf_rn(0.5f, sl.d, c.d);
+	r.p = __fmaf_rn(0.5f, sl.p, c.p);
+	r.x = __fmaf_rn(0.5f, sl.x, c.x);
+	r.a = __fmaf_rn(0.5f, sl.a, c.a);
+#pragma unroll
+	for (int k = 0; k < 3; ++k) r.v[k] = __fmaf_rn(0.5f, sl.v[k], c.v[k]);
+	return r;
+}
+__device__ __forceinline__ Prim face_right(const Prim& c, const Prim& sr) {
+	Prim r;
+	r.d = __fmaf_rn(-0.5f, sr.d, c.d);
+	r.p = __fmaf_rn(-0.5f, sr.p, c.p);
+	r.x = __fmaf_rn(-0.5f, sr.x, c.x);
+	r.a = __fmaf_rn(-0.5f, sr.a, c.a);
+#pragma unroll
+	for (int k = 0; k < 3; ++k) r.v[k] = __fmaf_rn(-0.5f, sr.v[k], c.v[k]);
+	return r;
 }
 
 struct Flux {
@@ -416,26 +445,45 @@ __device__ __forceinline__ Prim get(const SmemQ& s, int slot, int ly, int lx) {
 	return q;
 }
 
+// A Prim in a [7][n] float array of shared memory, at index k.
+__device__ __forceinline__ void put7(float* a, int n, int k, const Prim& q) {
+	a[DEN * n + k] = q.d;
+	a[PRE * n + k] = q.p;
+	a[HII * n + k] = q.x;
+	a[ADV * n + k] = q.a;
+#pragma unroll
+	for (int j = 0; j < 3; ++j) a[(VEL + j) * n + k] = q.v[j];
+}
+__device__ __forceinline__ Prim get7(const float* a, int n, int k) {
+	Prim q;
+	q.d = a[DEN * n + k];
+	q.p = a[PRE * n + k];
+	q.x = a[HII * n + k];
+	q.a = a[ADV * n + k];
+#pragma unroll
+	for (int j = 0; j < 3; ++j) q.v[j] = a[(VEL + j) * n + k];
+	return q;
+}
+__device__ __forceinline__ Prim shfl_up7(const Prim& q) {
+	Prim r;
+	r.d = __shfl_up_sync(0xffffffffu, q.d, 1);
+	r.p = __shfl_up_sync(0xffffffffu, q.p, 1);
+	r.x = __shfl_up_sync(0xffffffffu, q.x, 1);
+	r.a = __shfl_up_sync(0xffffffffu, q.a, 1);
+#pragma unroll
+	for (int j = 0; j < 3; ++j) r.v[j] = __shfl_up_sync(0xffffffffu, q.v[j], 1);
+	return r;
+}
+
 __device__ __forceinline__ double dmin_(double a, double b) { return (b < a) ? b : a; }
 
 }  // namespace f32
 
 using namespace f32;
 
-// Reconstruction + Riemann solve for one face (the single call site of the
-// solver in the kernel keeps the instruction footprint small).
-template <int LIM, int RS>
-__device__ __forceinline__ void face_flux(int order, int lim_rt, int rs_rt, const LimThr& th, const Prim& c0, const Prim& c1,
-                                          const Prim& c2,
-                                          const Prim& c3, int dim, float gamma, float* F) {
-	Prim L, R;
-	if (order == 1) {
-		const int lim = LIM >= 0 ? LIM : lim_rt;
-		reconstruct(lim, th, c0, c1, c2, c3, L, R);
-	} else {
-		L = c1;
-		R = c2;
-	}
+// Riemann solve for one face from its reconstructed states.
+template <int RS>
+__device__ __forceinline__ void face_flux(int rs_rt, const Prim& L, const Prim& R, int dim, float gamma, float* F) {
 	riemann32(RS >= 0 ? RS : rs_rt, L, R, dim, gamma, F);
 }
 
@@ -452,10 +500,15 @@ __global__ void __launch_bounds__(BX* BY, 2)
                        int zchunk) {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	SmemQ& s = *reinterpret_cast<SmemQ*>(smem_raw);
-	float* Fx = reinterpret_cast<float*>(smem_raw + sizeof(SmemQ));   // [7][BY][BX+1]
-	float* Fy = Fx + 7 * BY * (BX + 1);                                  // [7][BY+1][BX]
-	float* Fz = Fy + 7 * (BY + 1) * BX;                                  // [2][7][BY][BX]
+	float* Fx = reinterpret_cast<float*>(smem_raw + sizeof(SmemQ));  // [7][BY][BX + 1] x-face fluxes
+	float* Fy = Fx + 7 * BY * (BX + 1);                               // [7][BY + 1][BX] y-face fluxes
+	float* Fz = Fy + 7 * (BY + 1) * BX;                               // [7][BY * BX] flux of each column's face z + 1/2
+	float* Sx = Fz + 7 * BY * BX;                                     // [7][BY * BX] x slopes of the tile
+	float* Sy = Sx + 7 * BY * BX;                                     // [7][BY * BX] y slopes of the tile
+	float* Ex = Sy + 7 * BY * BX;                                     // [7][2 * BY] x slopes of cells x0 - 1, x0 + BX
+	float* Ey = Ex + 7 * 2 * BY;                                      // [7][2 * BX] y slopes of cells y0 - 1, y0 + BY
 	const int tx = threadIdx.x % BX, ty = threadIdx.x / BX;
+	const int lx = tx + HALO, ly = ty + HALO;
 	const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY;
 	const int z0 = blockIdx.z * zchunk;
 	const int nd = P.nd;
@@ -470,11 +523,20 @@ __global__ void __launch_bounds__(BX* BY, 2)
 	const long long N = P.N;
 	const int gx = x0 + tx, gy = y0 + ty;
 	const bool active = gx < P.nx && gy < P.ny;
-	const int order = P.order, lim_rt = P.limiter, rs_rt = P.riemann;
+	const bool rec = P.order == 1;
+	const int lim = LIM >= 0 ? LIM : P.limiter, rs_rt = P.riemann;
 	const LimThr th{(float)(1.0e-30 / (P.f32_rho0 * P.f32_rho0)), (float)(1.0e-30 / (P.f32_p0 * P.f32_p0)), 1.0e-30f,
 	                (float)(1.0e-30 / (P.f32_v0 * P.f32_v0))};
-	// face counts of one plane (x faces, y faces, z faces at z + 1/2)
-	const int nfx = (BX + 1) * BY, nfy = nd > 1 ? BX * (BY + 1) : 0, nfz = nd > 2 ? BX * BY : 0;
+	// faces of this thread: x at gx - 1/2 and y at gy - 1/2 where they are
+	// faces of the grid; the tile's last x face (x0 + BX - 1/2) of each row and
+	// last y face (y0 + BY - 1/2) of each column are computed by warps 0-1
+	const bool fx_ok = gx <= P.nx && gy < P.ny;
+	const bool fy_ok = nd > 1 && gx < P.nx && gy <= P.ny;
+	const int te = threadIdx.x;  // last faces: te < BX y face of column te; BX <= te < BX + BY x face of row te - BX
+	const bool fe_ok = te < BX ? (nd > 1 && x0 + te < P.nx && y0 + BY <= P.ny)
+	                           : (te < BX + BY && x0 + BX <= P.nx && y0 + te - BX < P.ny);
+	// edge slopes (cells just outside the tile): the last 80 threads
+	const int ts = (int)threadIdx.x - (BX * BY - 2 * (BX + BY));
 	double tmin = 1.0e308;
 	bool bad = false;
 
@@ -494,72 +556,130 @@ __global__ void __launch_bounds__(BX* BY, 2)
 	}
 
 	auto slot_of = [](int z) { return ((z % NPLANE) + NPLANE) % NPLANE; };
+	Prim zero;
+	zero.d = zero.p = zero.x = zero.a = zero.v[0] = zero.v[1] = zero.v[2] = 0.f;
+	Prim szc = zero;  // z slope of this column's cell in the current plane
+	float fzlo[7];    // flux through the column's face z - 1/2
+#pragma unroll
+	for (int i = 0; i < 7; ++i) fzlo[i] = 0.f;
+	// 3-D: the pass starts one plane early (z0 - 1), where it only forms the
+	// flux through z0 - 1/2, so that every z face goes through the same code
 	if (nd > 2) {
-		for (int z = z0 - 2; z <= z0 + 1; ++z) load_plane<STAGE>(P, SP, SC, Uq, s, slot_of(z), x0, y0, z);
+		for (int z = z0 - 2; z <= z0; ++z) load_plane<STAGE>(P, SP, SC, Uq, s, slot_of(z), x0, y0, z);
+		__syncthreads();
+		if (rec)
+			szc = slope_of(lim, th, get(s, slot_of(z0 - 2), ly, lx), get(s, slot_of(z0 - 1), ly, lx),
+			               get(s, slot_of(z0), ly, lx));
+		__syncthreads();  // plane z0 - 2 is read: its slot takes plane z0 + 1
 	} else {
 		load_plane<STAGE>(P, SP, SC, Uq, s, 0, x0, y0, 0);
-	}
-	__syncthreads();
-	if (nd > 2) {
-		// flux through the face z0 - 1/2 into Fz[0]
-		Prim c0 = get(s, slot_of(z0 - 2), ty + HALO, tx + HALO), c1 = get(s, slot_of(z0 - 1), ty + HALO, tx + HALO);
-		Prim c2 = get(s, slot_of(z0), ty + HALO, tx + HALO), c3 = get(s, slot_of(z0 + 1), ty + HALO, tx + HALO);
-		float F[7];
-		face_flux<LIM, RS>(order, lim_rt, rs_rt, th, c0, c1, c2, c3, 2, gamma, F);
-#pragma unroll
-		for (int i = 0; i < 7; ++i) Fz[i * BX * BY + threadIdx.x] = F[i];
+		__syncthreads();
 	}
 
-	for (int z = z0; z < z1; ++z) {
+	for (int z = nd > 2 ? z0 - 1 : z0; z < z1; ++z) {
 		const int sc = nd > 2 ? slot_of(z) : 0;
-		const int zb = (z - z0) & 1;  // Fz buffer holding the face z - 1/2
+		const bool plane = z >= z0;  // x/y faces and the update of this plane
 		if (nd > 2) {
 			load_plane<STAGE>(P, SP, SC, Uq, s, slot_of(z + 2), x0, y0, z + 2);
 			__syncthreads();
 		}
-		for (int f = threadIdx.x; f < nfx + nfy + nfz; f += blockDim.x) {
-			int dim, a, b;
-			Prim c0, c1, c2, c3;
-			if (f < nfx) {
-				dim = 0;
-				b = f / (BX + 1);
-				a = f - b * (BX + 1);
-				if (x0 + a > P.nx || y0 + b >= P.ny) continue;
-				int ly = b + HALO;
-				c0 = get(s, sc, ly, a); c1 = get(s, sc, ly, a + 1); c2 = get(s, sc, ly, a + 2); c3 = get(s, sc, ly, a + 3);
-			} else if (f < nfx + nfy) {
-				dim = 1;
-				int g = f - nfx;
-				b = g / BX;
-				a = g - b * BX;
-				if (x0 + a >= P.nx || y0 + b > P.ny) continue;
-				int lx = a + HALO;
-				c0 = get(s, sc, b, lx); c1 = get(s, sc, b + 1, lx); c2 = get(s, sc, b + 2, lx); c3 = get(s, sc, b + 3, lx);
-			} else {
-				dim = 2;
-				int g = f - nfx - nfy;
-				b = g / BX;
-				a = g - b * BX;
-				if (x0 + a >= P.nx || y0 + b >= P.ny) continue;
-				int lx = a + HALO, ly = b + HALO;
-				c0 = get(s, slot_of(z - 1), ly, lx); c1 = get(s, sc, ly, lx);
-				c2 = get(s, slot_of(z + 1), ly, lx); c3 = get(s, slot_of(z + 2), ly, lx);
-			}
-			float F[7];
-			face_flux<LIM, RS>(order, lim_rt, rs_rt, th, c0, c1, c2, c3, dim, gamma, F);
-			if (dim == 0) {
-#pragma unroll
-				for (int i = 0; i < 7; ++i) Fx[(i * BY + b) * (BX + 1) + a] = F[i];
-			} else if (dim == 1) {
-#pragma unroll
-				for (int i = 0; i < 7; ++i) Fy[(i * (BY + 1) + b) * BX + a] = F[i];
-			} else {
-#pragma unroll
-				for (int i = 0; i < 7; ++i) Fz[((zb ^ 1) * 7 + i) * BX * BY + b * BX + a] = F[i];
+		// slopes: this cell in x, y and (of the next plane's cell) z; the cells
+		// just outside the tile in x and y
+		Prim szn = zero;
+		if (rec) {
+			const Prim qc = get(s, sc, ly, lx);
+			if (nd > 2)
+				szn = slope_of(lim, th, qc, get(s, slot_of(z + 1), ly, lx), get(s, slot_of(z + 2), ly, lx));
+		}
+		if (rec && plane) {
+			const Prim qc = get(s, sc, ly, lx);
+			put7(Sx, BY * BX, threadIdx.x, slope_of(lim, th, get(s, sc, ly, lx - 1), qc, get(s, sc, ly, lx + 1)));
+			if (nd > 1)
+				put7(Sy, BY * BX, threadIdx.x, slope_of(lim, th, get(s, sc, ly - 1, lx), qc, get(s, sc, ly + 1, lx)));
+			if (ts >= 0 && ts < 2 * BY) {
+				const int e = ts / BY, r = ts - e * BY, ex = e ? HALO + BX : HALO - 1;
+				put7(Ex, 2 * BY, ts,
+				     slope_of(lim, th, get(s, sc, r + HALO, ex - 1), get(s, sc, r + HALO, ex), get(s, sc, r + HALO, ex + 1)));
+			} else if (ts >= 2 * BY && nd > 1) {
+				const int u = ts - 2 * BY, e = u / BX, col = u - e * BX, ey = e ? HALO + BY : HALO - 1;
+				put7(Ey, 2 * BX, u,
+				     slope_of(lim, th, get(s, sc, ey - 1, col + HALO), get(s, sc, ey, col + HALO), get(s, sc, ey + 1, col + HALO)));
 			}
 		}
 		__syncthreads();
-		if (active) {
+		// faces: the x face below, the y face below and the z face above this
+		// cell, then (warps 0-1) the tile's last y and x faces, all through one
+		// call of the solver
+#pragma unroll 1
+		for (int k = 0; k < 4; ++k) {
+			Prim ql, qr, sl = zero, sr = zero;
+			int dim;
+			bool ok;
+			float* dst;
+			int stride;
+			if (k == 0) {  // x face gx - 1/2, between cells lx - 1 and lx of row ly
+				ok = fx_ok && plane;
+				dim = 0;
+				ql = get(s, sc, ly, lx - 1);
+				qr = get(s, sc, ly, lx);
+				if (rec && ok) {
+					sl = tx > 0 ? get7(Sx, BY * BX, threadIdx.x - 1) : get7(Ex, 2 * BY, ty);
+					sr = get7(Sx, BY * BX, threadIdx.x);
+				}
+				dst = Fx + ty * (BX + 1) + tx;
+				stride = BY * (BX + 1);
+			} else if (k == 1) {  // y face gy - 1/2, between rows ly - 1 and ly of column lx
+				ok = fy_ok && plane;
+				dim = 1;
+				ql = get(s, sc, ly - 1, lx);
+				qr = get(s, sc, ly, lx);
+				if (rec && ok) {
+					sl = ty > 0 ? get7(Sy, BY * BX, threadIdx.x - BX) : get7(Ey, 2 * BX, tx);
+					sr = get7(Sy, BY * BX, threadIdx.x);
+				}
+				dst = Fy + ty * BX + tx;
+				stride = (BY + 1) * BX;
+			} else if (k == 2) {  // z face z + 1/2 of this column
+				ok = nd > 2;
+				dim = 2;
+				ql = get(s, sc, ly, lx);
+				qr = ok ? get(s, slot_of(z + 1), ly, lx) : ql;
+				sl = szc;
+				sr = szn;
+				dst = Fz + threadIdx.x;
+				stride = BY * BX;
+			} else if (te < BX) {  // y face y0 + BY - 1/2 of column te
+				ok = fe_ok && plane;
+				dim = 1;
+				ql = get(s, sc, HALO + BY - 1, te + HALO);
+				qr = get(s, sc, HALO + BY, te + HALO);
+				if (rec && ok) {
+					sl = get7(Sy, BY * BX, (BY - 1) * BX + te);
+					sr = get7(Ey, 2 * BX, BX + te);
+				}
+				dst = Fy + BY * BX + te;
+				stride = (BY + 1) * BX;
+			} else {  // x face x0 + BX - 1/2 of row te - BX
+				ok = fe_ok && plane;
+				dim = 0;
+				const int r = min(te - BX, BY - 1);
+				ql = get(s, sc, r + HALO, HALO + BX - 1);
+				qr = get(s, sc, r + HALO, HALO + BX);
+				if (rec && ok) {
+					sl = get7(Sx, BY * BX, r * BX + BX - 1);
+					sr = get7(Ex, 2 * BY, BY + r);
+				}
+				dst = Fx + r * (BX + 1) + BX;
+				stride = BY * (BX + 1);
+			}
+			if (!ok) continue;
+			float f[7];
+			face_flux<RS>(rs_rt, rec ? face_left(ql, sl) : ql, rec ? face_right(qr, sr) : qr, dim, gamma, f);
+#pragma unroll
+			for (int i = 0; i < 7; ++i) dst[i * stride] = f[i];
+		}
+		__syncthreads();
+		if (active && plane) {
 			const long long id = gx + (long long)P.nx * (gy + (long long)P.ny * z);
 			float udot[7];
 #pragma unroll
@@ -572,10 +692,9 @@ __global__ void __launch_bounds__(BX* BY, 2)
 			}
 			if (nd > 2) {
 #pragma unroll
-				for (int i = 0; i < 7; ++i)
-					udot[i] += azl * Fz[(zb * 7 + i) * BX * BY + threadIdx.x] - azr * Fz[((zb ^ 1) * 7 + i) * BX * BY + threadIdx.x];
+				for (int i = 0; i < 7; ++i) udot[i] += azl * fzlo[i] - azr * Fz[i * BY * BX + threadIdx.x];
 			}
-			Prim qc = get(s, sc, ty + HALO, tx + HALO);
+			const Prim qc = get(s, sc, ly, lx);
 			if (S.grav) {
 				for (int k = 0; k < 3; ++k) {
 					float g = (float)S.grav[(long long)k * N + id] * gscale;
@@ -636,6 +755,11 @@ __global__ void __launch_bounds__(BX* BY, 2)
 				tmin = dmin_(tmin, 0.5 / inv_t);
 			}
 		}
+		if (nd > 2) {
+#pragma unroll
+			for (int i = 0; i < 7; ++i) fzlo[i] = Fz[i * BY * BX + threadIdx.x];
+		}
+		szc = szn;
 		__syncthreads();
 	}
 	if (bad) atomicOr(S.err, ERRB_NAN);
@@ -649,7 +773,7 @@ __global__ void __launch_bounds__(BX* BY, 2)
 }
 
 size_t hydro_stage_fp32_smem() {
-	return sizeof(SmemQ) + sizeof(float) * 7 * (BY * (BX + 1) + (BY + 1) * BX + 2 * BX * BY);
+	return sizeof(SmemQ) + sizeof(float) * 7 * (BY * (BX + 1) + (BY + 1) * BX + 3 * BY * BX + 2 * BY + 2 * BX);
 }
 
 template <int STAGE, typename TS, int LIM, int RS>
