@@ -382,7 +382,14 @@ void sub_step(trg_ctx* c, double h, bool hasCalculatedHeatFlux, int comp) {
 				// FP64 fallback, part 1: list the high-contrast cells and compute
 				// their faces in FP64 from this sub-step's primitives
 				cudaMemsetAsync(c->S.fb_count, 0, sizeof(unsigned), c->stream);
-				LAUNCH(KF(k_fb_flags), c->P.N, 256, c->P, c->S, c->fb_contrast);
+				{
+					cudaEvent_t fa = nullptr, fbv = nullptr;
+					if (c->profiling) { fa = pool_event(c); fbv = pool_event(c); cudaEventRecord(fa, c->stream); }
+					const dim3 g((c->P.nx + 31) / 32, (c->P.ny + 7) / 8, (c->P.nz + FB_ZCHUNK - 1) / FB_ZCHUNK);
+					KF(k_fb_flags)<<<g, 256, 0, c->stream>>>(c->P, c->S, c->fb_contrast);
+					if (c->profiling) { cudaEventRecord(fbv, c->stream); c->recs.push_back({"k_fb_flags", fa, fbv}); }
+					c->launches++;
+				}
 				LAUNCH(KF(k_fb_faces), 148LL * 8 * 128, 128, c->P, c->S);
 			}
 			if (c->profiling) { ea = pool_event(c); eb = pool_event(c); cudaEventRecord(ea, c->stream); }

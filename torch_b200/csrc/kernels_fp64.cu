@@ -1558,34 +1558,73 @@ __device__ __forceinline__ long long clamp_nb(const Params& P, const int* ijk, i
 	else t[2] = v;
 	return flat_id(P, t[0], t[1], t[2]);
 }
+// The flag of a cell: its pressure and those of its neighbours up to 2 cells
+// away along each axis (indices clamped to the grid) span a ratio above
+// `contrast`.  A CTA owns a 32 x 8 tile of columns and marches along z through
+// FB_ZCHUNK planes: each plane's pressures, with two clamped cells of halo in x
+// and y, are staged in shared memory once; the z neighbours come from a window
+// of the column's pressures kept in registers.
 __global__ void __launch_bounds__(256) k_fb_flags(Params P, State S, double contrast) {
-	const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-	if (id >= P.N) return;
-	int ijk[3];
-	cell_ijk(P, id, ijk);
-	double pmin = FLD(S.Q, PRE, id), pmax = pmin;
-#pragma unroll
-	for (int dim = 0; dim < 3; ++dim)
-		if (dim < P.nd) {
-#pragma unroll
-			for (int off = -2; off <= 2; ++off) {
-				if (off == 0) continue;
-				const double p = FLD(S.Q, PRE, clamp_nb(P, ijk, dim, off));
-				pmin = smin(pmin, p);
-				pmax = smax(pmax, p);
-			}
+	__shared__ double tile[8 + 4][32 + 4];
+	const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
+	const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 8;
+	const int x = x0 + lane, y = y0 + row;
+	const int nx = P.nx, ny = P.ny, nz = P.nz, nd = P.nd;
+	const int xc = min(x, nx - 1), yc = min(y, ny - 1);
+	const bool in = x < nx && y < ny;
+	const int z0 = blockIdx.z * FB_ZCHUNK, z1 = min(z0 + FB_ZCHUNK, nz);
+	const double* pre = S.Q + (long long)PRE * P.N;
+	auto at = [&](int i, int j, int k) {
+		i = i < 0 ? 0 : (i >= nx ? nx - 1 : i);
+		j = j < 0 ? 0 : (j >= ny ? ny - 1 : j);
+		k = k < 0 ? 0 : (k >= nz ? nz - 1 : k);
+		return pre[i + (long long)nx * (j + (long long)ny * k)];
+	};
+	// the column's pressures at z - 2 .. z + 2 (clamped)
+	double w0 = 0, w1 = 0, w2 = 0, w3 = 0;
+	if (nd > 2) {
+		w0 = at(xc, yc, z0 - 2);
+		w1 = at(xc, yc, z0 - 1);
+		w2 = at(xc, yc, z0);
+		w3 = at(xc, yc, z0 + 1);
+	}
+	for (int z = z0; z < z1; ++z) {
+		for (int k = threadIdx.x; k < 12 * 36; k += 256) {
+			const int ly = k / 36, lx = k - ly * 36;
+			tile[ly][lx] = at(x0 + lx - 2, nd > 1 ? y0 + ly - 2 : 0, z);
 		}
-	const bool f = pmax > contrast * pmin;
-	S.fb_flag[id] = f ? 1 : 0;
-	const unsigned m = __activemask();
-	const unsigned ballot = __ballot_sync(m, f);
-	if (!ballot) return;
-	const int leader = __ffs(ballot) - 1;
-	unsigned base = 0;
-	if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(S.fb_count, (unsigned)__popc(ballot));
-	base = __shfl_sync(m, base, leader);
-	if (f) S.fb_list[base + __popc(ballot & ((1u << (threadIdx.x & 31)) - 1))] = (int)id;
-	if (P.stats_on && (int)(threadIdx.x & 31) == leader) atomicAdd(S.stats + TRG_STAT_FP64_CELLS, (unsigned long long)__popc(ballot));
+		const double w4 = nd > 2 ? at(xc, yc, z + 2) : 0.0;
+		__syncthreads();
+		const int lx = lane + 2, ly = row + 2;
+		const double pc = tile[ly][lx];
+		double pmin = pc, pmax = pc;
+		pmin = smin(smin(smin(pmin, tile[ly][lx - 1]), smin(tile[ly][lx - 2], tile[ly][lx + 1])), tile[ly][lx + 2]);
+		pmax = smax(smax(smax(pmax, tile[ly][lx - 1]), smax(tile[ly][lx - 2], tile[ly][lx + 1])), tile[ly][lx + 2]);
+		if (nd > 1) {
+			pmin = smin(smin(smin(pmin, tile[ly - 1][lx]), smin(tile[ly - 2][lx], tile[ly + 1][lx])), tile[ly + 2][lx]);
+			pmax = smax(smax(smax(pmax, tile[ly - 1][lx]), smax(tile[ly - 2][lx], tile[ly + 1][lx])), tile[ly + 2][lx]);
+		}
+		if (nd > 2) {
+			pmin = smin(smin(smin(pmin, w0), smin(w1, w3)), w4);
+			pmax = smax(smax(smax(pmax, w0), smax(w1, w3)), w4);
+			w0 = w1;
+			w1 = w2;
+			w2 = w3;
+			w3 = w4;
+		}
+		__syncthreads();  // the tile is read: the next plane may overwrite it
+		const bool f = in && pmax > contrast * pmin;
+		const long long id = xc + (long long)nx * (yc + (long long)ny * z);
+		if (in) S.fb_flag[id] = f ? 1 : 0;
+		const unsigned ballot = __ballot_sync(0xffffffffu, f);
+		if (!ballot) continue;
+		const int leader = __ffs(ballot) - 1;
+		unsigned base = 0;
+		if (lane == leader) base = atomicAdd(S.fb_count, (unsigned)__popc(ballot));
+		base = __shfl_sync(0xffffffffu, base, leader);
+		if (f) S.fb_list[base + __popc(ballot & ((1u << lane) - 1))] = (int)id;
+		if (P.stats_on && lane == leader) atomicAdd(S.stats + TRG_STAT_FP64_CELLS, (unsigned long long)__popc(ballot));
+	}
 }
 // FP64 face fluxes (into S.F) of every listed cell's faces.
 __global__ void __launch_bounds__(128) k_fb_faces(Params P, State S) {

@@ -39,6 +39,9 @@ enum : unsigned {
 	ERRB_NAN = 1u, ERRB_PICARD = 2u, ERRB_DT = 4u, ERRB_FLUX = 8u, ERRB_TC = 16u,
 };
 
+// Planes per CTA of the FP32 form's fallback flag pass (k_fb_flags).
+constexpr int FB_ZCHUNK = 16;
+
 // Cubic spline table (SplineData, src/Integrators/SplineData.cpp) built on the host.
 struct Spline {
 	int n, log_mode;
