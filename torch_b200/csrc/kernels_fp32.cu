@@ -610,8 +610,9 @@ __global__ void __launch_bounds__(BX* BY, 2)
 		// faces: the x face below, the y face below and the z face above this
 		// cell, then (warps 0-1) the tile's last y and x faces, all through one
 		// call of the solver
+		const int nk = te < BX + BY ? 4 : 3;  // only threads 0 .. BX + BY - 1 take a last face
 #pragma unroll 1
-		for (int k = 0; k < 4; ++k) {
+		for (int k = 0; k < nk; ++k) {
 			Prim ql, qr, sl = zero, sr = zero;
 			int dim;
 			bool ok;
@@ -678,6 +679,10 @@ __global__ void __launch_bounds__(BX* BY, 2)
 #pragma unroll
 			for (int i = 0; i < 7; ++i) dst[i * stride] = f[i];
 		}
+		// the cell itself for the source terms, read before the barrier: after
+		// it, nothing of this plane is read, so the next plane's load may reuse
+		// the slot without another barrier
+		const Prim qc = get(s, sc, ly, lx);
 		__syncthreads();
 		if (active && plane) {
 			const long long id = gx + (long long)P.nx * (gy + (long long)P.ny * z);
@@ -694,7 +699,6 @@ __global__ void __launch_bounds__(BX* BY, 2)
 #pragma unroll
 				for (int i = 0; i < 7; ++i) udot[i] += azl * fzlo[i] - azr * Fz[i * BY * BX + threadIdx.x];
 			}
-			const Prim qc = get(s, sc, ly, lx);
 			if (S.grav) {
 				for (int k = 0; k < 3; ++k) {
 					float g = (float)S.grav[(long long)k * N + id] * gscale;
@@ -760,7 +764,8 @@ __global__ void __launch_bounds__(BX* BY, 2)
 			for (int i = 0; i < 7; ++i) fzlo[i] = Fz[i * BY * BX + threadIdx.x];
 		}
 		szc = szn;
-		__syncthreads();
+		// no barrier here: the next plane's load writes only the slot of plane
+		// z, and the flux and slope arrays are rewritten after the next barrier
 	}
 	if (bad) atomicOr(S.err, ERRB_NAN);
 	if (STAGE == 2) {
