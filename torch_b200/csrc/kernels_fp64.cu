@@ -873,7 +873,14 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 	}
 }
 
-__global__ void __launch_bounds__(128) k_rad_shell_fp64(Params P, State S, const int* __restrict__ cells, int count,
+// The fast build fits 7 CTAs per SM (28 warps, one spilled register pair) for
+// the latency-bound large shells; the exact build keeps its registers.
+#ifdef TRG_FAST_MATH
+#define TRG_RAD_SHELL_MINB 7
+#else
+#define TRG_RAD_SHELL_MINB 1
+#endif
+__global__ void __launch_bounds__(128, TRG_RAD_SHELL_MINB) k_rad_shell_fp64(Params P, State S, const int* __restrict__ cells, int count,
                                                        double h) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= count) return;
