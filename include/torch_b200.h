@@ -184,7 +184,9 @@ int trg_heating(trg_ctx* c, double* H);
  * state, time, time step and the split's counters - as one binary blob of
  * trg_checkpoint_bytes(c) bytes.  trg_checkpoint_load restores it into a
  * context created with the same parameters and grid; stepping on is
- * bit-identical to the run that was saved. */
+ * bit-identical to the run that was saved.  The blob holds the device layout
+ * of R and T and a format version (2); a blob of another version is rejected
+ * with TRG_ERR_ARG. */
 long long trg_checkpoint_bytes(const trg_ctx* c);
 int trg_checkpoint_save(trg_ctx* c, void* buf, long long bytes);
 int trg_checkpoint_load(trg_ctx* c, const void* buf, long long bytes);
