@@ -73,6 +73,8 @@ __device__ __forceinline__ float load_u(const float* U, long long idx, const Sto
 __device__ __forceinline__ float load_u(const double* U, long long idx, const StoreScale& sc, int f) {
 	return (float)(__ldg(&U[idx]) * sc.is[sc.cls(f)]);
 }
+__device__ __forceinline__ float scaled_u(float u, const StoreScale&, int) { return u; }
+__device__ __forceinline__ float scaled_u(double u, const StoreScale& sc, int f) { return (float)(u * sc.is[sc.cls(f)]); }
 __device__ __forceinline__ void store_u(float* U, long long idx, float v, const StoreScale&, int) { U[idx] = v; }
 __device__ __forceinline__ void store_u(double* U, long long idx, float v, const StoreScale& sc, int f) {
 	U[idx] = (double)v * sc.s[sc.cls(f)];
@@ -433,6 +435,72 @@ __device__ __forceinline__ void load_plane(const Params& P, const Scaled& SP, co
 	}
 }
 
+// Asynchronous staging of a plane (cp.async): the raw conserved state of the
+// plane's cells, with the boundary rule applied to the source index, is
+// copied into a shared-memory buffer [7][SY * SX] while the CTA computes the
+// current plane, and turned into primitives in the ring slot afterwards.
+// The cells and the source rule are those of load_plane.
+template <typename TS>
+__device__ __forceinline__ void cp_async_elem(TS* dst, const TS* src) {
+	const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+	if (sizeof(TS) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+	else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+template <typename TS>
+__device__ __forceinline__ void plane_fetch(const Params& P, const TS* __restrict__ U, TS* raw, int x0, int y0, int z) {
+	int zc, zside;
+	const int zs = P.nd > 2 ? bc_src(P, 2, z, P.nz, zc, zside) : 0;
+	const long long N = P.N;
+	for (int idx = threadIdx.x; idx < SX * SY; idx += blockDim.x) {
+		const int ly = idx / SX, lx = idx - ly * SX;
+		const bool xh = lx < HALO || lx >= HALO + BX, yh = ly < HALO || ly >= HALO + BY;
+		if (xh && yh) continue;
+		int xc, xside, yc, yside;
+		const int xs = bc_src(P, 0, x0 + lx - HALO, P.nx, xc, xside);
+		const int ys = P.nd > 1 ? bc_src(P, 1, y0 + ly - HALO, P.ny, yc, yside) : 0;
+		if (xs < 0 || xs >= P.nx || ys < 0 || ys >= P.ny) continue;
+		const long long id = xs + (long long)P.nx * (ys + (long long)P.ny * zs);
+#pragma unroll
+		for (int f = 0; f < 7; ++f) cp_async_elem(raw + f * (SX * SY) + idx, U + f * N + id);
+	}
+	cp_async_commit();
+}
+template <int STAGE, typename TS>
+__device__ __forceinline__ void plane_convert(const Params& P, const Scaled& SP, const StoreScale& SC, const TS* raw,
+                                              SmemQ& s, int slot, int x0, int y0, int z) {
+	int zc, zside;
+	if (P.nd > 2) bc_src(P, 2, z, P.nz, zc, zside);
+	else zc = -1;
+	for (int idx = threadIdx.x; idx < SX * SY; idx += blockDim.x) {
+		const int ly = idx / SX, lx = idx - ly * SX;
+		const bool xh = lx < HALO || lx >= HALO + BX, yh = ly < HALO || ly >= HALO + BY;
+		if (xh && yh) continue;
+		int xc, xside, yc, yside;
+		const int xs = bc_src(P, 0, x0 + lx - HALO, P.nx, xc, xside);
+		const int ys = P.nd > 1 ? bc_src(P, 1, y0 + ly - HALO, P.ny, yc, yside) : 0;
+		if (P.nd <= 1) yc = -1;
+		if (xs < 0 || xs >= P.nx || ys < 0 || ys >= P.ny) continue;
+		float u[7];
+#pragma unroll
+		for (int f = 0; f < 7; ++f) u[f] = scaled_u(raw[f * (SX * SY) + idx], SC, f);
+		Prim q = prim_from_cons(u, (float)P.gamma, P.nd);
+		if (STAGE == 1) fix_prim(SP, q, u[DEN]);
+		apply_flip(q, 0, xc, xside);
+		if (P.nd > 1) apply_flip(q, 1, yc, yside);
+		if (P.nd > 2) apply_flip(q, 2, zc, zside);
+		s.v[slot][DEN][ly][lx] = q.d;
+		s.v[slot][PRE][ly][lx] = q.p;
+		s.v[slot][HII][ly][lx] = q.x;
+		s.v[slot][ADV][ly][lx] = q.a;
+		s.v[slot][VEL + 0][ly][lx] = q.v[0];
+		s.v[slot][VEL + 1][ly][lx] = q.v[1];
+		s.v[slot][VEL + 2][ly][lx] = q.v[2];
+	}
+}
+
 __device__ __forceinline__ Prim get(const SmemQ& s, int slot, int ly, int lx) {
 	Prim q;
 	q.d = s.v[slot][DEN][ly][lx];
@@ -481,6 +549,14 @@ __device__ __forceinline__ double dmin_(double a, double b) { return (b < a) ? b
 
 using namespace f32;
 
+// Byte offset of the plane staging buffer in the kernel's shared memory:
+// after the ring and the flux and slope arrays, 16-byte aligned.
+__host__ __device__ constexpr size_t hydro_stage_raw_offset() {
+	return (sizeof(f32::SmemQ) + sizeof(float) * 7 * (f32::BY * (f32::BX + 1) + (f32::BY + 1) * f32::BX +
+	                                                  3 * f32::BY * f32::BX + 2 * f32::BY + 2 * f32::BX) + 15) /
+	       16 * 16;
+}
+
 // Riemann solve for one face from its reconstructed states.
 template <int RS>
 __device__ __forceinline__ void face_flux(int rs_rt, const Prim& L, const Prim& R, int dim, float gamma, float* F) {
@@ -507,6 +583,7 @@ __global__ void __launch_bounds__(BX* BY, 2)
 	float* Sy = Sx + 7 * BY * BX;                                     // [7][BY * BX] y slopes of the tile
 	float* Ex = Sy + 7 * BY * BX;                                     // [7][2 * BY] x slopes of cells x0 - 1, x0 + BX
 	float* Ey = Ex + 7 * 2 * BY;                                      // [7][2 * BX] y slopes of cells y0 - 1, y0 + BY
+	TS* raw = reinterpret_cast<TS*>(smem_raw + hydro_stage_raw_offset());  // [7][SY * SX] next plane, staged
 	const int tx = threadIdx.x % BX, ty = threadIdx.x / BX;
 	const int lx = tx + HALO, ly = ty + HALO;
 	const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY;
@@ -571,18 +648,20 @@ __global__ void __launch_bounds__(BX* BY, 2)
 			szc = slope_of(lim, th, get(s, slot_of(z0 - 2), ly, lx), get(s, slot_of(z0 - 1), ly, lx),
 			               get(s, slot_of(z0), ly, lx));
 		__syncthreads();  // plane z0 - 2 is read: its slot takes plane z0 + 1
+		load_plane<STAGE>(P, SP, SC, Uq, s, slot_of(z0 + 1), x0, y0, z0 + 1);
 	} else {
 		load_plane<STAGE>(P, SP, SC, Uq, s, 0, x0, y0, 0);
-		__syncthreads();
 	}
 
+	// Plane z + 3 is staged (cp.async) while plane z is computed and turned into
+	// primitives after its update, into the slot of plane z, which nothing
+	// reads after the flux barrier.
 	for (int z = nd > 2 ? z0 - 1 : z0; z < z1; ++z) {
 		const int sc = nd > 2 ? slot_of(z) : 0;
 		const bool plane = z >= z0;  // x/y faces and the update of this plane
-		if (nd > 2) {
-			load_plane<STAGE>(P, SP, SC, Uq, s, slot_of(z + 2), x0, y0, z + 2);
-			__syncthreads();
-		}
+		const bool stage_next = nd > 2 && z + 1 < z1;
+		__syncthreads();  // planes z .. z + 2 are in the ring; the staging buffer is free
+		if (stage_next) plane_fetch(P, Uq, raw, x0, y0, z + 3);
 		// slopes: this cell in x, y and (of the next plane's cell) z; the cells
 		// just outside the tile in x and y
 		Prim szn = zero;
@@ -683,6 +762,7 @@ __global__ void __launch_bounds__(BX* BY, 2)
 		// it, nothing of this plane is read, so the next plane's load may reuse
 		// the slot without another barrier
 		const Prim qc = get(s, sc, ly, lx);
+		if (stage_next) cp_async_wait_all();  // this thread's copies of plane z + 3 have landed
 		__syncthreads();
 		if (active && plane) {
 			const long long id = gx + (long long)P.nx * (gy + (long long)P.ny * z);
@@ -764,8 +844,9 @@ __global__ void __launch_bounds__(BX* BY, 2)
 			for (int i = 0; i < 7; ++i) fzlo[i] = Fz[i * BY * BX + threadIdx.x];
 		}
 		szc = szn;
-		// no barrier here: the next plane's load writes only the slot of plane
-		// z, and the flux and slope arrays are rewritten after the next barrier
+		// no barrier before this: only the slot of plane z is written, and the
+		// flux and slope arrays are rewritten after the next barrier
+		if (stage_next) plane_convert<STAGE>(P, SP, SC, raw, s, slot_of(z + 3), x0, y0, z + 3);
 	}
 	if (bad) atomicOr(S.err, ERRB_NAN);
 	if (STAGE == 2) {
@@ -778,7 +859,8 @@ __global__ void __launch_bounds__(BX* BY, 2)
 }
 
 size_t hydro_stage_fp32_smem() {
-	return sizeof(SmemQ) + sizeof(float) * 7 * (BY * (BX + 1) + (BY + 1) * BX + 3 * BY * BX + 2 * BY + 2 * BX);
+	// the staging buffer is sized for the FP64 state of the radiation-hydro form
+	return hydro_stage_raw_offset() + sizeof(double) * 7 * SX * SY;
 }
 
 template <int STAGE, typename TS, int LIM, int RS>
