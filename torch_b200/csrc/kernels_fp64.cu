@@ -494,15 +494,20 @@ __global__ void __launch_bounds__(256) k_advance_fp64(Params P, State S, double 
 
 // ------------------------------------------------------------------ radiation
 // Radiation.cpp:243-251.
-// emT = exp(-T), passed in where T is fixed across calls.
+// emT = exp(-T), passed in where T is fixed across calls.  Beyond the
+// ionisation front exp(-T) underflows to 0 (T >= 750 in both builds' exp),
+// and then the rate is exactly +0 whatever delT: the second exponential is
+// skipped (a NaN delT still propagates).
 __device__ __forceinline__ double photoionisation_rate_e(double nHI, double emT, double delT, double shellVol,
                                                          double photonRate) {
 	if (nHI == 0 || shellVol == 0) return 0.0;
+	if (emT == 0 && delT == delT) return 0.0;
 	double emdT = d_exp(-delT);
 	return photonRate * emT * (1.0 - emdT) / (nHI * shellVol);
 }
 __device__ __forceinline__ double photoionisation_rate(double nHI, double T, double delT, double shellVol, double photonRate) {
 	if (nHI == 0 || shellVol == 0) return 0.0;
+	if (T >= 750.0 && delT == delT) return 0.0;
 	return photoionisation_rate_e(nHI, d_exp(-T), delT, shellVol, photonRate);
 }
 
