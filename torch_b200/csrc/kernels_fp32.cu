@@ -532,16 +532,6 @@ __device__ __forceinline__ Prim get7(const float* a, int n, int k) {
 	for (int j = 0; j < 3; ++j) q.v[j] = a[(VEL + j) * n + k];
 	return q;
 }
-__device__ __forceinline__ Prim shfl_up7(const Prim& q) {
-	Prim r;
-	r.d = __shfl_up_sync(0xffffffffu, q.d, 1);
-	r.p = __shfl_up_sync(0xffffffffu, q.p, 1);
-	r.x = __shfl_up_sync(0xffffffffu, q.x, 1);
-	r.a = __shfl_up_sync(0xffffffffu, q.a, 1);
-#pragma unroll
-	for (int j = 0; j < 3; ++j) r.v[j] = __shfl_up_sync(0xffffffffu, q.v[j], 1);
-	return r;
-}
 
 __device__ __forceinline__ double dmin_(double a, double b) { return (b < a) ? b : a; }
 
