@@ -141,6 +141,21 @@ def test_fp64_hii_region_24_cubed_20_steps():
     assert_close(common.state_dict(s), ref, 3, what="hii24")
 
 
+@pytest.mark.parametrize("precision", [torch_b200.PRECISION_FP64, torch_b200.PRECISION_FP32])
+def test_shell_overlap_keeps_results_bitwise(monkeypatch, precision):
+    """The shells of a sweep start while the previous shell runs (programmatic
+    dependent launch) and wait for it inside the kernel; with the overlap
+    switched off (TRG_SHELL_OVERLAP=0, read when a context is created) every
+    field of the state is bitwise the same."""
+    tp, ic = workloads.hii_region(n=24, seed=5)
+    monkeypatch.delenv("TRG_SHELL_OVERLAP", raising=False)
+    a = run_product(tp, ic, 12, precision=precision, batched=True)
+    monkeypatch.setenv("TRG_SHELL_OVERLAP", "0")
+    b = run_product(tp, ic, 12, precision=precision, batched=True)
+    for g in ("U", "Q", "R", "T"):
+        assert np.array_equal(common.state_dict(a)[g], common.state_dict(b)[g]), g
+
+
 def test_run_steps_is_deterministic():
     tp, ic = workloads.sedov(n=16)
     a = run_product(tp, ic, 5, batched=True)
