@@ -522,9 +522,17 @@ __device__ __forceinline__ double collisional_ionisation_rate(const Params& P, d
 __device__ __forceinline__ void doric(double dt, double& HII_avg, double& HII, double Api, double nHII_aB, double nHII_Aci) {
 	double xeq, inv_ti, epsilon = 1.0e-8;
 	double HII_old = HII;
+	inv_ti = Api + nHII_Aci + nHII_aB;
+#ifdef TRG_FAST_MATH
+	// one division, 1 / (dt / t_i), for xeq and the time average (when
+	// dt / t_i < 1e-8 neither is used)
+	const double ti_dt = 1.0 / (dt * inv_ti);
+	if (nHII_aB == 0.0) xeq = 1.0;
+	else xeq = (Api + nHII_Aci) * (ti_dt * dt);
+#else
 	if (nHII_aB == 0.0) xeq = 1.0;
 	else xeq = (Api + nHII_Aci) / (Api + nHII_Aci + nHII_aB);
-	inv_ti = Api + nHII_Aci + nHII_aB;
+#endif
 	if (dt * inv_ti < 1.0e-8) {
 		HII = HII_old;
 		HII = smax(smin(HII, 1.0), 0.0);
@@ -535,7 +543,11 @@ __device__ __forceinline__ void doric(double dt, double& HII_avg, double& HII, d
 		HII = xeq + (HII_old - xeq) * e;
 		HII = smax(smin(HII, 1.0), 0.0);
 		if (1.0 - HII < epsilon) HII = 1.0 - epsilon;
+#ifdef TRG_FAST_MATH
+		HII_avg = xeq + (HII_old - xeq) * (1.0 - e) * ti_dt;
+#else
 		HII_avg = xeq + (HII_old - xeq) * (1.0 - e) / (dt * inv_ti);
+#endif
 		HII_avg = smax(smin(HII_avg, 1.0), 0.0);
 		if (1.0 - HII_avg < epsilon) HII_avg = 1.0 - epsilon;
 	}
@@ -613,12 +625,20 @@ __device__ __forceinline__ double tau_interp(const Params& P, const double* tau,
 	double w[4];
 	for (int i = 0; i < 4; ++i) w[i] = w0[i] / smax(P.tau0, tau[i]);
 	double sum_w = w[0] + w[1] + w[2] + w[3];
+#ifdef TRG_FAST_MATH
+	// sum(w tau) / sum(w): one normalising division (sum_w > 0: the weights w0
+	// of an inner cell sum to 1)
+	double num = 0.0;
+	for (int i = 0; i < 4; ++i) num += w[i] * tau[i];
+	return num / sum_w;
+#else
 	double newtau = 0.0;
 	for (int i = 0; i < 4; ++i) {
 		w[i] = w[i] / sum_w;
 		newtau += w[i] * tau[i];
 	}
 	return newtau;
+#endif
 }
 // A zero-weight neighbour contributes 0 * tau = 0 whatever its tau, and may
 // belong to the shell being swept: it is not read.  Neighbour optical depths

@@ -177,7 +177,11 @@ __device__ __forceinline__ void FfromQ(double* f, const double* q, double gamma,
 // Fluid::calcTemperature, Fluid.cpp:71-74.
 __device__ __forceinline__ double calc_temperature(const Params& P, double hii, double pre, double den) {
 	double mu_inv = P.X * (hii + 1.0) + (1.0 - P.X) * 0.25;
+#ifdef TRG_FAST_MATH
+	return pre / (den * mu_inv * P.specificGasConstant);  // one division instead of three
+#else
 	return (pre / den) * (1.0 / mu_inv) / P.specificGasConstant;
+#endif
 }
 
 // Fluid::fixPrimitives for one cell, Fluid.cpp:138-150 (floor uses U[DEN]).
@@ -234,8 +238,14 @@ __device__ __forceinline__ double splint(const Spline& s, double x2) {
 		else klo = k;
 	}
 	double h = s.x[khi] - s.x[klo];
+#ifdef TRG_FAST_MATH
+	const double ih = 1.0 / h;
+	double a = (s.x[khi] - x2) * ih;
+	double b = (x2 - s.x[klo]) * ih;
+#else
 	double a = (s.x[khi] - x2) / h;
 	double b = (x2 - s.x[klo]) / h;
+#endif
 	return a * s.y[klo] + b * s.y[khi] + ((a * a * a - a) * s.y2[klo] + (b * b * b - b) * s.y2[khi]) * (h * h) / 6.0;
 }
 
