@@ -622,12 +622,26 @@ __device__ __forceinline__ void sweep_wait() {
 // Radiation::updateTauSC, Radiation.cpp:353-373: the weighted interpolation of
 // the inner neighbours' optical depths tau[i] (zero where not read).
 __device__ __forceinline__ double tau_interp(const Params& P, const double* tau, const double* w0) {
+#ifdef TRG_FAST_MATH
+	// sum(w0 tau / m) / sum(w0 / m), m = max(tau0, tau), with numerator and
+	// denominator multiplied by the product of the four m: one division (the
+	// weights w0 of an inner cell sum to 1, so the denominator is positive).
+	// Optical depths large enough for the product to overflow take the
+	// per-neighbour divisions.
+	double m[4];
+	for (int i = 0; i < 4; ++i) m[i] = smax(P.tau0, tau[i]);
+	const double m01 = m[0] * m[1], m23 = m[2] * m[3];
+	if (m01 * m23 < 1.0e300) {
+		const double p0 = m[1] * m23, p1 = m[0] * m23, p2 = m[3] * m01, p3 = m[2] * m01;
+		const double num = w0[0] * p0 * tau[0] + w0[1] * p1 * tau[1] + w0[2] * p2 * tau[2] + w0[3] * p3 * tau[3];
+		const double den = w0[0] * p0 + w0[1] * p1 + w0[2] * p2 + w0[3] * p3;
+		return num / den;
+	}
+#endif
 	double w[4];
 	for (int i = 0; i < 4; ++i) w[i] = w0[i] / smax(P.tau0, tau[i]);
 	double sum_w = w[0] + w[1] + w[2] + w[3];
 #ifdef TRG_FAST_MATH
-	// sum(w tau) / sum(w): one normalising division (sum_w > 0: the weights w0
-	// of an inner cell sum to 1)
 	double num = 0.0;
 	for (int i = 0; i < 4; ++i) num += w[i] * tau[i];
 	return num / sum_w;
@@ -770,6 +784,7 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 	const double dt = h * S.scal[0];
 	bool star = false, front = false, inner = false;
 	double q_den = 0, q_pre = 0, q_hii = 0, ds = 0, n_H = 0, T = 1, alphaB = 0, A_ci = 0, tau_avg = 0, shellVol = 0;
+	double nH_cell = 0;
 	long long nb[4] = {-1, -1, -1, -1};
 	double w[4] = {0, 0, 0, 0};
 	if (valid) {
@@ -786,8 +801,15 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 		q_pre = FLD(S.Q, PRE, id);
 		q_hii = FLD(S.Q, HII, id);
 		ds = S.ds[id];
+#ifdef TRG_FAST_MATH
+		nH_cell = P.X * q_den / P.hydrogenMass;
+#endif
 		if (!star) {
+#ifdef TRG_FAST_MATH
+			n_H = nH_cell;
+#else
 			n_H = P.X * q_den / P.hydrogenMass;
+#endif
 			T = calc_temperature(P, q_hii, q_pre, q_den);
 			alphaB = spline_eval(S.tables->rad_recomb, T);
 			A_ci = collisional_ionisation_rate(P, T);
@@ -845,7 +867,13 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 			double nHII_aB = HII_avg * n_H * alphaB;
 			double nHII_Aci = HII_avg * n_H * A_ci;
 			doric(dt, HII_avg, x_new, A_pi, nHII_aB, nHII_Aci);
-			if ((fabs((HII_avg - HII_avg_old) / HII_avg) < 1.0e-3 || (HII_avg < 1.0e-5) || A_pi == 0)) converged = true;
+#ifdef TRG_FAST_MATH
+			// the same test without its division
+			const bool small_step = fabs(HII_avg - HII_avg_old) < 1.0e-3 * fabs(HII_avg);
+#else
+			const bool small_step = fabs((HII_avg - HII_avg_old) / HII_avg) < 1.0e-3;
+#endif
+			if ((small_step || (HII_avg < 1.0e-5) || A_pi == 0)) converged = true;
 			if (learned) {
 				// the first iteration from the prediction is its residual test:
 				// accept, or restart the plain iteration from x_HII
@@ -889,7 +917,11 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 			}
 		}
 	}
-	double nH = P.X * q_den / P.hydrogenMass;
+#ifdef TRG_FAST_MATH
+	const double nH = nH_cell;
+#else
+	const double nH = P.X * q_den / P.hydrogenMass;
+#endif
 	store_taus(S, id, tau, (1.0 - hii_new) * nH * P.photoIonXsec * ds, tau_a, (1.0 - hii_a_new) * nH * P.photoIonXsec * ds);
 	if (DIAG && P.stats_on) {
 		stat_picard(S.stats, iters);
