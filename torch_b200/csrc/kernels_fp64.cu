@@ -1230,6 +1230,37 @@ __device__ __forceinline__ void b_colden_shell_fp64(const Params& P, const State
 	double newcolden = 0.0;
 	if (inner) {
 		double colden[4] = {0, 0, 0, 0}, w[4];
+#ifdef TRG_FAST_MATH
+		for (int i = 0; i < 4; ++i)
+			if (nb_read(nb, w0, i)) {
+				const double2 c = __ldcg(reinterpret_cast<const double2*>(S.T + nb[i] * 2));  // COL_DEN, DCOL_DEN
+				colden[i] = c.x + c.y;
+			}
+		// The interpolation is the weighted harmonic mean sum(w0) / sum(w0 / c)
+		// over the non-zero c; numerator and denominator scaled by the product
+		// of those c take one division (per-neighbour divisions where that
+		// product would overflow).
+		double m[4];
+		for (int i = 0; i < 4; ++i) m[i] = colden[i] == 0 ? 1.0 : colden[i];
+		const double m01 = m[0] * m[1], m23 = m[2] * m[3], prod = m01 * m23;
+		if (prod < 1.0e300) {
+			const double p[4] = {m[1] * m23, m[0] * m23, m[3] * m01, m[2] * m01};
+			double num = 0, den = 0;
+			for (int i = 0; i < 4; ++i)
+				if (colden[i] != 0) {
+					num += w0[i];
+					den += w0[i] * p[i];
+				}
+			newcolden = den != 0 ? num * prod / den : 0.0;
+		} else {
+			for (int i = 0; i < 4; ++i) w[i] = colden[i] == 0 ? 0 : w0[i] / colden[i];
+			double sum_w = w[0] + w[1] + w[2] + w[3];
+			for (int i = 0; i < 4 && sum_w != 0; ++i) {
+				w[i] = w[i] / sum_w;
+				newcolden += w[i] * colden[i];
+			}
+		}
+#else
 		for (int i = 0; i < 4; ++i) {
 			if (nb_read(nb, w0, i)) {
 				const double2 c = __ldcg(reinterpret_cast<const double2*>(S.T + nb[i] * 2));  // COL_DEN, DCOL_DEN
@@ -1242,6 +1273,7 @@ __device__ __forceinline__ void b_colden_shell_fp64(const Params& P, const State
 			w[i] = w[i] / sum_w;
 			newcolden += w[i] * colden[i];
 		}
+#endif
 	}
 	reinterpret_cast<double2*>(S.T + id * 2)[0] = make_double2(newcolden, dcolden);
 }
@@ -1498,7 +1530,11 @@ __device__ __forceinline__ void b_dt_reduce_fp64(const Params& P, const State& S
 		double inv_t = 0;
 		double ss = sqrt(P.gamma * q_pre / q_den);
 		#pragma unroll
+#ifdef TRG_FAST_MATH
+		for (int dim = 0; dim < 3; ++dim) if (dim < P.nd) inv_t += (fabs(FLD(S.Q, VEL + dim, id)) + ss) * (1.0 / P.dx[dim]);
+#else
 		for (int dim = 0; dim < 3; ++dim) if (dim < P.nd) inv_t += (fabs(FLD(S.Q, VEL + dim, id)) + ss) / P.dx[dim];
+#endif
 		if (inv_t == 0) inv_t = 1.0 / P.dt_max;
 		th = 0.5 / inv_t;
 		int ijk[3];
