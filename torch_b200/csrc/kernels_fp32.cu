@@ -16,9 +16,10 @@
 // every face flux is evaluated once.  A thread owns one cell of the plane (a
 // warp owns one row): it computes the cell's limited slope once per direction
 // (a face takes the slopes of its two cells), its low x, low y and high z
-// faces, and its update.  x neighbours' slopes and fluxes move by warp
-// shuffle, y neighbours' through shared memory, and the z slope and z flux of
-// the column stay in registers from one plane to the next.
+// faces, and its update; the neighbours' slopes and fluxes pass through
+// shared memory, while the z slope of the column and the flux through its
+// lower z face stay in registers from one plane to the next.  The plane three
+// ahead is staged with cp.async while the current one is computed.
 //
 // The rotated solver is written in directional form: HLL with normal n1 and
 // HLLC with normal n2 are the reference's rotate / 1-D solve / rotate-back
