@@ -72,3 +72,14 @@ def compare_states(got: dict, ref: dict, nd: int, groups=("U", "Q", "R", "T")):
 
 def state_dict(s):
     return {"U": s.U, "Q": s.Q, "R": s.R, "T": s.T, "Tmin": s.Tmin}
+
+
+def ifront_cells(hii, n):
+    """I-front distance (cells) from a star at the centre of an n^3 grid along
+    +x: the first cell with HII < 0.5, linearly interpolated (the rule of the
+    reference's scripts/misc/calc_if.py:43-56)."""
+    x = np.asarray(hii).reshape(n, n, n)[n // 2, n // 2, n // 2:]
+    for i in range(1, len(x)):
+        if x[i] < 0.5:
+            return (i - 1) + (x[i - 1] - 0.5) / (x[i - 1] - x[i])
+    return float(len(x))

@@ -93,6 +93,24 @@ def test_fp32_form_radiation_hydro_hii_region():
     assert ed <= 1e-4 and ep <= 1e-4
 
 
+def test_fp32_form_hii64_300_steps():
+    """The 3-D HII region at 64^3 with radiation and cooling, 300 steps: the
+    FP32 form (FP32 fluxes, increments added to the FP64 state) against the
+    FP64 form.  Density and pressure relative L1 <= 1e-4 (the bar of the FP32
+    form) and the I-front radius along +x within 0.5 cell."""
+    n = 64
+    tp, ic = workloads.hii_region(n=n, seed=5)
+    a = run(tp, ic, 300, torch_b200.PRECISION_FP32)
+    b = run(tp, ic, 300, torch_b200.PRECISION_FP64)
+    g = tp.heatCapacityRatio
+    ed = common.rel_l1(a.U[0], b.U[0])
+    ep = common.rel_l1(pressure(a.U, g, 3), pressure(b.U, g, 3))
+    fa, fb = common.ifront_cells(a.Q[2], n), common.ifront_cells(b.Q[2], n)
+    print(f"hii64 rad-hydro 300 steps: den {ed:.2e} pre {ep:.2e} ifront {fa:.3f} vs {fb:.3f}")
+    assert ed <= 1e-4 and ep <= 1e-4, (ed, ep)
+    assert abs(fa - fb) <= 0.5
+
+
 def test_fp32_form_radiation_hydro_config1():
     """The shipped 2-D cylindrical blister with radiation and cooling.  Its
     cooling step turns rounding differences into O(1e-4) pressure differences

@@ -536,6 +536,64 @@ __device__ __forceinline__ Prim get7(const float* a, int n, int k) {
 
 __device__ __forceinline__ double dmin_(double a, double b) { return (b < a) ? b : a; }
 
+// Fluid::advSolution + fixSolution (Fluid.cpp:80-136) of one cell of the FP64
+// state, in FP64: U_out = fix(U_base + inc), the increment inc = dt L(Q) formed
+// in FP32 (scaled units) by the caller.  With `write_q` also the primitives
+// that globalQfromU + fixPrimitives (Fluid.cpp:138-165) would form from the
+// fixed state, taken from the fix itself (equal up to rounding: the fix has
+// already applied the floors).  One reciprocal of the density replaces the
+// reference's divisions, and the temperature floor is tested as
+// pre < T_floor mu_inv R den.  Fields are formed one at a time, as they are
+// needed, to keep the register footprint of the calling kernel small.
+// Returns false where the reference throws.
+__device__ __forceinline__ bool update_state64(const Params& P, const State& S, const StoreScale& SC,
+                                               const double* __restrict__ Ub, double* __restrict__ Uo, long long id,
+                                               float dtf, const float* udot, bool write_q) {
+	const long long N = P.N;
+	const int nd = P.nd;
+	auto nu = [&](int f) { return __ldg(&Ub[f * N + id]) + (double)(dtf * udot[f]) * SC.s[SC.cls(f)]; };
+	const double d = nu(DEN), e = nu(PRE);
+	const double inv = 1.0 / d;
+	const double hii = smax(smin(nu(HII) * inv, 1.0), 0.0);
+	const double adv = smax(smin(nu(ADV) * inv, 1.0), 0.0);
+	const double den = smax(d, P.dfloor);
+	double v[3] = {0, 0, 0};
+#pragma unroll
+	for (int k = 0; k < 3; ++k)
+		if (k < nd) v[k] = nu(VEL + k) * inv;
+	double ke = ((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]) * (0.5 * d);
+	double pre = (e - ke) * (P.gamma - 1.0);
+	ke *= den * inv;
+	if (pre < P.pfloor) pre = P.pfloor;
+	const double mu_inv = P.X * (hii + 1.0) + (1.0 - P.X) * 0.25;
+	const double pt = mu_inv * P.specificGasConstant * den * P.tfloor;
+	if (pre < pt) pre = pt;
+	const double E = pre / (P.gamma - 1.0) + ke;
+	Uo[DEN * N + id] = den;
+	Uo[PRE * N + id] = E;
+	Uo[HII * N + id] = hii * den;
+	Uo[ADV * N + id] = adv * den;
+	bool ok = isfinite(d) && isfinite(e) && den != 0 && E != 0 && isfinite(E) && isfinite(hii * den) &&
+	          isfinite(adv * den);
+#pragma unroll
+	for (int k = 0; k < 3; ++k)
+		if (k < nd) {
+			const double m = den * v[k];
+			Uo[(VEL + k) * N + id] = m;
+			ok &= isfinite(m);
+		}
+	if (write_q) {
+		FLD(S.Q, DEN, id) = den;
+		FLD(S.Q, PRE, id) = pre;
+		FLD(S.Q, HII, id) = hii;
+		FLD(S.Q, ADV, id) = adv;
+#pragma unroll
+		for (int k = 0; k < 3; ++k)
+			if (k < nd) FLD(S.Q, VEL + k, id) = v[k];
+	}
+	return ok;
+}
+
 }  // namespace f32
 
 using namespace f32;
@@ -779,9 +837,6 @@ __global__ void __launch_bounds__(BX* BY, 2)
 			}
 			if (P.geometry == G_CYL) udot[VEL + 0] += qc.p * rgeo;
 			else if (P.geometry == G_SPH) udot[VEL + 0] += qc.p * rgeo;
-			float ub[7];
-#pragma unroll
-			for (int i = 0; i < 7; ++i) ub[i] = load_u(Ubase, i * N + id, SC, i);
 			if (P.star_on && P.mdot != 0) {
 				int cijk[3] = {gx, gy, z};
 				double cxc[3];
@@ -790,30 +845,31 @@ __global__ void __launch_bounds__(BX* BY, 2)
 					float mdot = (float)(P.mdot / (P.f32_rho0 * P.f32_v0));
 					udot[DEN] += mdot;
 					udot[PRE] += (float)(P.edot / (P.f32_p0 * P.f32_v0));
-					udot[HII] += (ub[HII] / ub[DEN]) * mdot;
+					udot[HII] += (load_u(Ubase, HII * N + id, SC, HII) / load_u(Ubase, DEN * N + id, SC, DEN)) * mdot;
 					udot[ADV] += mdot;
 				}
 			}
 			float u[7];
+			if constexpr (sizeof(TS) == sizeof(double)) {
+				// hydro sub-step of a radiation-hydro run on the FP64 state: the
+				// FP32 increment dt L(Q) is added to the unrounded FP64 state and
+				// fixSolution runs in FP64, so a cell keeps its FP64 digits where
+				// the flux divergence is small (Fluid::advSolution, Fluid.cpp:80-87,
+				// updates U in FP64).  The FP64 primitives of the fixed state are
+				// written as well (what globalQfromU + fixPrimitives of the next
+				// sub-step would compute), so that pass is skipped; cells of the
+				// FP64 fallback keep their old Q for its update.
+				bad |= !update_state64(P, S, SC, Ubase, Uout, id, dtf, udot, !(S.fb_flag && S.fb_flag[id]));
+				if (STAGE == 2) {
 #pragma unroll
-			for (int i = 0; i < 7; ++i) u[i] = ub[i] + dtf * udot[i];
-			bad |= !fix_cons(SP, u);
+					for (int i = 0; i < 7; ++i) u[i] = (float)(Uout[i * N + id] * SC.is[SC.cls(i)]);
+				}
+			} else {
 #pragma unroll
-			for (int i = 0; i < 7; ++i) store_u(Uout, i * N + id, u[i], SC, i);
-			if (sizeof(TS) == sizeof(double) && !(S.fb_flag && S.fb_flag[id])) {
-				// hydro sub-step of a radiation-hydro run: also the FP64 primitives
-				// of the new state with floors (what globalQfromU + fixPrimitives
-				// of the next sub-step would compute), so that pass is skipped;
-				// cells of the FP64 fallback keep their old Q for its update
-				Prim q = prim_from_cons(u, gamma, nd);
-				fix_prim(SP, q, u[DEN]);
-				FLD(S.Q, DEN, id) = (double)q.d * P.f32_rho0;
-				FLD(S.Q, PRE, id) = (double)q.p * P.f32_p0;
-				FLD(S.Q, HII, id) = (double)q.x;
-				FLD(S.Q, ADV, id) = (double)q.a;
+				for (int i = 0; i < 7; ++i) u[i] = load_u(Ubase, i * N + id, SC, i) + dtf * udot[i];
+				bad |= !fix_cons(SP, u);
 #pragma unroll
-				for (int k = 0; k < 3; ++k)
-					if (k < nd) FLD(S.Q, VEL + k, id) = (double)q.v[k] * P.f32_v0;
+				for (int i = 0; i < 7; ++i) store_u(Uout, i * N + id, u[i], SC, i);
 			}
 			if (STAGE == 2) {
 				// the next step's CFL limit from Q(U1) with floors (Torch::fullStep:
