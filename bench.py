@@ -228,11 +228,18 @@ def run_reference_arm(args, rank):
     t0 = time.perf_counter()
     rate, kind, cores, desc = cpu_sample(args.workload, n_sample, max(1, total_steps), procs)
     wall = time.perf_counter() - t0
+    config = workload_config(args.workload, args.n, "fp64", 1)
+    # the rate is the metric of the named workload; the CPU time is measured
+    # on a bounded sample of it (independent single-rank processes, no MPI)
+    config["workload"] = (f"{args.workload} {args.n}^3 rate, timed on a sample: {cores} independent "
+                          f"{n_sample}^3 grids, one single-rank reference process each")
+    config["sample_cells"] = n_sample ** 3 * cores
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / max(1, total_steps),
+        "ms_per_step_of": f"the sample ({cores} x {n_sample}^3 cells), not a {args.n}^3 step",
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(args.workload, args.n, "fp64", 1),
+        "config": config,
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": desc},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -378,37 +385,50 @@ def run_batch(args, world, rank, local, pg):
 
 def time_learned(args, sim32, N, world, local, pg):
     """FP32 form with the learned starting iterate, after the plain FP32 timing:
-    six more FP32 steps record the plain solve's front cells, a network is
-    trained on them on the GPU, then K more FP32 steps are timed with it.
-    Solver counters of two further steps with and without the network follow
-    the timed region."""
+    further FP32 steps record the plain solve's front cells until
+    --learned-records records (or 400 steps), a network is trained on them on
+    the GPU, then K steps are timed with it and K more without it (the plain
+    form from nearly the same state: the harvest steps moved the front).
+    Solver counters of two further steps with and without the network
+    follow."""
     import torch
     import torch_b200
-    # training set: the plain solve's front cells over a few more FP32 steps
-    sim32.harvest(1 << 23)
-    sim32.run_steps(6)
+    sim32.harvest(int(args.learned_records))
+    harvest_steps = 0
+    while harvest_steps < 400:
+        sim32.run_steps(10)
+        harvest_steps += 10
+        if sim32.harvest_read(count_only=True) >= args.learned_records:
+            break
     recs, _ = sim32.harvest_read()
     sim32.harvest(0)
     t0 = time.perf_counter()
     net = torch_b200.Mlp(device=local, seed=11)
-    hist = net.train(recs, epochs=30, batch=4096, lr=2e-3, seed=12)
+    hist = net.train(recs, epochs=30, batch=8192, lr=2e-3, seed=12)
     torch.cuda.synchronize(local)
     train_s = time.perf_counter() - t0
-    sim32.learned_start(net)
     dt_next = sim32.dt_max
-    sim32.run_steps(1)  # captures the sweep graphs with the learned kernel
     stream = torch.cuda.ExternalStream(sim32.stream_handle(), device=f"cuda:{local}")
-    barrier(pg)
-    torch.cuda.synchronize(local)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    sim32.enqueue_steps(args.steps, dt_next)
-    ev1.record(stream)
-    sim32.synchronize()
-    torch.cuda.synchronize(local)
-    barrier(pg)
-    ms = max_over_ranks(pg, ev0.elapsed_time(ev1), local)
+
+    def timed():
+        sim32.run_steps(1)  # captures the sweep graphs of this form
+        barrier(pg)
+        torch.cuda.synchronize(local)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        sim32.enqueue_steps(args.steps, dt_next)
+        ev1.record(stream)
+        sim32.synchronize()
+        torch.cuda.synchronize(local)
+        barrier(pg)
+        return max_over_ranks(pg, ev0.elapsed_time(ev1), local)
+
+    sim32.learned_start(net)
+    ms = timed()
+    sim32.learned_start(None)
+    ms_plain = timed()
     sim32.stats_enable(True)
+    sim32.learned_start(net)
     sim32.run_steps(2)
     st = sim32.stats(reset=True)
     sim32.learned_start(None)
@@ -417,14 +437,16 @@ def time_learned(args, sim32, N, world, local, pg):
     sim32.stats_enable(False)
     net.close()
     return {"value": N * args.steps * world / (ms / 1e3), "ms_per_step": ms / args.steps,
-            "training": {"records": int(len(recs)), "epochs": 30, "seconds": train_s,
-                         "loss_first_last": [float(hist[0]), float(hist[-1])]},
+            "plain_fp32_same_state": {"value": N * args.steps * world / (ms_plain / 1e3),
+                                      "ms_per_step": ms_plain / args.steps},
+            "training": {"records": int(len(recs)), "harvest_steps": harvest_steps, "epochs": 30,
+                         "seconds": train_s, "loss_first_last": [float(hist[0]), float(hist[-1])]},
             "front_cells": st["front_cells"], "learned_cells": st["learned_cells"],
             "accepted": st["learned_accepted"] / max(1, st["learned_cells"]),
             "front_iters_per_cell": st["front_iters"] / max(1, st["front_cells"]),
             "front_iters_per_cell_plain": st_plain["front_iters"] / max(1, st_plain["front_cells"]),
             "picard_max": st["picard_max"], "picard_max_plain": st_plain["picard_max"],
-            "note": "counters from two steps after the timed region with the network, then two without it"}
+            "note": "counters from two steps after the timed regions with the network, then two without it"}
 
 
 def ifront_cells(hii, n):
@@ -646,6 +668,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", dest="learned", action="store_false",
                     help="skip the FP32 + learned-start measurement")
+    ap.add_argument("--learned-records", type=float, default=1e7,
+                    help="front-cell solves harvested for the learned start's training set")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -52,6 +52,7 @@ extern "C" {
 #define TRG_ERR_FLUX 6         /* Riemann solver produced a NaN HII flux */
 #define TRG_ERR_OOM 7          /* device allocation failed */
 #define TRG_ERR_TC 8           /* a tensor-core (tcgen05) wait expired */
+#define TRG_ERR_SUBCYCLE 9     /* a cell needs more thermal sub-cycles than the work queue runs */
 
 #define TRG_PRECISION_FP64 0   /* every kernel in FP64, reference operation order, no FMA */
 #define TRG_PRECISION_FP32 1   /* hydro in FP32 (compensated E - KE), FP64 for ionisation, dt, sums */
@@ -108,6 +109,15 @@ typedef struct trg_ctx trg_ctx;
 int trg_create(const trg_params* p, const double* den, const double* pre, const double* hii,
                const double* v0, const double* v1, const double* v2, const double* grav,
                trg_ctx** out);
+/* The arguments Torch::setUpLua (src/Torch/Torch.cpp:196-228) passes to the
+ * Lua setup function initialise(x, y, z, xs, ys, zs) of a run with
+ * parameters p: every cell's centre (x, y, z: N each, cgs, flat index
+ * i + nx*(j + ny*k), any may be NULL) and the star's position (star_xyz[3],
+ * may be NULL), formed as the reference forms them (cell index coordinates
+ * times the code-unit grid spacing, converted back to cgs).  Host only: needs
+ * no GPU.  The setup function's nine results per cell become trg_create's
+ * den, pre, hii, v0, v1, v2 and grav. */
+int trg_setup_positions(const trg_params* p, double* x, double* y, double* z, double* star_xyz);
 int trg_full_step(trg_ctx* c, double dt_next_checkpoint, double* dt_taken);
 int trg_run_steps(trg_ctx* c, int nsteps, double dt_next_checkpoint, double* dts_out);
 int trg_component(trg_ctx* c, int comp, int phase, double dt, double* out);
@@ -165,6 +175,34 @@ enum {
  * strong shocks, where FP32 flux differences keep too few digits.  The count
  * of such updates is the TRG_STAT_FP64_CELLS counter. */
 int trg_fp32_contrast(trg_ctx* c, double contrast);
+
+/* Thermal sub-cycles through a work queue (no counterpart in the reference,
+ * whose Thermodynamics::integrate, src/Integrators/Thermodynamics.cpp:266-337,
+ * loops over the cells): with min_subcycles > 0, cells whose closed-form
+ * sub-cycle count (:304-310) is at least min_subcycles leave the in-place pass
+ * for a queue, binned by the bit length of their count, heaviest first, which
+ * a persistent kernel drains (each warp takes 32 cells of similar count).
+ * Results are bitwise those of the in-place pass; a cell with more than 2^26
+ * sub-cycles is reported as TRG_ERR_SUBCYCLE.  0 (the default) switches the
+ * queue off.  Single grids only (batches run the sub-cycles in place). */
+int trg_thermo_queue(trg_ctx* c, int min_subcycles);
+
+/* Global FP64 conservation sums (no counterpart in the reference): total
+ * mass sum(rho V) and total energy sum(E V) over the grid's cells (code
+ * units; V the cell volume of Grid::computeCellVolume,
+ * src/Fluid/Grid.cpp:876-905).  Every product is formed exactly and the sum
+ * is carried in double-double in a fixed order, so the result is
+ * deterministic and is the exact sum rounded once.  trg_conservation_sums
+ * returns the sums of the current state (either pointer may be NULL).  With
+ * trg_conservation_enable(c, 1) every full step also records the sums of the
+ * state it starts from (in the FP64 forms as a side product of the time-step
+ * reduction, Torch::calculateTimeStep); trg_conservation_history copies up
+ * to max_entries records [n][2] (mass, energy), record k being the state
+ * after k steps, and sets *n_entries to the number of steps recorded so far
+ * (NaN for steps run while recording was off). */
+int trg_conservation_sums(trg_ctx* c, double* mass, double* energy);
+int trg_conservation_enable(trg_ctx* c, int on);
+int trg_conservation_history(trg_ctx* c, double* out, long long max_entries, long long* n_entries);
 
 /* Heating and cooling diagnostics (Thermodynamics::fillHeatingArrays,
  * src/Integrators/Thermodynamics.cpp:419-461, as printed by
@@ -270,6 +308,11 @@ typedef struct trg_batch trg_batch;
 int trg_batch_create(trg_ctx* const* grids, int ngrids, trg_batch** out);
 int trg_batch_run_steps(trg_batch* b, int nsteps, double dt_next_checkpoint);
 int trg_batch_enqueue_steps(trg_batch* b, int nsteps, double dt_next_checkpoint);
+/* One captured CUDA graph per timestep (default on): the steps of a batch
+ * after its first are replayed from graphs captured once per position of the
+ * operator split's rotating component order (bitwise the same results as the
+ * launches themselves, which `on` = 0 restores). */
+int trg_batch_step_graphs(trg_batch* b, int on);
 int trg_batch_synchronize(trg_batch* b);
 void* trg_batch_stream(const trg_batch* b);
 long long trg_batch_kernel_launches(const trg_batch* b);
@@ -282,19 +325,26 @@ void trg_batch_destroy(trg_batch* b);
 /* No counterpart in the reference.  One FP32 RK2 hydro step - the two fused
  * stage kernels of the FP32 form - from U_in to U_out, both caller-owned
  * device arrays of [7][N] doubles in code units (the layout of trg_get_state;
- * U_in == U_out is allowed), for time step dt, on `stream` (a cudaStream_t,
- * NULL for the default stream), using the parameters of context c.  It
- * allocates no device memory: for callers that may not allocate once they run
- * (their device memory is reserved up front by their own allocator, or
- * cudaMalloc's implicit synchronisation is not allowed on their stepping
- * path).  Its intermediate state lives in a static device array of at most
- * TRG_NOALLOC_MAX_CELLS cells (about 14 MiB, held by every GPU that loads the
- * library until exit); larger grids are rejected with TRG_ERR_ARG.  All calls
- * share that array: calls that overlap on the GPU race.  The first call on a
- * device looks the array's address up, so make it before any stream capture.
- * The call waits for its stream and returns the step's error status. */
+ * U_in == U_out is allowed), for time step dt (positive and finite), on
+ * `stream` (a cudaStream_t, NULL for the default stream), using the
+ * parameters of context c.  Hydrodynamics only: a context with radiation or
+ * cooling on is rejected with TRG_ERR_ARG.  If dt_next is not NULL it
+ * receives the time step the next call may take: the CFL limit of the new
+ * state (Hydrodynamics::calculateTimeStep), at most dt_max - the caller
+ * chooses dt, and this is the stable choice.  It allocates no device memory:
+ * for callers that may not allocate once they run (their device memory is
+ * reserved up front by their own allocator, or cudaMalloc's implicit
+ * synchronisation is not allowed on their stepping path).  Its intermediate
+ * state lives in a static device array of at most TRG_NOALLOC_MAX_CELLS
+ * cells (about 14 MiB, held by every GPU that loads the library until exit);
+ * larger grids are rejected with TRG_ERR_ARG.  All calls share that array:
+ * calls that overlap on the GPU race.  The call switches to the context's
+ * device and restores the caller's current device before it returns; it
+ * waits for its stream (it reads the error status back), so it must not be
+ * made while a stream is being captured. */
 #define TRG_NOALLOC_MAX_CELLS 262144
-int trg_hydro_step_fp32_noalloc(trg_ctx* c, const double* U_in, double* U_out, double dt, void* stream);
+int trg_hydro_step_fp32_noalloc(trg_ctx* c, const double* U_in, double* U_out, double dt, double* dt_next,
+                                void* stream);
 
 #ifdef __cplusplus
 }

@@ -21,7 +21,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 LIB_PM_PATH = os.path.join(HERE, "_build", "liboracle_pm.so")
 REF_BIN = os.path.join(HERE, "_ref", "torch_ref")
-REF_TREE = "/root/reference"
+# the reference source tree: $TORCH_REFERENCE, default /root/reference
+REF_TREE = os.environ.get("TORCH_REFERENCE", "/root/reference")
 
 
 class OrcParams(C.Structure):
@@ -92,6 +93,8 @@ def _load(portable_math: bool = False):
         _lib.orc_destroy.argtypes = [C.c_void_p]
         _lib.orc_causal_order.restype = C.c_long
         _lib.orc_causal_order.argtypes = [C.c_void_p, C.c_void_p, C.c_long]
+        _lib.orc_cell_volumes.restype = C.c_long
+        _lib.orc_cell_volumes.argtypes = [C.c_void_p, C.c_void_p, C.c_long]
     return _libs[portable_math]
 
 
@@ -157,8 +160,10 @@ class Oracle:
         err = C.create_string_buffer(512)
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in
                 (ic.den, ic.pre, ic.hii, ic.vel[0], ic.vel[1], ic.vel[2])]
-        self._keep = arrs
-        self.ctx = lib.orc_create(C.byref(p), *[_ptr(a) for a in arrs], None, err, 512)
+        grav = getattr(ic, "grav", None)
+        garr = None if grav is None else np.ascontiguousarray(grav, dtype=np.float64)
+        self._keep = arrs + [garr]
+        self.ctx = lib.orc_create(C.byref(p), *[_ptr(a) for a in arrs], _ptr(garr), err, 512)
         if not self.ctx:
             raise RuntimeError("oracle: " + err.value.decode())
         self.lib = lib
@@ -185,6 +190,12 @@ class Oracle:
         n = self.lib.orc_causal_order(self.ctx, _ptr(out), self.N)
         return out[:n]
 
+    def cell_volumes(self) -> np.ndarray:
+        """Cell volumes in code units (Grid::computeCellVolume, Grid.cpp:876-905)."""
+        out = np.zeros(self.N)
+        self.lib.orc_cell_volumes(self.ctx, _ptr(out), self.N)
+        return out
+
     def close(self):
         if self.ctx:
             self.lib.orc_destroy(self.ctx)
@@ -195,6 +206,23 @@ class Oracle:
             self.close()
         except Exception:
             pass
+
+
+def exact_sum_of_products(a, b) -> float:
+    """sum_i a_i b_i of two FP64 arrays, computed exactly (rational
+    arithmetic) and rounded once to the nearest double: the checker of the
+    library's global conservation sums."""
+    from fractions import Fraction
+    total = Fraction(0)
+    for x, y in zip(np.asarray(a, dtype=np.float64).tolist(), np.asarray(b, dtype=np.float64).tolist()):
+        total += Fraction(x) * Fraction(y)
+    return float(total)
+
+
+def conservation_sums(U, vol):
+    """Exact global (mass, energy) = (sum rho V, sum E V) of a conserved state
+    U [7][N] with cell volumes vol [N]."""
+    return exact_sum_of_products(U[0], vol), exact_sum_of_products(U[1], vol)
 
 
 def read_trgs(path: str) -> State:
@@ -217,7 +245,8 @@ def read_trgs(path: str) -> State:
 
 
 def run_reference(params_path: str, ic_path: Optional[str], steps: int, workdir: str,
-                  setup_path: Optional[str] = None, timeout: float = 600, print2d: Optional[str] = None) -> State:
+                  setup_path: Optional[str] = None, timeout: float = 600, print2d: Optional[str] = None,
+                  setup_dump: Optional[str] = None) -> State:
     """Runs the reference binary on a case in a fresh process and returns its final state
     (with `print2d`, the reference also writes its checkpoint files of that state there)."""
     binp = build_reference()
@@ -231,6 +260,8 @@ def run_reference(params_path: str, ic_path: Optional[str], steps: int, workdir:
         cmd.append(f"--setup={setup_path}")
     if print2d:
         cmd.append(f"--print2d={print2d}")
+    if setup_dump:
+        cmd.append(f"--setup-dump={setup_dump}")
     r = subprocess.run(cmd, cwd=workdir, capture_output=True, text=True, timeout=timeout)
     if r.returncode != 0:
         raise RuntimeError(f"reference failed ({r.returncode}): {r.stderr[-2000:]}")

@@ -17,6 +17,9 @@
  *                                  The checkpoint scheduler is not run: every
  *                                  step is offered dt_next_checkpoint = dt_max.
  *
+ * With --setup-dump=FILE (and --setup) it also writes the raw values the Lua
+ * setup function returned for every cell (see below).
+ *
  * Output: a binary state dump (format "TRGS", see write_state below) of the
  * interior cells in the reference's flat index order (x fastest); with
  * --print2d=DIR also the reference's own checkpoint files of the final state
@@ -43,6 +46,7 @@
 #include "Integrators/Radiation.hpp"
 #include "Integrators/Thermodynamics.hpp"
 #include "MPI/MPI_Wrapper.hpp"
+#include "selene/include/selene.h"
 #undef private
 #undef protected
 
@@ -95,7 +99,7 @@ static void write_state(const std::string& path, Torch& torch, const std::vector
 }
 
 int main(int argc, char** argv) {
-	std::string params, setup, ic, out, out0, print2d;
+	std::string params, setup, ic, out, out0, print2d, setup_dump;
 	long steps = 0;
 	int print_params = 0;
 	for (int i = 1; i < argc; ++i) {
@@ -107,10 +111,11 @@ int main(int argc, char** argv) {
 		else if ((v = arg_value(argv[i], "--out="))) out = v;
 		else if ((v = arg_value(argv[i], "--out0="))) out0 = v;
 		else if ((v = arg_value(argv[i], "--print2d="))) print2d = v;
+		else if ((v = arg_value(argv[i], "--setup-dump="))) setup_dump = v;
 		else if (strcmp(argv[i], "--print-params") == 0) print_params = 1;
 		else {
 			fprintf(stderr, "usage: torch_ref --params=P.lua [--setup=S.lua] [--ic=IC_000.txt] "
-			                "--steps=N --out=final.bin [--out0=initial.bin] [--print2d=DIR]\n");
+			                "--steps=N --out=final.bin [--out0=initial.bin] [--print2d=DIR] [--setup-dump=FILE]\n");
 			return 2;
 		}
 	}
@@ -154,6 +159,33 @@ int main(int argc, char** argv) {
 
 		Torch torch;
 		torch.initialise(p);
+		if (!setup_dump.empty() && !setup.empty()) {
+			/* The raw values of the Lua setup function (cgs, before toCodeUnits),
+			 * evaluated with the arguments Torch::setUpLua passes
+			 * (src/Torch/Torch.cpp:196-228): [9][N] doubles, x fastest. */
+			Grid& grid = torch.fluid.getGrid();
+			const size_t N = (size_t)grid.ncells[0] * grid.ncells[1] * grid.ncells[2];
+			std::vector<double> vals(9 * N);
+			sel::State luaState{true};
+			if (!luaState.Load(setup))
+				throw std::runtime_error("cannot load " + setup);
+			for (size_t id = 0; id < N; ++id) {
+				GridCell& cell = grid.getCell((int)id);
+				std::array<double, 3> xc, xs;
+				for (int i = 0; i < 3; ++i) {
+					xc[i] = torch.consts->converter.fromCodeUnits(cell.xc[i] * grid.dx[i], 0, 1, 0);
+					xs[i] = torch.consts->converter.fromCodeUnits(torch.fluid.getStar().xc[i] * grid.dx[i], 0, 1, 0);
+				}
+				double r[9];
+				sel::tie(r[0], r[1], r[2], r[3], r[4], r[5], r[6], r[7], r[8]) =
+					luaState["initialise"](xc[0], xc[1], xc[2], xs[0], xs[1], xs[2]);
+				for (int k = 0; k < 9; ++k) vals[k * N + id] = r[k];
+			}
+			FILE* f = fopen(setup_dump.c_str(), "wb");
+			if (!f || fwrite(vals.data(), sizeof(double), vals.size(), f) != vals.size())
+				throw std::runtime_error("cannot write " + setup_dump);
+			fclose(f);
+		}
 
 		/* Torch::run() prologue, src/Torch/Torch.cpp:245-264, minus snapshot I/O. */
 		torch.fluid.globalQfromU();

@@ -1809,6 +1809,12 @@ long orc_causal_order(const orc_ctx* c, int* out, long cap) {
 	return c->ncausal;
 }
 
+long orc_cell_volumes(const orc_ctx* c, double* out, long cap) {
+	long n = c->N < cap ? c->N : cap;
+	if (out) memcpy(out, c->vol, sizeof(double) * n);
+	return c->N;
+}
+
 void orc_destroy(orc_ctx* c) {
 	if (!c) return;
 	free(c->U); free(c->Q); free(c->W); free(c->UDOT); free(c->R); free(c->T);

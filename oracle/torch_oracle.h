@@ -80,6 +80,10 @@ void orc_destroy(orc_ctx* c);
  * returns the list length. */
 long orc_causal_order(const orc_ctx* c, int* out, long cap);
 
+/* Cell volumes (Grid::computeCellVolume, Grid.cpp:876-905) in code units:
+ * writes up to cap values in flat-index order and returns the cell count. */
+long orc_cell_volumes(const orc_ctx* c, double* out, long cap);
+
 #ifdef __cplusplus
 }
 #endif

@@ -32,11 +32,19 @@ def load_golden(name):
     """Returns (tp, ic, steps, arrays) for tests/golden/<name>.npz."""
     z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
     tp = config.parse_parameters(str(z["params_lua"]))
-    with tempfile.TemporaryDirectory() as d:
-        path = os.path.join(d, "ic_000.txt")
-        with open(path, "w") as f:
-            f.write(str(z["ic_text"]))
-        ic = config.read_initial_conditions(path)
+    if "setup_lua" in z:
+        # Lua-setup case: the reference's own evaluation of the script, cgs
+        v = z["setup_vals"]
+        ic = config.make_initial_conditions(tuple(tp.ncells), tp.sideLength / tp.ncells[0], v[0], v[1], v[2],
+                                            v[3:6].copy())
+        ic.side_length = tp.sideLength
+        ic.grav = v[6:9].copy()
+    else:
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "ic_000.txt")
+            with open(path, "w") as f:
+                f.write(str(z["ic_text"]))
+            ic = config.read_initial_conditions(path)
     arrays = {k: z[k] for k in ("U", "Q", "R", "T", "Tmin", "dts", "time")}
     return tp, ic, int(z["steps"]), arrays
 

@@ -45,3 +45,17 @@ def test_two_gloo_ranks_reduce_and_reference_arm_on_rank0():
         assert p.exitcode == 0
     assert [r for r, *_ in res] == [0, 1]
     assert all(w == 2 and m == 20.0 and rc == 0 for _, w, m, rc in res)
+
+
+def test_reference_arm_line_names_its_sample(capsys):
+    """The reference arm's JSON line: the workload's metric, measured on a
+    bounded sample that the line itself names (grid size and process count)."""
+    import json
+    sys.path.insert(0, ROOT)
+    import bench
+    args = types.SimpleNamespace(workload="hii", n=256, steps=1, warmup=0, gpus=1)
+    assert bench.run_reference_arm(args, 0) == 0
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert "sample" in line["config"]["workload"] and "32^3" in line["config"]["workload"]
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["cores"] >= 1

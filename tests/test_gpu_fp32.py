@@ -55,7 +55,8 @@ def test_fp32_cylindrical_blister_hydro_error_vs_fp64():
 
 
 @pytest.mark.parametrize("riemann,limiter,order", [("HLLC", "minmod", 1), ("HLL", "superbee", 0),
-                                                   ("RotatedHLLC", "monotonised_central", 1)])
+                                                   ("RotatedHLLC", "monotonised_central", 1),
+                                                   ("RotatedHLLC", "leer", 1), ("RotatedHLLC", "ospre", 1)])
 def test_fp32_solver_variants(riemann, limiter, order):
     tp, ic = workloads.sedov(n=24, riemann=riemann, limiter=limiter, order=order)
     rng = np.random.default_rng(3)
@@ -162,3 +163,13 @@ def test_fp64_fallback_for_high_pressure_contrast():
         print(f"contrast {contrast:g}: pre {errs[contrast]:.2e}, FP64 cell updates {st['fp64_cells']}")
         assert (st["fp64_cells"] > 0) == (contrast > 0)
     assert errs[1.0e3] <= 1e-6 and errs[1.0e3] <= errs[0.0]
+
+
+@pytest.mark.parametrize("name", ["grav2d_lua", "sedov2d_maxmod"])
+def test_fp32_form_on_golden_cases(name):
+    """Gravity source terms (a Lua-setup case) and the maxmod limiter in the
+    FP32 form against the FP64 form on the same input."""
+    tp, ic, steps, _ = common.load_golden(name)
+    ed, ep, eE, a, b = errors(tp, ic, steps)
+    print(f"{name} {steps} steps: den {ed:.2e} pre {ep:.2e}")
+    assert ed <= 1e-5 and ep <= 1e-5

@@ -60,3 +60,61 @@ def test_special_values(lib):
     assert np.isnan(lib.f_log(-1.0)) and np.isinf(lib.f_log(0.0))
     assert lib.f_pow(2.0, 0.0) == 1.0 and lib.f_pow(0.0, 1.6) == 0.0
     assert lib.f_exp(-740.0) > 0  # subnormal range
+
+
+VEC = r"""
+#include <math.h>
+#include "%s"
+void v_trg(int f, const double* x, const double* y, double* out, long n) {
+    for (long i = 0; i < n; ++i)
+        out[i] = f == 0 ? trg_exp(x[i]) : f == 1 ? trg_log(x[i]) : f == 2 ? trg_log10(x[i]) : trg_pow(x[i], y[i]);
+}
+void v_libm(int f, const double* x, const double* y, double* out, long n) {
+    for (long i = 0; i < n; ++i)
+        out[i] = f == 0 ? exp(x[i]) : f == 1 ? log(x[i]) : f == 2 ? log10(x[i]) : pow(x[i], y[i]);
+}
+""" % HDR
+
+
+def test_where_the_portable_math_differs_from_glibc():
+    """Where trg_math.h (the FP64 kernels' exp/log/log10/pow) and the host
+    glibc (the reference's libm) return different doubles, over the argument
+    ranges the radiation and cooling step uses: the fraction of differing
+    results and the largest difference in ulp, per function and range.  These
+    differences are what bound the FP64 form's agreement with the reference
+    beyond ~40 radiation-hydro steps (the reference's step amplifies single-ulp
+    differences); the figures are quoted in the design notes."""
+    d = tempfile.mkdtemp(prefix="trg_mathv_")
+    src = os.path.join(d, "v.c")
+    with open(src, "w") as f:
+        f.write(VEC)
+    so = os.path.join(d, "v.so")
+    subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", so, src, "-lm"], check=True)
+    L = C.CDLL(so)
+    for n in ("v_trg", "v_libm"):
+        getattr(L, n).argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long]
+    rng = np.random.default_rng(42)
+    n = 200000
+    cases = [
+        ("exp", 0, "x in [-745, 0] (exp(-tau), doric, cooling)", rng.uniform(-745, 0, n), None),
+        ("exp", 0, "x in [-1, 1]", rng.uniform(-1, 1, n), None),
+        ("log", 1, "x log-uniform in [1e-30, 1e30]", 10 ** rng.uniform(-30, 30, n), None),
+        ("log10", 2, "T log-uniform in [1, 1e9] (spline abscissae)", 10 ** rng.uniform(0, 9, n), None),
+        ("pow", 3, "x log-uniform in [1e-3, 1e6], y in [-3, 3]", 10 ** rng.uniform(-3, 6, n),
+         rng.uniform(-3, 3, n)),
+    ]
+    rows = []
+    for name, f, what, x, y in cases:
+        x = np.ascontiguousarray(x)
+        y = np.ascontiguousarray(y if y is not None else np.zeros(n))
+        a, b = np.zeros(n), np.zeros(n)
+        L.v_trg(f, x.ctypes.data, y.ctypes.data, a.ctypes.data, n)
+        L.v_libm(f, x.ctypes.data, y.ctypes.data, b.ctypes.data, n)
+        ok = b != 0
+        frac = float(np.mean(a[ok] != b[ok]))
+        worst = float(ulp_err(a[ok], b[ok]).max())
+        rows.append((name, what, frac, worst))
+        print(f"{name:6s} {what:50s} differing {100 * frac:6.2f}%  max {worst:.0f} ulp")
+        assert worst <= (64.0 if name == "pow" else 2.0)
+    # the libraries do differ: a build with trg_math.h cannot round like glibc everywhere
+    assert any(r[2] > 0 for r in rows)

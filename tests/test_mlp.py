@@ -136,10 +136,11 @@ def ifront_x(hii, n):
 @pytest.mark.gpu
 def test_learned_start_on_hii_region():
     """Harvest front-cell solves from the plain method, train on the GPU, then
-    run the same steps with the learned start: the network serves the front
-    cells it predicts to be slow; a prediction whose first Picard iteration
-    passes the convergence test is accepted, any other restarts the plain
-    iteration.  Reports the iterations per front cell with and without the
+    run the same steps with the learned start: before each sweep the network
+    runs once over the candidate front cells (chosen from the previous
+    sweep's optical depths) and serves those it predicts to be slow; a
+    prediction whose first Picard iteration passes the convergence test is
+    accepted, any other restarts the plain iteration.  Reports the iterations per front cell with and without the
     network and how far each moves the state from the plain run, beside a
     start one solver tolerance off; the I-front stays within 0.5 cell."""
     n, steps = 32, 40
@@ -179,7 +180,10 @@ def test_learned_start_on_hii_region():
     print(f"learned cells {st['learned_cells']} accepted {acc:.3f}; front iterations per cell: plain {it_plain:.3f} "
           f"learned {it_learned:.3f}")
     assert 0 < st["learned_cells"] <= st["front_cells"]
-    assert st_tol["learned_cells"] == st_tol["front_cells"] > 0
+    # the candidates are chosen before each sweep from the previous sweep's
+    # optical depths: the probe network (every candidate predicted slow)
+    # serves most of the front cells the sweep finds
+    assert 0.5 * st_tol["front_cells"] <= st_tol["learned_cells"] <= st_tol["front_cells"]
     dev = {k: common.rel_l1(s.U[i], s_plain.U[i]) for k, i in (("den", 0), ("E", 1), ("hii", 2))}
     tol = {k: common.rel_l1(s_tol.U[i], s_plain.U[i]) for k, i in (("den", 0), ("E", 1), ("hii", 2))}
     print("state vs plain after", steps, "steps, learned:", {k: f"{v:.2e}" for k, v in dev.items()},

@@ -113,3 +113,17 @@ def test_reference_algorithm_amplifies_ulp_noise():
         a.full_step()
         b.full_step()
     assert common.rel_l1(b.state().U[1], a.state().U[1]) > 1e-8
+
+
+def test_exact_sum_checker_rounds_once():
+    """The checker of the library's conservation sums is exact: a naive FP64
+    sum loses the small terms here, the exact one keeps them."""
+    a = np.array([1e16, 1.0, -1e16, 3.0])
+    b = np.array([1.0, 1.0, 1.0, 0.5])
+    assert float(np.sum(a * b)) != 2.5
+    assert oracle.exact_sum_of_products(a, b) == 2.5
+    o = oracle.Oracle(*common.load_golden("blister_small")[:2])
+    vol = o.cell_volumes()
+    o.close()
+    assert vol.shape == (30 * 40,)
+    assert np.all(vol > 0)

@@ -20,7 +20,8 @@ import numpy as np
 from . import config
 from .config import CONDITION, GEOMETRY, TorchParameters, enum_value
 
-__all__ = ["Torch", "TrgError", "library_path", "load_library", "TorchParameters", "config"]
+__all__ = ["Torch", "TrgError", "library_path", "load_library", "TorchParameters", "config",
+           "initial_conditions_from_lua", "setup_positions"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_NAME = "libtorch_b200.so"
@@ -32,7 +33,7 @@ COMP_HYDRO, COMP_RAD, COMP_THERMO, COMP_FLUID = 0, 1, 2, 3
 PHASE_PRE, PHASE_DT, PHASE_INTEGRATE, PHASE_SOURCES, PHASE_Q_FROM_U, PHASE_ADVANCE = 0, 1, 2, 3, 4, 5
 
 ERROR_NAMES = {1: "TRG_ERR_ARG", 2: "TRG_ERR_CUDA", 3: "TRG_ERR_NAN", 4: "TRG_ERR_PICARD",
-               5: "TRG_ERR_DT", 6: "TRG_ERR_FLUX", 7: "TRG_ERR_OOM"}
+               5: "TRG_ERR_DT", 6: "TRG_ERR_FLUX", 7: "TRG_ERR_OOM", 8: "TRG_ERR_TC", 9: "TRG_ERR_SUBCYCLE"}
 
 
 class TrgError(RuntimeError):
@@ -79,6 +80,7 @@ _lib = None
 # (name, restype, argtypes) for every entry point of include/torch_b200.h
 _SIGNATURES = [
     ("trg_create", C.c_int, [C.POINTER(TrgParams)] + [C.c_void_p] * 7 + [C.POINTER(C.c_void_p)]),
+    ("trg_setup_positions", C.c_int, [C.POINTER(TrgParams)] + [C.c_void_p] * 4),
     ("trg_full_step", C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_double)]),
     ("trg_run_steps", C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_void_p]),
     ("trg_component", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_double)]),
@@ -100,6 +102,7 @@ _SIGNATURES = [
     ("trg_checkpoint_bytes", C.c_longlong, [C.c_void_p]),
     ("trg_heating_enable", C.c_int, [C.c_void_p, C.c_int]),
     ("trg_fp32_contrast", C.c_int, [C.c_void_p, C.c_double]),
+    ("trg_thermo_queue", C.c_int, [C.c_void_p, C.c_int]),
     ("trg_heating", C.c_int, [C.c_void_p, C.c_void_p]),
     ("trg_checkpoint_save", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
     ("trg_checkpoint_load", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
@@ -117,6 +120,7 @@ _SIGNATURES = [
     ("trg_batch_create", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     ("trg_batch_run_steps", C.c_int, [C.c_void_p, C.c_int, C.c_double]),
     ("trg_batch_enqueue_steps", C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    ("trg_batch_step_graphs", C.c_int, [C.c_void_p, C.c_int]),
     ("trg_batch_synchronize", C.c_int, [C.c_void_p]),
     ("trg_batch_stream", C.c_void_p, [C.c_void_p]),
     ("trg_batch_kernel_launches", C.c_longlong, [C.c_void_p]),
@@ -128,7 +132,11 @@ _SIGNATURES = [
     ("trg_harvest", C.c_int, [C.c_void_p, C.c_long]),
     ("trg_harvest_read", C.c_long, [C.c_void_p, C.c_void_p, C.c_long]),
     ("trg_stats", C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong), C.c_int]),
-    ("trg_hydro_step_fp32_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
+    ("trg_conservation_sums", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    ("trg_conservation_enable", C.c_int, [C.c_void_p, C.c_int]),
+    ("trg_conservation_history", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.POINTER(C.c_longlong)]),
+    ("trg_hydro_step_fp32_noalloc", C.c_int,
+     [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.POINTER(C.c_double), C.c_void_p]),
 ]
 
 
@@ -284,6 +292,37 @@ class Mlp:
             pass
 
 
+def setup_positions(tp: TorchParameters):
+    """(x, y, z, star) in cgs as Torch::setUpLua passes them to the Lua setup
+    function (src/Torch/Torch.cpp:196-228), computed by the library's host
+    code (no GPU needed)."""
+    lib = load_library()
+    ncells = tuple(tp.ncells)
+    p = make_params(tp, tp.sideLength, ncells)
+    N = int(np.prod(ncells))
+    x, y, z, star = np.zeros(N), np.zeros(N), np.zeros(N), np.zeros(3)
+    rc = lib.trg_setup_positions(C.byref(p), _ptr(x), _ptr(y), _ptr(z), _ptr(star))
+    if rc != 0:
+        raise TrgError(rc, "trg_setup_positions: invalid grid parameters")
+    return x, y, z, star
+
+
+def initial_conditions_from_lua(tp: TorchParameters, setup) -> "config.InitialConditions":
+    """Initial conditions from a Lua setup script (a path or a
+    ``lua_setup.LuaScript``): the script's ``initialise(x, y, z, xs, ys, zs)``
+    evaluated for every cell of the grid ``tp`` describes, as
+    Torch::setUpLua does (src/Torch/Torch.cpp:196-228), gravity included."""
+    from . import lua_setup
+    script = setup if isinstance(setup, lua_setup.LuaScript) else lua_setup.LuaScript.from_file(setup)
+    x, y, z, star = setup_positions(tp)
+    v = lua_setup.evaluate_setup(script, x, y, z, star)
+    ic = config.make_initial_conditions(tuple(tp.ncells), tp.sideLength / tp.ncells[0], v["den"], v["pre"],
+                                        v["hii"], v["vel"])
+    ic.side_length = tp.sideLength
+    ic.grav = v["grav"]
+    return ic
+
+
 class Torch:
     """One run on one GPU: ``Torch::initialise`` then ``full_step`` calls.
 
@@ -360,11 +399,14 @@ class Torch:
         """Record up to `capacity` front-cell training records from the plain solve (0 stops)."""
         self._check(self.lib.trg_harvest(self.ctx, int(capacity)))
 
-    def harvest_read(self, max_records: int = 1 << 26):
-        """(records [k x 8] float32, total recorded) of the current harvest."""
+    def harvest_read(self, max_records: int = 1 << 26, count_only: bool = False):
+        """(records [k x 8] float32, total recorded) of the current harvest;
+        with count_only, just the number recorded so far."""
         n = int(self.lib.trg_harvest_read(self.ctx, None, 0))
         if n < 0:
             raise TrgError(-n, "trg_harvest_read failed")
+        if count_only:
+            return n
         k = min(n, int(max_records))
         out = np.zeros((k, 8), dtype=np.float32)
         if k:
@@ -376,6 +418,29 @@ class Torch:
     def fp32_contrast(self, contrast: float):
         """Pressure ratio above which the FP32 form updates a hydro cell in FP64 (0: off)."""
         self._check(self.lib.trg_fp32_contrast(self.ctx, float(contrast)))
+
+    def thermo_queue(self, min_subcycles: int):
+        """Cells with at least this many thermal sub-cycles run through the
+        work queue (0: all in place)."""
+        self._check(self.lib.trg_thermo_queue(self.ctx, int(min_subcycles)))
+
+    def conservation_sums(self):
+        """Global FP64 (mass, energy) = (sum rho V, sum E V) of the current state."""
+        m, e = C.c_double(0), C.c_double(0)
+        self._check(self.lib.trg_conservation_sums(self.ctx, C.byref(m), C.byref(e)))
+        return m.value, e.value
+
+    def conservation_enable(self, on: bool = True):
+        """Record the conservation sums of the state every step starts from."""
+        self._check(self.lib.trg_conservation_enable(self.ctx, int(on)))
+
+    def conservation_history(self) -> np.ndarray:
+        """[n, 2] recorded (mass, energy); row k is the state after k steps."""
+        n = C.c_longlong(0)
+        self._check(self.lib.trg_conservation_history(self.ctx, None, 0, C.byref(n)))
+        out = np.zeros((max(n.value, 1), 2))
+        self._check(self.lib.trg_conservation_history(self.ctx, _ptr(out), n.value, C.byref(n)))
+        return out[:n.value]
 
     def heating_enable(self, on: bool = True):
         """Keep the heating/cooling terms during the step (for heating())."""
@@ -487,6 +552,10 @@ class Batch:
 
     def enqueue_steps(self, nsteps: int, dt_next_checkpoint: float):
         self._check(self.lib.trg_batch_enqueue_steps(self.handle, int(nsteps), float(dt_next_checkpoint)))
+
+    def step_graphs(self, on: bool):
+        """One captured CUDA graph per timestep (on by default)."""
+        self._check(self.lib.trg_batch_step_graphs(self.handle, int(on)))
 
     def synchronize(self):
         self._check(self.lib.trg_batch_synchronize(self.handle))

@@ -374,6 +374,7 @@ class InitialConditions:
     pre: np.ndarray
     hii: np.ndarray
     vel: np.ndarray  # [3][N]
+    grav: Optional[np.ndarray] = None  # [3][N] or None (zero); only a Lua setup provides it
 
 
 def write_initial_conditions(path: str, ncells, dx_cgs: float, den, pre, hii, vel, time: float = 0.0):

@@ -80,6 +80,8 @@ struct trg_ctx {
 	float* U32 = nullptr;
 	float* U32s = nullptr;
 	unsigned char* mlp_img = nullptr;
+	int* lcand_buf = nullptr;
+	unsigned* lcand_n_buf = nullptr;
 	double* d_heat = nullptr;
 	int zchunk = 64;
 	std::vector<void*> allocs;
@@ -89,6 +91,19 @@ struct trg_ctx {
 	long long steps = 0;
 	long long launches = 0;
 	int dt_hist_cap = 0;
+	// global FP64 mass and energy sums: on-demand result (2 doubles), block
+	// partials, and (when on) the per-step record [cap][2] of the state each
+	// step starts from
+	// thermal sub-cycle work queue (allocated when first switched on)
+	int* thq_buf = nullptr;
+	int* thq_sorted_buf = nullptr;
+	unsigned char* thq_bin_buf = nullptr;
+	unsigned* thq_ctl_buf = nullptr;
+	double* cons_out = nullptr;
+	double* cons_part = nullptr;
+	double* cons_hist = nullptr;
+	long long cons_cap = 0;
+	bool cons_on = false;
 	std::string err;
 	// optional per-launch CUDA-event timing
 	bool profiling = false;
@@ -228,9 +243,15 @@ void q_from_u(trg_ctx* c, int sel, int fix) { LAUNCH(KF(k_q_from_u_fp64), c->P.N
 
 void colden_sweep_direct(trg_ctx* c) {
 	const auto& off = c->hs.off_all;
+	const bool sw = c->S.sw_col != nullptr;
+	if (sw) LAUNCH(KF(k_colden_sweep_prep), c->S.sw_col_n, 256, c->P, c->S, c->d_sweep_all, (int)c->S.sw_col_n, 0);
 	for (size_t s = 0; s + 1 < off.size(); ++s) {
 		int count = (int)(off[s + 1] - off[s]);
-		LAUNCH_SHELL(KF(k_colden_shell_fp64), count, 128, s > 0, c->P, c->S, c->d_sweep_all + off[s], count);
+		if (sw)
+			LAUNCH_SHELL(KF(k_colden_shell_sw), count, 128, s > 0, c->P, c->S, c->d_sweep_all + off[s], count,
+			             (long long)off[s]);
+		else
+			LAUNCH_SHELL(KF(k_colden_shell_fp64), count, 128, s > 0, c->P, c->S, c->d_sweep_all + off[s], count);
 	}
 }
 
@@ -291,29 +312,43 @@ void hydro_fluxes(trg_ctx* c) {
 	for (int d = 0; d < c->P.nd; ++d) LAUNCH(KF(k_faces_fp64), c->S.nfaces[d], 128, c->P, c->S, d);
 }
 
-// One shell of the radiation sweep: the plain kernel, or with a network
-// loaded the learned-start kernel (its tensor-core tile needs dynamic shared
-// memory and 64 TMEM columns per CTA).
-void rad_shell_launch(trg_ctx* c, const int* cells, int count, double h, bool overlap) {
-	if (c->S.mlp_img) {
-		cudaEvent_t ea = nullptr, eb = nullptr;
-		if (c->profiling) { ea = pool_event(c); eb = pool_event(c); cudaEventRecord(ea, c->stream); }
-		KF(k_rad_shell_learned)<<<grid_for(count, 128), 128, mlp::INFER_SMEM, c->stream>>>(c->P, c->S, cells, count, h);
-		if (c->profiling) { cudaEventRecord(eb, c->stream); c->recs.push_back({"k_rad_shell_learned", ea, eb}); }
-		c->launches++;
+// Single grids: the shells read their cells' own inputs in sweep order
+// (S.sw_rad, refreshed by k_rad_sweep_prep at the start of the sweep).
+void rad_shell_launch(trg_ctx* c, const int* cells, int count, double h, bool overlap, long long off) {
+	if (c->S.sw_rad) {
+		if (c->P.stats_on || c->S.harvest)
+			LAUNCH_SHELL(KF(k_rad_shell_sw_diag), count, 128, overlap, c->P, c->S, cells, count, h, off);
+		else if (c->S.mlp_img)
+			LAUNCH_SHELL(KF(k_rad_shell_sw_ls), count, 128, overlap, c->P, c->S, cells, count, h, off);
+		else
+			LAUNCH_SHELL(KF(k_rad_shell_sw), count, 128, overlap, c->P, c->S, cells, count, h, off);
 		return;
 	}
-	if (c->P.stats_on || c->S.harvest) LAUNCH_SHELL(KF(k_rad_shell_diag), count, 128, overlap, c->P, c->S, cells, count, h);
-	else LAUNCH_SHELL(KF(k_rad_shell_fp64), count, 128, overlap, c->P, c->S, cells, count, h);
+	if (c->P.stats_on || c->S.harvest)
+		LAUNCH_SHELL(KF(k_rad_shell_diag), count, 128, overlap, c->P, c->S, cells, count, h);
+	else
+		LAUNCH_SHELL(KF(k_rad_shell_fp64), count, 128, overlap, c->P, c->S, cells, count, h);
 }
 
 void rad_sweep_direct(trg_ctx* c, double h) {
 	int nw = (int)c->hs.wind_cells.size();
 	LAUNCH(KF(k_rad_wind_reset), nw, 128, c->P, c->S, c->d_wind, nw);
+	if (c->S.sw_rad) {
+		if (c->S.lstart) cudaMemsetAsync(c->S.lcand_n, 0, sizeof(unsigned), c->stream);
+		LAUNCH(KF(k_rad_sweep_prep), c->S.sw_rad_n, 256, c->P, c->S, c->d_sweep_nonwind, (int)c->S.sw_rad_n, 0);
+		if (c->S.lstart) {
+			// learned starting iterates of the listed candidates (persistent tcgen05 tiles)
+			cudaEvent_t ea = nullptr, eb = nullptr;
+			if (c->profiling) { ea = pool_event(c); eb = pool_event(c); cudaEventRecord(ea, c->stream); }
+			KF(k_learned_infer)<<<148, 128, mlp::INFER_SMEM, c->stream>>>(c->P, c->S, c->d_sweep_nonwind, h);
+			if (c->profiling) { cudaEventRecord(eb, c->stream); c->recs.push_back({"k_learned_infer", ea, eb}); }
+			c->launches++;
+		}
+	}
 	const auto& off = c->hs.off_nonwind;
 	for (size_t s = 0; s + 1 < off.size(); ++s) {
 		int count = (int)(off[s + 1] - off[s]);
-		rad_shell_launch(c, c->d_sweep_nonwind + off[s], count, h, s > 0);
+		rad_shell_launch(c, c->d_sweep_nonwind + off[s], count, h, s > 0, (long long)off[s]);
 	}
 }
 
@@ -353,16 +388,23 @@ void rad_integrate(trg_ctx* c, double h) {
 		}
 	}
 	if (c->P.star_on) {
-		int nw = (int)c->hs.wind_cells.size();
-		LAUNCH(KF(k_rad_wind_reset), nw, 128, c->P, c->S, c->d_wind, nw);
-		const auto& off = c->hs.off_nonwind;
-		for (size_t s = 0; s + 1 < off.size(); ++s) {
-			int count = (int)(off[s + 1] - off[s]);
-			rad_shell_launch(c, c->d_sweep_nonwind + off[s], count, h, s > 0);
-		}
+		rad_sweep_direct(c, h);
 	} else {
 		LAUNCH(KF(k_rad_no_star_fp64), c->P.N, 256, c->P, c->S, h);
 	}
+}
+
+// Thermodynamics::integrate: every cell's sub-cycles in place, or with the
+// work queue on, the cells with many sub-cycles drained by a persistent
+// kernel after the in-place pass.
+void thermo_integrate(trg_ctx* c, double h) {
+	if (c->S.thq) cudaMemsetAsync(c->S.thq_ctl, 0, THQ_CTL * sizeof(unsigned), c->stream);
+	LAUNCH(KF(k_thermo_integrate_fp64), c->P.N, 256, c->P, c->S, h);
+	if (!c->S.thq) return;
+	KF(k_thq_layout)<<<1, 32, 0, c->stream>>>(c->S);
+	KF(k_thq_scatter)<<<148 * 4, 256, 0, c->stream>>>(c->S);
+	KF(k_thq_drain)<<<148 * 8, 128, 0, c->stream>>>(c->P, c->S, h);
+	c->launches += 3;
 }
 
 void sub_step(trg_ctx* c, double h, bool hasCalculatedHeatFlux, int comp) {
@@ -414,7 +456,7 @@ void sub_step(trg_ctx* c, double h, bool hasCalculatedHeatFlux, int comp) {
 		c->q_fresh = c->mixed;
 		break;
 	default:
-		LAUNCH(KF(k_thermo_integrate_fp64), c->P.N, 256, c->P, c->S, h);
+		thermo_integrate(c, h);
 		LAUNCH(KF(k_thermo_update_fp64), c->P.N, 256, c->P, c->S, h, c->mixed ? 2 : 0);
 		c->q_fresh = c->mixed;
 		break;
@@ -432,10 +474,26 @@ void hydro_step(trg_ctx* c) {
 	LAUNCH(KF(k_hydro_update_fp64), c->P.N, 256, c->P, c->S, 1.0, 0, 0, 0);
 }
 
+// Global FP64 mass and energy sums of the state the current step starts from
+// into the per-step record: the partials come from the time-step reduction
+// (fused) or, where none ran, from a pass of their own.
+void cons_record(trg_ctx* c, bool fused) {
+	if (!fused) {
+		if (c->fp32) launch_cons_cells_f32(c->P, c->U32, c->cons_part, c->stream);
+		else launch_cons_cells_f64(c->P, c->S.U, c->cons_part, c->stream);
+		c->launches++;
+	}
+	if (c->steps < c->cons_cap) {
+		launch_cons_finalize(c->P, c->cons_part, c->cons_hist + 2 * c->steps, c->stream);
+		c->launches++;
+	}
+}
+
 void time_step(trg_ctx* c, double dt_next) {
 	// Torch::calculateTimeStep and the min with dt_next_checkpoint (Torch.cpp:304-339, :394)
 	int step = c->steps < c->dt_hist_cap ? (int)c->steps : -1;
 	if (c->first_time) {
+		if (c->cons_on) cons_record(c, false);
 		LAUNCH_SCALAR(KF(k_dt_finalize), c->P, c->S, dt_next, 1, step);
 		c->first_time = 0;
 		return;
@@ -447,6 +505,7 @@ void time_step(trg_ctx* c, double dt_next) {
 	}
 	LAUNCH_SCALAR(KF(k_dt_reset), c->P, c->S);
 	LAUNCH(KF(k_dt_reduce_fp64), c->P.N, 256, c->P, c->S, first_cell);
+	if (c->cons_on) cons_record(c, true);
 	LAUNCH_SCALAR(KF(k_dt_finalize), c->P, c->S, dt_next, 0, step);
 }
 
@@ -455,6 +514,7 @@ void enqueue_full_step_fp32(trg_ctx* c, double dt_next) {
 	// the previous corrector reduced (FP64), the two RK2 stages are one fused
 	// kernel each.
 	int step = c->steps < c->dt_hist_cap ? (int)c->steps : -1;
+	if (c->cons_on) cons_record(c, false);
 	LAUNCH_SCALAR(KF(k_dt_finalize), c->P, c->S, dt_next, c->first_time, step);
 	c->first_time = 0;
 	LAUNCH_SCALAR(KF(k_dt_reset), c->P, c->S);
@@ -523,10 +583,28 @@ int check_device_error(trg_ctx* c) {
 	if (e & ERRB_PICARD) return set_error(c, TRG_ERR_PICARD, "update_HIIfrac: implicit method not converging");
 	if (e & ERRB_DT) return set_error(c, TRG_ERR_DT, "Radiation::calculateTimeStep: invalid timestep");
 	if (e & ERRB_TC) return set_error(c, TRG_ERR_TC, "learned start: tensor-core wait expired");
+	if (e & ERRB_SUBCYCLE)
+		return set_error(c, TRG_ERR_SUBCYCLE, "Thermodynamics::integrate: a cell needs more thermal sub-cycles than "
+		                                      "the work queue runs (2^26)");
 	return TRG_OK;
 }
 
+int ensure_cons_hist(trg_ctx* c, long long needed) {
+	if (!c->cons_on || needed <= c->cons_cap) return 0;
+	long long cap = std::max<long long>(needed, 2LL * c->cons_cap + 1024);
+	double* nh = nullptr;
+	if (dalloc(c, &nh, 2 * cap)) return TRG_ERR_OOM;
+	CUDA_TRY(cudaMemsetAsync(nh, 0xff, sizeof(double) * 2 * cap, c->stream));  // NaN: step not recorded
+	if (c->cons_hist && c->steps > 0)
+		CUDA_TRY(cudaMemcpyAsync(nh, c->cons_hist, sizeof(double) * 2 * std::min<long long>(c->steps, c->cons_cap),
+		                         cudaMemcpyDeviceToDevice, c->stream));
+	c->cons_hist = nh;
+	c->cons_cap = cap;
+	return 0;
+}
+
 int ensure_dt_hist(trg_ctx* c, long long needed) {
+	if (int rc = ensure_cons_hist(c, needed)) return rc;
 	if (needed <= c->dt_hist_cap) return 0;
 	int cap = (int)std::max<long long>(needed, 2LL * c->dt_hist_cap + 1024);
 	double* nh = nullptr;
@@ -636,6 +714,15 @@ int trg_create(const trg_params* p, const double* den, const double* pre, const 
 		CUDA_TRY(cudaMemcpyAsync(c->d_wind, c->hs.wind_cells.data(), c->hs.wind_cells.size() * sizeof(int),
 		                         cudaMemcpyHostToDevice, st));
 	if ((rc = ensure_dt_hist(c, 1024))) return rc;
+	if (c->P.star_on) {
+		// sweep-ordered own-cell inputs of the causal sweeps, with their fixed parts
+		S.sw_col_n = (long long)c->hs.sweep_all.size();
+		S.sw_rad_n = (long long)c->hs.sweep_nonwind.size();
+		if ((rc = dalloc(c, &S.sw_col, 2 * S.sw_col_n)) || (rc = dalloc(c, &S.sw_rad, SW_RAD_ROWS * S.sw_rad_n)))
+			return rc;
+		LAUNCH(trg::exact::k_colden_sweep_prep, S.sw_col_n, 256, c->P, c->S, c->d_sweep_all, (int)S.sw_col_n, 1);
+		LAUNCH(trg::exact::k_rad_sweep_prep, S.sw_rad_n, 256, c->P, c->S, c->d_sweep_nonwind, (int)S.sw_rad_n, 1);
+	}
 	if (p->precision == TRG_PRECISION_FP32 && c->hs.nactive > 1) {
 		if (c->P.nd < 2) return set_error(c, TRG_ERR_ARG, "the FP32 form needs a 2-D or 3-D grid");
 		c->mixed = true;
@@ -756,7 +843,7 @@ int trg_component(trg_ctx* c, int comp, int phase, double dt, double* out) {
 	case TRG_PHASE_INTEGRATE:
 		if (comp == TRG_COMP_HYDRO) hydro_fluxes(c);
 		else if (comp == TRG_COMP_RAD) rad_integrate(c, 1.0);
-		else if (comp == TRG_COMP_THERMO) LAUNCH(KF(k_thermo_integrate_fp64), c->P.N, 256, c->P, c->S, 1.0);
+		else if (comp == TRG_COMP_THERMO) thermo_integrate(c, 1.0);
 		break;
 	case TRG_PHASE_SOURCES:
 		if (comp == TRG_COMP_HYDRO)
@@ -904,6 +991,11 @@ double trg_time(const trg_ctx* c) {
 	return t;
 }
 
+int trg_setup_positions(const trg_params* p, double* x, double* y, double* z, double* star_xyz) {
+	if (!p) return TRG_ERR_ARG;
+	return setup_positions(*p, x, y, z, star_xyz).empty() ? TRG_OK : TRG_ERR_ARG;
+}
+
 double trg_dt_max(const trg_ctx* c) { return c ? c->hs.dt_max : 0; }
 long trg_ncells(const trg_ctx* c) { return c ? (long)c->P.N : 0; }
 static void drop_graphs(trg_ctx* c) {
@@ -938,9 +1030,76 @@ int trg_stats(trg_ctx* c, unsigned long long* out, int reset) {
 	return TRG_OK;
 }
 
+int trg_thermo_queue(trg_ctx* c, int min_subcycles) {
+	if (!c || min_subcycles < 0) return TRG_ERR_ARG;
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	if (min_subcycles == 0) {
+		c->S.thq = nullptr;
+		return TRG_OK;
+	}
+	if (!c->thq_buf) {
+		const long long N = c->P.N;
+		if (dalloc(c, &c->thq_buf, N) || dalloc(c, &c->thq_sorted_buf, N) || dalloc(c, &c->thq_bin_buf, N) ||
+		    dalloc(c, &c->thq_ctl_buf, THQ_CTL))
+			return TRG_ERR_OOM;
+	}
+	c->S.thq = c->thq_buf;
+	c->S.thq_sorted = c->thq_sorted_buf;
+	c->S.thq_binof = c->thq_bin_buf;
+	c->S.thq_ctl = c->thq_ctl_buf;
+	c->S.thq_min = min_subcycles;
+	return TRG_OK;
+}
+
 int trg_fp32_contrast(trg_ctx* c, double contrast) {
 	if (!c || !(contrast >= 0)) return TRG_ERR_ARG;
 	c->fb_contrast = contrast;
+	return TRG_OK;
+}
+
+static int cons_buffers(trg_ctx* c) {
+	if (!c->cons_part && dalloc(c, &c->cons_part, 4 * cons_nparts(c->P))) return TRG_ERR_OOM;
+	if (!c->cons_out && dalloc(c, &c->cons_out, 2)) return TRG_ERR_OOM;
+	return TRG_OK;
+}
+
+int trg_conservation_sums(trg_ctx* c, double* mass, double* energy) {
+	if (!c) return TRG_ERR_ARG;
+	if (int rc = cons_buffers(c)) return rc;
+	if (c->fp32) launch_cons_cells_f32(c->P, c->U32, c->cons_part, c->stream);
+	else launch_cons_cells_f64(c->P, c->S.U, c->cons_part, c->stream);
+	launch_cons_finalize(c->P, c->cons_part, c->cons_out, c->stream);
+	double h[2] = {0, 0};
+	CUDA_TRY(cudaMemcpyAsync(h, c->cons_out, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	CUDA_TRY(cudaGetLastError());
+	if (mass) *mass = h[0];
+	if (energy) *energy = h[1];
+	return TRG_OK;
+}
+
+int trg_conservation_enable(trg_ctx* c, int on) {
+	if (!c) return TRG_ERR_ARG;
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	if (on) {
+		if (int rc = cons_buffers(c)) return rc;
+		c->cons_on = true;
+		c->S.cons_part = c->cons_part;
+		if (int rc = ensure_cons_hist(c, c->steps + 1024)) return rc;
+	} else {
+		c->cons_on = false;
+		c->S.cons_part = nullptr;
+	}
+	return TRG_OK;
+}
+
+int trg_conservation_history(trg_ctx* c, double* out, long long max_entries, long long* n_entries) {
+	if (!c || (max_entries > 0 && !out)) return TRG_ERR_ARG;
+	const long long n = std::min<long long>(c->steps, c->cons_cap);
+	const long long k = std::min<long long>(n, std::max<long long>(max_entries, 0));
+	if (k > 0) CUDA_TRY(cudaMemcpyAsync(out, c->cons_hist, sizeof(double) * 2 * k, cudaMemcpyDeviceToHost, c->stream));
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	if (n_entries) *n_entries = n;
 	return TRG_OK;
 }
 
@@ -976,6 +1135,7 @@ int trg_learned_start(trg_ctx* c, const trg_mlp* m) {
 	CUDA_TRY(cudaStreamSynchronize(c->stream));
 	if (!m) {
 		c->S.mlp_img = nullptr;
+		c->S.lstart = nullptr;
 		drop_graphs(c);
 		return TRG_OK;
 	}
@@ -983,8 +1143,14 @@ int trg_learned_start(trg_ctx* c, const trg_mlp* m) {
 	const unsigned char* src = mlp_device_image(m, &dev);
 	if (dev != c->raw.device) return set_error(c, TRG_ERR_ARG, "trg_learned_start: network on another device");
 	if (!c->mlp_img && dalloc(c, &c->mlp_img, mlp::IMG_INFER_BYTES)) return TRG_ERR_OOM;
+	if (!c->S.sw_rad) return set_error(c, TRG_ERR_ARG, "trg_learned_start: the run has no radiation sweep");
+	if (!c->lcand_buf && (dalloc(c, &c->lcand_buf, c->S.sw_rad_n) || dalloc(c, &c->lcand_n_buf, 1)))
+		return TRG_ERR_OOM;
 	CUDA_TRY(cudaMemcpy(c->mlp_img, src, mlp::IMG_INFER_BYTES, cudaMemcpyDeviceToDevice));
 	c->S.mlp_img = c->mlp_img;
+	c->S.lstart = c->S.sw_rad + SW_LSTART * c->S.sw_rad_n;
+	c->S.lcand = c->lcand_buf;
+	c->S.lcand_n = c->lcand_n_buf;
 	drop_graphs(c);
 	return TRG_OK;
 }
@@ -1103,6 +1269,20 @@ struct trg_batch {
 	int G = 0;
 	std::vector<trg_ctx*> grids;
 	trg_ctx* v = nullptr;  // the batch's own context: flags of grid 0, tables of all grids
+	// One captured CUDA graph per timestep: the operator split visits the
+	// components in an order that rotates with the step counter, so a step is
+	// one of `ncomps` fixed launch sequences (after the first step and the
+	// radiation time step's one-off first call).  Each is captured the first
+	// time it is needed and replayed after.
+	struct StepGraph {
+		cudaGraphExec_t exec = nullptr;
+		long long nodes = 0;
+		double dt_next = 0;
+		bool q_fresh0 = false, colden_valid0 = false;  // host-side state the capture started from
+		bool q_fresh1 = false, colden_valid1 = false;  // and ended with
+	};
+	StepGraph step_graph[3];
+	bool step_graphs = true;
 };
 
 namespace {
@@ -1211,6 +1391,8 @@ int trg_batch_create(trg_ctx* const* grids, int G, trg_batch** out) {
 		Ss[g] = grids[g]->S;
 		Ss[g].err = v->S.err;
 		Ss[g].stats = v->S.stats;
+		Ss[g].cons_part = nullptr;
+		Ss[g].thq = nullptr;  // batches run the sub-cycles in place
 	}
 	// batched sweeps and wind list
 	std::vector<int> wind;
@@ -1243,18 +1425,101 @@ int trg_batch_create(trg_ctx* const* grids, int G, trg_batch** out) {
 	v->P.stats_on = 0;
 	for (int d = 0; d < 3; ++d) v->S.nfaces[d] = face_off[d][G];
 	v->S.mlp_img = nullptr;
+	v->S.lstart = nullptr;
 	v->S.harvest = nullptr;
 	v->S.harvest_n = nullptr;
 	v->S.dt_hist = nullptr;
+	v->S.cons_part = nullptr;
+	v->S.sw_rad = v->S.sw_col = nullptr;  // batches read each grid's cells in place
+	v->S.thq = nullptr;
+	v->S.sw_rad_n = v->S.sw_col_n = 0;
 	*out = b;
 	return TRG_OK;
 }
 
+namespace {
+void batch_drop_step_graphs(trg_batch* b) {
+	for (auto& g : b->step_graph) {
+		if (g.exec) cudaGraphExecDestroy(g.exec);
+		g = trg_batch::StepGraph();
+	}
+}
+
+// One timestep of a batch: the step's captured graph when it can be replayed,
+// else the launches themselves (capturing them first when the step has a
+// fixed launch sequence).
+void batch_step(trg_batch* b, double dt_next) {
+	trg_ctx* v = b->v;
+	const bool rad_once = v->P.radiation_on && v->P.star_on && v->P.K1 != 0.0 && v->rad_once_pending;
+	if (!b->step_graphs || v->first_time || rad_once || v->profiling) {
+		enqueue_full_step(v, dt_next);
+		return;
+	}
+	const int n = v->hs.nactive;
+	const int phase = n > 1 ? (v->stepCounter + 1) % n : 0;
+	trg_batch::StepGraph& g = b->step_graph[phase];
+	if (g.exec && g.dt_next == dt_next && g.q_fresh0 == v->q_fresh && g.colden_valid0 == v->colden_valid) {
+		cudaGraphLaunch(g.exec, v->stream);
+		if (n > 1) v->stepCounter = phase;
+		v->steps++;
+		v->q_fresh = g.q_fresh1;
+		v->colden_valid = g.colden_valid1;
+		v->launches += g.nodes;
+		return;
+	}
+	if (g.exec) cudaGraphExecDestroy(g.exec);
+	g = trg_batch::StepGraph();
+	g.dt_next = dt_next;
+	g.q_fresh0 = v->q_fresh;
+	g.colden_valid0 = v->colden_valid;
+	// the sweeps go into the step's graph directly (not as graphs of their own)
+	const bool use_graphs = v->use_graphs;
+	v->use_graphs = false;
+	const long long before = v->launches;
+	cudaGraph_t graph = nullptr;
+	bool captured = false;
+	if (cudaStreamBeginCapture(v->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+		enqueue_full_step(v, dt_next);
+		captured = cudaStreamEndCapture(v->stream, &graph) == cudaSuccess && graph;
+	}
+	v->use_graphs = use_graphs;
+	if (captured && cudaGraphInstantiate(&g.exec, graph, 0) != cudaSuccess) g.exec = nullptr;
+	if (graph) cudaGraphDestroy(graph);
+	cudaGetLastError();
+	g.nodes = v->launches - before;
+	g.q_fresh1 = v->q_fresh;
+	g.colden_valid1 = v->colden_valid;
+	if (g.exec) {
+		cudaGraphLaunch(g.exec, v->stream);  // the capture recorded the step without running it
+		return;
+	}
+	// capture failed: run this step's launches directly; the host state the
+	// capture advanced is rewound first
+	g = trg_batch::StepGraph();
+	b->step_graphs = false;
+	v->steps--;
+	v->launches = before;
+	if (n > 1) v->stepCounter = (v->stepCounter + n - 1) % n;
+	v->q_fresh = g.q_fresh0;
+	v->colden_valid = g.colden_valid0;
+	enqueue_full_step(v, dt_next);
+}
+}  // namespace
+
 int trg_batch_enqueue_steps(trg_batch* b, int nsteps, double dt_next_checkpoint) {
 	if (!b || nsteps < 0) return TRG_ERR_ARG;
-	for (int s = 0; s < nsteps; ++s) enqueue_full_step(b->v, dt_next_checkpoint);
+	for (int s = 0; s < nsteps; ++s) batch_step(b, dt_next_checkpoint);
 	trg_ctx* c = b->v;
 	CUDA_TRY(cudaGetLastError());
+	return TRG_OK;
+}
+
+int trg_batch_step_graphs(trg_batch* b, int on) {
+	if (!b) return TRG_ERR_ARG;
+	trg_ctx* c = b->v;
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	batch_drop_step_graphs(b);
+	b->step_graphs = on != 0;
 	return TRG_OK;
 }
 
@@ -1289,6 +1554,7 @@ void trg_batch_destroy(trg_batch* b) {
 	trg_ctx* v = b->v;
 	if (v) {
 		if (v->stream) cudaStreamSynchronize(v->stream);
+		batch_drop_step_graphs(b);
 		// the grids continue on their own from where the batch left them
 		for (auto* g : b->grids) {
 			g->steps = v->steps;

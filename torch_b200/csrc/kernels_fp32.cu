@@ -55,6 +55,11 @@ struct Scaled {
 };
 
 __device__ __forceinline__ float fminf_(float a, float b) { return (b < a) ? b : a; }
+// Division and reciprocal of the FP32 form: the hardware approximation (one
+// reciprocal and one multiply, within 2 ulp for divisors of magnitude in
+// [2^-126, 2^126], which the scaled units keep every divisor of this file in).
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ float frcp(float b) { return __fdividef(1.0f, b); }
 __device__ __forceinline__ float fmaxf_(float a, float b) { return (a < b) ? b : a; }
 
 // Conserved-state storage of the FP32 kernels: float arrays hold the scaled
@@ -96,7 +101,7 @@ __device__ __forceinline__ void two_prod(float a, float b, float& p, float& e) {
 __device__ __forceinline__ Prim prim_from_cons(const float* u, float gamma, int nd) {
 	Prim q;
 	q.d = u[DEN];
-	float inv = 1.0f / u[DEN];
+	float inv = frcp(u[DEN]);
 	float s = 0.f, se = 0.f;
 #pragma unroll
 	for (int k = 0; k < 3; ++k) {
@@ -129,14 +134,14 @@ __device__ __forceinline__ void fix_prim(const Scaled& P, Prim& q, float u_den) 
 	q.d = fmaxf_(q.d, P.dfloor);
 	q.p = fmaxf_(q.p, P.pfloor);
 	float mu_inv = P.X * (q.x + 1.f) + (1.f - P.X) * 0.25f;
-	float temperature = q.p / (mu_inv * P.Rg * q.d);
-	if (temperature < P.tfloor) q.p = mu_inv * P.Rg * u_den * P.tfloor;
+	// temperature = p / (mu_inv Rg rho) below the floor
+	if (q.p < P.tfloor * (mu_inv * P.Rg * q.d)) q.p = mu_inv * P.Rg * u_den * P.tfloor;
 }
 
 // Fluid::fixSolution in FP32 (compensated kinetic energy as in prim_from_cons).
 __device__ __forceinline__ bool fix_cons(const Scaled& P, float* u) {
 	if (!isfinite(u[DEN]) || !isfinite(u[PRE])) return false;
-	float inv = 1.0f / u[DEN];
+	float inv = frcp(u[DEN]);
 	float hii = fmaxf_(fminf_(u[HII] * inv, 1.f), 0.f);
 	float adv = fmaxf_(fminf_(u[ADV] * inv, 1.f), 0.f);
 	float den = fmaxf_(u[DEN], P.dfloor);
@@ -150,10 +155,9 @@ __device__ __forceinline__ bool fix_cons(const Scaled& P, float* u) {
 	ke *= 0.5f * den;
 	if (pre < P.pfloor) pre = P.pfloor;
 	float mu_inv = P.X * (hii + 1.f) + (1.f - P.X) * 0.25f;
-	float temperature = pre / (mu_inv * P.Rg * den);
-	if (temperature < P.tfloor) pre = mu_inv * P.Rg * den * P.tfloor;
+	if (pre < P.tfloor * (mu_inv * P.Rg * den)) pre = mu_inv * P.Rg * den * P.tfloor;
 	u[DEN] = den;
-	u[PRE] = pre / (P.gamma - 1.f) + ke;
+	u[PRE] = fdiv(pre, P.gamma - 1.f) + ke;
 	u[HII] = hii * den;
 	u[ADV] = adv * den;
 #pragma unroll
@@ -174,7 +178,7 @@ __device__ __forceinline__ bool fix_cons(const Scaled& P, float* u) {
 // the same flux from both.
 __device__ __forceinline__ float albada(float a, float b, float thr) {
 	float ab = __fmul_rn(a, b);
-	return ab <= thr ? 0.f : __fmul_rn(ab, __fadd_rn(a, b)) / __fmaf_rn(a, a, __fmul_rn(b, b));
+	return ab <= thr ? 0.f : fdiv(__fmul_rn(ab, __fadd_rn(a, b)), __fmaf_rn(a, a, __fmul_rn(b, b)));
 }
 __device__ __forceinline__ float minmod_(float a, float b) {
 	return (a * b > 0) ? (fabsf(a) < fabsf(b) ? a : b) : 0.f;
@@ -190,12 +194,12 @@ __device__ __forceinline__ float limiter32(int kind, float a, float b, float thr
 	case 3: return maxmod_(a, b);
 	case 4: {
 		if (b == 0) return 0.f;
-		float r = fabsf(a / b);
-		return __fmaf_rn(b, r, a) / __fadd_rn(1.f, r);
+		float r = fabsf(fdiv(a, b));
+		return fdiv(__fmaf_rn(b, r, a), __fadd_rn(1.f, r));
 	}
 	case 5: {
 		const float ab = __fmul_rn(a, b), t = __fmaf_rn(a, a, ab);
-		return (ab <= thr) ? 0.f : __fmul_rn(__fmul_rn(1.5f, b), t) / __fmaf_rn(b, b, t);
+		return (ab <= thr) ? 0.f : fdiv(__fmul_rn(__fmul_rn(1.5f, b), t), __fmaf_rn(b, b, t));
 	}
 	default: return albada(a, b, thr);
 	}
@@ -262,9 +266,9 @@ __device__ __forceinline__ void face_pre(const Prim& L, const Prim& R, float gam
 	cons_of(R, g1inv, f.UR);
 	f.sl = sqrtf(L.d);
 	f.sr = sqrtf(R.d);
-	f.inv = 1.f / (f.sl + f.sr);
+	f.inv = frcp(f.sl + f.sr);
 	f.nu2 = 0.5f * f.sr * f.sl * f.inv * f.inv;
-	float aL2 = gamma * L.p / L.d, aR2 = gamma * R.p / R.d;
+	float aL2 = fdiv(gamma * L.p, L.d), aR2 = fdiv(gamma * R.p, R.d);
 	f.c2 = (f.sl * aL2 + f.sr * aR2) * f.inv;
 }
 // Physical flux of a state (conserved U) along unit normal n.
@@ -295,7 +299,7 @@ __device__ __forceinline__ void hll_n(const Prim& L, const Prim& R, const FacePr
 	} else if (SL >= 0) {
 		for (int i = 0; i < 7; ++i) F[i] = FL[i];
 	} else {
-		float inv = 1.f / (SR - SL);
+		float inv = frcp(SR - SL);
 		for (int i = 0; i < 7; ++i) F[i] = (SR * FL[i] - SL * FR[i] + SL * SR * (f.UR[i] - f.UL[i])) * inv;
 	}
 }
@@ -311,17 +315,17 @@ __device__ __forceinline__ void hllc_n(const Prim& L, const Prim& R, const FaceP
 		for (int i = 0; i < 7; ++i) F[i] = FR[i];
 	} else {
 		float mL = L.d * (SL - unL), mR = R.d * (SR - unR);
-		float Sc = (R.p - L.p + mL * unL - mR * unR) / (mL - mR);
+		float Sc = fdiv(R.p - L.p + mL * unL - mR * unR, mL - mR);
 		bool left = Sc >= 0;
 		const Prim& K = left ? L : R;
 		const float* UK = left ? f.UL : f.UR;
 		const float* FK = left ? FL : FR;
 		float SK = left ? SL : SR, unK = left ? unL : unR;
 		float mK = K.d * (SK - unK);
-		float A = mK / (SK - Sc);
+		float A = fdiv(mK, SK - Sc);
 		float Us[7];
 		Us[DEN] = A;
-		Us[PRE] = A * (UK[PRE] / K.d + (Sc - unK) * (Sc + K.p / mK));
+		Us[PRE] = A * (fdiv(UK[PRE], K.d) + (Sc - unK) * (Sc + fdiv(K.p, mK)));
 		Us[HII] = A * K.x;
 		Us[ADV] = A * K.a;
 		for (int k = 0; k < 3; ++k) Us[VEL + k] = A * (K.v[k] + (Sc - unK) * n[k]);
@@ -352,11 +356,11 @@ __device__ __forceinline__ void riemann32(int kind, const Prim& L, const Prim& R
 	if (pp == 0.f) { hll_n(L, R, f, d, F); return; }        // dv parallel to d
 	if (par == 0.f) { hllc_n(L, R, f, d, F); return; }     // dv normal to d
 	const float r = sqrtf(rr), s = sqrtf(pp);
-	const float inv_r = 1.f / r;
+	const float inv_r = frcp(r);
 	const float sg = par < 0 ? -1.f : 1.f;
 	const float n1[3] = {sg * dv[0] * inv_r, sg * dv[1] * inv_r, sg * dv[2] * inv_r};
 	const float cosv = fabsf(par) * inv_r, sinv = s * inv_r;
-	const float k2 = par * inv_r / s;
+	const float k2 = fdiv(par * inv_r, s);
 	const float n2[3] = {sinv * d[0] - k2 * perp[0], sinv * d[1] - k2 * perp[1], sinv * d[2] - k2 * perp[2]};
 	float F1[7], F2[7];
 	hll_n(L, R, f, n1, F1);
@@ -399,40 +403,77 @@ __device__ __forceinline__ void apply_flip(Prim& q, int dim, int cond, int side)
 	}
 }
 
+// The staged cells of the CTA's x/y box (halo included, corners left out: no
+// stencil reads them) and their sources under the boundary rule depend on
+// the CTA's position only, not on the plane: a thread works out its (at most
+// two) box positions once, before the z march.  Per position: the source
+// offset xs + nx ys within a plane (-1: not staged - a corner, or beyond a
+// ragged grid edge) and the velocity flips the boundary rule applies there.
+constexpr int STAGE_PER_THREAD = (SX * SY + BX * BY - 1) / (BX * BY);
+struct StageMap {
+	int off[STAGE_PER_THREAD];
+	int flags[STAGE_PER_THREAD];  // x condition + 1 (3 bits), x side, y condition + 1 (3 bits), y side
+};
+__device__ __forceinline__ StageMap stage_map(const Params& P, int x0, int y0) {
+	StageMap m;
+#pragma unroll
+	for (int j = 0; j < STAGE_PER_THREAD; ++j) {
+		const int idx = threadIdx.x + j * BX * BY;
+		m.off[j] = -1;
+		m.flags[j] = 0;
+		if (idx >= SX * SY) continue;
+		const int ly = idx / SX, lx = idx - ly * SX;
+		const bool xh = lx < HALO || lx >= HALO + BX, yh = ly < HALO || ly >= HALO + BY;
+		if (xh && yh) continue;  // corners: never part of a stencil
+		int xc, xside, yc = -1, yside = 0;
+		const int xs = bc_src(P, 0, x0 + lx - HALO, P.nx, xc, xside);
+		const int ys = P.nd > 1 ? bc_src(P, 1, y0 + ly - HALO, P.ny, yc, yside) : 0;
+		if (P.nd <= 1) yc = -1;
+		if (xs < 0 || xs >= P.nx || ys < 0 || ys >= P.ny) continue;  // tile beyond a ragged grid edge
+		m.off[j] = xs + P.nx * ys;
+		m.flags[j] = (xc + 1) | (xside << 3) | ((yc + 1) << 4) | (yside << 7);
+	}
+	return m;
+}
+__device__ __forceinline__ void apply_flips(const Params& P, Prim& q, int flags, int zc, int zside) {
+	apply_flip(q, 0, (flags & 7) - 1, (flags >> 3) & 1);
+	if (P.nd > 1) apply_flip(q, 1, ((flags >> 4) & 7) - 1, (flags >> 7) & 1);
+	if (P.nd > 2) apply_flip(q, 2, zc, zside);
+}
+__device__ __forceinline__ void put_prim(SmemQ& s, int slot, int idx, const Prim& q) {
+	float* b = &s.v[slot][0][0][0] + idx;
+	b[DEN * SX * SY] = q.d;
+	b[PRE * SX * SY] = q.p;
+	b[HII * SX * SY] = q.x;
+	b[ADV * SX * SY] = q.a;
+	b[(VEL + 0) * SX * SY] = q.v[0];
+	b[(VEL + 1) * SX * SY] = q.v[1];
+	b[(VEL + 2) * SX * SY] = q.v[2];
+}
+// Source plane of z under the boundary rule (2-D grids: plane 0).
+__device__ __forceinline__ int plane_src(const Params& P, int z, int& zc, int& zside) {
+	zc = -1;
+	zside = 0;
+	return P.nd > 2 ? bc_src(P, 2, z, P.nz, zc, zside) : 0;
+}
+
 // Loads plane z (global index, may be a ghost plane) of the CTA's x/y box into ring slot.
 template <int STAGE, typename TS>
 __device__ __forceinline__ void load_plane(const Params& P, const Scaled& SP, const StoreScale& SC,
-                                           const TS* __restrict__ U, SmemQ& s, int slot, int x0, int y0, int z) {
+                                           const TS* __restrict__ U, SmemQ& s, int slot, const StageMap& m, int z) {
 	int zc, zside;
-	int zs = P.nd > 2 ? bc_src(P, 2, z, P.nz, zc, zside) : 0;
-	if (P.nd <= 2) zc = -1;
+	const TS* Up = U + (long long)P.nx * P.ny * plane_src(P, z, zc, zside);
 	const long long N = P.N;
-	for (int idx = threadIdx.x; idx < SX * SY; idx += blockDim.x) {
-		int ly = idx / SX, lx = idx - ly * SX;
-		bool xh = lx < HALO || lx >= HALO + BX, yh = ly < HALO || ly >= HALO + BY;
-		if (xh && yh) continue;  // corners: never part of a stencil
-		int gx = x0 + lx - HALO, gy = y0 + ly - HALO;
-		int xc, xside, yc, yside;
-		int xs = bc_src(P, 0, gx, P.nx, xc, xside);
-		int ys = P.nd > 1 ? bc_src(P, 1, gy, P.ny, yc, yside) : 0;
-		if (P.nd <= 1) yc = -1;
-		if (xs < 0 || xs >= P.nx || ys < 0 || ys >= P.ny) continue;  // tile beyond a ragged grid edge
-		long long id = xs + (long long)P.nx * (ys + (long long)P.ny * zs);
+#pragma unroll
+	for (int j = 0; j < STAGE_PER_THREAD; ++j) {
+		if (m.off[j] < 0) continue;
 		float u[7];
 #pragma unroll
-		for (int f = 0; f < 7; ++f) u[f] = load_u(U, f * N + id, SC, f);
+		for (int f = 0; f < 7; ++f) u[f] = load_u(Up, f * N + m.off[j], SC, f);
 		Prim q = prim_from_cons(u, (float)P.gamma, P.nd);
 		if (STAGE == 1) fix_prim(SP, q, u[DEN]);
-		apply_flip(q, 0, xc, xside);
-		if (P.nd > 1) apply_flip(q, 1, yc, yside);
-		if (P.nd > 2) apply_flip(q, 2, zc, zside);
-		s.v[slot][DEN][ly][lx] = q.d;
-		s.v[slot][PRE][ly][lx] = q.p;
-		s.v[slot][HII][ly][lx] = q.x;
-		s.v[slot][ADV][ly][lx] = q.a;
-		s.v[slot][VEL + 0][ly][lx] = q.v[0];
-		s.v[slot][VEL + 1][ly][lx] = q.v[1];
-		s.v[slot][VEL + 2][ly][lx] = q.v[2];
+		apply_flips(P, q, m.flags[j], zc, zside);
+		put_prim(s, slot, threadIdx.x + j * BX * BY, q);
 	}
 }
 
@@ -451,54 +492,36 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 template <typename TS>
-__device__ __forceinline__ void plane_fetch(const Params& P, const TS* __restrict__ U, TS* raw, int x0, int y0, int z) {
+__device__ __forceinline__ void plane_fetch(const Params& P, const TS* __restrict__ U, TS* raw, const StageMap& m,
+                                            int z) {
 	int zc, zside;
-	const int zs = P.nd > 2 ? bc_src(P, 2, z, P.nz, zc, zside) : 0;
+	const TS* Up = U + (long long)P.nx * P.ny * plane_src(P, z, zc, zside);
 	const long long N = P.N;
-	for (int idx = threadIdx.x; idx < SX * SY; idx += blockDim.x) {
-		const int ly = idx / SX, lx = idx - ly * SX;
-		const bool xh = lx < HALO || lx >= HALO + BX, yh = ly < HALO || ly >= HALO + BY;
-		if (xh && yh) continue;
-		int xc, xside, yc, yside;
-		const int xs = bc_src(P, 0, x0 + lx - HALO, P.nx, xc, xside);
-		const int ys = P.nd > 1 ? bc_src(P, 1, y0 + ly - HALO, P.ny, yc, yside) : 0;
-		if (xs < 0 || xs >= P.nx || ys < 0 || ys >= P.ny) continue;
-		const long long id = xs + (long long)P.nx * (ys + (long long)P.ny * zs);
 #pragma unroll
-		for (int f = 0; f < 7; ++f) cp_async_elem(raw + f * (SX * SY) + idx, U + f * N + id);
+	for (int j = 0; j < STAGE_PER_THREAD; ++j) {
+		if (m.off[j] < 0) continue;
+		const int idx = threadIdx.x + j * BX * BY;
+#pragma unroll
+		for (int f = 0; f < 7; ++f) cp_async_elem(raw + f * (SX * SY) + idx, Up + f * N + m.off[j]);
 	}
 	cp_async_commit();
 }
 template <int STAGE, typename TS>
 __device__ __forceinline__ void plane_convert(const Params& P, const Scaled& SP, const StoreScale& SC, const TS* raw,
-                                              SmemQ& s, int slot, int x0, int y0, int z) {
+                                              SmemQ& s, int slot, const StageMap& m, int z) {
 	int zc, zside;
-	if (P.nd > 2) bc_src(P, 2, z, P.nz, zc, zside);
-	else zc = -1;
-	for (int idx = threadIdx.x; idx < SX * SY; idx += blockDim.x) {
-		const int ly = idx / SX, lx = idx - ly * SX;
-		const bool xh = lx < HALO || lx >= HALO + BX, yh = ly < HALO || ly >= HALO + BY;
-		if (xh && yh) continue;
-		int xc, xside, yc, yside;
-		const int xs = bc_src(P, 0, x0 + lx - HALO, P.nx, xc, xside);
-		const int ys = P.nd > 1 ? bc_src(P, 1, y0 + ly - HALO, P.ny, yc, yside) : 0;
-		if (P.nd <= 1) yc = -1;
-		if (xs < 0 || xs >= P.nx || ys < 0 || ys >= P.ny) continue;
+	plane_src(P, z, zc, zside);
+#pragma unroll
+	for (int j = 0; j < STAGE_PER_THREAD; ++j) {
+		if (m.off[j] < 0) continue;
+		const int idx = threadIdx.x + j * BX * BY;
 		float u[7];
 #pragma unroll
 		for (int f = 0; f < 7; ++f) u[f] = scaled_u(raw[f * (SX * SY) + idx], SC, f);
 		Prim q = prim_from_cons(u, (float)P.gamma, P.nd);
 		if (STAGE == 1) fix_prim(SP, q, u[DEN]);
-		apply_flip(q, 0, xc, xside);
-		if (P.nd > 1) apply_flip(q, 1, yc, yside);
-		if (P.nd > 2) apply_flip(q, 2, zc, zside);
-		s.v[slot][DEN][ly][lx] = q.d;
-		s.v[slot][PRE][ly][lx] = q.p;
-		s.v[slot][HII][ly][lx] = q.x;
-		s.v[slot][ADV][ly][lx] = q.a;
-		s.v[slot][VEL + 0][ly][lx] = q.v[0];
-		s.v[slot][VEL + 1][ly][lx] = q.v[1];
-		s.v[slot][VEL + 2][ly][lx] = q.v[2];
+		apply_flips(P, q, m.flags[j], zc, zside);
+		put_prim(s, slot, idx, q);
 	}
 }
 
@@ -681,6 +704,7 @@ __global__ void __launch_bounds__(BX* BY, 2)
 		else if (P.geometry == G_SPH) rgeo = (float)((face_area(P, xc, 0, 1) - face_area(P, xc, 0, 0)) / vol);
 	}
 
+	const StageMap smap = stage_map(P, x0, y0);
 	auto slot_of = [](int z) { return ((z % NPLANE) + NPLANE) % NPLANE; };
 	Prim zero;
 	zero.d = zero.p = zero.x = zero.a = zero.v[0] = zero.v[1] = zero.v[2] = 0.f;
@@ -691,15 +715,15 @@ __global__ void __launch_bounds__(BX* BY, 2)
 	// 3-D: the pass starts one plane early (z0 - 1), where it only forms the
 	// flux through z0 - 1/2, so that every z face goes through the same code
 	if (nd > 2) {
-		for (int z = z0 - 2; z <= z0; ++z) load_plane<STAGE>(P, SP, SC, Uq, s, slot_of(z), x0, y0, z);
+		for (int z = z0 - 2; z <= z0; ++z) load_plane<STAGE>(P, SP, SC, Uq, s, slot_of(z), smap, z);
 		__syncthreads();
 		if (rec)
 			szc = slope_of(lim, th, get(s, slot_of(z0 - 2), ly, lx), get(s, slot_of(z0 - 1), ly, lx),
 			               get(s, slot_of(z0), ly, lx));
 		__syncthreads();  // plane z0 - 2 is read: its slot takes plane z0 + 1
-		load_plane<STAGE>(P, SP, SC, Uq, s, slot_of(z0 + 1), x0, y0, z0 + 1);
+		load_plane<STAGE>(P, SP, SC, Uq, s, slot_of(z0 + 1), smap, z0 + 1);
 	} else {
-		load_plane<STAGE>(P, SP, SC, Uq, s, 0, x0, y0, 0);
+		load_plane<STAGE>(P, SP, SC, Uq, s, 0, smap, 0);
 	}
 
 	// Plane z + 3 is staged (cp.async) while plane z is computed and turned into
@@ -710,7 +734,7 @@ __global__ void __launch_bounds__(BX* BY, 2)
 		const bool plane = z >= z0;  // x/y faces and the update of this plane
 		const bool stage_next = nd > 2 && z + 1 < z1;
 		__syncthreads();  // planes z .. z + 2 are in the ring; the staging buffer is free
-		if (stage_next) plane_fetch(P, Uq, raw, x0, y0, z + 3);
+		if (stage_next) plane_fetch(P, Uq, raw, smap, z + 3);
 		// slopes: this cell in x, y and (of the next plane's cell) z; the cells
 		// just outside the tile in x and y
 		Prim szn = zero;
@@ -893,7 +917,7 @@ __global__ void __launch_bounds__(BX* BY, 2)
 		szc = szn;
 		// no barrier before this: only the slot of plane z is written, and the
 		// flux and slope arrays are rewritten after the next barrier
-		if (stage_next) plane_convert<STAGE>(P, SP, SC, raw, s, slot_of(z + 3), x0, y0, z + 3);
+		if (stage_next) plane_convert<STAGE>(P, SP, SC, raw, s, slot_of(z + 3), smap, z + 3);
 	}
 	if (bad) atomicOr(S.err, ERRB_NAN);
 	if (STAGE == 2) {

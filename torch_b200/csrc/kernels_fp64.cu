@@ -769,34 +769,47 @@ __device__ __forceinline__ double inv_logit10(float l) {
 // (update_HIIfrac, :375-478) and the new optical depths.  Every cell of a
 // shell reads only cells of inner shells, so a shell is fully parallel.
 //
-// LEARNED: CTAs that hold a front cell run the tensor-core network on their
-// 128 cells (dynamic shared memory mlp::INFER_SMEM, TMEM 64 columns) and start
-// the front cells' Picard iteration from the predicted time-averaged
-// fraction.  The prediction is accepted when the first iteration from it
-// meets the solver's own convergence test (its residual is below the solver
-// tolerance); otherwise the cell restarts the plain iteration from x_HII, so
-// that a rejected prediction leaves the plain result unchanged.
+// Learned start (S.lstart set, LS or DIAG builds): a front cell whose entry of
+// S.lstart holds a prediction (written by k_learned_infer before the sweep)
+// starts its Picard iteration there.  The prediction is accepted when the
+// first iteration from it meets the solver's own convergence test (its
+// residual is below the solver tolerance); otherwise the cell restarts the
+// plain iteration from x_HII, so that a rejected prediction leaves the plain
+// result unchanged.
 // DIAG: the counters and the training-set recording are compiled in (a
 // lean build without them keeps the sweep's instruction footprint small).
-template <bool LEARNED, bool DIAG>
-__device__ __forceinline__ void rad_shell(const Params& P, const State& S, const long long id, const bool valid,
-                                          double h) {
+// SW: the cell's own inputs come from the sweep-ordered arrays (S.sw_rad,
+// `sw` pointing at this cell's column, stride `swn`), formed by
+// k_rad_sweep_prep with this function's own arithmetic.
+template <bool DIAG, bool SW = false, bool LS = false>
+__device__ __forceinline__ void rad_shell(const Params& P, const State& S, const long long id, double h,
+                                          double* sw = nullptr, long long swn = 0) {
 	const double dt = h * S.scal[0];
 	bool star = false, front = false, inner = false;
 	double q_den = 0, q_pre = 0, q_hii = 0, ds = 0, n_H = 0, T = 1, alphaB = 0, A_ci = 0, tau_avg = 0, shellVol = 0;
 	double nH_cell = 0;
 	long long nb[4] = {-1, -1, -1, -1};
 	double w[4] = {0, 0, 0, 0};
-	if (valid) {
-		// everything that does not depend on the inner shells
-		int ijk[3];
-		double xc[3];
-		cell_ijk(P, id, ijk);
-		cell_xc(P, ijk, xc);
-		inner = dist2_cells(P, xc) > 0.95;
-		if (inner) neighbours(P, ijk, xc, nb, w);
-		// Radiation::isStar (Radiation.cpp:682-684): z compares an int with a double.
-		star = (int)xc[0] == (int)P.sxc[0] && (int)xc[1] == (int)P.sxc[1] && (double)(int)xc[2] == P.sxc[2];
+	// everything that does not depend on the inner shells
+	int ijk[3];
+	double xc[3];
+	cell_ijk(P, id, ijk);
+	cell_xc(P, ijk, xc);
+	inner = dist2_cells(P, xc) > 0.95;
+	if (inner) neighbours(P, ijk, xc, nb, w);
+	// Radiation::isStar (Radiation.cpp:682-684): z compares an int with a double.
+	star = (int)xc[0] == (int)P.sxc[0] && (int)xc[1] == (int)P.sxc[1] && (double)(int)xc[2] == P.sxc[2];
+	if (SW) {
+		nH_cell = sw[0];
+		q_hii = sw[3 * swn];
+		ds = sw[4 * swn];
+		if (!star) {
+			n_H = nH_cell;
+			alphaB = sw[swn];
+			A_ci = sw[2 * swn];
+			shellVol = sw[5 * swn];
+		}
+	} else {
 		q_den = FLD(S.Q, DEN, id);
 		q_pre = FLD(S.Q, PRE, id);
 		q_hii = FLD(S.Q, HII, id);
@@ -817,32 +830,22 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 		}
 	}
 	sweep_wait();
-	if (!LEARNED && !valid) return;
 	double tau = 0, tau_a = 0;
-	if (valid) {
-		if (inner) tau_sc2(P, S, nb, w, tau, tau_a);
-		if (!star) {
-			tau_avg = tau_a;
-			front = front_cell(tau_avg, q_hii);
-		}
+	if (inner) tau_sc2(P, S, nb, w, tau, tau_a);
+	if (!star) {
+		tau_avg = tau_a;
+		front = front_cell(tau_avg, q_hii);
 	}
 	double start = q_hii;
 	bool learned = false, used_learned = false;
-	if (LEARNED) {
-		if (__syncthreads_or(front)) {
-			extern __shared__ __align__(128) unsigned char sm_mlp[];
-			float f[5] = {0, 0, 0, 0, 0}, y[3];
-			if (front) learned_features(P, n_H, T, q_hii, tau_avg, ds, shellVol, dt, f);
-			if (!mlp::infer_tile(sm_mlp, reinterpret_cast<const uint4*>(S.mlp_img), f, y)) {
-				if (threadIdx.x == 0) atomicOr(S.err, ERRB_TC);
-			} else if (front && y[2] > 1.0f) {
-				// predicted to need more than two plain iterations: start from the prediction
-				start = inv_logit10(logit10(q_hii) + y[0]);
-				learned = used_learned = true;
-			}
+	if (SW && (LS || DIAG) && front && S.lstart) {
+		const double st = sw[SW_LSTART * swn];
+		if (st == st) {
+			start = st;
+			learned = used_learned = true;
 		}
-		if (!valid) return;
 	}
+	if (SW) sw[SW_TAU_A * swn] = tau_a;  // the next sweep's learned-start candidates are chosen from it
 	unsigned iters = 0;
 	double hii_new = 1, hii_a_new = 1;
 	if (star) {
@@ -904,12 +907,13 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 		hii_new = x_new;
 		if (x_new > 0.001) FLD(S.Q, ADV, id) = 1;
 		iters += (unsigned)miter * 10006u + (unsigned)niter;
-		if (LEARNED && DIAG && P.stats_on && used_learned) stat_add(S.stats, TRG_STAT_LEARNED_ITERS, iters);
-		if (!LEARNED && DIAG && front && S.harvest) {
+		if (DIAG && P.stats_on && used_learned) stat_add(S.stats, TRG_STAT_LEARNED_ITERS, iters);
+		if (DIAG && front && S.harvest && !used_learned) {
 			// training record: 5 inputs, then the converged <x>, x and the iteration count
 			unsigned long long slot = atomicAdd(S.harvest_n, 1ull);
 			if (slot < (unsigned long long)S.harvest_cap) {
 				float* r = S.harvest + slot * 8;
+				if (SW) T = calc_temperature(P, q_hii, FLD(S.Q, PRE, id), FLD(S.Q, DEN, id));
 				learned_features(P, n_H, T, q_hii, tau_avg, ds, shellVol, dt, r);
 				r[5] = logit10(HII_avg) - logit10(q_hii);
 				r[6] = logit10(x_new) - logit10(q_hii);
@@ -920,7 +924,7 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 #ifdef TRG_FAST_MATH
 	const double nH = nH_cell;
 #else
-	const double nH = P.X * q_den / P.hydrogenMass;
+	const double nH = SW ? nH_cell : P.X * q_den / P.hydrogenMass;
 #endif
 	store_taus(S, id, tau, (1.0 - hii_new) * nH * P.photoIonXsec * ds, tau_a, (1.0 - hii_a_new) * nH * P.photoIonXsec * ds);
 	if (DIAG && P.stats_on) {
@@ -945,24 +949,120 @@ __global__ void TRG_RAD_SHELL_BOUNDS k_rad_shell_fp64(Params P, State S, const i
 	if (TRG_BATCHED && P.batch) {
 		const int e = cells[t];
 		const int g = e >> BATCH_CELL_BITS;
-		rad_shell<false, false>(P.batch->P[g], P.batch->S[g], e & BATCH_CELL_MASK, true, h);
+		rad_shell<false>(P.batch->P[g], P.batch->S[g], e & BATCH_CELL_MASK, h);
 		return;
 	}
-	rad_shell<false, false>(P, S, cells[t], true, h);
+	rad_shell<false>(P, S, cells[t], h);
 }
 // The same with the solver counters and training-set recording compiled in.
 __global__ void __launch_bounds__(128) k_rad_shell_diag(Params P, State S, const int* __restrict__ cells, int count,
                                                        double h) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= count) return;
-	rad_shell<false, true>(P, S, cells[t], true, h);
+	rad_shell<true>(P, S, cells[t], h);
 }
-// Single grids only (the tensor-core tile needs all 128 threads of a CTA).
-__global__ void __launch_bounds__(128) k_rad_shell_learned(Params P, State S, const int* __restrict__ cells, int count,
-                                                          double h) {
+
+// ----------------------------------------------- learned starting iterate
+// Before each radiation sweep with a network loaded, k_rad_sweep_prep lists
+// the candidate front cells (by the previous sweep's TAU_A and x_HII, the
+// front criterion) as sweep positions and clears every prediction slot; this
+// kernel runs the network over the candidates, 128 per tile (tcgen05, one
+// tile per CTA at a time, persistent over the tiles): inputs log n_H, log T,
+// x_HII, log of the optically thin photoionisation rate at that TAU_A, log
+// dt; cells predicted to need more than two plain iterations get the
+// predicted time-averaged fraction as their starting iterate.  More than
+// LCAND_MAX candidates (the first sweep of a run, before any optical depth
+// exists, lists every neutral cell) means no predictions for that sweep.
+__global__ void __launch_bounds__(128) k_learned_infer(Params P, State S, const int* __restrict__ cells, double h) {
+	extern __shared__ __align__(128) unsigned char sm_mlp[];
+	const unsigned n = *S.lcand_n;
+	if (n > (unsigned)LCAND_MAX) return;
+	const double dt = h * S.scal[0];
+	const long long sn = S.sw_rad_n;
+	for (unsigned tile = blockIdx.x; tile * 128u < n; tile += gridDim.x) {
+		const unsigned t = tile * 128u + threadIdx.x;
+		const bool valid = t < n;
+		const int pos = valid ? S.lcand[t] : 0;
+		float f[5] = {0, 0, 0, 0, 0}, y[3];
+		double q_hii = 0;
+		if (valid) {
+			const long long id = cells[pos];
+			const double* sw = S.sw_rad + pos;
+			const double q_den = FLD(S.Q, DEN, id), q_pre = FLD(S.Q, PRE, id);
+			q_hii = sw[3 * sn];
+			const double T = calc_temperature(P, q_hii, q_pre, q_den);
+			learned_features(P, sw[0], T, q_hii, sw[SW_TAU_A * sn], sw[4 * sn], sw[5 * sn], dt, f);
+		}
+		const bool ok = mlp::infer_tile(sm_mlp, reinterpret_cast<const uint4*>(S.mlp_img), f, y);
+		if (__syncthreads_or(!ok)) {  // the whole CTA leaves together
+			if (threadIdx.x == 0) atomicOr(S.err, ERRB_TC);
+			return;
+		}
+		if (valid && y[2] > 1.0f) S.sw_rad[SW_LSTART * sn + pos] = inv_logit10(logit10(q_hii) + y[0]);
+	}
+}
+
+// The cell's own inputs of the radiation sweep in sweep order (S.sw_rad):
+// what rad_shell computes from the cell's density, pressure and fraction
+// before waiting for the inner shells, with its arithmetic: n_H, the case-B
+// recombination rate and the collisional ionisation rate at the cell's
+// temperature, and x_HII; with `init` also the fixed path length and shell
+// volume.  One parallel pass before each sweep (single grids only).
+__global__ void __launch_bounds__(256) k_rad_sweep_prep(Params P, State S, const int* __restrict__ cells, int n,
+                                                         int init) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
-	const bool valid = t < count;
-	rad_shell<true, true>(P, S, valid ? cells[t] : 0, valid, h);
+	if (t >= n) return;
+	const long long id = cells[t];
+	const long long sn = S.sw_rad_n;
+	double* sw = S.sw_rad + t;
+	const double q_den = FLD(S.Q, DEN, id), q_pre = FLD(S.Q, PRE, id), q_hii = FLD(S.Q, HII, id);
+	const double n_H = P.X * q_den / P.hydrogenMass;
+	const double T = calc_temperature(P, q_hii, q_pre, q_den);
+	sw[0] = n_H;
+	sw[sn] = spline_eval(S.tables->rad_recomb, T);
+	sw[2 * sn] = collisional_ionisation_rate(P, T);
+	sw[3 * sn] = q_hii;
+	if (init) {
+		sw[4 * sn] = S.ds[id];
+		sw[5 * sn] = S.shellVol[id];
+		sw[SW_TAU_A * sn] = RFLD(S.R, R_TAU_A, id);
+	}
+	if (S.lstart) {
+		// learned start: no prediction yet; a cell at the front by the
+		// previous sweep's optical depth becomes a candidate (its sweep position)
+		sw[SW_LSTART * sn] = __longlong_as_double(0x7ff8000000000000LL);
+		const bool cand = front_cell(sw[SW_TAU_A * sn], q_hii);
+		const unsigned ballot = __ballot_sync(__activemask(), cand);
+		if (cand) {
+			const int lane = threadIdx.x & 31, leader = __ffs(ballot) - 1;
+			unsigned base = 0;
+			if (lane == leader) base = atomicAdd(S.lcand_n, (unsigned)__popc(ballot));
+			base = __shfl_sync(ballot, base, leader);
+			S.lcand[base + __popc(ballot & ((1u << lane) - 1))] = t;
+		}
+	}
+}
+// A radiation shell reading its cells' own inputs from S.sw_rad; `off` is the
+// shell's offset in the non-wind sweep list.
+__global__ void TRG_RAD_SHELL_BOUNDS k_rad_shell_sw(Params P, State S, const int* __restrict__ cells, int count,
+                                                     double h, long long off) {
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= count) return;
+	rad_shell<false, true>(P, S, cells[t], h, S.sw_rad + off + t, S.sw_rad_n);
+}
+// The same with the solver counters and training-set recording compiled in.
+__global__ void __launch_bounds__(128) k_rad_shell_sw_diag(Params P, State S, const int* __restrict__ cells,
+                                                           int count, double h, long long off) {
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= count) return;
+	rad_shell<true, true>(P, S, cells[t], h, S.sw_rad + off + t, S.sw_rad_n);
+}
+// The same, front cells starting from the learned prediction (S.lstart).
+__global__ void TRG_RAD_SHELL_BOUNDS k_rad_shell_sw_ls(Params P, State S, const int* __restrict__ cells, int count,
+                                                        double h, long long off) {
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= count) return;
+	rad_shell<false, true, true>(P, S, cells[t], h, S.sw_rad + off + t, S.sw_rad_n);
 }
 
 // Radiation::transferRadiation2 (Radiation.cpp:508-567) for the implicit2 and
@@ -1216,7 +1316,9 @@ __device__ __forceinline__ double th_cooling(const Params& P, const State& S, do
 }
 
 // One shell of Thermodynamics::rayTrace / updateColDen (Thermodynamics.cpp:339-417).
-__device__ __forceinline__ void b_colden_shell_fp64(const Params& P, const State& S, long long id) {
+// `own`: the cell's ds rho / m_H in the sweep-ordered array, or null.
+__device__ __forceinline__ void b_colden_shell_fp64(const Params& P, const State& S, long long id,
+                                                    const double* own = nullptr) {
 	int ijk[3];
 	double xc[3];
 	cell_ijk(P, id, ijk);
@@ -1225,7 +1327,7 @@ __device__ __forceinline__ void b_colden_shell_fp64(const Params& P, const State
 	long long nb[4];
 	double w0[4];
 	if (inner) neighbours(P, ijk, xc, nb, w0);
-	const double dcolden = (FLD(S.Q, DEN, id) / P.hydrogenMass) * S.ds[id];
+	const double dcolden = own ? *own : (FLD(S.Q, DEN, id) / P.hydrogenMass) * S.ds[id];
 	sweep_wait();
 	double newcolden = 0.0;
 	if (inner) {
@@ -1276,6 +1378,23 @@ __device__ __forceinline__ void b_colden_shell_fp64(const Params& P, const State
 #endif
 	}
 	reinterpret_cast<double2*>(S.T + id * 2)[0] = make_double2(newcolden, dcolden);
+}
+// The cell's own column density of the sweep in sweep order (S.sw_col):
+// ds rho / m_H, as b_colden_shell_fp64 forms it; with `init` also the fixed
+// path lengths.  One parallel pass before each column-density sweep.
+__global__ void __launch_bounds__(256) k_colden_sweep_prep(Params P, State S, const int* __restrict__ cells, int n,
+                                                            int init) {
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= n) return;
+	const long long id = cells[t];
+	if (init) S.sw_col[S.sw_col_n + t] = S.ds[id];
+	S.sw_col[t] = (FLD(S.Q, DEN, id) / P.hydrogenMass) * S.sw_col[S.sw_col_n + t];
+}
+__global__ void __launch_bounds__(128) k_colden_shell_sw(Params P, State S, const int* __restrict__ cells, int count,
+                                                          long long off) {
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= count) return;
+	b_colden_shell_fp64(P, S, cells[t], S.sw_col + off + t);
 }
 __global__ void __launch_bounds__(128) k_colden_shell_fp64(Params P, State S, const int* __restrict__ cells, int count) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1336,74 +1455,168 @@ __global__ void __launch_bounds__(256) k_thermo_rates_fp64(Params P, State S) {
 }
 
 // Thermodynamics::integrate (pressure subcycling), Thermodynamics.cpp:266-337, non-wind cells.
-__device__ __forceinline__ void b_thermo_integrate_fp64(const Params& P, const State& S, long long id, double h) {
-	if (!P.thermo_subcycling) return;
+// Thermodynamics::integrate (pressure subcycling), Thermodynamics.cpp:266-337,
+// for one cell, split in three: the set-up (the first explicit step and the
+// closed-form sub-cycle count, :285-310), the sub-cycles (:312-331) and the
+// result (:334-335).  The work queue below runs the same three pieces.
+struct ThermoCell {
+	double qpre, ne, nn, nH, x, Tmin, heat, pre2temp, temp2pre, rate2dpre, dpre2rate, pressure, subT;
+	int nsteps;  // sub-cycles still to run (0: none)
+};
+// false: a wind cell or one below the HII switch (nothing, or T_RATE = 0, to write)
+// `count`: update the sub-cycle counters (the drain, which repeats the set-up
+// of a queued cell, does not count it again)
+__device__ __forceinline__ bool thermo_setup(const Params& P, const State& S, long long id, double h, ThermoCell& c,
+                                             bool count = true) {
 	int ijk[3];
 	double xc[3];
 	cell_ijk(P, id, ijk);
 	cell_xc(P, ijk, xc);
-	if (is_wind(P, id, ijk, xc)) return;
+	if (is_wind(P, id, ijk, xc)) return false;
 	if (FLD(S.Q, ADV, id) < P.thermo_hii_switch) {
 		if (S.H)
 			for (int i = 0; i < NH; ++i) FLD(S.H, i, id) = 0;
 		TFLD(S.T, T_RATE, id) = 0;
-		return;
+		return false;
 	}
 	const double dt = h * S.scal[0];
 	double qden = FLD(S.Q, DEN, id), qpre = FLD(S.Q, PRE, id), x = FLD(S.Q, HII, id);
-	double Tmin = S.Tmin[id];
-	double rate0 = TFLD(S.T, T_RATE, id), heat = TFLD(S.T, T_HEAT, id);
-	double nH = P.X * qden / P.hydrogenMass;
-	double ne = nH * (x);
-	double nn = nH * (1.0 - x);
+	c.qpre = qpre;
+	c.x = x;
+	c.Tmin = S.Tmin[id];
+	double rate0 = TFLD(S.T, T_RATE, id);
+	c.heat = TFLD(S.T, T_HEAT, id);
+	c.nH = P.X * qden / P.hydrogenMass;
+	c.ne = c.nH * (x);
+	c.nn = c.nH * (1.0 - x);
 	double dti = fabs(0.10 * FLD(S.U, PRE, id) / rate0);
 	double mu_inv = P.X * (x + 1.0) + (1.0 - P.X) * 0.25;
-	double pre2temp = 1.0 / (mu_inv * P.specificGasConstant * qden);
-	double temp2pre = (mu_inv * P.specificGasConstant * qden);
-	double rate2dpre = smin(dt, dti) * (P.gamma - 1.0);
-	double dpre2rate = 1.0 / rate2dpre;
-	double pressure = qpre + rate0 * rate2dpre;
-	double subT = pressure * pre2temp;
-	if (pressure < P.pfloor || subT < Tmin) {
-		double pfl = smax(Tmin * temp2pre, P.pfloor);
-		subT = pfl * pre2temp;
-		pressure = pfl;
+	c.pre2temp = 1.0 / (mu_inv * P.specificGasConstant * qden);
+	c.temp2pre = (mu_inv * P.specificGasConstant * qden);
+	c.rate2dpre = smin(dt, dti) * (P.gamma - 1.0);
+	c.dpre2rate = 1.0 / c.rate2dpre;
+	c.pressure = qpre + rate0 * c.rate2dpre;
+	c.subT = c.pressure * c.pre2temp;
+	if (c.pressure < P.pfloor || c.subT < c.Tmin) {
+		double pfl = smax(c.Tmin * c.temp2pre, P.pfloor);
+		c.subT = pfl * c.pre2temp;
+		c.pressure = pfl;
 	}
+	c.nsteps = 0;
 	if (dt > dti) {
 		double dtdti = dt / dti;
 		int nsteps = dtdti - (int)dtdti > 0 ? (int)(dtdti + 1.0) : (int)(dtdti + 0.5);
-		--nsteps;
-		if (P.stats_on) {
+		c.nsteps = nsteps - 1;
+		if (count && P.stats_on) {
 			stat_add(S.stats, TRG_STAT_THERMO_CELLS, 1u);
-			stat_add(S.stats, TRG_STAT_THERMO_SUBCYCLES, (unsigned)nsteps);
-			stat_max(S.stats, TRG_STAT_THERMO_MAX, (unsigned)nsteps);
-		}
-		for (int i = 0; i < nsteps; ++i) {
-			double r = th_cooling(P, S, heat, ne, nn, nH, x, subT);
-			r = P.heating_amp * soft_landing(r, subT, Tmin);
-			pressure += r * rate2dpre;
-			subT = pressure * pre2temp;
-			if (pressure < P.pfloor || subT < Tmin) {
-				double pfl = smax(Tmin * temp2pre, P.pfloor);
-				subT = pfl * pre2temp;
-				pressure = pfl;
-			}
+			stat_add(S.stats, TRG_STAT_THERMO_SUBCYCLES, (unsigned)c.nsteps);
+			stat_max(S.stats, TRG_STAT_THERMO_MAX, (unsigned)c.nsteps);
 		}
 	}
-	TFLD(S.T, T_RATE, id) = (pressure - qpre) * dpre2rate;
+	return true;
+}
+__device__ __forceinline__ void thermo_subcycles(const Params& P, const State& S, ThermoCell& c) {
+	for (int i = 0; i < c.nsteps; ++i) {
+		double r = th_cooling(P, S, c.heat, c.ne, c.nn, c.nH, c.x, c.subT);
+		r = P.heating_amp * soft_landing(r, c.subT, c.Tmin);
+		c.pressure += r * c.rate2dpre;
+		c.subT = c.pressure * c.pre2temp;
+		if (c.pressure < P.pfloor || c.subT < c.Tmin) {
+			double pfl = smax(c.Tmin * c.temp2pre, P.pfloor);
+			c.subT = pfl * c.pre2temp;
+			c.pressure = pfl;
+		}
+	}
+}
+__device__ __forceinline__ void thermo_finish(const Params& P, const State& S, long long id, const ThermoCell& c) {
+	TFLD(S.T, T_RATE, id) = (c.pressure - c.qpre) * c.dpre2rate;
 	if (S.H) FLD(S.H, H_TOT, id) = TFLD(S.T, T_RATE, id);  // Thermodynamics.cpp:335
+}
+
+// Work queue of the uneven sub-cycles (single grids, when S.thq is set): a
+// cell with at least S.thq_min sub-cycles is not run in place but appended
+// to the queue with the bit length of its count (its bin); the bins are then
+// laid out heaviest first, and a persistent kernel drains them, each warp
+// taking 32 consecutive entries, so that the lanes of a warp run sub-cycle
+// loops of similar length and the longest loops start first.
+__device__ __forceinline__ int thq_bin(int nsteps) { return min(31 - __clz(nsteps), THQ_BINS - 1); }
+__device__ __forceinline__ void thq_push(const State& S, long long id, int nsteps) {
+	const unsigned slot = atomicAdd(&S.thq_ctl[THQ_COUNT], 1u);
+	const int b = thq_bin(nsteps);
+	S.thq[slot] = (int)id;
+	S.thq_binof[slot] = (unsigned char)b;
+	atomicAdd(&S.thq_ctl[THQ_BIN + b], 1u);
+}
+
+__device__ __forceinline__ void b_thermo_integrate_fp64(const Params& P, const State& S, long long id, double h,
+                                                        bool queue) {
+	if (!P.thermo_subcycling) return;
+	ThermoCell c;
+	if (!thermo_setup(P, S, id, h, c)) return;
+	if (queue && c.nsteps >= S.thq_min) {
+		thq_push(S, id, c.nsteps);
+		return;
+	}
+	thermo_subcycles(P, S, c);
+	thermo_finish(P, S, id, c);
 }
 __global__ void __launch_bounds__(256) k_thermo_integrate_fp64(Params P, State S, double h) {
 	if (TRG_BATCHED && P.batch) {
 		const BatchTable& B = *P.batch;
 		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
 		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
-		if (lid < B.P[g].N) b_thermo_integrate_fp64(B.P[g], B.S[g], lid, h);
+		if (lid < B.P[g].N) b_thermo_integrate_fp64(B.P[g], B.S[g], lid, h, false);
 		return;
 	}
 	const long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
 	if (id >= P.N) return;
-	b_thermo_integrate_fp64(P, S, id, h);
+	b_thermo_integrate_fp64(P, S, id, h, S.thq != nullptr);
+}
+
+// Bin offsets of the queue, heaviest bin first, and the drain head.
+__global__ void k_thq_layout(State S) {
+	if (threadIdx.x != 0) return;
+	unsigned pos = 0;
+	for (int b = THQ_BINS - 1; b >= 0; --b) {
+		S.thq_ctl[THQ_CURSOR + b] = pos;
+		pos += S.thq_ctl[THQ_BIN + b];
+	}
+	S.thq_ctl[THQ_HEAD] = 0;
+}
+// Entries into their bins' ranges (the order within a bin does not matter:
+// the cells are independent).
+__global__ void __launch_bounds__(256) k_thq_scatter(State S) {
+	const unsigned n = S.thq_ctl[THQ_COUNT];
+	for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+		const unsigned pos = atomicAdd(&S.thq_ctl[THQ_CURSOR + S.thq_binof[t]], 1u);
+		S.thq_sorted[pos] = S.thq[t];
+	}
+}
+// Persistent drain: warps take 32 entries at a time until the queue is empty.
+// A cell whose count exceeds THQ_MAX_SUBCYCLES is not run: the error word
+// reports it (the loop of every cell is bounded).
+__global__ void __launch_bounds__(128) k_thq_drain(Params P, State S, double h) {
+	const unsigned n = S.thq_ctl[THQ_COUNT];
+	const int lane = threadIdx.x & 31;
+	for (;;) {
+		unsigned base = 0;
+		if (lane == 0) base = atomicAdd(&S.thq_ctl[THQ_HEAD], 32u);
+		base = __shfl_sync(0xffffffffu, base, 0);
+		if (base >= n) return;
+		const unsigned t = base + lane;
+		if (t < n) {
+			const long long id = S.thq_sorted[t];
+			ThermoCell c;
+			if (thermo_setup(P, S, id, h, c, false)) {
+				if (c.nsteps > THQ_MAX_SUBCYCLES) {
+					atomicOr(S.err, ERRB_SUBCYCLE);
+				} else {
+					thermo_subcycles(P, S, c);
+					thermo_finish(P, S, id, c);
+				}
+			}
+		}
+	}
 }
 
 // Thermodynamics::updateSourceTerms (Thermodynamics.cpp:478-485) then advSolution + fixSolution.
@@ -1511,20 +1724,36 @@ __device__ __forceinline__ double block_min(double v) {
 // exact and order independent; they are combined with atomicMin on the bit
 // pattern.  first_cell: the first non-wind cell in causal order on the first
 // radiation call (the reference's static `once`), else -1.
-__device__ __forceinline__ void b_dt_reduce_fp64(const Params& P, const State& S, long long id, long long first_cell);
+//
+// With cons_part set (single grids only) the pass also forms the block's
+// partial of the global FP64 mass and energy sums of the state (U), the
+// conservation check of the step.
+__device__ __forceinline__ void b_dt_reduce_fp64(const Params& P, const State& S, long long id, long long first_cell,
+                                                 double* cons_part);
 __global__ void __launch_bounds__(256) k_dt_reduce_fp64(Params P, State S, long long first_cell) {
 	if (TRG_BATCHED && P.batch) {
 		// grid ranges are padded to whole blocks: the block reduction stays within one grid
 		const BatchTable& B = *P.batch;
 		const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
 		const long long lid = blockIdx.x * (long long)blockDim.x + threadIdx.x - B.cell_off[g];
-		b_dt_reduce_fp64(B.P[g], B.S[g], lid, first_cell >= 0 ? B.first_cell[g] : -1);
+		b_dt_reduce_fp64(B.P[g], B.S[g], lid, first_cell >= 0 ? B.first_cell[g] : -1, nullptr);
 		return;
 	}
-	b_dt_reduce_fp64(P, S, blockIdx.x * (long long)blockDim.x + threadIdx.x, first_cell);
+	b_dt_reduce_fp64(P, S, blockIdx.x * (long long)blockDim.x + threadIdx.x, first_cell, S.cons_part);
 }
-__device__ __forceinline__ void b_dt_reduce_fp64(const Params& P, const State& S, long long id, long long first_cell) {
+__device__ __forceinline__ void b_dt_reduce_fp64(const Params& P, const State& S, long long id, long long first_cell,
+                                                 double* cons_part) {
 	double th = 1.0e308, tr = 1.0e308, tt = 1.0e308;
+	DD cm = {0.0, 0.0}, ce = {0.0, 0.0};
+	if (cons_part && id < P.N) {
+		int ijk[3];
+		double xc[3];
+		cell_ijk(P, id, ijk);
+		cell_xc(P, ijk, xc);
+		const double vol = cell_volume_rn(P, xc[0]);
+		cm = dd_prod(FLD(S.U, DEN, id), vol);
+		ce = dd_prod(FLD(S.U, PRE, id), vol);
+	}
 	if (id < P.N) {
 		double q_den = FLD(S.Q, DEN, id), q_pre = FLD(S.Q, PRE, id), q_hii = FLD(S.Q, HII, id);
 		double inv_t = 0;
@@ -1577,6 +1806,7 @@ __device__ __forceinline__ void b_dt_reduce_fp64(const Params& P, const State& S
 			}
 		}
 	}
+	if (cons_part) block_cons_partial(cm, ce, cons_part, blockIdx.x);
 	th = block_min(th);
 	__syncthreads();
 	tr = block_min(tr);

@@ -17,10 +17,14 @@
 //     start at zero (the error word, the time-step minima) is cleared by each
 //     call, and calls that overlap on the GPU race on the array;
 //   * the first call on a device looks the array's device address up
-//     (cudaGetSymbolAddress, with that device current); make that first call
-//     before any stream capture.
+//     (cudaGetSymbolAddress, with that device current);
+//   * every call waits for its stream (it reads the error word and the next
+//     time-step limit back), so it must not be made while a stream is being
+//     captured;
+//   * hydrodynamics only: contexts with radiation or cooling are rejected.
 #include <cuda_runtime.h>
 
+#include <cstring>
 #include <mutex>
 #include <string>
 
@@ -74,7 +78,21 @@ __global__ void k_noalloc_begin(double* scal, unsigned* err, double dt, double d
 
 using namespace trg;
 
-extern "C" int trg_hydro_step_fp32_noalloc(trg_ctx* c, const double* U_in, double* U_out, double dt, void* stream) {
+namespace {
+// Restores the calling thread's current device on every return path.
+struct DeviceGuard {
+	int prev = -1;
+	DeviceGuard() {
+		if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+	}
+	~DeviceGuard() {
+		if (prev >= 0) cudaSetDevice(prev);
+	}
+};
+}  // namespace
+
+extern "C" int trg_hydro_step_fp32_noalloc(trg_ctx* c, const double* U_in, double* U_out, double dt,
+                                           double* dt_next, void* stream) {
 	if (!c || !U_in || !U_out) return TRG_ERR_ARG;
 	const Params& P = ctx_params(c);
 	if (P.N > kMaxCells)
@@ -83,6 +101,13 @@ extern "C" int trg_hydro_step_fp32_noalloc(trg_ctx* c, const double* U_in, doubl
 		                    " cells exceeds the limit of " + std::to_string(kMaxCells) + " cells");
 	if (P.nd < 2)
 		return ctx_fail(c, TRG_ERR_ARG, "trg_hydro_step_fp32_noalloc: needs a 2-D or 3-D grid");
+	if (P.radiation_on || P.cooling_on)
+		return ctx_fail(c, TRG_ERR_ARG,
+		                "trg_hydro_step_fp32_noalloc: advances hydrodynamics only; the context has radiation or "
+		                "cooling on");
+	if (!(dt > 0) || !(dt <= 1.0e308))
+		return ctx_fail(c, TRG_ERR_ARG, "trg_hydro_step_fp32_noalloc: dt must be positive and finite");
+	DeviceGuard guard;
 	cudaError_t e = cudaSetDevice(ctx_device(c));
 	float* base = nullptr;
 	if (e == cudaSuccess) e = scratch_address(ctx_device(c), &base);
@@ -104,12 +129,20 @@ extern "C" int trg_hydro_step_fp32_noalloc(trg_ctx* c, const double* U_in, doubl
 	launch_hydro_stage_fp32(1, P, S, U0, U0, Us, zchunk, st);
 	launch_hydro_stage_fp32(2, P, S, Us, U0, U0, zchunk, st);
 	k_f32_to_f64<<<(unsigned)((7 * N + 255) / 256), 256, 0, st>>>(P, U0, U_out);
-	unsigned h_err = 0;
+	// header bytes 16..67: the CFL minimum (scal[2], bits of a positive double)
+	// up to the error word (float 16 = byte 64), read back in one copy
+	unsigned char hdr[52];
 	e = cudaGetLastError();
-	if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, err, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+	if (e == cudaSuccess)
+		e = cudaMemcpyAsync(hdr, reinterpret_cast<unsigned char*>(base) + 16, sizeof hdr, cudaMemcpyDeviceToHost, st);
 	if (e == cudaSuccess) e = cudaStreamSynchronize(st);
 	if (e != cudaSuccess)
 		return ctx_fail(c, TRG_ERR_CUDA, std::string("trg_hydro_step_fp32_noalloc: ") + cudaGetErrorString(e));
+	unsigned h_err = 0;
+	double cfl = 0;
+	memcpy(&cfl, hdr, sizeof cfl);
+	memcpy(&h_err, hdr + 48, sizeof h_err);
 	if (h_err & ERRB_NAN) return ctx_fail(c, TRG_ERR_NAN, "checkValues/fixSolution: invalid cell state");
+	if (dt_next) *dt_next = cfl < P.dt_max ? cfl : P.dt_max;
 	return TRG_OK;
 }

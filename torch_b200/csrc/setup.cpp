@@ -517,4 +517,47 @@ std::string host_setup(const trg_params& p, const double* den, const double* pre
 	return "";
 }
 
+// The arguments Torch::setUpLua passes to the Lua setup function
+// initialise(x, y, z, xs, ys, zs) (src/Torch/Torch.cpp:196-228): each cell's
+// centre and the star's position, cell index coordinates times the grid
+// spacing in code units, converted back to cgs (Converter::fromCodeUnits,
+// length index 1).  Coordinates beyond nd are 0.
+std::string setup_positions(const trg_params& p, double* x, double* y, double* z, double* star) {
+	if (p.nd < 1 || p.nd > 3) return "nd must be 1, 2 or 3";
+	for (int i = 0; i < 3; ++i)
+		if (p.ncells[i] < 1) return "ncells must be positive";
+	if ((p.nd < 3 && p.ncells[2] != 1) || (p.nd < 2 && p.ncells[1] != 1)) return "ncells beyond nd must be 1";
+	Converter cv;
+	cv.set_rho_pressure_time(p.dscale, p.pscale, p.tscale);
+	const double side = cv.to_code(p.side_length, 0, 1, 0);
+	double dx[3] = {0, 0, 0};
+	for (int i = 0; i < p.nd; ++i) dx[i] = side / (double)p.ncells[0];  // Grid.cpp:470-471
+	// fromCodeUnits(v, 0, 1, 0) multiplies by the length unit once (Converter.cpp:35-62)
+	auto from_code_length = [&](double v) { return v * cv.L; };
+	double sxc[3];
+	for (int i = 0; i < 3; ++i) {  // Star::initialise, Star.cpp:13-25
+		const double mod = (p.face_snap[i] && (p.star_pos[i] == 0)) ? 0.5 : 0;
+		sxc[i] = p.star_pos[i] + 0.5 - mod;
+	}
+	if (p.nd < 3) sxc[2] = 0;
+	if (p.nd < 2) sxc[1] = 0;
+	if (star)
+		for (int i = 0; i < 3; ++i) star[i] = from_code_length(sxc[i] * dx[i]);
+	const long long nx = p.ncells[0], ny = p.ncells[1], nz = p.ncells[2];
+	double* out[3] = {x, y, z};
+	for (long long k = 0; k < nz; ++k)
+		for (long long j = 0; j < ny; ++j)
+			for (long long i = 0; i < nx; ++i) {
+				const long long id = i + nx * (j + ny * k);
+				const long long ijk[3] = {i, j, k};
+				for (int d = 0; d < 3; ++d) {
+					if (!out[d]) continue;
+					double xc = (double)ijk[d];  // Grid::buildCells, Grid.cpp:525-548
+					if (d < p.nd) xc += 0.5;
+					out[d][id] = from_code_length(xc * dx[d]);
+				}
+			}
+	return "";
+}
+
 }  // namespace trg

@@ -28,4 +28,8 @@ struct HostSetup {
 std::string host_setup(const trg_params& p, const double* den, const double* pre, const double* hii, const double* v0,
                        const double* v1, const double* v2, const double* grav, HostSetup& out);
 
+// Cell and star positions (cgs) as Torch::setUpLua passes them to the Lua
+// setup function; empty string on success.
+std::string setup_positions(const trg_params& p, double* x, double* y, double* z, double* star);
+
 }  // namespace trg

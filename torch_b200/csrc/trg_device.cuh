@@ -286,6 +286,89 @@ __device__ __forceinline__ void stat_picard(unsigned long long* st, unsigned ite
 	for (int k = 0; k < 8; ++k) stat_add(st, TRG_STAT_PICARD_HIST + k, iters > 0 && b == k);
 }
 
+// ------------------------------------------------------- conservation sums
+// Global FP64 mass and energy sums, sum(rho V) and sum(E V) over the cells.
+// Each cell's product is formed exactly (a double-double, two_prod) and the
+// sums are carried as double-double pairs combined in a fixed tree order, so
+// the result is deterministic (independent of scheduling) and equals the
+// exact sum of the products to within about 2^-100 relative before its final
+// rounding.  Every operation is an explicit round-to-nearest intrinsic, so
+// the exact and the fast build (FMA contraction) compute the same bits.
+struct DD {
+	double hi, lo;
+};
+__device__ __forceinline__ DD dd_two_sum(double a, double b) {
+	const double s = __dadd_rn(a, b);
+	const double bb = __dsub_rn(s, a);
+	return {s, __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb))};
+}
+__device__ __forceinline__ DD dd_fast_two_sum(double a, double b) {  // |a| >= |b| or a == 0
+	const double s = __dadd_rn(a, b);
+	return {s, __dsub_rn(b, __dsub_rn(s, a))};
+}
+__device__ __forceinline__ DD dd_add(DD a, DD b) {
+	const DD s = dd_two_sum(a.hi, b.hi), t = dd_two_sum(a.lo, b.lo);
+	const DD u = dd_fast_two_sum(s.hi, __dadd_rn(s.lo, t.hi));
+	return dd_fast_two_sum(u.hi, __dadd_rn(u.lo, t.lo));
+}
+__device__ __forceinline__ DD dd_prod(double a, double b) {
+	const double p = __dmul_rn(a, b);
+	return {p, __fma_rn(a, b, -p)};
+}
+// Grid::computeCellVolume (Grid.cpp:876-905) with every operation rounded
+// separately (no contraction in either build), the value the sums weight by.
+__device__ __forceinline__ double cell_volume_rn(const Params& P, double rc) {
+	const double PI = 3.14159265359;
+	if (P.geometry == G_CART) {
+		double volume = 1.0;
+#pragma unroll
+		for (int i = 0; i < 3; ++i)
+			if (i < P.nd) volume = __dmul_rn(volume, P.dx[i]);
+		return volume;
+	}
+	const double r2 = __dadd_rn(__dmul_rn(rc, P.dx[0]), __dmul_rn(0.5, P.dx[0]));
+	const double r1 = __dsub_rn(__dmul_rn(rc, P.dx[0]), __dmul_rn(0.5, P.dx[0]));
+	if (P.geometry == G_CYL) {
+		double volume = __dmul_rn(__dmul_rn(PI, __dsub_rn(r2, r1)), __dadd_rn(r2, r1));
+		if (P.nd >= 2) volume = __dmul_rn(volume, P.dx[1]);
+		return volume;
+	}
+	const double s = __dadd_rn(__dadd_rn(__dmul_rn(r2, r2), __dmul_rn(r1, r2)), __dmul_rn(r1, r1));
+	return __ddiv_rn(__dmul_rn(__dmul_rn(__dmul_rn(4.0, PI), __dsub_rn(r2, r1)), s), 3.0);
+}
+// Sums (m, e) over a block of 256 threads in a fixed order; thread 0 writes
+// the block's partial (m.hi, m.lo, e.hi, e.lo) to part[4 * slot].  Every
+// thread of the block must call it.
+__device__ __forceinline__ void block_cons_partial(DD m, DD e, double* part, long long slot) {
+	__shared__ double red[8][4];
+	for (int o = 16; o > 0; o >>= 1) {
+		const DD mo = {__shfl_down_sync(0xffffffffu, m.hi, o), __shfl_down_sync(0xffffffffu, m.lo, o)};
+		const DD eo = {__shfl_down_sync(0xffffffffu, e.hi, o), __shfl_down_sync(0xffffffffu, e.lo, o)};
+		m = dd_add(m, mo);
+		e = dd_add(e, eo);
+	}
+	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+	if (lane == 0) {
+		red[wid][0] = m.hi;
+		red[wid][1] = m.lo;
+		red[wid][2] = e.hi;
+		red[wid][3] = e.lo;
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		DD ms = {red[0][0], red[0][1]}, es = {red[0][2], red[0][3]};
+		const int nw = (blockDim.x + 31) >> 5;
+		for (int w = 1; w < nw; ++w) {
+			ms = dd_add(ms, DD{red[w][0], red[w][1]});
+			es = dd_add(es, DD{red[w][2], red[w][3]});
+		}
+		part[4 * slot + 0] = ms.hi;
+		part[4 * slot + 1] = ms.lo;
+		part[4 * slot + 2] = es.hi;
+		part[4 * slot + 3] = es.lo;
+	}
+}
+
 // Grid of a batched launch whose (padded) range holds position `pos`:
 // the last g with off[g] <= pos.
 __device__ __forceinline__ int batch_slot(const long long* off, int G, long long pos) {

@@ -12,7 +12,9 @@
 	__global__ void k_advance_fp64(Params P, State S, double dt); \
 	__global__ void k_rad_wind_reset(Params P, State S, const int* cells, int count); \
 	__global__ void k_rad_shell_fp64(Params P, State S, const int* cells, int count, double h); \
-	__global__ void k_rad_shell_learned(Params P, State S, const int* cells, int count, double h); \
+	__global__ void k_learned_infer(Params P, State S, const int* cells, double h); \
+	__global__ void k_rad_shell_sw_diag(Params P, State S, const int* cells, int count, double h, long long off); \
+	__global__ void k_rad_shell_sw_ls(Params P, State S, const int* cells, int count, double h, long long off); \
 	__global__ void k_rad_shell_diag(Params P, State S, const int* cells, int count, double h); \
 	__global__ void k_rad_no_star_fp64(Params P, State S, double h); \
 	__global__ void k_rad_tau_shell(Params P, State S, const int* cells, int count); \
@@ -20,8 +22,15 @@
 	__global__ void k_rad_heating_fp64(Params P, State S); \
 	__global__ void k_rad_update_fp64(Params P, State S, double h, int mode); \
 	__global__ void k_colden_shell_fp64(Params P, State S, const int* cells, int count); \
+	__global__ void k_colden_shell_sw(Params P, State S, const int* cells, int count, long long off); \
+	__global__ void k_colden_sweep_prep(Params P, State S, const int* cells, int n, int init); \
+	__global__ void k_rad_shell_sw(Params P, State S, const int* cells, int count, double h, long long off); \
+	__global__ void k_rad_sweep_prep(Params P, State S, const int* cells, int n, int init); \
 	__global__ void k_thermo_rates_fp64(Params P, State S); \
 	__global__ void k_thermo_integrate_fp64(Params P, State S, double h); \
+	__global__ void k_thq_layout(State S); \
+	__global__ void k_thq_scatter(State S); \
+	__global__ void k_thq_drain(Params P, State S, double h); \
 	__global__ void k_thermo_update_fp64(Params P, State S, double h, int mode); \
 	__global__ void k_heating_arrays_fp64(Params P, State S); \
 	__global__ void k_fb_flags(Params P, State S, double contrast); \
@@ -46,6 +55,13 @@ size_t hydro_stage_fp32_smem();
 void launch_hydro_substep_fp32(const Params& P, const State& S, const double* U, double* Uout, double h, int zchunk,
                                cudaStream_t stream);
 __global__ void k_f64_to_f32(Params P, const double* a, float* b);
+// global FP64 mass and energy sums (conservation.cu): block partials of a
+// state, and the fold of the partials (also those of k_dt_reduce_fp64) into
+// out[0] = sum(rho V), out[1] = sum(E V)
+long long cons_nparts(const Params& P);
+void launch_cons_cells_f64(const Params& P, const double* U, double* part, cudaStream_t st);
+void launch_cons_cells_f32(const Params& P, const float* U, double* part, cudaStream_t st);
+void launch_cons_finalize(const Params& P, const double* part, double* out, cudaStream_t st);
 }  // namespace trg
 // network image of a trained model (mlp.cu) and the device it lives on
 const unsigned char* mlp_device_image(const trg_mlp* m, int* device);

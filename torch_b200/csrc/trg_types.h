@@ -36,8 +36,19 @@ enum { RS_HLLC = 0, RS_ROTATED = 1, RS_HLL = 2 };
 
 // Device error word bits (host maps them to TRG_ERR_*).
 enum : unsigned {
-	ERRB_NAN = 1u, ERRB_PICARD = 2u, ERRB_DT = 4u, ERRB_FLUX = 8u, ERRB_TC = 16u,
+	ERRB_NAN = 1u, ERRB_PICARD = 2u, ERRB_DT = 4u, ERRB_FLUX = 8u, ERRB_TC = 16u, ERRB_SUBCYCLE = 32u,
 };
+
+// Work queue of the thermal sub-cycles: control words (State::thq_ctl) and
+// limits.  Bins hold counts of bit length b (2^b .. 2^(b+1) - 1 sub-cycles).
+constexpr int THQ_BINS = 32;
+enum { THQ_COUNT = 0, THQ_HEAD = 1, THQ_BIN = 2, THQ_CURSOR = THQ_BIN + THQ_BINS, THQ_CTL = THQ_CURSOR + THQ_BINS };
+constexpr int THQ_MAX_SUBCYCLES = 1 << 26;
+
+// Rows of State::sw_rad beyond the six per-cell inputs, and the largest
+// candidate list the learned start serves in one sweep.
+constexpr int SW_TAU_A = 6, SW_LSTART = 7, SW_RAD_ROWS = 8;
+constexpr int LCAND_MAX = 1 << 21;
 
 // Planes per CTA of the FP32 form's fallback flag pass (k_fb_flags).
 constexpr int FB_ZCHUNK = 16;
@@ -116,8 +127,13 @@ struct State {
 	// heating / cooling diagnostics [NH][N], kept up to date during the step
 	// when non-null (trg_heating_enable)
 	double* H;
-	// learned starting iterate: the network's inference image (null = plain solve)
+	// learned starting iterate: the network's inference image (null = plain
+	// solve); when set, lstart is non-null (the predictions live in sw_rad
+	// row SW_LSTART) and lcand lists the candidate sweep positions
 	const unsigned char* mlp_img;
+	double* lstart;
+	int* lcand;
+	unsigned* lcand_n;
 	// FP32 form, radiation-hydro runs: cells whose hydro stencil spans a
 	// pressure contrast FP32 cannot difference are updated in FP64 instead
 	// (flag per cell, compacted list and its length)
@@ -128,6 +144,33 @@ struct State {
 	float* harvest;
 	long long harvest_cap;
 	unsigned long long* harvest_n;
+	// Causal sweeps of a single grid: each cell's own inputs in sweep order
+	// (index = the cell's position in the sweep list), so that the
+	// latency-bound shell kernels read them contiguously; a parallel pass
+	// refreshes the per-step ones before each sweep.
+	//   sw_rad [8][sw_rad_n] over the non-wind sweep list: n_H, the case-B
+	//          recombination rate, the collisional ionisation rate, x_HII
+	//          (per sweep), path length ds, shell volume (fixed), TAU_A of the
+	//          last sweep, the learned starting fraction of the coming sweep
+	//          (NaN: none);
+	//   sw_col [2][sw_col_n] over the sweep list of all cells: the cell's own
+	//          column density ds rho / m_H (per sweep), ds (fixed).
+	// Thermal sub-cycle work queue (null: every cell runs its sub-cycles in
+	// place): cells with at least thq_min sub-cycles, their bins, the cells
+	// laid out bin by bin, and the control words (THQ_*)
+	int* thq;
+	unsigned char* thq_binof;
+	int* thq_sorted;
+	unsigned* thq_ctl;
+	int thq_min;
+	double* sw_rad;
+	long long sw_rad_n;
+	double* sw_col;
+	long long sw_col_n;
+	// global FP64 mass and energy sums (null: off): the time-step reduction
+	// also leaves per-block double-double partials of sum(rho V) and sum(E V)
+	// here, 4 doubles per 256-cell block (mass hi, lo, energy hi, lo)
+	double* cons_part;
 };
 
 // Many independent grids advanced by one launch per stage.  Cell and face
