@@ -218,6 +218,33 @@ def cpu_sample(workload, n_sample, steps, procs):
     return rate, kind, procs, desc
 
 
+def cpu_sample_batch(cases, steps):
+    """The reference build on a sample of batch grids, one single-rank process
+    per grid, all at once on the host cores: cell-updates/s of the sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if not os.path.exists(oracle.REF_BIN):
+        raise FileNotFoundError("reference build unavailable")
+    cells = sum(int(np.prod(ic.ncells)) for _, ic in cases)
+    with tempfile.TemporaryDirectory() as d:
+        cmds = []
+        for i, (tp, ic) in enumerate(cases):
+            di = os.path.join(d, f"g{i}")
+            os.makedirs(di)
+            pp, icp = _write_case(di, tp, ic)
+            cmds.append(([oracle.REF_BIN, f"--params={pp}", f"--ic={icp}", f"--steps={steps}"], di))
+        t0 = time.perf_counter()
+        ps = [subprocess.Popen(c, cwd=di, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL) for c, di in cmds]
+        rcs = [p.wait() for p in ps]
+        wall = time.perf_counter() - t0
+    if any(rcs):
+        raise RuntimeError(f"reference sample failed: {rcs}")
+    return {"value": cells * steps / wall, "unit": UNIT, "cores": min(len(cases), os.cpu_count() or 1),
+            "kind": "reference",
+            "sample": f"the first {len(cases)} grids of the batch, {steps} full steps, one single-rank reference "
+                      f"process per grid (MPI absent), run together; includes set-up"}
+
+
 def run_reference_arm(args, rank):
     if rank != 0:
         return 0
@@ -311,8 +338,9 @@ def form_error(sim_a, sim_b, gamma, nd):
 
 def run_batch(args, world, rank, local, pg):
     """Independent 2-D cylindrical HII-region grids of uneven sizes, FP64,
-    advanced one launch per stage for all grids; beside it the same grids
-    stepped one by one (`unbatched`, on a bounded sample of grids)."""
+    advanced one launch per stage for all grids, each timestep replayed from
+    a captured CUDA graph; beside it the same grids stepped one by one
+    (`unbatched`, on a bounded sample of grids)."""
     import torch
     import torch_b200
     from torch_b200 import workloads
@@ -325,7 +353,6 @@ def run_batch(args, world, rank, local, pg):
     stream = torch.cuda.ExternalStream(b.stream_handle(), device=f"cuda:{local}")
     b.run_steps(args.warmup, dt_next)
     launches0 = b.kernel_launches()
-    b.profile(True)
     clocks = ClockSampler(local)
     clocks.start()
     barrier(pg)
@@ -340,15 +367,66 @@ def run_batch(args, world, rank, local, pg):
     clk = clocks.stop()
     ms = max_over_ranks(pg, ev0.elapsed_time(ev1), local)
     launches = b.kernel_launches() - launches0
+    # per-kernel times from an event-bracketed pass of the same number of
+    # steps after the timed region (per-launch events would keep the timed
+    # steps from being replayed as graphs)
+    b.profile(True)
+    b.enqueue_steps(args.steps, dt_next)
+    b.synchronize()
     prof = {}
     for name in PROFILE_NAMES:
         tt, cc = b.profile_read(name)
         if cc:
             prof[name] = {"ms": tt, "launches": cc}
     b.profile(False)
+    # end to end through the batch's public API: per step every grid's
+    # conserved state in from pinned host memory, the step, and out again
+    hbuf = [torch.empty((7, g.N), dtype=torch.float64).pin_memory() for g in grids]
+    for i, g in enumerate(grids):
+        b.get_conserved(i, hbuf[i].data_ptr())
+    b.synchronize()
+    e2e_steps = max(1, args.e2e_steps)
+    torch.cuda.synchronize(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        for i in range(len(grids)):
+            b.set_conserved(i, hbuf[i].data_ptr())
+        b.enqueue_steps(1, dt_next)
+        for i in range(len(grids)):
+            b.get_conserved(i, hbuf[i].data_ptr())
+    e1.record(stream)
+    b.synchronize()
+    e2e_ms = max_over_ranks(pg, e0.elapsed_time(e1), local)
+    ubytes = sum(7 * 8 * g.N for g in grids)
+    e2e = {"value": cells * e2e_steps * world / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": ubytes,
+           "d2h_bytes_per_step": ubytes, "steps": e2e_steps,
+           "note": "per step through the batch API: pinned H2D of every grid's U, one batch step, D2H of U"}
     b.close()
     for g in grids:
         g.close()
+    # roofline of the HBM-bound kernel with the largest share among those with a
+    # stated algorithmic byte count per cell (FP64 form)
+    per_cell = {"k_hydro_update_fp64": 280.0, "k_faces_fp64": 112.0, "k_q_from_u": 112.0}
+    roofline = None
+    cand = [(v["ms"], k) for k, v in prof.items() if k in per_cell]
+    if cand:
+        _, kname = max(cand)
+        launches_k = prof[kname]["launches"]
+        bytes_launch = per_cell[kname] * cells
+        avg_ms = prof[kname]["ms"] / launches_k
+        peak, src = hbm_peak()
+        achieved = bytes_launch / (avg_ms / 1e3) / 1e9
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": None, "kernel": kname, "peak_source": src, "avg_launch_ms": avg_ms,
+                    "launches": launches_k, "algorithmic_bytes_per_launch": bytes_launch,
+                    "note": "batch-wide launch (all grids); per-kernel times from an event-bracketed pass"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_sample_batch(cases[:16], args.cpu_steps)
+        except Exception as e:  # a missing CPU baseline must not hide the GPU number
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable", "sample": str(e)[:200]}
     # the same kind of grids stepped one context at a time (first 16 grids)
     sample = cases[:min(16, len(cases))]
     singles = [torch_b200.Torch(tp, ic) for tp, ic in sample]
@@ -377,7 +455,7 @@ def run_batch(args, world, rank, local, pg):
             "kernels": prof,
             "unbatched": {"value": ucells * args.steps / wall, "grids": len(sample),
                           "note": "the first grids stepped one context after another, host wall clock"},
-            "roofline": None, "cpu_baseline": None, "e2e": None,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
         }
         print(json.dumps(line), flush=True)
     return 0

@@ -313,6 +313,13 @@ int trg_batch_enqueue_steps(trg_batch* b, int nsteps, double dt_next_checkpoint)
  * operator split's rotating component order (bitwise the same results as the
  * launches themselves, which `on` = 0 restores). */
 int trg_batch_step_graphs(trg_batch* b, int on);
+/* The conserved state U [7][N_g] of grid g of the batch, copied in or out on
+ * the batch's stream, ordered with its steps (asynchronous with respect to
+ * the host: pinned host buffers, and trg_batch_synchronize before reading a
+ * result).  A state copied in is the start of the next step, as
+ * trg_set_conserved is for a single grid. */
+int trg_batch_set_conserved(trg_batch* b, int g, const double* U);
+int trg_batch_get_conserved(trg_batch* b, int g, double* U);
 int trg_batch_synchronize(trg_batch* b);
 void* trg_batch_stream(const trg_batch* b);
 long long trg_batch_kernel_launches(const trg_batch* b);

@@ -121,6 +121,8 @@ _SIGNATURES = [
     ("trg_batch_run_steps", C.c_int, [C.c_void_p, C.c_int, C.c_double]),
     ("trg_batch_enqueue_steps", C.c_int, [C.c_void_p, C.c_int, C.c_double]),
     ("trg_batch_step_graphs", C.c_int, [C.c_void_p, C.c_int]),
+    ("trg_batch_set_conserved", C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    ("trg_batch_get_conserved", C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     ("trg_batch_synchronize", C.c_int, [C.c_void_p]),
     ("trg_batch_stream", C.c_void_p, [C.c_void_p]),
     ("trg_batch_kernel_launches", C.c_longlong, [C.c_void_p]),
@@ -552,6 +554,15 @@ class Batch:
 
     def enqueue_steps(self, nsteps: int, dt_next_checkpoint: float):
         self._check(self.lib.trg_batch_enqueue_steps(self.handle, int(nsteps), float(dt_next_checkpoint)))
+
+    def set_conserved(self, g: int, U_ptr: int):
+        """Copy grid g's conserved state in from host memory at U_ptr (pinned
+        for an asynchronous copy), on the batch's stream."""
+        self._check(self.lib.trg_batch_set_conserved(self.handle, int(g), C.c_void_p(U_ptr)))
+
+    def get_conserved(self, g: int, U_ptr: int):
+        """Copy grid g's conserved state out to host memory at U_ptr, on the batch's stream."""
+        self._check(self.lib.trg_batch_get_conserved(self.handle, int(g), C.c_void_p(U_ptr)))
 
     def step_graphs(self, on: bool):
         """One captured CUDA graph per timestep (on by default)."""

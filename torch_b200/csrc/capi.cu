@@ -337,10 +337,11 @@ void rad_sweep_direct(trg_ctx* c, double h) {
 		if (c->S.lstart) cudaMemsetAsync(c->S.lcand_n, 0, sizeof(unsigned), c->stream);
 		LAUNCH(KF(k_rad_sweep_prep), c->S.sw_rad_n, 256, c->P, c->S, c->d_sweep_nonwind, (int)c->S.sw_rad_n, 0);
 		if (c->S.lstart) {
-			// learned starting iterates of the listed candidates (persistent tcgen05 tiles)
+			// learned starting iterates of the listed candidates (one tcgen05 tile per CTA)
 			cudaEvent_t ea = nullptr, eb = nullptr;
 			if (c->profiling) { ea = pool_event(c); eb = pool_event(c); cudaEventRecord(ea, c->stream); }
-			KF(k_learned_infer)<<<148, 128, mlp::INFER_SMEM, c->stream>>>(c->P, c->S, c->d_sweep_nonwind, h);
+			KF(k_learned_infer)<<<LCAND_MAX / 128, 128, mlp::INFER_SMEM, c->stream>>>(c->P, c->S,
+			                                                                          c->d_sweep_nonwind, h);
 			if (c->profiling) { cudaEventRecord(eb, c->stream); c->recs.push_back({"k_learned_infer", ea, eb}); }
 			c->launches++;
 		}
@@ -1272,16 +1273,16 @@ struct trg_batch {
 	// One captured CUDA graph per timestep: the operator split visits the
 	// components in an order that rotates with the step counter, so a step is
 	// one of `ncomps` fixed launch sequences (after the first step and the
-	// radiation time step's one-off first call).  Each is captured the first
-	// time it is needed and replayed after.
+	// radiation time step's one-off first call), given whether Q and the
+	// column densities are up to date when it starts.  Each is captured the
+	// first time it is needed and replayed after.
 	struct StepGraph {
 		cudaGraphExec_t exec = nullptr;
 		long long nodes = 0;
 		double dt_next = 0;
-		bool q_fresh0 = false, colden_valid0 = false;  // host-side state the capture started from
-		bool q_fresh1 = false, colden_valid1 = false;  // and ended with
+		bool q_fresh1 = false, colden_valid1 = false;  // host-side state the step ends with
 	};
-	StepGraph step_graph[3];
+	StepGraph step_graph[3][2][2];  // [position][Q up to date][column densities up to date]
 	bool step_graphs = true;
 };
 
@@ -1439,10 +1440,12 @@ int trg_batch_create(trg_ctx* const* grids, int G, trg_batch** out) {
 
 namespace {
 void batch_drop_step_graphs(trg_batch* b) {
-	for (auto& g : b->step_graph) {
-		if (g.exec) cudaGraphExecDestroy(g.exec);
-		g = trg_batch::StepGraph();
-	}
+	for (auto& a : b->step_graph)
+		for (auto& bb : a)
+			for (auto& g : bb) {
+				if (g.exec) cudaGraphExecDestroy(g.exec);
+				g = trg_batch::StepGraph();
+			}
 }
 
 // One timestep of a batch: the step's captured graph when it can be replayed,
@@ -1457,8 +1460,8 @@ void batch_step(trg_batch* b, double dt_next) {
 	}
 	const int n = v->hs.nactive;
 	const int phase = n > 1 ? (v->stepCounter + 1) % n : 0;
-	trg_batch::StepGraph& g = b->step_graph[phase];
-	if (g.exec && g.dt_next == dt_next && g.q_fresh0 == v->q_fresh && g.colden_valid0 == v->colden_valid) {
+	trg_batch::StepGraph& g = b->step_graph[phase][v->q_fresh ? 1 : 0][v->colden_valid ? 1 : 0];
+	if (g.exec && g.dt_next == dt_next) {
 		cudaGraphLaunch(g.exec, v->stream);
 		if (n > 1) v->stepCounter = phase;
 		v->steps++;
@@ -1470,8 +1473,7 @@ void batch_step(trg_batch* b, double dt_next) {
 	if (g.exec) cudaGraphExecDestroy(g.exec);
 	g = trg_batch::StepGraph();
 	g.dt_next = dt_next;
-	g.q_fresh0 = v->q_fresh;
-	g.colden_valid0 = v->colden_valid;
+	const bool q_fresh0 = v->q_fresh, colden_valid0 = v->colden_valid;
 	// the sweeps go into the step's graph directly (not as graphs of their own)
 	const bool use_graphs = v->use_graphs;
 	v->use_graphs = false;
@@ -1500,8 +1502,8 @@ void batch_step(trg_batch* b, double dt_next) {
 	v->steps--;
 	v->launches = before;
 	if (n > 1) v->stepCounter = (v->stepCounter + n - 1) % n;
-	v->q_fresh = g.q_fresh0;
-	v->colden_valid = g.colden_valid0;
+	v->q_fresh = q_fresh0;
+	v->colden_valid = colden_valid0;
 	enqueue_full_step(v, dt_next);
 }
 }  // namespace
@@ -1511,6 +1513,24 @@ int trg_batch_enqueue_steps(trg_batch* b, int nsteps, double dt_next_checkpoint)
 	for (int s = 0; s < nsteps; ++s) batch_step(b, dt_next_checkpoint);
 	trg_ctx* c = b->v;
 	CUDA_TRY(cudaGetLastError());
+	return TRG_OK;
+}
+
+int trg_batch_set_conserved(trg_batch* b, int g, const double* U) {
+	if (!b || g < 0 || g >= b->G || !U) return TRG_ERR_ARG;
+	trg_ctx* c = b->v;
+	trg_ctx* grid = b->grids[g];
+	CUDA_TRY(cudaMemcpyAsync(grid->S.U, U, 7 * grid->P.N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+	c->q_fresh = false;  // the next step rebuilds Q, and the column densities, from the new state
+	c->colden_valid = false;
+	return TRG_OK;
+}
+
+int trg_batch_get_conserved(trg_batch* b, int g, double* U) {
+	if (!b || g < 0 || g >= b->G || !U) return TRG_ERR_ARG;
+	trg_ctx* c = b->v;
+	trg_ctx* grid = b->grids[g];
+	CUDA_TRY(cudaMemcpyAsync(U, grid->S.U, 7 * grid->P.N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
 	return TRG_OK;
 }
 

@@ -966,40 +966,40 @@ __global__ void __launch_bounds__(128) k_rad_shell_diag(Params P, State S, const
 // Before each radiation sweep with a network loaded, k_rad_sweep_prep lists
 // the candidate front cells (by the previous sweep's TAU_A and x_HII, the
 // front criterion) as sweep positions and clears every prediction slot; this
-// kernel runs the network over the candidates, 128 per tile (tcgen05, one
-// tile per CTA at a time, persistent over the tiles): inputs log n_H, log T,
-// x_HII, log of the optically thin photoionisation rate at that TAU_A, log
-// dt; cells predicted to need more than two plain iterations get the
-// predicted time-averaged fraction as their starting iterate.  More than
-// LCAND_MAX candidates (the first sweep of a run, before any optical depth
-// exists, lists every neutral cell) means no predictions for that sweep.
+// kernel runs the network over the candidates, one tcgen05 tile of 128 per
+// CTA (a CTA allocates tensor memory once: infer_tile gives up the
+// allocation permit after its allocation, so no CTA runs a second tile; the
+// grid covers LCAND_MAX candidates and CTAs beyond the list return at once):
+// inputs log n_H, log T, x_HII, log of the optically thin photoionisation
+// rate at that TAU_A, log dt; cells predicted to need more than two plain
+// iterations get the predicted time-averaged fraction as their starting
+// iterate.  More than LCAND_MAX candidates (the first sweep of a run, before
+// any optical depth exists, lists every neutral cell) means no predictions
+// for that sweep.
 __global__ void __launch_bounds__(128) k_learned_infer(Params P, State S, const int* __restrict__ cells, double h) {
 	extern __shared__ __align__(128) unsigned char sm_mlp[];
 	const unsigned n = *S.lcand_n;
-	if (n > (unsigned)LCAND_MAX) return;
+	if (n > (unsigned)LCAND_MAX || blockIdx.x * 128u >= n) return;  // uniform over the CTA
 	const double dt = h * S.scal[0];
 	const long long sn = S.sw_rad_n;
-	for (unsigned tile = blockIdx.x; tile * 128u < n; tile += gridDim.x) {
-		const unsigned t = tile * 128u + threadIdx.x;
-		const bool valid = t < n;
-		const int pos = valid ? S.lcand[t] : 0;
-		float f[5] = {0, 0, 0, 0, 0}, y[3];
-		double q_hii = 0;
-		if (valid) {
-			const long long id = cells[pos];
-			const double* sw = S.sw_rad + pos;
-			const double q_den = FLD(S.Q, DEN, id), q_pre = FLD(S.Q, PRE, id);
-			q_hii = sw[3 * sn];
-			const double T = calc_temperature(P, q_hii, q_pre, q_den);
-			learned_features(P, sw[0], T, q_hii, sw[SW_TAU_A * sn], sw[4 * sn], sw[5 * sn], dt, f);
-		}
-		const bool ok = mlp::infer_tile(sm_mlp, reinterpret_cast<const uint4*>(S.mlp_img), f, y);
-		if (__syncthreads_or(!ok)) {  // the whole CTA leaves together
-			if (threadIdx.x == 0) atomicOr(S.err, ERRB_TC);
-			return;
-		}
-		if (valid && y[2] > 1.0f) S.sw_rad[SW_LSTART * sn + pos] = inv_logit10(logit10(q_hii) + y[0]);
+	const unsigned t = blockIdx.x * 128u + threadIdx.x;
+	const bool valid = t < n;
+	const int pos = valid ? S.lcand[t] : 0;
+	float f[5] = {0, 0, 0, 0, 0}, y[3];
+	double q_hii = 0;
+	if (valid) {
+		const long long id = cells[pos];
+		const double* sw = S.sw_rad + pos;
+		const double q_den = FLD(S.Q, DEN, id), q_pre = FLD(S.Q, PRE, id);
+		q_hii = sw[3 * sn];
+		const double T = calc_temperature(P, q_hii, q_pre, q_den);
+		learned_features(P, sw[0], T, q_hii, sw[SW_TAU_A * sn], sw[4 * sn], sw[5 * sn], dt, f);
 	}
+	if (!mlp::infer_tile(sm_mlp, reinterpret_cast<const uint4*>(S.mlp_img), f, y)) {
+		if (threadIdx.x == 0) atomicOr(S.err, ERRB_TC);
+		return;
+	}
+	if (valid && y[2] > 1.0f) S.sw_rad[SW_LSTART * sn + pos] = inv_logit10(logit10(q_hii) + y[0]);
 }
 
 // The cell's own inputs of the radiation sweep in sweep order (S.sw_rad):

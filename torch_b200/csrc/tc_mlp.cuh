@@ -130,7 +130,10 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, int limi
 	return false;
 }
 
-// TMEM allocation by one full warp; the base address lands in *slot.
+// TMEM allocation by one full warp; the base address lands in *slot.  The
+// CTA then gives up its allocation permit: a CTA allocates once in its life
+// (a second tcgen05.alloc after the relinquish is not allowed), so every
+// kernel here runs at most one allocating tile per CTA.
 __device__ __forceinline__ void tmem_alloc(uint32_t slot_saddr, int ncols) {
 	asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot_saddr), "r"(ncols)
 	             : "memory");
