@@ -175,6 +175,12 @@ enum {
  * strong shocks, where FP32 flux differences keep too few digits.  The count
  * of such updates is the TRG_STAT_FP64_CELLS counter. */
 int trg_fp32_contrast(trg_ctx* c, double contrast);
+/* FP32 form with radiation or cooling (no counterpart in the reference): the
+ * fused hydro pass stages each plane of a CTA whose haloed box lies inside
+ * the grid with one tiled TMA copy (on, the default) or, off, with per-cell
+ * asynchronous copies like the CTAs at the grid's edges.  Bitwise the same
+ * results either way. */
+int trg_fp32_tma(trg_ctx* c, int on);
 
 /* Thermal sub-cycles through a work queue (no counterpart in the reference,
  * whose Thermodynamics::integrate, src/Integrators/Thermodynamics.cpp:266-337,

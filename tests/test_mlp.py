@@ -192,3 +192,51 @@ def test_learned_start_on_hii_region():
     print(f"I-front: plain {r_plain:.3f} learned {r_learned:.3f} cells")
     assert abs(r_plain - r_learned) <= 0.5
     assert dev["den"] <= 1e-3 and dev["E"] <= 1e-2
+
+
+@pytest.mark.gpu
+def test_learned_start_gain_after_training_at_scale():
+    """The gain the trained network gives: 128^3 HII region, FP32 form.  The
+    plain solve records about a million front-cell solves over 200 steps,
+    the network trains on them on the GPU, then the same 16 steps run from
+    the same saved state with and without it.  The network must cut the
+    Picard iterations per front cell (every rejected prediction costs one
+    extra iteration, so this is a net gain), and the I-front and the state
+    stay with the plain run's."""
+    n = 128
+    tp, ic = workloads.hii_region(n=n, seed=6)
+    t = torch_b200.Torch(tp, ic, precision=torch_b200.PRECISION_FP32)
+    t.harvest(1 << 21)
+    t.run_steps(200)
+    rec, total = t.harvest_read()
+    t.harvest(0)
+    blob = t.checkpoint()
+    print("records", total)
+    assert total > 200000
+    m = torch_b200.Mlp(seed=7)
+    hist = m.train(rec, epochs=30, batch=8192, lr=2e-3, seed=8)
+    print("training loss", hist[0], hist[-1])
+    runs = {}
+    for name, net in (("plain", None), ("learned", m)):
+        t.restore(blob)
+        t.learned_start(net)
+        t.stats_enable(True)
+        t.run_steps(16)
+        runs[name] = (t.stats(reset=True), t.state())
+        t.stats_enable(False)
+    t.learned_start(None)
+    t.close()
+    m.close()
+    st_p, s_p = runs["plain"]
+    st_l, s_l = runs["learned"]
+    it_p = st_p["front_iters"] / max(1, st_p["front_cells"])
+    it_l = st_l["front_iters"] / max(1, st_l["front_cells"])
+    acc = st_l["learned_accepted"] / max(1, st_l["learned_cells"])
+    print(f"front cells {st_p['front_cells']}: Picard iterations per front cell plain {it_p:.3f}, learned {it_l:.3f}; "
+          f"predictions accepted {acc:.3f} of {st_l['learned_cells']}")
+    assert st_l["learned_cells"] > 0
+    assert it_l < it_p
+    fp, fl = common.ifront_cells(s_p.Q[2], n), common.ifront_cells(s_l.Q[2], n)
+    print(f"I-front plain {fp:.4f} learned {fl:.4f} cells; density L1 {common.rel_l1(s_l.U[0], s_p.U[0]):.2e}")
+    assert abs(fp - fl) <= 0.5
+    assert common.rel_l1(s_l.U[0], s_p.U[0]) <= 1e-4

@@ -103,6 +103,7 @@ _SIGNATURES = [
     ("trg_heating_enable", C.c_int, [C.c_void_p, C.c_int]),
     ("trg_fp32_contrast", C.c_int, [C.c_void_p, C.c_double]),
     ("trg_thermo_queue", C.c_int, [C.c_void_p, C.c_int]),
+    ("trg_fp32_tma", C.c_int, [C.c_void_p, C.c_int]),
     ("trg_heating", C.c_int, [C.c_void_p, C.c_void_p]),
     ("trg_checkpoint_save", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
     ("trg_checkpoint_load", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong]),
@@ -420,6 +421,10 @@ class Torch:
     def fp32_contrast(self, contrast: float):
         """Pressure ratio above which the FP32 form updates a hydro cell in FP64 (0: off)."""
         self._check(self.lib.trg_fp32_contrast(self.ctx, float(contrast)))
+
+    def fp32_tma(self, on: bool):
+        """FP32 hydro pass on the FP64 state: stage planes by TMA where possible (default on)."""
+        self._check(self.lib.trg_fp32_tma(self.ctx, int(on)))
 
     def thermo_queue(self, min_subcycles: int):
         """Cells with at least this many thermal sub-cycles run through the

@@ -584,6 +584,7 @@ int check_device_error(trg_ctx* c) {
 	if (e & ERRB_PICARD) return set_error(c, TRG_ERR_PICARD, "update_HIIfrac: implicit method not converging");
 	if (e & ERRB_DT) return set_error(c, TRG_ERR_DT, "Radiation::calculateTimeStep: invalid timestep");
 	if (e & ERRB_TC) return set_error(c, TRG_ERR_TC, "learned start: tensor-core wait expired");
+	if (e & ERRB_ASYNC) return set_error(c, TRG_ERR_CUDA, "hydro pass: a TMA plane copy did not complete in time");
 	if (e & ERRB_SUBCYCLE)
 		return set_error(c, TRG_ERR_SUBCYCLE, "Thermodynamics::integrate: a cell needs more thermal sub-cycles than "
 		                                      "the work queue runs (2^26)");
@@ -975,6 +976,13 @@ int trg_checkpoint_load(trg_ctx* c, const void* buf, long long bytes) {
 	c->stepCounter = h.stepCounter;
 	int rc = ensure_dt_hist(c, c->steps + 1);
 	if (rc) return rc;
+	// the sweep-ordered copy of the optical depths (the learned start's
+	// candidate test) from the restored state
+	if (c->S.sw_rad) {
+		if (c->S.lstart) CUDA_TRY(cudaMemsetAsync(c->S.lcand_n, 0, sizeof(unsigned), c->stream));
+		LAUNCH(KF(k_rad_sweep_prep), c->S.sw_rad_n, 256, c->P, c->S, c->d_sweep_nonwind, (int)c->S.sw_rad_n, 1);
+	}
+	CUDA_TRY(cudaDeviceSynchronize());  // the copies above went through the default stream
 	return TRG_OK;
 }
 
@@ -1028,6 +1036,13 @@ int trg_stats(trg_ctx* c, unsigned long long* out, int reset) {
 		CUDA_TRY(cudaMemsetAsync(c->S.stats, 0, TRG_NSTATS * sizeof(unsigned long long), c->stream));
 		CUDA_TRY(cudaStreamSynchronize(c->stream));
 	}
+	return TRG_OK;
+}
+
+int trg_fp32_tma(trg_ctx* c, int on) {
+	if (!c) return TRG_ERR_ARG;
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	c->P.hydro_tma = on ? 1 : 0;
 	return TRG_OK;
 }
 

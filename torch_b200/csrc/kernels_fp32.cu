@@ -19,7 +19,10 @@
 // faces, and its update; the neighbours' slopes and fluxes pass through
 // shared memory, while the z slope of the column and the flux through its
 // lower z face stay in registers from one plane to the next.  The plane three
-// ahead is staged with cp.async while the current one is computed.
+// ahead is staged while the current one is computed: by one tiled TMA copy
+// (cp.async.bulk.tensor, the whole haloed box of all seven fields) in CTAs
+// whose box lies inside the grid, by per-cell cp.async through the boundary
+// rule in the others.
 //
 // The rotated solver is written in directional form: HLL with normal n1 and
 // HLLC with normal n2 are the reference's rotate / 1-D solve / rotate-back
@@ -29,7 +32,10 @@
 // Pressure from total energy uses a compensated subtraction: the kinetic
 // energy is formed as a float pair with error-free products and sums, so that
 // E - KE loses no more than E's own rounding.
+#include <cuda.h>
 #include <cuda_runtime.h>
+
+#include <mutex>
 
 #include "trg_device.cuh"
 #include "trg_kernels.h"
@@ -339,38 +345,96 @@ __device__ __forceinline__ void hllc_n(const Prim& L, const Prim& R, const FaceP
 // n2 x d == 0 exactly), and n2 is built from them without cancellation:
 //   n1 = sign(dv_par) dv / |dv|,  |n1 . d| = |dv_par| / |dv| = cos,
 //   n2 = (d |dv|^2 - dv_par dv) / (|dv| |dv_perp|),  n2 . d = |dv_perp| / |dv| = sin.
+// Every case is F = w1 HLL(n1) + w2 HLLC(n2): the rotated flux (w1 = cos,
+// w2 = sin), pure HLLC across the face (|dv| < 1e-6 or dv normal to the face:
+// w1 = 0, n2 = d) or pure HLL along it (dv parallel to the face normal:
+// w2 = 0, n1 = d); a solve with weight 0 is skipped, so the exact flux of the
+// pure cases is kept, and each solver is inlined once.
 // No array is indexed with the run-time dim, so everything stays in registers.
 __device__ __forceinline__ void riemann32(int kind, const Prim& L, const Prim& R, int dim, float gamma, float* F) {
 	const float g1inv = 1.f / (gamma - 1.f);
 	const float d[3] = {dim == 0 ? 1.f : 0.f, dim == 1 ? 1.f : 0.f, dim == 2 ? 1.f : 0.f};
 	FacePre f;
 	face_pre(L, R, gamma, g1inv, f);
-	if (kind == RS_HLLC) { hllc_n(L, R, f, d, F); return; }
-	if (kind == RS_HLL) { hll_n(L, R, f, d, F); return; }
-	const float dv[3] = {R.v[0] - L.v[0], R.v[1] - L.v[1], R.v[2] - L.v[2]};
-	const float par = dv[0] * d[0] + dv[1] * d[1] + dv[2] * d[2];  // exact: one term is non-zero
-	const float perp[3] = {dv[0] - par * d[0], dv[1] - par * d[1], dv[2] - par * d[2]};  // exact
-	const float pp = perp[0] * perp[0] + perp[1] * perp[1] + perp[2] * perp[2];
-	const float rr = par * par + pp;
-	if (rr < 1.0e-12f) { hllc_n(L, R, f, d, F); return; }  // |dv| < 1e-6
-	if (pp == 0.f) { hll_n(L, R, f, d, F); return; }        // dv parallel to d
-	if (par == 0.f) { hllc_n(L, R, f, d, F); return; }     // dv normal to d
-	const float r = sqrtf(rr), s = sqrtf(pp);
-	const float inv_r = frcp(r);
-	const float sg = par < 0 ? -1.f : 1.f;
-	const float n1[3] = {sg * dv[0] * inv_r, sg * dv[1] * inv_r, sg * dv[2] * inv_r};
-	const float cosv = fabsf(par) * inv_r, sinv = s * inv_r;
-	const float k2 = fdiv(par * inv_r, s);
-	const float n2[3] = {sinv * d[0] - k2 * perp[0], sinv * d[1] - k2 * perp[1], sinv * d[2] - k2 * perp[2]};
-	float F1[7], F2[7];
-	hll_n(L, R, f, n1, F1);
-	hllc_n(L, R, f, n2, F2);
+	float n1[3] = {d[0], d[1], d[2]}, n2[3] = {d[0], d[1], d[2]};
+	float w1 = kind == RS_HLL ? 1.f : 0.f, w2 = kind == RS_HLLC ? 1.f : 0.f;
+	if (kind == RS_ROTATED) {
+		const float dv[3] = {R.v[0] - L.v[0], R.v[1] - L.v[1], R.v[2] - L.v[2]};
+		const float par = dv[0] * d[0] + dv[1] * d[1] + dv[2] * d[2];  // exact: one term is non-zero
+		const float perp[3] = {dv[0] - par * d[0], dv[1] - par * d[1], dv[2] - par * d[2]};  // exact
+		const float pp = perp[0] * perp[0] + perp[1] * perp[1] + perp[2] * perp[2];
+		const float rr = par * par + pp;
+		if (rr < 1.0e-12f || par == 0.f) {  // |dv| < 1e-6, or dv normal to d: HLLC
+			w2 = 1.f;
+		} else if (pp == 0.f) {  // dv parallel to d: HLL
+			w1 = 1.f;
+		} else {
+			const float r = sqrtf(rr), s = sqrtf(pp);
+			const float inv_r = frcp(r);
+			const float sg = par < 0 ? -1.f : 1.f;
 #pragma unroll
-	for (int i = 0; i < 7; ++i) F[i] = cosv * F1[i] + sinv * F2[i];
+			for (int k = 0; k < 3; ++k) n1[k] = sg * dv[k] * inv_r;
+			w1 = fabsf(par) * inv_r;
+			w2 = s * inv_r;
+			const float k2 = fdiv(par * inv_r, s);
+#pragma unroll
+			for (int k = 0; k < 3; ++k) n2[k] = w2 * d[k] - k2 * perp[k];
+		}
+	}
+	float F1[7], F2[7];
+#pragma unroll
+	for (int i = 0; i < 7; ++i) F1[i] = F2[i] = 0.f;
+	if (w1 != 0.f) hll_n(L, R, f, n1, F1);
+	if (w2 != 0.f) hllc_n(L, R, f, n2, F2);
+#pragma unroll
+	for (int i = 0; i < 7; ++i) F[i] = w1 * F1[i] + w2 * F2[i];
 }
 
+// A Prim, or a flux, in shared memory as two 16-byte halves kept in two
+// arrays of the same index (fields 0-3, then 4-6 and a pad): consecutive
+// threads read and write them with conflict-free 16-byte accesses, two per
+// cell instead of seven.
+struct V8 {
+	float4* a;
+	float4* b;
+	__device__ __forceinline__ Prim get(int k) const {
+		const float4 u = a[k], w = b[k];
+		Prim q;
+		q.d = u.x;
+		q.p = u.y;
+		q.x = u.z;
+		q.a = u.w;
+		q.v[0] = w.x;
+		q.v[1] = w.y;
+		q.v[2] = w.z;
+		return q;
+	}
+	__device__ __forceinline__ void put(int k, const Prim& q) const {
+		a[k] = make_float4(q.d, q.p, q.x, q.a);
+		b[k] = make_float4(q.v[0], q.v[1], q.v[2], 0.f);
+	}
+	__device__ __forceinline__ void get_f(int k, float* f) const {
+		const float4 u = a[k], w = b[k];
+		f[0] = u.x;
+		f[1] = u.y;
+		f[2] = u.z;
+		f[3] = u.w;
+		f[4] = w.x;
+		f[5] = w.y;
+		f[6] = w.z;
+	}
+	__device__ __forceinline__ void put_f(int k, const float* f) const {
+		a[k] = make_float4(f[0], f[1], f[2], f[3]);
+		b[k] = make_float4(f[4], f[5], f[6], 0.f);
+	}
+};
+// V8 arrays of a CTA: the three-plane ring of primitives (the x/y box of each
+// plane, index ly * SX + lx), face fluxes, slopes.
+constexpr int N_FX = BY * (BX + 1), N_FY = (BY + 1) * BX, N_S = BY * BX, N_EX = 2 * BY, N_EY = 2 * BX;
 struct SmemQ {
-	float v[NPLANE][7][SY][SX];
+	float4 a[NPLANE][SY * SX];
+	float4 b[NPLANE][SY * SX];
+	__device__ __forceinline__ V8 ring(int slot) { return V8{a[slot], b[slot]}; }
 };
 
 // Source position (with the boundary rule) of coordinate c along dim.
@@ -440,16 +504,7 @@ __device__ __forceinline__ void apply_flips(const Params& P, Prim& q, int flags,
 	if (P.nd > 1) apply_flip(q, 1, ((flags >> 4) & 7) - 1, (flags >> 7) & 1);
 	if (P.nd > 2) apply_flip(q, 2, zc, zside);
 }
-__device__ __forceinline__ void put_prim(SmemQ& s, int slot, int idx, const Prim& q) {
-	float* b = &s.v[slot][0][0][0] + idx;
-	b[DEN * SX * SY] = q.d;
-	b[PRE * SX * SY] = q.p;
-	b[HII * SX * SY] = q.x;
-	b[ADV * SX * SY] = q.a;
-	b[(VEL + 0) * SX * SY] = q.v[0];
-	b[(VEL + 1) * SX * SY] = q.v[1];
-	b[(VEL + 2) * SX * SY] = q.v[2];
-}
+__device__ __forceinline__ void put_prim(SmemQ& s, int slot, int idx, const Prim& q) { s.ring(slot).put(idx, q); }
 // Source plane of z under the boundary rule (2-D grids: plane 0).
 __device__ __forceinline__ int plane_src(const Params& P, int z, int& zc, int& zside) {
 	zc = -1;
@@ -491,6 +546,46 @@ __device__ __forceinline__ void cp_async_elem(TS* dst, const TS* src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// Tiled TMA staging of a plane (FP64 state, CTAs whose haloed box lies inside
+// the grid): one cp.async.bulk.tensor copy of the box x0 - 2 .. x0 + 33,
+// y0 - 2 .. y0 + 9 of source plane zs, all seven fields, into the staging
+// buffer in its [7][SY][SX] layout, completing on an mbarrier.  The x
+// coordinate x0 - 2 with x0 a multiple of 32 is a multiple of 2 elements of
+// 8 bytes, so the copy starts on a 16-byte boundary.
+constexpr unsigned TMA_BYTES = 7u * SX * SY * 8u;
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void tma_bar_init(uint64_t* bar) {
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+	asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void tma_plane(const CUtensorMap* tmap, void* dst, uint64_t* bar, int x, int y, int z) {
+	// generic-proxy reads of the buffer (the previous plane's conversion) are
+	// ordered before the async-proxy writes of this copy
+	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(TMA_BYTES)
+	             : "memory");
+	asm volatile(
+	    "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+	    "%5}], [%6];" ::"r"(smem_addr(dst)),
+	    "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(z), "r"(0), "r"(smem_addr(bar))
+	    : "memory");
+}
+// Bounded wait for the copy of the given phase: false if it did not complete
+// within the limit (the caller reports it; the kernel never hangs).
+__device__ __forceinline__ bool tma_wait(uint64_t* bar, uint32_t phase) {
+	for (int i = 0; i < (1 << 22); ++i) {
+		uint32_t ok;
+		asm volatile(
+		    "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+		    "selp.b32 %0, 1, 0, P1;\n\t}\n"
+		    : "=r"(ok)
+		    : "r"(smem_addr(bar)), "r"(phase)
+		    : "memory");
+		if (ok) return true;
+	}
+	return false;
+}
+
 template <typename TS>
 __device__ __forceinline__ void plane_fetch(const Params& P, const TS* __restrict__ U, TS* raw, const StageMap& m,
                                             int z) {
@@ -525,37 +620,7 @@ __device__ __forceinline__ void plane_convert(const Params& P, const Scaled& SP,
 	}
 }
 
-__device__ __forceinline__ Prim get(const SmemQ& s, int slot, int ly, int lx) {
-	Prim q;
-	q.d = s.v[slot][DEN][ly][lx];
-	q.p = s.v[slot][PRE][ly][lx];
-	q.x = s.v[slot][HII][ly][lx];
-	q.a = s.v[slot][ADV][ly][lx];
-	q.v[0] = s.v[slot][VEL + 0][ly][lx];
-	q.v[1] = s.v[slot][VEL + 1][ly][lx];
-	q.v[2] = s.v[slot][VEL + 2][ly][lx];
-	return q;
-}
-
-// A Prim in a [7][n] float array of shared memory, at index k.
-__device__ __forceinline__ void put7(float* a, int n, int k, const Prim& q) {
-	a[DEN * n + k] = q.d;
-	a[PRE * n + k] = q.p;
-	a[HII * n + k] = q.x;
-	a[ADV * n + k] = q.a;
-#pragma unroll
-	for (int j = 0; j < 3; ++j) a[(VEL + j) * n + k] = q.v[j];
-}
-__device__ __forceinline__ Prim get7(const float* a, int n, int k) {
-	Prim q;
-	q.d = a[DEN * n + k];
-	q.p = a[PRE * n + k];
-	q.x = a[HII * n + k];
-	q.a = a[ADV * n + k];
-#pragma unroll
-	for (int j = 0; j < 3; ++j) q.v[j] = a[(VEL + j) * n + k];
-	return q;
-}
+__device__ __forceinline__ Prim get(SmemQ& s, int slot, int ly, int lx) { return s.ring(slot).get(ly * SX + lx); }
 
 __device__ __forceinline__ double dmin_(double a, double b) { return (b < a) ? b : a; }
 
@@ -622,11 +687,11 @@ __device__ __forceinline__ bool update_state64(const Params& P, const State& S, 
 using namespace f32;
 
 // Byte offset of the plane staging buffer in the kernel's shared memory:
-// after the ring and the flux and slope arrays, 16-byte aligned.
+// after the ring and the flux and slope arrays.
 __host__ __device__ constexpr size_t hydro_stage_raw_offset() {
-	return (sizeof(f32::SmemQ) + sizeof(float) * 7 * (f32::BY * (f32::BX + 1) + (f32::BY + 1) * f32::BX +
-	                                                  3 * f32::BY * f32::BX + 2 * f32::BY + 2 * f32::BX) + 15) /
-	       16 * 16;
+	return (sizeof(f32::SmemQ) + 2 * sizeof(float4) * (f32::N_FX + f32::N_FY + 2 * f32::N_S + f32::N_EX + f32::N_EY) +
+	        127) /
+	       128 * 128;  // 128-byte aligned: the destination of the TMA plane copy
 }
 
 // Riemann solve for one face from its reconstructed states.
@@ -642,20 +707,28 @@ __device__ __forceinline__ void face_flux(int rs_rt, const Prim& L, const Prim& 
 //          corrector (h = 1).
 // TS: storage type (float: scaled units; double: code units).
 // LIM / RS: limiter and Riemann solver fixed at compile time (-1: chosen at run time).
+// tmap / use_tma: the tensor map of the FP64 state Uq for the TMA plane
+// staging (use_tma = 0: per-cell cp.async staging everywhere).
 template <int STAGE, typename TS, int LIM, int RS>
 __global__ void __launch_bounds__(BX* BY, 2)
     k_hydro_stage_fp32(Params P, State S, const TS* __restrict__ Uq, const TS* Ubase, TS* Uout, double hfac,
-                       int zchunk) {
-	extern __shared__ __align__(16) unsigned char smem_raw[];
+                       int zchunk, const __grid_constant__ CUtensorMap tmap, int use_tma) {
+	extern __shared__ __align__(128) unsigned char smem_raw[];
 	SmemQ& s = *reinterpret_cast<SmemQ*>(smem_raw);
-	float* Fx = reinterpret_cast<float*>(smem_raw + sizeof(SmemQ));  // [7][BY][BX + 1] x-face fluxes
-	float* Fy = Fx + 7 * BY * (BX + 1);                               // [7][BY + 1][BX] y-face fluxes
-	float* Fz = Fy + 7 * (BY + 1) * BX;                               // [7][BY * BX] flux of each column's face z + 1/2
-	float* Sx = Fz + 7 * BY * BX;                                     // [7][BY * BX] x slopes of the tile
-	float* Sy = Sx + 7 * BY * BX;                                     // [7][BY * BX] y slopes of the tile
-	float* Ex = Sy + 7 * BY * BX;                                     // [7][2 * BY] x slopes of cells x0 - 1, x0 + BX
-	float* Ey = Ex + 7 * 2 * BY;                                      // [7][2 * BX] y slopes of cells y0 - 1, y0 + BY
+	float4* v8 = reinterpret_cast<float4*>(smem_raw + sizeof(SmemQ));
+	const V8 Fx{v8, v8 + N_FX};                      // [BY][BX + 1] x-face fluxes
+	v8 += 2 * N_FX;
+	const V8 Fy{v8, v8 + N_FY};                      // [BY + 1][BX] y-face fluxes
+	v8 += 2 * N_FY;
+	const V8 Sx{v8, v8 + N_S};                       // [BY * BX] x slopes of the tile
+	v8 += 2 * N_S;
+	const V8 Sy{v8, v8 + N_S};                       // [BY * BX] y slopes of the tile
+	v8 += 2 * N_S;
+	const V8 Ex{v8, v8 + N_EX};                      // [2 * BY] x slopes of cells x0 - 1, x0 + BX
+	v8 += 2 * N_EX;
+	const V8 Ey{v8, v8 + N_EY};                      // [2 * BX] y slopes of cells y0 - 1, y0 + BY
 	TS* raw = reinterpret_cast<TS*>(smem_raw + hydro_stage_raw_offset());  // [7][SY * SX] next plane, staged
+	uint64_t* tbar = reinterpret_cast<uint64_t*>(smem_raw + hydro_stage_raw_offset() + sizeof(double) * 7 * SX * SY);
 	const int tx = threadIdx.x % BX, ty = threadIdx.x / BX;
 	const int lx = tx + HALO, ly = ty + HALO;
 	const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY;
@@ -705,6 +778,12 @@ __global__ void __launch_bounds__(BX* BY, 2)
 	}
 
 	const StageMap smap = stage_map(P, x0, y0);
+	// TMA staging: FP64 state, 3-D, the CTA's haloed x/y box inside the grid
+	const bool tma = sizeof(TS) == sizeof(double) && use_tma && nd > 2 && x0 >= HALO && x0 + BX + HALO <= P.nx &&
+	                 y0 >= HALO && y0 + BY + HALO <= P.ny;
+	uint32_t tphase = 0;
+	bool tma_late = false;
+	if (tma && threadIdx.x == 0) tma_bar_init(tbar);  // ordered before use by the first barrier below
 	auto slot_of = [](int z) { return ((z % NPLANE) + NPLANE) % NPLANE; };
 	Prim zero;
 	zero.d = zero.p = zero.x = zero.a = zero.v[0] = zero.v[1] = zero.v[2] = 0.f;
@@ -734,7 +813,16 @@ __global__ void __launch_bounds__(BX* BY, 2)
 		const bool plane = z >= z0;  // x/y faces and the update of this plane
 		const bool stage_next = nd > 2 && z + 1 < z1;
 		__syncthreads();  // planes z .. z + 2 are in the ring; the staging buffer is free
-		if (stage_next) plane_fetch(P, Uq, raw, smap, z + 3);
+		if (stage_next) {
+			if (tma) {
+				if (threadIdx.x == 0) {
+					int zc, zside;
+					tma_plane(&tmap, raw, tbar, x0 - HALO, y0 - HALO, plane_src(P, z + 3, zc, zside));
+				}
+			} else {
+				plane_fetch(P, Uq, raw, smap, z + 3);
+			}
+		}
 		// slopes: this cell in x, y and (of the next plane's cell) z; the cells
 		// just outside the tile in x and y
 		Prim szn = zero;
@@ -745,73 +833,66 @@ __global__ void __launch_bounds__(BX* BY, 2)
 		}
 		if (rec && plane) {
 			const Prim qc = get(s, sc, ly, lx);
-			put7(Sx, BY * BX, threadIdx.x, slope_of(lim, th, get(s, sc, ly, lx - 1), qc, get(s, sc, ly, lx + 1)));
+			Sx.put(threadIdx.x, slope_of(lim, th, get(s, sc, ly, lx - 1), qc, get(s, sc, ly, lx + 1)));
 			if (nd > 1)
-				put7(Sy, BY * BX, threadIdx.x, slope_of(lim, th, get(s, sc, ly - 1, lx), qc, get(s, sc, ly + 1, lx)));
+				Sy.put(threadIdx.x, slope_of(lim, th, get(s, sc, ly - 1, lx), qc, get(s, sc, ly + 1, lx)));
 			if (ts >= 0 && ts < 2 * BY) {
 				const int e = ts / BY, r = ts - e * BY, ex = e ? HALO + BX : HALO - 1;
-				put7(Ex, 2 * BY, ts,
+				Ex.put(ts,
 				     slope_of(lim, th, get(s, sc, r + HALO, ex - 1), get(s, sc, r + HALO, ex), get(s, sc, r + HALO, ex + 1)));
 			} else if (ts >= 2 * BY && nd > 1) {
 				const int u = ts - 2 * BY, e = u / BX, col = u - e * BX, ey = e ? HALO + BY : HALO - 1;
-				put7(Ey, 2 * BX, u,
+				Ey.put(u,
 				     slope_of(lim, th, get(s, sc, ey - 1, col + HALO), get(s, sc, ey, col + HALO), get(s, sc, ey + 1, col + HALO)));
 			}
 		}
 		__syncthreads();
-		// faces: the x face below, the y face below and the z face above this
-		// cell, then (warps 0-1) the tile's last y and x faces, all through one
-		// call of the solver
-		const int nk = te < BX + BY ? 4 : 3;  // only threads 0 .. BX + BY - 1 take a last face
+		// faces: the x face below and the y face below this cell, then (warps
+		// 0-1) the tile's last y and x faces, through one call of the solver;
+		// then the z face above this cell through a second one, its flux kept
+		// in registers (this thread's own update and, as the flux below, the
+		// next plane's)
+		const int nk = te < BX + BY ? 3 : 2;  // only threads 0 .. BX + BY - 1 take a last face
 #pragma unroll 1
 		for (int k = 0; k < nk; ++k) {
 			Prim ql, qr, sl = zero, sr = zero;
 			int dim;
 			bool ok;
-			float* dst;
-			int stride;
+			V8 dst;
+			int di;
 			if (k == 0) {  // x face gx - 1/2, between cells lx - 1 and lx of row ly
 				ok = fx_ok && plane;
 				dim = 0;
 				ql = get(s, sc, ly, lx - 1);
 				qr = get(s, sc, ly, lx);
 				if (rec && ok) {
-					sl = tx > 0 ? get7(Sx, BY * BX, threadIdx.x - 1) : get7(Ex, 2 * BY, ty);
-					sr = get7(Sx, BY * BX, threadIdx.x);
+					sl = tx > 0 ? Sx.get(threadIdx.x - 1) : Ex.get(ty);
+					sr = Sx.get(threadIdx.x);
 				}
-				dst = Fx + ty * (BX + 1) + tx;
-				stride = BY * (BX + 1);
+				dst = Fx;
+				di = ty * (BX + 1) + tx;
 			} else if (k == 1) {  // y face gy - 1/2, between rows ly - 1 and ly of column lx
 				ok = fy_ok && plane;
 				dim = 1;
 				ql = get(s, sc, ly - 1, lx);
 				qr = get(s, sc, ly, lx);
 				if (rec && ok) {
-					sl = ty > 0 ? get7(Sy, BY * BX, threadIdx.x - BX) : get7(Ey, 2 * BX, tx);
-					sr = get7(Sy, BY * BX, threadIdx.x);
+					sl = ty > 0 ? Sy.get(threadIdx.x - BX) : Ey.get(tx);
+					sr = Sy.get(threadIdx.x);
 				}
-				dst = Fy + ty * BX + tx;
-				stride = (BY + 1) * BX;
-			} else if (k == 2) {  // z face z + 1/2 of this column
-				ok = nd > 2;
-				dim = 2;
-				ql = get(s, sc, ly, lx);
-				qr = ok ? get(s, slot_of(z + 1), ly, lx) : ql;
-				sl = szc;
-				sr = szn;
-				dst = Fz + threadIdx.x;
-				stride = BY * BX;
+				dst = Fy;
+				di = ty * BX + tx;
 			} else if (te < BX) {  // y face y0 + BY - 1/2 of column te
 				ok = fe_ok && plane;
 				dim = 1;
 				ql = get(s, sc, HALO + BY - 1, te + HALO);
 				qr = get(s, sc, HALO + BY, te + HALO);
 				if (rec && ok) {
-					sl = get7(Sy, BY * BX, (BY - 1) * BX + te);
-					sr = get7(Ey, 2 * BX, BX + te);
+					sl = Sy.get((BY - 1) * BX + te);
+					sr = Ey.get(BX + te);
 				}
-				dst = Fy + BY * BX + te;
-				stride = (BY + 1) * BX;
+				dst = Fy;
+				di = BY * BX + te;
 			} else {  // x face x0 + BX - 1/2 of row te - BX
 				ok = fe_ok && plane;
 				dim = 0;
@@ -819,38 +900,51 @@ __global__ void __launch_bounds__(BX* BY, 2)
 				ql = get(s, sc, r + HALO, HALO + BX - 1);
 				qr = get(s, sc, r + HALO, HALO + BX);
 				if (rec && ok) {
-					sl = get7(Sx, BY * BX, r * BX + BX - 1);
-					sr = get7(Ex, 2 * BY, BY + r);
+					sl = Sx.get(r * BX + BX - 1);
+					sr = Ex.get(BY + r);
 				}
-				dst = Fx + r * (BX + 1) + BX;
-				stride = BY * (BX + 1);
+				dst = Fx;
+				di = r * (BX + 1) + BX;
 			}
 			if (!ok) continue;
 			float f[7];
 			face_flux<RS>(rs_rt, rec ? face_left(ql, sl) : ql, rec ? face_right(qr, sr) : qr, dim, gamma, f);
-#pragma unroll
-			for (int i = 0; i < 7; ++i) dst[i * stride] = f[i];
+			dst.put_f(di, f);
+		}
+		float fz[7];  // flux through this column's face z + 1/2
+		if (nd > 2) {
+			const Prim ql = get(s, sc, ly, lx), qr = get(s, slot_of(z + 1), ly, lx);
+			face_flux<RS>(rs_rt, rec ? face_left(ql, szc) : ql, rec ? face_right(qr, szn) : qr, 2, gamma, fz);
 		}
 		// the cell itself for the source terms, read before the barrier: after
 		// it, nothing of this plane is read, so the next plane's load may reuse
 		// the slot without another barrier
 		const Prim qc = get(s, sc, ly, lx);
-		if (stage_next) cp_async_wait_all();  // this thread's copies of plane z + 3 have landed
+		if (stage_next) {  // plane z + 3 has landed (this thread's copies, or the CTA's TMA copy)
+			if (tma) {
+				tma_late |= !tma_wait(tbar, tphase);
+				tphase ^= 1u;
+			} else {
+				cp_async_wait_all();
+			}
+		}
 		__syncthreads();
 		if (active && plane) {
 			const long long id = gx + (long long)P.nx * (gy + (long long)P.ny * z);
-			float udot[7];
+			float udot[7], fl[7], fr[7];
+			Fx.get_f(ty * (BX + 1) + tx, fl);
+			Fx.get_f(ty * (BX + 1) + tx + 1, fr);
 #pragma unroll
-			for (int i = 0; i < 7; ++i)
-				udot[i] = axl * Fx[(i * BY + ty) * (BX + 1) + tx] - axr * Fx[(i * BY + ty) * (BX + 1) + tx + 1];
+			for (int i = 0; i < 7; ++i) udot[i] = axl * fl[i] - axr * fr[i];
 			if (nd > 1) {
+				Fy.get_f(ty * BX + tx, fl);
+				Fy.get_f((ty + 1) * BX + tx, fr);
 #pragma unroll
-				for (int i = 0; i < 7; ++i)
-					udot[i] += ayl * Fy[(i * (BY + 1) + ty) * BX + tx] - ayr * Fy[(i * (BY + 1) + ty + 1) * BX + tx];
+				for (int i = 0; i < 7; ++i) udot[i] += ayl * fl[i] - ayr * fr[i];
 			}
 			if (nd > 2) {
 #pragma unroll
-				for (int i = 0; i < 7; ++i) udot[i] += azl * fzlo[i] - azr * Fz[i * BY * BX + threadIdx.x];
+				for (int i = 0; i < 7; ++i) udot[i] += azl * fzlo[i] - azr * fz[i];
 			}
 			if (S.grav) {
 				for (int k = 0; k < 3; ++k) {
@@ -912,7 +1006,7 @@ __global__ void __launch_bounds__(BX* BY, 2)
 		}
 		if (nd > 2) {
 #pragma unroll
-			for (int i = 0; i < 7; ++i) fzlo[i] = Fz[i * BY * BX + threadIdx.x];
+			for (int i = 0; i < 7; ++i) fzlo[i] = fz[i];
 		}
 		szc = szn;
 		// no barrier before this: only the slot of plane z is written, and the
@@ -920,6 +1014,7 @@ __global__ void __launch_bounds__(BX* BY, 2)
 		if (stage_next) plane_convert<STAGE>(P, SP, SC, raw, s, slot_of(z + 3), smap, z + 3);
 	}
 	if (bad) atomicOr(S.err, ERRB_NAN);
+	if (tma_late) atomicOr(S.err, ERRB_ASYNC);
 	if (STAGE == 2) {
 		for (int o = 16; o > 0; o >>= 1) tmin = dmin_(tmin, __shfl_down_sync(0xffffffffu, tmin, o));
 		if ((threadIdx.x & 31) == 0) {
@@ -930,8 +1025,40 @@ __global__ void __launch_bounds__(BX* BY, 2)
 }
 
 size_t hydro_stage_fp32_smem() {
-	// the staging buffer is sized for the FP64 state of the radiation-hydro form
-	return hydro_stage_raw_offset() + sizeof(double) * 7 * SX * SY;
+	// the staging buffer is sized for the FP64 state of the radiation-hydro
+	// form, followed by the TMA copy's mbarrier
+	return hydro_stage_raw_offset() + sizeof(double) * 7 * SX * SY + 16;
+}
+
+// Tensor map of an FP64 state [7][nz][ny][nx] for the TMA plane staging: a
+// 4-D tensor (x, y, z, field), box SX x SY x 1 x 7.  False where the driver
+// entry point is unavailable or the strides are not multiples of 16 bytes
+// (odd nx): the kernel then stages with cp.async.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled_fn() {
+	static EncodeTiledFn fn = nullptr;
+	static std::once_flag once;
+	std::call_once(once, [] {
+		void* p = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+		    q == cudaDriverEntryPointSuccess)
+			fn = reinterpret_cast<EncodeTiledFn>(p);
+	});
+	return fn;
+}
+static bool state_tensor_map(const Params& P, const double* U, CUtensorMap* m) {
+	EncodeTiledFn enc = encode_tiled_fn();
+	if (!enc || P.nd != 3 || (P.nx & 1) || P.nx < SX || P.ny < SY) return false;
+	const cuuint64_t dims[4] = {(cuuint64_t)P.nx, (cuuint64_t)P.ny, (cuuint64_t)P.nz, 7};
+	const cuuint64_t strides[3] = {(cuuint64_t)P.nx * 8, (cuuint64_t)P.nx * P.ny * 8, (cuuint64_t)P.N * 8};
+	const cuuint32_t box[4] = {SX, SY, 1, 7};
+	const cuuint32_t estr[4] = {1, 1, 1, 1};
+	return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(U), dims, strides, box, estr,
+	           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+	           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 template <int STAGE, typename TS, int LIM, int RS>
@@ -940,9 +1067,15 @@ static void launch_one(const Params& P, const State& S, const TS* Uq, const TS* 
 	size_t smem = hydro_stage_fp32_smem();
 	int zc = P.nd > 2 ? zchunk : 1;
 	dim3 grid((P.nx + BX - 1) / BX, (P.ny + BY - 1) / BY, P.nd > 2 ? (P.nz + zc - 1) / zc : 1);
+	CUtensorMap tmap;
+	memset(&tmap, 0, sizeof(tmap));
+	int use_tma = 0;
+	if (sizeof(TS) == sizeof(double) && P.hydro_tma)
+		use_tma = state_tensor_map(P, reinterpret_cast<const double*>(Uq), &tmap) ? 1 : 0;
 	cudaFuncSetAttribute(k_hydro_stage_fp32<STAGE, TS, LIM, RS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 	                     (int)smem);
-	k_hydro_stage_fp32<STAGE, TS, LIM, RS><<<grid, BX * BY, smem, stream>>>(P, S, Uq, Ubase, Uout, hfac, zc);
+	k_hydro_stage_fp32<STAGE, TS, LIM, RS><<<grid, BX * BY, smem, stream>>>(P, S, Uq, Ubase, Uout, hfac, zc, tmap,
+	                                                                         use_tma);
 }
 
 // the reference's configured and default pair (albada, RotatedHLLC) is compiled

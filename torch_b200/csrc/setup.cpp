@@ -295,6 +295,7 @@ std::string host_setup(const trg_params& p, const double* den, const double* pre
 	P.coupling = p.coupling;
 	P.rt_scheme = p.rt_scheme;
 	P.thermo_subcycling = p.thermo_subcycling;
+	P.hydro_tma = 1;
 	for (int i = 0; i < 3; ++i) P.star_pos[i] = p.star_pos[i];
 	P.wind_radius = p.star_on ? p.wind_cell_radius : 0;
 	// Star::initialise, Star.cpp:13-40

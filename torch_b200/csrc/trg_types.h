@@ -37,6 +37,7 @@ enum { RS_HLLC = 0, RS_ROTATED = 1, RS_HLL = 2 };
 // Device error word bits (host maps them to TRG_ERR_*).
 enum : unsigned {
 	ERRB_NAN = 1u, ERRB_PICARD = 2u, ERRB_DT = 4u, ERRB_FLUX = 8u, ERRB_TC = 16u, ERRB_SUBCYCLE = 32u,
+	ERRB_ASYNC = 64u,  // an asynchronous (TMA) copy did not complete within its wait limit
 };
 
 // Work queue of the thermal sub-cycles: control words (State::thq_ctl) and
@@ -98,6 +99,9 @@ struct Params {
 	double f32_rho0, f32_p0, f32_v0;
 	// diagnostic counters (State::stats) are updated only when this is set
 	int stats_on;
+	// FP32 hydro pass on the FP64 state: stage planes by TMA where possible
+	// (else per-cell cp.async)
+	int hydro_tma;
 	// batched launch over many grids (null for one grid): kernels take each
 	// grid's Params and State from this table
 	const BatchTable* batch;
