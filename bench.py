@@ -63,12 +63,19 @@ def build_workload(name, n):
         return workloads.sedov(n=n)
     if name == "hii":
         return workloads.hii_region(n=n)
+    if name == "blister":  # the shipped 2-D cylindrical setup (150 x 200), whatever n
+        return workloads.blister()
     raise ValueError(name)
 
 
 def workload_config(name, n, precision, replicas):
     base = {"workload": f"{name} {n}^3", "cells": n ** 3, "precision": precision,
             "parallelism": f"replicas x{replicas}", "l2": "inputs larger than L2 (no flush)"}
+    if name == "blister":
+        base.update({"workload": "blister 150x200 (2-D cylindrical, the shipped setup)", "cells": 30000,
+                     "l2": "inputs smaller than L2", "setup": "config/torch-config.lua + torch-setup.lua values",
+                     "time": "operator split H/T/R"})
+        return base
     if name == "sedov":
         base.update({"setup": "hydro-only Sedov blast, rho 1e-20, P 1e-12, E 1e51 erg in r<=3dx, outflow",
                      "reconstruction": "piecewise-linear albada (spatial_order 1)", "riemann": "RotatedHLLC",
@@ -282,6 +289,8 @@ def time_form(args, precision, tp, ic, local, pg, profile_names):
     sim = torch_b200.Torch(tp, ic, precision=precision, device=local)
     if precision == torch_b200.PRECISION_FP32 and getattr(args, "fp32_contrast", None) is not None and tp.radiation_on:
         sim.fp32_contrast(args.fp32_contrast)
+    if getattr(args, "thermo_queue", 0) and tp.cooling_on:
+        sim.thermo_queue(args.thermo_queue)
     sim.tile = sim.autotune()
     dt_next = sim.dt_max
     stream = torch.cuda.ExternalStream(sim.stream_handle(), device=f"cuda:{local}")
@@ -337,16 +346,19 @@ def form_error(sim_a, sim_b, gamma, nd):
 
 
 def run_batch(args, world, rank, local, pg):
-    """Independent 2-D cylindrical HII-region grids of uneven sizes, FP64,
-    advanced one launch per stage for all grids, each timestep replayed from
-    a captured CUDA graph; beside it the same grids stepped one by one
-    (`unbatched`, on a bounded sample of grids)."""
+    """Independent 2-D cylindrical HII-region grids of uneven sizes, in the
+    FP32 form (FP32 hydro, FP64 radiation and cooling; --precision fp64 for
+    the FP64 form), advanced one launch per stage for all grids, each
+    timestep replayed from a captured CUDA graph; beside it the same grids
+    stepped one by one (`unbatched`, on a bounded sample of grids)."""
     import torch
     import torch_b200
     from torch_b200 import workloads
 
     cases = workloads.blister_batch(G=args.grids, seed=2024 + rank)
-    grids = [torch_b200.Torch(tp, ic) for tp, ic in cases]
+    prec = torch_b200.PRECISION_FP64 if args.precision == "fp64" else torch_b200.PRECISION_FP32
+    form = "fp64" if prec == torch_b200.PRECISION_FP64 else "fp32"
+    grids = [torch_b200.Torch(tp, ic, precision=prec) for tp, ic in cases]
     cells = sum(g.N for g in grids)
     dt_next = min(g.dt_max for g in grids)
     b = torch_b200.Batch(grids)
@@ -407,7 +419,9 @@ def run_batch(args, world, rank, local, pg):
         g.close()
     # roofline of the HBM-bound kernel with the largest share among those with a
     # stated algorithmic byte count per cell (FP64 form)
-    per_cell = {"k_hydro_update_fp64": 280.0, "k_faces_fp64": 112.0, "k_q_from_u": 112.0}
+    # (the FP32 form's batch hydro pass: read U, write U1 and Q, then U1 back to U)
+    per_cell = {"k_hydro_update_fp64": 280.0, "k_faces_fp64": 112.0, "k_q_from_u": 112.0,
+                "k_hydro_stage_fp32": 280.0}
     roofline = None
     cand = [(v["ms"], k) for k, v in prof.items() if k in per_cell]
     if cand:
@@ -429,7 +443,7 @@ def run_batch(args, world, rank, local, pg):
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable", "sample": str(e)[:200]}
     # the same kind of grids stepped one context at a time (first 16 grids)
     sample = cases[:min(16, len(cases))]
-    singles = [torch_b200.Torch(tp, ic) for tp, ic in sample]
+    singles = [torch_b200.Torch(tp, ic, precision=prec) for tp, ic in sample]
     for s in singles:
         s.run_steps(args.warmup, dt_next)
     torch.cuda.synchronize(local)
@@ -446,9 +460,10 @@ def run_batch(args, world, rank, local, pg):
         line = {
             "metric": "cell-updates/s batched grids", "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if form == "fp32" else "f64",
+            "data": "synthetic",
             "config": {"workload": f"batch of {args.grids} 2-D cylindrical HII-region grids", "cells": cells,
-                       "precision": "fp64", "parallelism": f"replicas x{world}",
+                       "precision": form, "parallelism": f"replicas x{world}",
                        "sizes": "nx U[64,256], ny U[64,320], Q log-U[1e47,1e49], alpha U[0,2], rc U[0.005,0.05] pc",
                        "l2": "inputs larger than L2 (no flush)"},
             "gpu_launches": int(launches), "launches_per_step": launches / max(1, args.steps), "clocks": clk,
@@ -733,7 +748,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["hii", "sedov", "batch"], default="hii")
+    ap.add_argument("--workload", choices=["hii", "sedov", "batch", "blister"], default="hii")
+    ap.add_argument("--thermo-queue", type=int, default=0,
+                    help="thermal sub-cycles of cells with at least this many run through the work queue (0: off)")
     ap.add_argument("--grids", type=int, default=256, help="grids of the batch workload")
     ap.add_argument("--fp32-contrast", type=float, default=None,
                     help="pressure ratio above which the FP32 form updates a hydro cell in FP64 (library default 1e3)")

@@ -67,3 +67,29 @@ def test_batch_step_graphs_keep_results_bitwise():
     for a, c in zip(*out):
         for k in ("U", "Q", "R", "T"):
             assert np.array_equal(getattr(a, k), getattr(c, k)), k
+
+
+def test_fp32_form_batch_against_fp64_single_grids():
+    """A batch of 2-D grids in the FP32 form (FP32 hydro pass over all grids
+    in one launch per sub-step; FP64 radiation, cooling and time step) against
+    each grid stepped alone in the FP64 form: density and pressure relative
+    L1 within 1e-4 per grid, I-front rows within 0.5 cell."""
+    cases = workloads.blister_batch(G=4, seed=5, nx_range=(40, 72), ny_range=(40, 80))
+    steps = 20
+    ref = []
+    for tp, ic in cases:
+        t = torch_b200.Torch(tp, ic)
+        t.run_steps(steps, 1e300)
+        ref.append(t.state())
+        t.close()
+    grids = [torch_b200.Torch(tp, ic, precision=torch_b200.PRECISION_FP32) for tp, ic in cases]
+    b = torch_b200.Batch(grids)
+    b.run_steps(steps, 1e300)
+    b.close()
+    for (tp, ic), g, r in zip(cases, grids, ref):
+        s = g.state()
+        g.close()
+        ed = common.rel_l1(s.U[0], r.U[0])
+        ep = common.rel_l1(s.Q[1], r.Q[1])
+        print(f"grid {ic.ncells[:2]}: density {ed:.2e} pressure {ep:.2e}")
+        assert ed <= 1e-4 and ep <= 1e-4

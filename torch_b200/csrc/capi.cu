@@ -77,6 +77,7 @@ struct trg_ctx {
 	// per-grid scalar kernels (dt, time) run on this many threads: 1, or the
 	// number of grids of a batch
 	int nscalar = 1;
+	int batch_tiles = 0;  // batch context, FP32 form: CTA tiles of the hydro pass
 	float* U32 = nullptr;
 	float* U32s = nullptr;
 	unsigned char* mlp_img = nullptr;
@@ -417,6 +418,17 @@ void sub_step(trg_ctx* c, double h, bool hasCalculatedHeatFlux, int comp) {
 	}
 	switch (comp) {
 	case COMP_HYDRO:
+		if (c->mixed && c->P.batch) {
+			// FP32 hydro pass over every grid of the batch, U into U1, then back
+			cudaEvent_t ea = nullptr, eb = nullptr;
+			if (c->profiling) { ea = pool_event(c); eb = pool_event(c); cudaEventRecord(ea, c->stream); }
+			launch_hydro_substep_fp32_batch(c->P, c->P.batch, c->batch_tiles, h, c->stream);
+			if (c->profiling) { cudaEventRecord(eb, c->stream); c->recs.push_back({"k_hydro_stage_fp32", ea, eb}); }
+			c->launches += 2;
+			c->q_fresh = true;
+			c->colden_valid = false;
+			break;
+		}
 		if (c->mixed) {
 			// FP32 hydro pass on the FP64 state, into U1, then swap
 			cudaEvent_t ea = nullptr, eb = nullptr;
@@ -1299,6 +1311,7 @@ struct trg_batch {
 	};
 	StepGraph step_graph[3][2][2];  // [position][Q up to date][column densities up to date]
 	bool step_graphs = true;
+	int ntiles = 0;  // FP32 form: CTA tiles of the batch's hydro pass
 };
 
 namespace {
@@ -1354,7 +1367,12 @@ int trg_batch_create(trg_ctx* const* grids, int G, trg_batch** out) {
 	for (int g = 0; g < G; ++g) {
 		trg_ctx* c = grids[g];
 		if (!c) return TRG_ERR_ARG;
-		if (c->fp32 || c->mixed) return set_error(c, TRG_ERR_ARG, "trg_batch_create: batches run the FP64 form");
+		if (c->fp32)
+			return set_error(c, TRG_ERR_ARG, "trg_batch_create: batches run radiation-hydro grids (FP64 or FP32 form)");
+		if (c->mixed != grids[0]->mixed)
+			return set_error(c, TRG_ERR_ARG, "trg_batch_create: grids of a batch share one precision form");
+		if (c->mixed && c->P.nd != 2)
+			return set_error(c, TRG_ERR_ARG, "trg_batch_create: FP32-form batches take 2-D grids");
 		if (c->P.N > (long long)BATCH_CELL_MASK + 1)
 			return set_error(c, TRG_ERR_ARG, "trg_batch_create: a batched grid holds at most 4194304 cells");
 		if (c->steps != 0 || !c->first_time)
@@ -1382,7 +1400,8 @@ int trg_batch_create(trg_ctx* const* grids, int G, trg_batch** out) {
 	v->hs.nactive = grids[0]->hs.nactive;
 	for (int i = 0; i < 3; ++i) v->hs.active[i] = grids[0]->hs.active[i];
 	v->nscalar = G;
-	v->fastk = false;
+	v->fastk = false;  // batches run the exact build's radiation and cooling kernels (batch dispatch)
+	v->mixed = grids[0]->mixed;
 	v->dt_hist_cap = 0;
 	// offsets of the padded cell and face ranges
 	std::vector<long long> cell_off(G + 1, 0), face_off[3], first_cell(G, -1);
@@ -1408,6 +1427,7 @@ int trg_batch_create(trg_ctx* const* grids, int G, trg_batch** out) {
 		Ss[g].err = v->S.err;
 		Ss[g].stats = v->S.stats;
 		Ss[g].cons_part = nullptr;
+		Ss[g].fb_flag = nullptr;  // FP32-form batches have no FP64 fallback pass
 		Ss[g].thq = nullptr;  // batches run the sub-cycles in place
 	}
 	// batched sweeps and wind list
@@ -1435,6 +1455,20 @@ int trg_batch_create(trg_ctx* const* grids, int G, trg_batch** out) {
 	tab.cell_off = dcell;
 	for (int d = 0; d < 3; ++d) tab.face_off[d] = dface[d];
 	tab.first_cell = dfirst;
+	tab.tiles = nullptr;
+	tab.ntiles = 0;
+	if (v->mixed) {
+		std::vector<BatchTile> tiles;
+		for (int g = 0; g < G; ++g)
+			for (int ty = 0; ty < (grids[g]->P.ny + 7) / 8; ++ty)
+				for (int tx = 0; tx < (grids[g]->P.nx + 31) / 32; ++tx) tiles.push_back({g, tx, ty, 0});
+		BatchTile* dtiles = nullptr;
+		if ((rc = upload(v, &dtiles, tiles))) return bail(rc);
+		tab.tiles = dtiles;
+		tab.ntiles = (int)tiles.size();
+		b->ntiles = tab.ntiles;
+		v->batch_tiles = tab.ntiles;
+	}
 	if ((rc = upload(v, &dtab, std::vector<BatchTable>(1, tab)))) return bail(rc);
 	v->P.batch = dtab;
 	v->P.N = cell_off[G];

@@ -709,10 +709,12 @@ __device__ __forceinline__ void face_flux(int rs_rt, const Prim& L, const Prim& 
 // LIM / RS: limiter and Riemann solver fixed at compile time (-1: chosen at run time).
 // tmap / use_tma: the tensor map of the FP64 state Uq for the TMA plane
 // staging (use_tma = 0: per-cell cp.async staging everywhere).
+// The body runs the CTA's tile (bx, by, bz) of one grid (P, S): the kernel's
+// own block index for a single grid, an entry of the tile table for a batch.
 template <int STAGE, typename TS, int LIM, int RS>
-__global__ void __launch_bounds__(BX* BY, 2)
-    k_hydro_stage_fp32(Params P, State S, const TS* __restrict__ Uq, const TS* Ubase, TS* Uout, double hfac,
-                       int zchunk, const __grid_constant__ CUtensorMap tmap, int use_tma) {
+__device__ __forceinline__ void hydro_stage_body(const Params& P, const State& S, const TS* __restrict__ Uq,
+                                                 const TS* Ubase, TS* Uout, double hfac, int zchunk,
+                                                 const CUtensorMap* tmap, int use_tma, int bx, int by, int bz) {
 	extern __shared__ __align__(128) unsigned char smem_raw[];
 	SmemQ& s = *reinterpret_cast<SmemQ*>(smem_raw);
 	float4* v8 = reinterpret_cast<float4*>(smem_raw + sizeof(SmemQ));
@@ -731,8 +733,8 @@ __global__ void __launch_bounds__(BX* BY, 2)
 	uint64_t* tbar = reinterpret_cast<uint64_t*>(smem_raw + hydro_stage_raw_offset() + sizeof(double) * 7 * SX * SY);
 	const int tx = threadIdx.x % BX, ty = threadIdx.x / BX;
 	const int lx = tx + HALO, ly = ty + HALO;
-	const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY;
-	const int z0 = blockIdx.z * zchunk;
+	const int x0 = bx * BX, y0 = by * BY;
+	const int z0 = bz * zchunk;
 	const int nd = P.nd;
 	const int z1 = nd > 2 ? min(z0 + zchunk, P.nz) : 1;
 	const float gamma = (float)P.gamma;
@@ -817,7 +819,7 @@ __global__ void __launch_bounds__(BX* BY, 2)
 			if (tma) {
 				if (threadIdx.x == 0) {
 					int zc, zside;
-					tma_plane(&tmap, raw, tbar, x0 - HALO, y0 - HALO, plane_src(P, z + 3, zc, zside));
+					tma_plane(tmap, raw, tbar, x0 - HALO, y0 - HALO, plane_src(P, z + 3, zc, zside));
 				}
 			} else {
 				plane_fetch(P, Uq, raw, smap, z + 3);
@@ -1022,6 +1024,53 @@ __global__ void __launch_bounds__(BX* BY, 2)
 			atomicMin(&slots[0], (unsigned long long)__double_as_longlong(tmin));
 		}
 	}
+}
+
+template <int STAGE, typename TS, int LIM, int RS>
+__global__ void __launch_bounds__(BX* BY, 2)
+    k_hydro_stage_fp32(Params P, State S, const TS* __restrict__ Uq, const TS* Ubase, TS* Uout, double hfac,
+                       int zchunk, const __grid_constant__ CUtensorMap tmap, int use_tma) {
+	hydro_stage_body<STAGE, TS, LIM, RS>(P, S, Uq, Ubase, Uout, hfac, zchunk, &tmap, use_tma, blockIdx.x, blockIdx.y,
+	                                     blockIdx.z);
+}
+
+// Hydro sub-step of the FP32 form on the FP64 states of a batch of 2-D grids:
+// one CTA per entry (grid, tile x, tile y) of the batch's tile table; each
+// grid's U into its U1.
+template <int LIM, int RS>
+__global__ void __launch_bounds__(BX* BY, 2) k_hydro_substep_fp32_batch(const BatchTable* __restrict__ B, double hfac) {
+	const BatchTile t = B->tiles[blockIdx.x];
+	const Params& P = B->P[t.g];
+	const State& S = B->S[t.g];
+	hydro_stage_body<1, double, LIM, RS>(P, S, S.U, S.U, S.U1, hfac, 1, nullptr, 0, t.tx, t.ty, 0);
+}
+// Every grid's U1 into its U (the batch keeps each grid's U where its own
+// context has it).
+__global__ void __launch_bounds__(256) k_batch_u1_to_u(Params Pv) {
+	const BatchTable& B = *Pv.batch;
+	const long long pos = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
+	const long long id = pos - B.cell_off[g];
+	const Params& P = B.P[g];
+	if (id >= P.N) return;
+	const State& S = B.S[g];
+#pragma unroll
+	for (int f = 0; f < 7; ++f) S.U[f * P.N + id] = S.U1[f * P.N + id];
+}
+
+void launch_hydro_substep_fp32_batch(const Params& Pv, const BatchTable* B, int ntiles, double h, cudaStream_t stream) {
+	const size_t smem = hydro_stage_fp32_smem();
+	const bool fast = Pv.limiter == 6 && Pv.riemann == RS_ROTATED;
+	if (fast) {
+		cudaFuncSetAttribute(k_hydro_substep_fp32_batch<6, RS_ROTATED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                     (int)smem);
+		k_hydro_substep_fp32_batch<6, RS_ROTATED><<<ntiles, BX * BY, smem, stream>>>(B, h);
+	} else {
+		cudaFuncSetAttribute(k_hydro_substep_fp32_batch<-1, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                     (int)smem);
+		k_hydro_substep_fp32_batch<-1, -1><<<ntiles, BX * BY, smem, stream>>>(B, h);
+	}
+	k_batch_u1_to_u<<<(unsigned)((Pv.N + 255) / 256), 256, 0, stream>>>(Pv);
 }
 
 size_t hydro_stage_fp32_smem() {

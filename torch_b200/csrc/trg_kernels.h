@@ -55,6 +55,9 @@ size_t hydro_stage_fp32_smem();
 void launch_hydro_substep_fp32(const Params& P, const State& S, const double* U, double* Uout, double h, int zchunk,
                                cudaStream_t stream);
 __global__ void k_f64_to_f32(Params P, const double* a, float* b);
+// FP32 form of a batch of 2-D grids: the hydro sub-step of every grid (U -> U1,
+// then U1 copied back to U)
+void launch_hydro_substep_fp32_batch(const Params& Pv, const BatchTable* B, int ntiles, double h, cudaStream_t stream);
 // global FP64 mass and energy sums (conservation.cu): block partials of a
 // state, and the fold of the partials (also those of k_dt_reduce_fp64) into
 // out[0] = sum(rho V), out[1] = sum(E V)

@@ -192,6 +192,12 @@ struct BatchTable {
 	const long long* cell_off;   // [G + 1]
 	const long long* face_off[3];  // [G + 1] per dimension
 	const long long* first_cell;   // [G] first non-wind cell in causal order
+	// FP32 form (2-D grids): the CTA tiles of all grids' FP32 hydro pass
+	const struct BatchTile* tiles;
+	int ntiles;
+};
+struct BatchTile {
+	int g, tx, ty, pad;  // grid, tile index along x and y
 };
 
 }  // namespace trg
