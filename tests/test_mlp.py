@@ -196,32 +196,38 @@ def test_learned_start_on_hii_region():
 
 @pytest.mark.gpu
 def test_learned_start_gain_after_training_at_scale():
-    """The gain the trained network gives: 128^3 HII region, FP32 form.  The
-    plain solve records about a million front-cell solves over 200 steps,
-    the network trains on them on the GPU, then the same 16 steps run from
-    the same saved state with and without it.  The network must cut the
-    Picard iterations per front cell (every rejected prediction costs one
-    extra iteration, so this is a net gain), and the I-front and the state
-    stay with the plain run's."""
-    n = 128
-    tp, ic = workloads.hii_region(n=n, seed=6)
+    """The gain the trained network gives on the 256^3 HII region (lognormal
+    cloud, seed 12345, 2 pc box), FP32 form: the plain solve records front-cell
+    solves in 10-step blocks until 10^7 records (or 400 steps), the network
+    trains on them on the GPU (30 epochs), then the same 8 steps run from the
+    same saved state with and without it.  The network must cut the Picard
+    iterations per front cell (a rejected prediction costs one extra
+    iteration, so this is a net gain), and the I-front and the state stay with
+    the plain run's.  (On the same cloud at 128^3, cells twice as large, the
+    plain solve already needs fewer iterations and the network gains nothing.)"""
+    n = 256
+    tp, ic = workloads.hii_region(n=n, seed=12345)
     t = torch_b200.Torch(tp, ic, precision=torch_b200.PRECISION_FP32)
-    t.harvest(1 << 21)
-    t.run_steps(200)
+    t.harvest(10_000_000)
+    steps = 0
+    while steps < 400 and t.harvest_read(count_only=True) < 10_000_000:
+        t.run_steps(10)
+        steps += 10
     rec, total = t.harvest_read()
     t.harvest(0)
     blob = t.checkpoint()
-    print("records", total)
-    assert total > 200000
-    m = torch_b200.Mlp(seed=7)
-    hist = m.train(rec, epochs=30, batch=8192, lr=2e-3, seed=8)
+    print("records", total, "harvest steps", steps)
+    assert total > 1_000_000
+    m = torch_b200.Mlp(seed=11)
+    hist = m.train(rec, epochs=30, batch=8192, lr=2e-3, seed=12)
+    del rec
     print("training loss", hist[0], hist[-1])
     runs = {}
     for name, net in (("plain", None), ("learned", m)):
         t.restore(blob)
         t.learned_start(net)
         t.stats_enable(True)
-        t.run_steps(16)
+        t.run_steps(8)
         runs[name] = (t.stats(reset=True), t.state())
         t.stats_enable(False)
     t.learned_start(None)
