@@ -95,7 +95,15 @@ def _load(portable_math: bool = False):
         _lib.orc_causal_order.argtypes = [C.c_void_p, C.c_void_p, C.c_long]
         _lib.orc_cell_volumes.restype = C.c_long
         _lib.orc_cell_volumes.argtypes = [C.c_void_p, C.c_void_p, C.c_long]
+        _lib.orc_set_libm_noise.argtypes = [C.c_double]
     return _libs[portable_math]
+
+
+def set_libm_noise(fraction: float) -> None:
+    """Test hook of the host-libm oracle: from now on a fixed, input-determined
+    fraction of its exp/log/log10/pow results is moved by one ulp (0: off).
+    Process-wide: it applies to every host-libm Oracle of this process."""
+    _load(False).orc_set_libm_noise(float(fraction))
 
 
 def params_struct(tp, side_length: Optional[float] = None, ncells=None) -> OrcParams:
@@ -150,8 +158,9 @@ class Oracle:
     """The C restatement, driven like Torch::run (one context per run).
 
     portable_math=False: host libm, bit-exact with the reference build.
-    portable_math=True: the IEEE-only exp/log/log10/pow that the FP64 GPU
-    kernels use, i.e. the GPU's bit-exact CPU twin."""
+    portable_math=True: the exp/log/log10/pow of torch_b200/csrc/trg_math.h
+    (correctly rounded, IEEE operations only) that the FP64 GPU kernels use,
+    i.e. the GPU's bit-exact CPU twin."""
 
     def __init__(self, tp, ic, portable_math: bool = False):
         lib = _load(portable_math)

@@ -21,11 +21,31 @@
 #define m_log trg_log
 #define m_log10 trg_log10
 #define m_pow trg_pow
+void orc_set_libm_noise(double fraction) { (void)fraction; }
 #else
-#define m_exp exp
-#define m_log log
-#define m_log10 log10
-#define m_pow pow
+/* Host libm, with an optional test hook (orc_set_libm_noise): a fixed,
+ * input-determined fraction of the results moved by one ulp, to show how the
+ * step amplifies single-ulp differences between math libraries. */
+#include <stdint.h>
+#include <string.h>
+static double g_libm_noise = 0.0;
+void orc_set_libm_noise(double fraction) { g_libm_noise = fraction; }
+static double libm_noise(double x, double salt, double r) {
+	if (g_libm_noise <= 0.0 || !isfinite(r) || r == 0.0) return r;
+	uint64_t b;
+	double k = x + salt;
+	memcpy(&b, &k, sizeof b);
+	b *= 0xff51afd7ed558ccdULL; /* 64-bit mixing (multiply, xor-shift) */
+	b ^= b >> 33;
+	b *= 0xc4ceb9fe1a85ec53ULL;
+	b ^= b >> 33;
+	if ((double)(b >> 11) * 0x1p-53 >= g_libm_noise) return r;
+	return nextafter(r, (b & 1) ? INFINITY : -INFINITY);
+}
+static double m_exp(double x) { return libm_noise(x, 0.0, exp(x)); }
+static double m_log(double x) { return libm_noise(x, 1.0, log(x)); }
+static double m_log10(double x) { return libm_noise(x, 2.0, log10(x)); }
+static double m_pow(double x, double y) { return libm_noise(x * 1.000001 + y, 3.0, pow(x, y)); }
 #endif
 #include <stdio.h>
 #include <stdlib.h>

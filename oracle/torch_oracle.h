@@ -74,6 +74,9 @@ double orc_dt_max(const orc_ctx* c);
 long orc_ncells(const orc_ctx* c);
 const char* orc_last_error(const orc_ctx* c);
 void orc_destroy(orc_ctx* c);
+/* Test hook of the host-libm build: moves a fixed, input-determined fraction
+ * of the step's exp/log/log10/pow results by one ulp (0: off). */
+void orc_set_libm_noise(double fraction);
 
 /* Order in which the reference visits interior cells in its causal sweeps
  * (Grid::buildCausal, Grid.cpp:568-574): writes up to cap flat indices and

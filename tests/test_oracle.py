@@ -96,23 +96,55 @@ def test_portable_math_oracle_matches_golden_to_1e10():
         assert max(errs.values()) <= 1e-10, (name, max(errs.values()))
 
 
+def test_portable_math_twin_matches_reference_libm_for_100_steps():
+    """The oracle built with trg_math.h (the FP64 kernels' correctly rounded
+    exp/log/pow and fdlibm-reduction log10; the GPU's bit-exact twin) against
+    the oracle on the host glibc (bit-exact with the reference build), 100
+    steps of the shipped config 1 and 100 steps of a 24^3 HII region: every
+    conserved and radiation field within relative L1 1e-10 - although the
+    two libraries still differ in ~1e-3 of the results (where glibc is not
+    correctly rounded, tests/test_math.py)."""
+    from torch_b200 import workloads
+    for (tp, ic), nd in ((workloads.blister(), 2), (workloads.hii_region(n=24, seed=9), 3)):
+        a = oracle.Oracle(tp, ic)
+        b = oracle.Oracle(tp, ic, portable_math=True)
+        for _ in range(100):
+            a.full_step()
+            b.full_step()
+        sa, sb = a.state(), b.state()
+        errs = [common.rel_l1(sb.U[i], sa.U[i]) for i in range(4 + nd)]
+        errs += [common.rel_l1(sb.R[i], sa.R[i]) for i in range(5)]
+        print("max relative L1 after 100 steps:", max(errs))
+        assert max(errs) <= 1e-10
+
+
 def test_reference_algorithm_amplifies_ulp_noise():
-    """Two oracle builds that differ only in the math library (glibc versus the
-    IEEE-only trg_math.h, both within 2 ulp) agree to 1e-10 for 40 steps of
-    config 1 and then drift apart: the reference's step is chaotic at the ulp
-    level, which bounds FP64 agreement between any two libm implementations."""
+    """The reference's step amplifies single-ulp libm differences: moving 1%
+    of the host libm's exp/log/log10/pow results by one ulp leaves config 1
+    unchanged at 1e-10 for 40 steps, then moves it by more than 1e-8 by step
+    100 (a thermal sub-cycle count is a ceil(), the implicit ionisation
+    solve stops on a relative-change test).  This is why the FP64 form's
+    functions must round like the host libm almost everywhere."""
     from torch_b200 import workloads
     tp, ic = workloads.blister()
     a = oracle.Oracle(tp, ic)
-    b = oracle.Oracle(tp, ic, portable_math=True)
-    for _ in range(40):
-        a.full_step()
-        b.full_step()
-    assert common.rel_l1(b.state().U[1], a.state().U[1]) <= 1e-10
-    for _ in range(60):
-        a.full_step()
-        b.full_step()
-    assert common.rel_l1(b.state().U[1], a.state().U[1]) > 1e-8
+    oracle.set_libm_noise(0.01)
+    try:
+        b = oracle.Oracle(tp, ic)
+        # the noise is process-wide: step the two alternately with it off / on
+        def step_pair():
+            oracle.set_libm_noise(0.0)
+            a.full_step()
+            oracle.set_libm_noise(0.01)
+            b.full_step()
+        for _ in range(40):
+            step_pair()
+        assert common.rel_l1(b.state().U[1], a.state().U[1]) <= 1e-10
+        for _ in range(60):
+            step_pair()
+        assert common.rel_l1(b.state().U[1], a.state().U[1]) > 1e-8
+    finally:
+        oracle.set_libm_noise(0.0)
 
 
 def test_exact_sum_checker_rounds_once():
