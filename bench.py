@@ -379,6 +379,7 @@ def run_batch(args, world, rank, local, pg):
     clk = clocks.stop()
     ms = max_over_ranks(pg, ev0.elapsed_time(ev1), local)
     launches = b.kernel_launches() - launches0
+    learned = time_batch_learned(args, b, cases, prec, cells, world, local, pg, dt_next) if args.learned else None
     # per-kernel times from an event-bracketed pass of the same number of
     # steps after the timed region (per-launch events would keep the timed
     # steps from being replayed as graphs)
@@ -470,20 +471,90 @@ def run_batch(args, world, rank, local, pg):
             "kernels": prof,
             "unbatched": {"value": ucells * args.steps / wall, "grids": len(sample),
                           "note": "the first grids stepped one context after another, host wall clock"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "learned": learned,
         }
         print(json.dumps(line), flush=True)
     return 0
 
 
-def time_learned(args, sim32, N, world, local, pg):
+def time_batch_learned(args, b, cases, prec, cells, world, local, pg, dt_next):
+    """The batch with the learned starting iterate: a network trained on the
+    front-cell solves of the first four grids, each stepped alone for 40
+    steps, then K batch steps timed with it and K more without it (the plain
+    batch from nearly the same state)."""
+    import torch
+    import torch_b200
+    recs = []
+    for tp, ic in cases[:4]:
+        t = torch_b200.Torch(tp, ic, precision=prec, device=local)
+        t.harvest(1 << 20)
+        t.run_steps(40, dt_next)
+        r, _ = t.harvest_read()
+        recs.append(r)
+        t.close()
+    recs = np.concatenate(recs)
+    t0 = time.perf_counter()
+    net = torch_b200.Mlp(device=local, seed=11)
+    net.train(recs, epochs=30, batch=4096, lr=2e-3, seed=12)
+    torch.cuda.synchronize(local)
+    train_s = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(b.stream_handle(), device=f"cuda:{local}")
+
+    def timed():
+        b.run_steps(1, dt_next)  # captures this form's step graphs
+        barrier(pg)
+        torch.cuda.synchronize(local)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.enqueue_steps(args.steps, dt_next)
+        e1.record(stream)
+        b.synchronize()
+        torch.cuda.synchronize(local)
+        barrier(pg)
+        return max_over_ranks(pg, e0.elapsed_time(e1), local)
+
+    b.learned_start(net)
+    ms = timed()
+    b.learned_start(None)
+    ms_plain = timed()
+    net.close()
+    return {"value": cells * args.steps * world / (ms / 1e3), "ms_per_step": ms / args.steps,
+            "plain_same_state": {"value": cells * args.steps * world / (ms_plain / 1e3),
+                                 "ms_per_step": ms_plain / args.steps},
+            "training": {"records": int(len(recs)), "grids": 4, "steps_each": 40, "epochs": 30,
+                         "seconds": train_s}}
+
+
+def timed_form(sim, args, local, pg, dt_next):
+    """K steps of a context on its own stream, timed with CUDA events on that
+    stream after one untimed step (which captures the sweep graphs), max over
+    ranks (ms)."""
+    import torch
+    stream = torch.cuda.ExternalStream(sim.stream_handle(), device=f"cuda:{local}")
+    sim.run_steps(1)
+    barrier(pg)
+    torch.cuda.synchronize(local)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    sim.enqueue_steps(args.steps, dt_next)
+    ev1.record(stream)
+    sim.synchronize()
+    torch.cuda.synchronize(local)
+    barrier(pg)
+    return max_over_ranks(pg, ev0.elapsed_time(ev1), local)
+
+
+def time_learned(args, sim32, N, world, local, pg, sim64=None):
     """FP32 form with the learned starting iterate, after the plain FP32 timing:
     further FP32 steps record the plain solve's front cells until
     --learned-records records (or 400 steps), a network is trained on them on
     the GPU, then K steps are timed with it and K more without it (the plain
     form from nearly the same state: the harvest steps moved the front).
-    Solver counters of two further steps with and without the network
-    follow."""
+    With sim64 (the FP64 form's context), the state the learned timing starts
+    from is also restored into the FP64 form and K of its steps are timed, so
+    that the learned FP32 form and the plain FP64 form are compared on the
+    same state.  Solver counters of two further steps with and without the
+    network follow."""
     import torch
     import torch_b200
     sim32.harvest(int(args.learned_records))
@@ -501,25 +572,21 @@ def time_learned(args, sim32, N, world, local, pg):
     torch.cuda.synchronize(local)
     train_s = time.perf_counter() - t0
     dt_next = sim32.dt_max
-    stream = torch.cuda.ExternalStream(sim32.stream_handle(), device=f"cuda:{local}")
 
     def timed():
-        sim32.run_steps(1)  # captures the sweep graphs of this form
-        barrier(pg)
-        torch.cuda.synchronize(local)
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        sim32.enqueue_steps(args.steps, dt_next)
-        ev1.record(stream)
-        sim32.synchronize()
-        torch.cuda.synchronize(local)
-        barrier(pg)
-        return max_over_ranks(pg, ev0.elapsed_time(ev1), local)
+        return timed_form(sim32, args, local, pg, dt_next)
 
+    blob = sim32.checkpoint() if sim64 is not None else None
     sim32.learned_start(net)
     ms = timed()
     sim32.learned_start(None)
     ms_plain = timed()
+    fp64_same = None
+    if sim64 is not None:
+        sim64.restore(blob)
+        del blob
+        ms64 = timed_form(sim64, args, local, pg, dt_next)
+        fp64_same = {"value": N * args.steps * world / (ms64 / 1e3), "ms_per_step": ms64 / args.steps}
     sim32.stats_enable(True)
     sim32.learned_start(net)
     sim32.run_steps(2)
@@ -532,6 +599,7 @@ def time_learned(args, sim32, N, world, local, pg):
     return {"value": N * args.steps * world / (ms / 1e3), "ms_per_step": ms / args.steps,
             "plain_fp32_same_state": {"value": N * args.steps * world / (ms_plain / 1e3),
                                       "ms_per_step": ms_plain / args.steps},
+            "plain_fp64_same_state": fp64_same,
             "training": {"records": int(len(recs)), "harvest_steps": harvest_steps, "epochs": 30,
                          "seconds": train_s, "loss_first_last": [float(hist[0]), float(hist[-1])]},
             "front_cells": st["front_cells"], "learned_cells": st["learned_cells"],
@@ -649,7 +717,7 @@ def run_ours(args, world, rank, local, pg):
         error["against"] = "plain FP64 form on the GPU (bit-exact twin of the FP64 oracle)"
     learned = None
     if args.learned and head == "fp32" and tp.radiation_on:
-        learned = time_learned(args, sims["fp32"], N, world, local, pg)
+        learned = time_learned(args, sims["fp32"], N, world, local, pg, sims.get("fp64"))
     for form, s in sims.items():
         if form != head:
             s.close()

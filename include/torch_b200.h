@@ -230,7 +230,10 @@ int trg_heating(trg_ctx* c, double* H);
  * context created with the same parameters and grid; stepping on is
  * bit-identical to the run that was saved.  The blob holds the device layout
  * of R and T and a format version (2); a blob of another version is rejected
- * with TRG_ERR_ARG. */
+ * with TRG_ERR_ARG.  The FP64 form and the FP32 form of a radiation or
+ * cooling run keep the same FP64 state, so either form continues the other's
+ * blob (switching precision mid-run); the hydro-only FP32 form's state is
+ * FP32 and its blobs restore only into that form. */
 long long trg_checkpoint_bytes(const trg_ctx* c);
 int trg_checkpoint_save(trg_ctx* c, void* buf, long long bytes);
 int trg_checkpoint_load(trg_ctx* c, const void* buf, long long bytes);
@@ -271,13 +274,15 @@ int trg_stats(trg_ctx* c, unsigned long long* out, int reset);
  * trg_mlp_gradient returns the summed gradient and loss of one pass over the
  * records without updating, for gradient checks.
  *
- * trg_learned_start(ctx, m) makes ctx's radiation sweeps start the Picard
- * iteration of the front cells (tau < 20, x_HII < 0.99) that m predicts to
- * need more than two plain iterations from m's predicted <x>: the prediction
- * is accepted when the first iteration from it passes the solver's own
- * convergence test (its residual is below the solver tolerance), else the
- * plain iteration restarts from x_HII.  m = NULL restores the plain solve.  m must live on ctx's device; its parameters are
- * copied, so later training does not change ctx until the next call.
+ * trg_learned_start(ctx, m) makes the front cells (tau < 20, x_HII < 0.99)
+ * of ctx's radiation sweeps that m predicts to need more than two plain
+ * iterations try m's predicted <x> beside their plain first Picard iteration:
+ * the prediction's iteration is accepted when it passes the solver's own
+ * convergence test (its residual is below the solver tolerance) and the
+ * plain one does not; otherwise the plain iteration goes on unchanged.
+ * m = NULL restores the plain solve.  m must live on ctx's device; its
+ * parameters are copied, so later training does not change ctx until the
+ * next call.
  * trg_harvest(ctx, capacity) makes the plain solve record front cells (at
  * most `capacity` records; 0 stops and frees); trg_harvest_read copies up to
  * `max` records out and returns how many were recorded in total. */
@@ -319,6 +324,12 @@ int trg_batch_enqueue_steps(trg_batch* b, int nsteps, double dt_next_checkpoint)
  * operator split's rotating component order (bitwise the same results as the
  * launches themselves, which `on` = 0 restores). */
 int trg_batch_step_graphs(trg_batch* b, int on);
+/* The learned starting iterate (trg_learned_start) for every grid of a batch
+ * of radiation grids (implicit scheme): before each radiation sweep one
+ * launch lists the candidate front cells of all grids and one runs the
+ * network over them; m = NULL restores the plain solve.  A batch with the
+ * network steps every grid as trg_learned_start steps it alone. */
+int trg_batch_learned_start(trg_batch* b, const trg_mlp* m);
 /* The conserved state U [7][N_g] of grid g of the batch, copied in or out on
  * the batch's stream, ordered with its steps (asynchronous with respect to
  * the host: pinned host buffers, and trg_batch_synchronize before reading a

@@ -69,6 +69,47 @@ def test_batch_step_graphs_keep_results_bitwise():
             assert np.array_equal(getattr(a, k), getattr(c, k)), k
 
 
+def test_batch_learned_start_matches_single_grids_bitwise():
+    """The learned starting iterate in a batch (one candidate launch and one
+    network launch per radiation sweep for all grids, predictions in per-cell
+    slots) steps every grid bit-for-bit as the same grid with the same network
+    stepped alone (candidates in sweep order); the network (trained on the
+    front-cell solves of one grid stepped alone) changes the result, so the
+    predictions are used."""
+    cases = workloads.blister_batch(G=4, seed=11, nx_range=(24, 48), ny_range=(24, 56))
+    steps = 20
+    t = torch_b200.Torch(*cases[0])
+    t.harvest(1 << 20)
+    t.run_steps(40, 1e300)
+    rec, total = t.harvest_read()
+    t.close()
+    assert total > 100
+    m = torch_b200.Mlp(seed=3)
+    m.train(rec, epochs=20, batch=1024, lr=2e-3, seed=5)
+    singles, plain = [], []
+    for tp, ic in cases:
+        for net, out in ((m, singles), (None, plain)):
+            t = torch_b200.Torch(tp, ic)
+            t.learned_start(net)
+            t.run_steps(steps, 1e300)
+            out.append(t.state())
+            t.close()
+    grids = [torch_b200.Torch(tp, ic) for tp, ic in cases]
+    b = torch_b200.Batch(grids)
+    b.learned_start(m)
+    b.run_steps(steps, 1e300)
+    b.synchronize()
+    for g, ref in zip(grids, singles):
+        got = g.state()
+        for k, v in fields(ref).items():
+            assert np.array_equal(fields(got)[k], v), k
+    b.close()
+    for g in grids:
+        g.close()
+    m.close()
+    assert any(not np.array_equal(a.R, p.R) for a, p in zip(singles, plain))
+
+
 def pressure(U, gamma):
     """P = (E - |m|^2 / (2 rho)) (gamma - 1) of a 2-D conserved state."""
     return (U[1] - (U[4] ** 2 + U[5] ** 2) / (2.0 * U[0])) * (gamma - 1.0)

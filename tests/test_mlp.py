@@ -138,11 +138,13 @@ def test_learned_start_on_hii_region():
     """Harvest front-cell solves from the plain method, train on the GPU, then
     run the same steps with the learned start: before each sweep the network
     runs once over the candidate front cells (chosen from the previous
-    sweep's optical depths) and serves those it predicts to be slow; a
-    prediction whose first Picard iteration passes the convergence test is
-    accepted, any other restarts the plain iteration.  Reports the iterations per front cell with and without the
-    network and how far each moves the state from the plain run, beside a
-    start one solver tolerance off; the I-front stays within 0.5 cell."""
+    sweep's optical depths) and serves those it predicts to be slow; beside
+    the plain first Picard iteration a served cell runs one from the
+    prediction, which is accepted when it passes the convergence test and the
+    plain one does not.  Reports the iterations per front cell with and
+    without the network and how far each moves the state from the plain run,
+    beside a start one solver tolerance off; the I-front stays within 0.5
+    cell."""
     n, steps = 32, 40
     tp, ic = workloads.hii_region(n=n, seed=4)
     plain = torch_b200.Torch(tp, ic)
@@ -201,10 +203,11 @@ def test_learned_start_gain_after_training_at_scale():
     solves in 10-step blocks until 10^7 records (or 400 steps), the network
     trains on them on the GPU (30 epochs), then the same 8 steps run from the
     same saved state with and without it.  The network must cut the Picard
-    iterations per front cell (a rejected prediction costs one extra
-    iteration, so this is a net gain), and the I-front and the state stay with
-    the plain run's.  (On the same cloud at 128^3, cells twice as large, the
-    plain solve already needs fewer iterations and the network gains nothing.)"""
+    iterations per front cell (its prediction is tried beside the plain first
+    iteration, so a rejected one costs no iteration), and the I-front and the
+    state stay with the plain run's.  (On the same cloud at 128^3, cells twice
+    as large, the plain solve already needs fewer iterations and the network
+    gains little.)"""
     n = 256
     tp, ic = workloads.hii_region(n=n, seed=12345)
     t = torch_b200.Torch(tp, ic, precision=torch_b200.PRECISION_FP32)

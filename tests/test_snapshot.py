@@ -83,6 +83,37 @@ def test_checkpoint_restart_is_bitwise(form):
 
 
 @pytest.mark.gpu
+def test_checkpoint_moves_between_fp64_and_fp32_forms():
+    """A radiation-hydro run switches precision mid-run: an FP64-form
+    checkpoint restored into an FP32-form context continues within the FP32
+    form's error of the FP64 run, and that context's checkpoint restored into
+    an FP64-form context holds the same state arrays bit for bit."""
+    from torch_b200 import workloads
+    tp, ic = workloads.hii_region(n=16, seed=3)
+    a = torch_b200.Torch(tp, ic, precision=torch_b200.PRECISION_FP64)
+    a.run_steps(6)
+    blob = a.checkpoint()
+    a.run_steps(6)
+    sa = a.state()
+    a.close()
+    b = torch_b200.Torch(tp, ic, precision=torch_b200.PRECISION_FP32)
+    b.restore(blob)
+    b.run_steps(6)
+    sb = b.state()
+    blob_b = b.checkpoint()
+    b.close()
+    for i in (0, 1, 2):
+        assert common.rel_l1(sb.U[i], sa.U[i]) <= 1e-5, i
+    assert abs(sb.time - sa.time) <= 1e-6 * sa.time  # the forms' CFL steps differ by rounding
+    c = torch_b200.Torch(tp, ic, precision=torch_b200.PRECISION_FP64)
+    c.restore(blob_b)
+    sc = c.state()
+    c.close()
+    for k in ("U", "R", "T"):
+        assert np.array_equal(getattr(sb, k), getattr(sc, k)), k
+
+
+@pytest.mark.gpu
 def test_checkpoint_rejects_other_grid():
     from torch_b200 import workloads
     tp, ic = workloads.hii_region(n=16, seed=3)

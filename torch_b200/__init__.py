@@ -122,6 +122,7 @@ _SIGNATURES = [
     ("trg_batch_run_steps", C.c_int, [C.c_void_p, C.c_int, C.c_double]),
     ("trg_batch_enqueue_steps", C.c_int, [C.c_void_p, C.c_int, C.c_double]),
     ("trg_batch_step_graphs", C.c_int, [C.c_void_p, C.c_int]),
+    ("trg_batch_learned_start", C.c_int, [C.c_void_p, C.c_void_p]),
     ("trg_batch_set_conserved", C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     ("trg_batch_get_conserved", C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     ("trg_batch_synchronize", C.c_int, [C.c_void_p]),
@@ -572,6 +573,11 @@ class Batch:
     def step_graphs(self, on: bool):
         """One captured CUDA graph per timestep (on by default)."""
         self._check(self.lib.trg_batch_step_graphs(self.handle, int(on)))
+
+    def learned_start(self, mlp):
+        """The learned starting iterate for every grid of the batch (an ``Mlp``
+        on the batch's device), or the plain solve again (None)."""
+        self._check(self.lib.trg_batch_learned_start(self.handle, mlp.handle if mlp is not None else None))
 
     def synchronize(self):
         self._check(self.lib.trg_batch_synchronize(self.handle))

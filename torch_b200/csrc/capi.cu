@@ -327,6 +327,8 @@ void rad_shell_launch(trg_ctx* c, const int* cells, int count, double h, bool ov
 	}
 	if (c->P.stats_on || c->S.harvest)
 		LAUNCH_SHELL(KF(k_rad_shell_diag), count, 128, overlap, c->P, c->S, cells, count, h);
+	else if (c->P.batch && c->S.mlp_img)
+		LAUNCH_SHELL(KF(k_rad_shell_fp64_ls), count, 128, overlap, c->P, c->S, cells, count, h);
 	else
 		LAUNCH_SHELL(KF(k_rad_shell_fp64), count, 128, overlap, c->P, c->S, cells, count, h);
 }
@@ -346,6 +348,12 @@ void rad_sweep_direct(trg_ctx* c, double h) {
 			if (c->profiling) { cudaEventRecord(eb, c->stream); c->recs.push_back({"k_learned_infer", ea, eb}); }
 			c->launches++;
 		}
+	} else if (c->P.batch && c->S.mlp_img) {
+		// a batch with a network: candidates of every grid, then the network over them
+		cudaMemsetAsync(c->S.lcand_n, 0, sizeof(unsigned), c->stream);
+		LAUNCH(KF(k_batch_learned_prep), c->P.N, 256, c->P, c->S);
+		KF(k_batch_learned_infer)<<<LCAND_MAX / 128, 128, mlp::INFER_SMEM, c->stream>>>(c->P, c->S, h);
+		c->launches++;
 	}
 	const auto& off = c->hs.off_nonwind;
 	for (size_t s = 0; s + 1 < off.size(); ++s) {
@@ -965,7 +973,11 @@ int trg_checkpoint_load(trg_ctx* c, const void* buf, long long bytes) {
 	memcpy(&h, buf, sizeof(h));
 	if (memcmp(h.magic, "TRGCKPT1", 8) != 0 || h.version != 2)
 		return set_error(c, TRG_ERR_ARG, "trg_checkpoint_load: not a checkpoint of this library");
-	if (h.form != ckpt_form(c) || h.N != c->P.N || h.nx != c->P.nx || h.ny != c->P.ny || h.nz != c->P.nz ||
+	// the FP64 form (0) and the FP32 form on the FP64 state (2) keep the same
+	// state arrays, so either continues the other's checkpoint; the FP32
+	// state of the hydro-only FP32 form (1) is its own
+	const bool same_state = h.form == ckpt_form(c) || (h.form != 1 && ckpt_form(c) != 1);
+	if (!same_state || h.N != c->P.N || h.nx != c->P.nx || h.ny != c->P.ny || h.nz != c->P.nz ||
 	    h.nd != c->P.nd || bytes < trg_checkpoint_bytes(c))
 		return set_error(c, TRG_ERR_ARG, "trg_checkpoint_load: the checkpoint is of another grid or form");
 	CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1312,6 +1324,10 @@ struct trg_batch {
 	StepGraph step_graph[3][2][2];  // [position][Q up to date][column densities up to date]
 	bool step_graphs = true;
 	int ntiles = 0;  // FP32 form: CTA tiles of the batch's hydro pass
+	std::vector<State> Ss;          // the grids' State copies (host), uploaded to dS
+	State* dS = nullptr;
+	std::vector<long long> cell_off;  // padded cell offsets of the grids
+	double* lpred = nullptr;          // learned start: one prediction slot per (padded) cell
 };
 
 namespace {
@@ -1470,6 +1486,9 @@ int trg_batch_create(trg_ctx* const* grids, int G, trg_batch** out) {
 		v->batch_tiles = tab.ntiles;
 	}
 	if ((rc = upload(v, &dtab, std::vector<BatchTable>(1, tab)))) return bail(rc);
+	b->Ss = Ss;
+	b->dS = dS;
+	b->cell_off = cell_off;
 	v->P.batch = dtab;
 	v->P.N = cell_off[G];
 	v->P.stats_on = 0;
@@ -1556,6 +1575,37 @@ void batch_step(trg_batch* b, double dt_next) {
 	enqueue_full_step(v, dt_next);
 }
 }  // namespace
+
+int trg_batch_learned_start(trg_batch* b, const trg_mlp* m) {
+	if (!b) return TRG_ERR_ARG;
+	trg_ctx* v = b->v;
+	trg_ctx* c = v;  // for CUDA_TRY
+	CUDA_TRY(cudaStreamSynchronize(v->stream));
+	if (m) {
+		if (!v->P.radiation_on || !v->P.star_on || v->P.rt_scheme != 0)
+			return set_error(v, TRG_ERR_ARG, "trg_batch_learned_start: the grids have no implicit radiation sweep");
+		int dev = -1;
+		const unsigned char* src = mlp_device_image(m, &dev);
+		if (dev != v->raw.device)
+			return set_error(v, TRG_ERR_ARG, "trg_batch_learned_start: network on another device");
+		if (!v->mlp_img && dalloc(v, &v->mlp_img, mlp::IMG_INFER_BYTES)) return TRG_ERR_OOM;
+		if (!b->lpred && dalloc(v, &b->lpred, v->P.N)) return TRG_ERR_OOM;
+		if (!v->lcand_buf && (dalloc(v, &v->lcand_buf, v->P.N) || dalloc(v, &v->lcand_n_buf, 1))) return TRG_ERR_OOM;
+		CUDA_TRY(cudaMemcpy(v->mlp_img, src, mlp::IMG_INFER_BYTES, cudaMemcpyDeviceToDevice));
+	}
+	for (int g = 0; g < b->G; ++g) {
+		b->Ss[g].mlp_img = m ? v->mlp_img : nullptr;
+		b->Ss[g].lstart = m ? b->lpred + b->cell_off[g] : nullptr;
+	}
+	CUDA_TRY(cudaMemcpy(b->dS, b->Ss.data(), b->Ss.size() * sizeof(State), cudaMemcpyHostToDevice));
+	v->S.mlp_img = m ? v->mlp_img : nullptr;
+	v->S.lstart = m ? b->lpred : nullptr;
+	v->S.lcand = m ? v->lcand_buf : nullptr;
+	v->S.lcand_n = m ? v->lcand_n_buf : nullptr;
+	batch_drop_step_graphs(b);
+	drop_graphs(v);
+	return TRG_OK;
+}
 
 int trg_batch_enqueue_steps(trg_batch* b, int nsteps, double dt_next_checkpoint) {
 	if (!b || nsteps < 0) return TRG_ERR_ARG;

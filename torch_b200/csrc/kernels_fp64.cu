@@ -3,8 +3,9 @@
 // This file is compiled twice.  The exact build (namespace trg::exact, the
 // plain-FP64 form) uses --fmad=false: every kernel reproduces the reference's
 // FP64 arithmetic in the reference's operation order, and exp/log/log10/pow
-// come from trg_math.h (IEEE +-*/ only), which the CPU oracle can share, so
-// that the GPU and CPU runs agree to the last bit.  The fast build
+// come from trg_math.h (correctly rounded, IEEE operations only, so they
+// return the host glibc's results wherever glibc rounds correctly), which the
+// CPU oracle shares, so that the GPU and CPU runs agree to the last bit.  The fast build
 // (trg::fast, -DTRG_FAST_MATH, FMA contraction on) serves the FP32 form, whose
 // radiation, cooling and time-step kernels stay FP64 but need not round like
 // the reference.
@@ -771,11 +772,11 @@ __device__ __forceinline__ double inv_logit10(float l) {
 //
 // Learned start (S.lstart set, LS or DIAG builds): a front cell whose entry of
 // S.lstart holds a prediction (written by k_learned_infer before the sweep)
-// starts its Picard iteration there.  The prediction is accepted when the
-// first iteration from it meets the solver's own convergence test (its
-// residual is below the solver tolerance); otherwise the cell restarts the
-// plain iteration from x_HII, so that a rejected prediction leaves the plain
-// result unchanged.
+// runs one Picard iteration from it beside the plain first iteration from
+// x_HII.  The prediction is accepted when its iteration meets the solver's own
+// convergence test (its residual is below the solver tolerance) and the plain
+// one does not; otherwise the plain iteration goes on as without it, so a
+// rejected prediction leaves the plain result and iteration count unchanged.
 // DIAG: the counters and the training-set recording are compiled in (a
 // lean build without them keeps the sweep's instruction footprint small).
 // SW: the cell's own inputs come from the sweep-ordered arrays (S.sw_rad,
@@ -838,8 +839,9 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 	}
 	double start = q_hii;
 	bool learned = false, used_learned = false;
-	if (SW && (LS || DIAG) && front && S.lstart) {
-		const double st = sw[SW_LSTART * swn];
+	if ((LS || DIAG) && front && S.lstart) {
+		// the prediction slot: in sweep order (single grids), or per cell (batches)
+		const double st = SW ? sw[SW_LSTART * swn] : S.lstart[id];
 		if (st == st) {
 			start = st;
 			learned = used_learned = true;
@@ -855,7 +857,7 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 	} else {
 		double A_pi = 0;
 		double x_new = q_hii;
-		double HII_avg = start;
+		double HII_avg = q_hii;
 		double HII_avg_old;
 		int niter = 0, miter = 0;
 		bool converged = false;
@@ -878,18 +880,33 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 #endif
 			if ((small_step || (HII_avg < 1.0e-5) || A_pi == 0)) converged = true;
 			if (learned) {
-				// the first iteration from the prediction is its residual test:
-				// accept, or restart the plain iteration from x_HII
+				// beside the plain first iteration (from x_HII), one iteration
+				// from the prediction: its residual test is the solver's own
+				// convergence test.  It is taken when the plain first iteration
+				// has not converged and the prediction's has; otherwise it is
+				// dropped and the plain iteration goes on untouched, so the
+				// prediction never costs an iteration.
 				learned = false;
+				double hp = start, xp = q_hii;
+				const double dtau_p = (1.0 - hp) * n_H * P.photoIonXsec * ds;
+				const double A_p = photoionisation_rate_e((1.0 - hp) * n_H, em_tau, dtau_p, shellVol, P.photonRate);
+				doric(dt, hp, xp, A_p, hp * n_H * alphaB, hp * n_H * A_ci);
+#ifdef TRG_FAST_MATH
+				const bool small_p = fabs(hp - start) < 1.0e-3 * fabs(hp);
+#else
+				const bool small_p = fabs((hp - start) / hp) < 1.0e-3;
+#endif
+				const bool take = !converged && (small_p || hp < 1.0e-5 || A_p == 0);
 				if (DIAG && P.stats_on) {
 					stat_add(S.stats, TRG_STAT_LEARNED_CELLS, 1u);
-					stat_add(S.stats, TRG_STAT_LEARNED_ACCEPTED, converged ? 1u : 0u);
+					stat_add(S.stats, TRG_STAT_LEARNED_ACCEPTED, take ? 1u : 0u);
 				}
-				if (converged) break;
-				iters = 1;
-				HII_avg = q_hii;
-				niter = 0;
-				continue;
+				if (take) {
+					HII_avg = hp;
+					x_new = xp;
+					A_pi = A_p;
+					break;
+				}
 			}
 			if (niter > 10005) {
 				miter++;
@@ -1002,6 +1019,39 @@ __global__ void __launch_bounds__(128) k_learned_infer(Params P, State S, const 
 	if (valid && y[2] > 1.0f) S.sw_rad[SW_LSTART * sn + pos] = inv_logit10(logit10(q_hii) + y[0]);
 }
 
+// The network over a batch's candidates (packed (grid, cell) entries): the
+// same inputs as k_learned_infer, each grid's cells read in place (n_H with
+// the radiation sweep's own arithmetic), the prediction into the cell's slot.
+__global__ void __launch_bounds__(128) k_batch_learned_infer(Params Pv, State Sv, double h) {
+#if TRG_BATCHED
+	extern __shared__ __align__(128) unsigned char sm_mlp[];
+	const unsigned n = *Sv.lcand_n;
+	if (n > (unsigned)LCAND_MAX || blockIdx.x * 128u >= n) return;  // uniform over the CTA
+	const BatchTable& B = *Pv.batch;
+	const unsigned t = blockIdx.x * 128u + threadIdx.x;
+	const bool valid = t < n;
+	const int e = valid ? Sv.lcand[t] : 0;
+	const int g = e >> BATCH_CELL_BITS;
+	const long long id = e & BATCH_CELL_MASK;
+	float f[5] = {0, 0, 0, 0, 0}, y[3];
+	double q_hii = 0;
+	if (valid) {
+		const Params& P = B.P[g];
+		const State& S = B.S[g];
+		const double q_den = FLD(S.Q, DEN, id), q_pre = FLD(S.Q, PRE, id);
+		q_hii = FLD(S.Q, HII, id);
+		const double n_H = P.X * q_den / P.hydrogenMass;
+		const double T = calc_temperature(P, q_hii, q_pre, q_den);
+		learned_features(P, n_H, T, q_hii, RFLD(S.R, R_TAU_A, id), S.ds[id], S.shellVol[id], h * S.scal[0], f);
+	}
+	if (!mlp::infer_tile(sm_mlp, reinterpret_cast<const uint4*>(Sv.mlp_img), f, y)) {
+		if (threadIdx.x == 0) atomicOr(Sv.err, ERRB_TC);
+		return;
+	}
+	if (valid && y[2] > 1.0f) B.S[g].lstart[id] = inv_logit10(logit10(q_hii) + y[0]);
+#endif
+}
+
 // The cell's own inputs of the radiation sweep in sweep order (S.sw_rad):
 // what rad_shell computes from the cell's density, pressure and fraction
 // before waiting for the inner shells, with its arithmetic: n_H, the case-B
@@ -1063,6 +1113,49 @@ __global__ void TRG_RAD_SHELL_BOUNDS k_rad_shell_sw_ls(Params P, State S, const 
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= count) return;
 	rad_shell<false, true, true>(P, S, cells[t], h, S.sw_rad + off + t, S.sw_rad_n);
+}
+
+// Learned start in batches (exact build, cells read in place): a front cell
+// of any grid whose per-cell slot S.lstart[id] holds a prediction (written by
+// k_batch_learned_infer before the sweep) tries it beside its plain first
+// iteration, as in single grids.
+__global__ void TRG_RAD_SHELL_BOUNDS k_rad_shell_fp64_ls(Params P, State S, const int* __restrict__ cells, int count,
+                                                         double h) {
+#if TRG_BATCHED
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= count || !P.batch) return;
+	const int e = cells[t];
+	const int g = e >> BATCH_CELL_BITS;
+	rad_shell<false, false, true>(P.batch->P[g], P.batch->S[g], e & BATCH_CELL_MASK, h);
+#endif
+}
+// Before each radiation sweep of a batch with a network loaded: every cell's
+// prediction slot is cleared, and the cells at the front by the previous
+// sweep's optical depth (TAU_A, kept in R) and x_HII become candidates, listed
+// as packed (grid, cell) entries.  One thread per cell of the padded ranges
+// (a 256-thread block never straddles two grids).
+__global__ void __launch_bounds__(256) k_batch_learned_prep(Params Pv, State Sv) {
+#if TRG_BATCHED
+	const BatchTable& B = *Pv.batch;
+	const long long pos = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	const int g = batch_slot(B.cell_off, B.G, blockIdx.x * (long long)blockDim.x);
+	const long long id = pos - B.cell_off[g];
+	const Params& P = B.P[g];
+	const State& S = B.S[g];
+	bool cand = false;
+	if (id < P.N) {
+		S.lstart[id] = __longlong_as_double(0x7ff8000000000000LL);
+		cand = front_cell(RFLD(S.R, R_TAU_A, id), FLD(S.Q, HII, id));
+	}
+	const unsigned ballot = __ballot_sync(0xffffffffu, cand);
+	if (cand) {
+		const int lane = threadIdx.x & 31, leader = __ffs(ballot) - 1;
+		unsigned base = 0;
+		if (lane == leader) base = atomicAdd(Sv.lcand_n, (unsigned)__popc(ballot));
+		base = __shfl_sync(ballot, base, leader);
+		Sv.lcand[base + __popc(ballot & ((1u << lane) - 1))] = (g << BATCH_CELL_BITS) | (int)id;
+	}
+#endif
 }
 
 // Radiation::transferRadiation2 (Radiation.cpp:508-567) for the implicit2 and

@@ -15,8 +15,8 @@
 #include "../../include/torch_b200.h"
 
 // Transcendentals of the radiation and cooling kernels.  The exact build
-// (FP64 form) uses the IEEE-only functions of trg_math.h, shared with the CPU
-// oracle; the fast build (FP32 form, compiled with TRG_FAST_MATH and FMA
+// (FP64 form) uses the correctly rounded functions of trg_math.h, shared with
+// the CPU oracle; the fast build (FP32 form, compiled with TRG_FAST_MATH and FMA
 // contraction) uses CUDA's double-precision library.
 #ifdef TRG_FAST_MATH
 #define d_exp(x) exp(x)

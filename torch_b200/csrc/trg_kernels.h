@@ -15,6 +15,9 @@
 	__global__ void k_learned_infer(Params P, State S, const int* cells, double h); \
 	__global__ void k_rad_shell_sw_diag(Params P, State S, const int* cells, int count, double h, long long off); \
 	__global__ void k_rad_shell_sw_ls(Params P, State S, const int* cells, int count, double h, long long off); \
+	__global__ void k_rad_shell_fp64_ls(Params P, State S, const int* cells, int count, double h); \
+	__global__ void k_batch_learned_prep(Params Pv, State Sv); \
+	__global__ void k_batch_learned_infer(Params Pv, State Sv, double h); \
 	__global__ void k_rad_shell_diag(Params P, State S, const int* cells, int count, double h); \
 	__global__ void k_rad_no_star_fp64(Params P, State S, double h); \
 	__global__ void k_rad_tau_shell(Params P, State S, const int* cells, int count); \
