@@ -587,6 +587,18 @@ def time_learned(args, sim32, N, world, local, pg, sim64=None):
         del blob
         ms64 = timed_form(sim64, args, local, pg, dt_next)
         fp64_same = {"value": N * args.steps * world / (ms64 / 1e3), "ms_per_step": ms64 / args.steps}
+    # where the difference goes: event-bracketed passes of K steps with and without it
+    breakdown = {}
+    for name, n_ in (("learned", net), ("plain", None)):
+        sim32.learned_start(n_)
+        sim32.run_steps(1)
+        sim32.profile(True)
+        sim32.enqueue_steps(args.steps, dt_next)
+        sim32.synchronize()
+        breakdown[name] = {k: round(sim32.profile_read(k)[0] / args.steps, 4)
+                           for k in ("graph_rad_sweep", "k_learned_infer", "k_hydro_stage_fp32", "k_rad_update",
+                                     "k_thermo", "graph_colden_sweep")}
+        sim32.profile(False)
     sim32.stats_enable(True)
     sim32.learned_start(net)
     sim32.run_steps(2)
@@ -607,6 +619,7 @@ def time_learned(args, sim32, N, world, local, pg, sim64=None):
             "front_iters_per_cell": st["front_iters"] / max(1, st["front_cells"]),
             "front_iters_per_cell_plain": st_plain["front_iters"] / max(1, st_plain["front_cells"]),
             "picard_max": st["picard_max"], "picard_max_plain": st_plain["picard_max"],
+            "ms_per_step_by_phase": breakdown,
             "note": "counters from two steps after the timed regions with the network, then two without it"}
 
 
@@ -826,7 +839,7 @@ def main():
                     help="instead of timing: error of the FP32 form against the FP64 form after this many steps")
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--precision", choices=["both", "fp32", "fp64"], default="both")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", dest="learned", action="store_false",

@@ -152,6 +152,21 @@ def test_shell_overlap_keeps_results_bitwise(monkeypatch, precision):
         assert np.array_equal(common.state_dict(a)[g], common.state_dict(b)[g]), g
 
 
+@pytest.mark.parametrize("precision", [torch_b200.PRECISION_FP64, torch_b200.PRECISION_FP32])
+def test_colden_overlap_keeps_results_bitwise(monkeypatch, precision):
+    """In steps whose radiation sub-step lies between a hydro and a thermal
+    sub-step, the thermal sub-step's column-density sweep runs on a side
+    stream beside the radiation sub-step; with that off (TRG_COLDEN_OVERLAP=0,
+    read when a context is created) every field is bitwise the same."""
+    tp, ic = workloads.hii_region(n=24, seed=6)
+    monkeypatch.delenv("TRG_COLDEN_OVERLAP", raising=False)
+    a = run_product(tp, ic, 12, precision=precision, batched=True)
+    monkeypatch.setenv("TRG_COLDEN_OVERLAP", "0")
+    b = run_product(tp, ic, 12, precision=precision, batched=True)
+    for g in ("U", "Q", "R", "T"):
+        assert np.array_equal(common.state_dict(a)[g], common.state_dict(b)[g]), g
+
+
 def test_run_steps_is_deterministic():
     tp, ic = workloads.sedov(n=16)
     a = run_product(tp, ic, 5, batched=True)

@@ -27,6 +27,10 @@ namespace {
 constexpr int COMP_HYDRO = 0, COMP_RAD = 1, COMP_THERMO = 2;
 }
 
+inline bool colden_overlap_default() {
+	const char* v = std::getenv("TRG_COLDEN_OVERLAP");
+	return !(v && v[0] == '0');
+}
 inline bool shell_overlap_default() {
 	const char* v = std::getenv("TRG_SHELL_OVERLAP");
 	return !(v && v[0] == '0');
@@ -48,7 +52,7 @@ struct trg_ctx {
 	bool fp32 = false;
 	bool mixed = false;
 	// FP32 form (either kind): the FP64 kernels come from the fast build
-	bool fastk = false;
+	int fastk = 0;  // kernel build: 0 exact, 1 fast, 2 fast with the batch dispatch
 	// FP32 form with radiation/cooling: Q already holds the primitives of the
 	// current U (written by the FP32 hydro sub-step), so the next
 	// globalQfromU + fixPrimitives pass can be skipped
@@ -64,6 +68,14 @@ struct trg_ctx {
 	// sweep at the start of a step (they touch disjoint fields)
 	cudaStream_t side = nullptr;
 	cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+	// in a split step whose radiation sub-step comes after a hydro sub-step and
+	// before the next thermal one, the column-density sweep that thermal
+	// sub-step needs runs on the side stream beside the radiation sweep (the
+	// density it reads is the hydro sub-step's, which radiation does not
+	// change); TRG_COLDEN_OVERLAP=0 keeps it in the thermal sub-step
+	bool colden_overlap = colden_overlap_default();
+	bool colden_join_pending = false;
+	cudaEvent_t ev_cfork = nullptr, ev_cjoin = nullptr;
 	// CUDA graphs of the shell sweeps (all shells of one sweep, launched as one)
 	cudaGraphExec_t g_colden = nullptr;
 	cudaGraphExec_t g_rad[2] = {nullptr, nullptr};
@@ -167,7 +179,7 @@ void profile_collect(trg_ctx* c) {
 }
 
 // the exact or the fast build of a kernels_fp64.cu kernel, by the context's form
-#define KF(name) (c->fastk ? trg::fast::name : trg::exact::name)
+#define KF(name) (c->fastk == 1 ? trg::fast::name : (c->fastk == 2 ? trg::fastb::name : trg::exact::name))
 
 #define LAUNCH(kernel, n, block, ...)                                                        \
 	do {                                                                                     \
@@ -295,6 +307,10 @@ void colden_sweep(trg_ctx* c) {
 
 void thermo_pre(trg_ctx* c) {
 	// Thermodynamics::preTimeStepCalculations: column densities, then rates.
+	if (c->colden_join_pending) {  // the sweep ran on the side stream
+		cudaStreamWaitEvent(c->stream, c->ev_cjoin, 0);
+		c->colden_join_pending = false;
+	}
 	if (c->P.star_on && !c->colden_valid) {
 		colden_sweep(c);
 		c->colden_valid = true;
@@ -343,7 +359,7 @@ void rad_sweep_direct(trg_ctx* c, double h) {
 			// learned starting iterates of the listed candidates (one tcgen05 tile per CTA)
 			cudaEvent_t ea = nullptr, eb = nullptr;
 			if (c->profiling) { ea = pool_event(c); eb = pool_event(c); cudaEventRecord(ea, c->stream); }
-			KF(k_learned_infer)<<<LCAND_MAX / 128, 128, mlp::INFER_SMEM, c->stream>>>(c->P, c->S,
+			KF(k_learned_infer)<<<INFER_CTAS, 128, mlp::INFER_SMEM, c->stream>>>(c->P, c->S,
 			                                                                          c->d_sweep_nonwind, h);
 			if (c->profiling) { cudaEventRecord(eb, c->stream); c->recs.push_back({"k_learned_infer", ea, eb}); }
 			c->launches++;
@@ -352,7 +368,7 @@ void rad_sweep_direct(trg_ctx* c, double h) {
 		// a batch with a network: candidates of every grid, then the network over them
 		cudaMemsetAsync(c->S.lcand_n, 0, sizeof(unsigned), c->stream);
 		LAUNCH(KF(k_batch_learned_prep), c->P.N, 256, c->P, c->S);
-		KF(k_batch_learned_infer)<<<LCAND_MAX / 128, 128, mlp::INFER_SMEM, c->stream>>>(c->P, c->S, h);
+		KF(k_batch_learned_infer)<<<INFER_CTAS, 128, mlp::INFER_SMEM, c->stream>>>(c->P, c->S, h);
 		c->launches++;
 	}
 	const auto& off = c->hs.off_nonwind;
@@ -417,7 +433,7 @@ void thermo_integrate(trg_ctx* c, double h) {
 	c->launches += 3;
 }
 
-void sub_step(trg_ctx* c, double h, bool hasCalculatedHeatFlux, int comp) {
+void sub_step(trg_ctx* c, double h, bool hasCalculatedHeatFlux, int comp, bool colden_ahead = false) {
 	// Torch::subStep, Torch.cpp:352-364
 	if (!hasCalculatedHeatFlux) {
 		if (!c->q_fresh) q_from_u(c, 0, 1);
@@ -471,6 +487,17 @@ void sub_step(trg_ctx* c, double h, bool hasCalculatedHeatFlux, int comp) {
 		c->colden_valid = false;
 		break;
 	case COMP_RAD:
+		if (colden_ahead) {
+			// the next thermal sub-step's column densities, beside this sub-step
+			cudaEventRecord(c->ev_cfork, c->stream);
+			cudaStreamWaitEvent(c->side, c->ev_cfork, 0);
+			std::swap(c->stream, c->side);
+			colden_sweep(c);
+			std::swap(c->stream, c->side);
+			cudaEventRecord(c->ev_cjoin, c->side);
+			c->colden_valid = true;
+			c->colden_join_pending = true;
+		}
 		rad_integrate(c, h);
 		// mode 2 (FP32 form): the update also leaves Q of the new state
 		LAUNCH(KF(k_rad_update_fp64), c->P.N, 256, c->P, c->S, h, c->mixed ? 2 : 0);
@@ -582,11 +609,34 @@ void enqueue_full_step(trg_ctx* c, double dt_next) {
 		hydro_step(c);
 	} else {
 		c->stepCounter = (c->stepCounter + 1) % ncomps;
+		// the symmetric split: components in the rotated order, then back
+		int seq[5];
+		double hs[5];
+		int ns = 0;
 		for (int i = 0; i < ncomps; ++i) {
-			double h = (i == ncomps - 1) ? 1.0 : 0.5;
-			sub_step(c, h, i == 0, c->hs.active[(i + c->stepCounter) % ncomps]);
+			seq[ns] = c->hs.active[(i + c->stepCounter) % ncomps];
+			hs[ns++] = (i == ncomps - 1) ? 1.0 : 0.5;
 		}
-		for (int i = ncomps - 2; i >= 0; --i) sub_step(c, 0.5, false, c->hs.active[(i + c->stepCounter) % ncomps]);
+		for (int i = ncomps - 2; i >= 0; --i) {
+			seq[ns] = c->hs.active[(i + c->stepCounter) % ncomps];
+			hs[ns++] = 0.5;
+		}
+		const bool can_overlap = c->colden_overlap && c->side && c->P.star_on && c->P.cooling_on;
+		for (int k = 0; k < ns; ++k) {
+			bool ahead = false;
+			if (can_overlap && seq[k] == COMP_RAD && !c->colden_valid) {
+				// the first thermal or hydro sub-step after this one: a thermal
+				// one needs the column densities of the current density
+				for (int j = k + 1; j < ns; ++j) {
+					if (seq[j] == COMP_HYDRO) break;
+					if (seq[j] == COMP_THERMO) {
+						ahead = true;
+						break;
+					}
+				}
+			}
+			sub_step(c, hs[k], k == 0, seq[k], ahead);
+		}
 	}
 	LAUNCH_SCALAR(KF(k_time_advance), c->P, c->S);
 	c->steps++;
@@ -684,6 +734,8 @@ int trg_create(const trg_params* p, const double* den, const double* pre, const 
 	CUDA_TRY(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
 	CUDA_TRY(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
 	CUDA_TRY(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+	CUDA_TRY(cudaEventCreateWithFlags(&c->ev_cfork, cudaEventDisableTiming));
+	CUDA_TRY(cudaEventCreateWithFlags(&c->ev_cjoin, cudaEventDisableTiming));
 	State& S = c->S;
 	std::memset(&S, 0, sizeof(S));
 	int rc = 0;
@@ -748,7 +800,7 @@ int trg_create(const trg_params* p, const double* den, const double* pre, const 
 	if (p->precision == TRG_PRECISION_FP32 && c->hs.nactive > 1) {
 		if (c->P.nd < 2) return set_error(c, TRG_ERR_ARG, "the FP32 form needs a 2-D or 3-D grid");
 		c->mixed = true;
-		c->fastk = true;
+		c->fastk = 1;
 		c->zchunk = ctx_fp32_zchunk(c);
 		if ((rc = dalloc(c, &c->S.fb_flag, N)) || (rc = dalloc(c, &c->S.fb_list, N)) ||
 		    (rc = dalloc(c, &c->S.fb_count, 1)))
@@ -756,7 +808,7 @@ int trg_create(const trg_params* p, const double* den, const double* pre, const 
 	} else if (p->precision == TRG_PRECISION_FP32) {
 		if (c->P.nd < 2) return set_error(c, TRG_ERR_ARG, "the FP32 form needs a 2-D or 3-D grid");
 		c->fp32 = true;
-		c->fastk = true;
+		c->fastk = 1;
 		// z chunk per CTA: about four waves of two 256-thread CTAs per SM
 		c->zchunk = ctx_fp32_zchunk(c);
 		if ((rc = dalloc(c, &c->U32, 7 * N)) || (rc = dalloc(c, &c->U32s, 7 * N))) return rc;
@@ -1297,6 +1349,8 @@ void trg_destroy(trg_ctx* c) {
 	if (c->side) cudaStreamSynchronize(c->side);
 	if (c->ev_fork) cudaEventDestroy(c->ev_fork);
 	if (c->ev_join) cudaEventDestroy(c->ev_join);
+	if (c->ev_cfork) cudaEventDestroy(c->ev_cfork);
+	if (c->ev_cjoin) cudaEventDestroy(c->ev_cjoin);
 	if (c->side) cudaStreamDestroy(c->side);
 	if (c->stream) cudaStreamDestroy(c->stream);
 	delete c;
@@ -1410,13 +1464,21 @@ int trg_batch_create(trg_ctx* const* grids, int G, trg_batch** out) {
 	trg_ctx* c = v;  // for CUDA_TRY
 	v->raw = grids[0]->raw;
 	CUDA_TRY(cudaSetDevice(v->raw.device));
-	if (cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(TRG_ERR_CUDA);
+	if (cudaStreamCreateWithFlags(&v->stream, cudaStreamNonBlocking) != cudaSuccess ||
+	    cudaStreamCreateWithFlags(&v->side, cudaStreamNonBlocking) != cudaSuccess ||
+	    cudaEventCreateWithFlags(&v->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+	    cudaEventCreateWithFlags(&v->ev_join, cudaEventDisableTiming) != cudaSuccess ||
+	    cudaEventCreateWithFlags(&v->ev_cfork, cudaEventDisableTiming) != cudaSuccess ||
+	    cudaEventCreateWithFlags(&v->ev_cjoin, cudaEventDisableTiming) != cudaSuccess)
+		return bail(TRG_ERR_CUDA);
 	v->P = grids[0]->P;
 	v->S = grids[0]->S;
 	v->hs.nactive = grids[0]->hs.nactive;
 	for (int i = 0; i < 3; ++i) v->hs.active[i] = grids[0]->hs.active[i];
 	v->nscalar = G;
-	v->fastk = false;  // batches run the exact build's radiation and cooling kernels (batch dispatch)
+	// batches run a build with the batch dispatch: the exact one (FP64 form)
+	// or the fast one with the dispatch (FP32 form)
+	v->fastk = grids[0]->mixed ? 2 : 0;
 	v->mixed = grids[0]->mixed;
 	v->dt_hist_cap = 0;
 	// offsets of the padded cell and face ranges
@@ -1596,6 +1658,8 @@ int trg_batch_learned_start(trg_batch* b, const trg_mlp* m) {
 	for (int g = 0; g < b->G; ++g) {
 		b->Ss[g].mlp_img = m ? v->mlp_img : nullptr;
 		b->Ss[g].lstart = m ? b->lpred + b->cell_off[g] : nullptr;
+		b->Ss[g].lcand = m ? v->lcand_buf : nullptr;  // the batch's candidate list and count
+		b->Ss[g].lcand_n = m ? v->lcand_n_buf : nullptr;
 	}
 	CUDA_TRY(cudaMemcpy(b->dS, b->Ss.data(), b->Ss.size() * sizeof(State), cudaMemcpyHostToDevice));
 	v->S.mlp_img = m ? v->mlp_img : nullptr;

@@ -787,6 +787,7 @@ __device__ __forceinline__ void hydro_stage_body(const Params& P, const State& S
 	bool tma_late = false;
 	if (tma && threadIdx.x == 0) tma_bar_init(tbar);  // ordered before use by the first barrier below
 	auto slot_of = [](int z) { return ((z % NPLANE) + NPLANE) % NPLANE; };
+	int s_z = nd > 2 ? slot_of(z0 - 1) : 0;  // ring slot of the loop's plane z, advanced with z
 	Prim zero;
 	zero.d = zero.p = zero.x = zero.a = zero.v[0] = zero.v[1] = zero.v[2] = 0.f;
 	Prim szc = zero;  // z slope of this column's cell in the current plane
@@ -811,7 +812,8 @@ __device__ __forceinline__ void hydro_stage_body(const Params& P, const State& S
 	// primitives after its update, into the slot of plane z, which nothing
 	// reads after the flux barrier.
 	for (int z = nd > 2 ? z0 - 1 : z0; z < z1; ++z) {
-		const int sc = nd > 2 ? slot_of(z) : 0;
+		const int sc = s_z;  // planes z + 1 and z + 2 in the next slots; z + 3 comes into sc
+		const int s_z1 = sc == NPLANE - 1 ? 0 : sc + 1, s_z2 = s_z1 == NPLANE - 1 ? 0 : s_z1 + 1;
 		const bool plane = z >= z0;  // x/y faces and the update of this plane
 		const bool stage_next = nd > 2 && z + 1 < z1;
 		__syncthreads();  // planes z .. z + 2 are in the ring; the staging buffer is free
@@ -831,7 +833,7 @@ __device__ __forceinline__ void hydro_stage_body(const Params& P, const State& S
 		if (rec) {
 			const Prim qc = get(s, sc, ly, lx);
 			if (nd > 2)
-				szn = slope_of(lim, th, qc, get(s, slot_of(z + 1), ly, lx), get(s, slot_of(z + 2), ly, lx));
+				szn = slope_of(lim, th, qc, get(s, s_z1, ly, lx), get(s, s_z2, ly, lx));
 		}
 		if (rec && plane) {
 			const Prim qc = get(s, sc, ly, lx);
@@ -915,7 +917,7 @@ __device__ __forceinline__ void hydro_stage_body(const Params& P, const State& S
 		}
 		float fz[7];  // flux through this column's face z + 1/2
 		if (nd > 2) {
-			const Prim ql = get(s, sc, ly, lx), qr = get(s, slot_of(z + 1), ly, lx);
+			const Prim ql = get(s, sc, ly, lx), qr = get(s, s_z1, ly, lx);
 			face_flux<RS>(rs_rt, rec ? face_left(ql, szc) : ql, rec ? face_right(qr, szn) : qr, 2, gamma, fz);
 		}
 		// the cell itself for the source terms, read before the barrier: after
@@ -1013,7 +1015,8 @@ __device__ __forceinline__ void hydro_stage_body(const Params& P, const State& S
 		szc = szn;
 		// no barrier before this: only the slot of plane z is written, and the
 		// flux and slope arrays are rewritten after the next barrier
-		if (stage_next) plane_convert<STAGE>(P, SP, SC, raw, s, slot_of(z + 3), smap, z + 3);
+		if (stage_next) plane_convert<STAGE>(P, SP, SC, raw, s, sc, smap, z + 3);
+		s_z = s_z1;
 	}
 	if (bad) atomicOr(S.err, ERRB_NAN);
 	if (tma_late) atomicOr(S.err, ERRB_ASYNC);

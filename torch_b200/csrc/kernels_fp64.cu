@@ -20,9 +20,11 @@
 #ifndef TRG_KNS
 #define TRG_KNS exact
 #endif
-// Batches run the plain-FP64 form only: the fast build leaves the batch
-// dispatch out, which keeps its kernels' instruction footprint small.
-#ifdef TRG_FAST_MATH
+// Batch dispatch (a kernel over the cells or shells of many grids): in the
+// exact build (FP64-form batches) and in a third build, fast arithmetic with
+// the dispatch (trg::fastb, FP32-form batches); the fast build of single
+// grids leaves it out, which keeps its kernels' instruction footprint small.
+#if defined(TRG_FAST_MATH) && !defined(TRG_FAST_BATCHED)
 #define TRG_BATCHED false
 #else
 #define TRG_BATCHED true
@@ -840,11 +842,17 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 	double start = q_hii;
 	bool learned = false, used_learned = false;
 	if ((LS || DIAG) && front && S.lstart) {
-		// the prediction slot: in sweep order (single grids), or per cell (batches)
-		const double st = SW ? sw[SW_LSTART * swn] : S.lstart[id];
-		if (st == st) {
-			start = st;
-			learned = used_learned = true;
+		// a candidate of this sweep (at the front by the previous sweep's optical
+		// depth, not yet overwritten) holds the network's output in its slot -
+		// in sweep order (single grids) or per cell (batches) - unless the
+		// candidate list overflowed and the network did not run
+		const double tau_prev = SW ? sw[SW_TAU_A * swn] : RFLD(S.R, R_TAU_A, id);
+		if (front_cell(tau_prev, q_hii) && *S.lcand_n <= (unsigned)LCAND_MAX) {
+			const double st = SW ? sw[SW_LSTART * swn] : S.lstart[id];
+			if (st == st) {
+				start = st;
+				learned = used_learned = true;
+			}
 		}
 	}
 	if (SW) sw[SW_TAU_A * swn] = tau_a;  // the next sweep's learned-start candidates are chosen from it
@@ -982,11 +990,11 @@ __global__ void __launch_bounds__(128) k_rad_shell_diag(Params P, State S, const
 // ----------------------------------------------- learned starting iterate
 // Before each radiation sweep with a network loaded, k_rad_sweep_prep lists
 // the candidate front cells (by the previous sweep's TAU_A and x_HII, the
-// front criterion) as sweep positions and clears every prediction slot; this
-// kernel runs the network over the candidates, one tcgen05 tile of 128 per
-// CTA (a CTA allocates tensor memory once: infer_tile gives up the
-// allocation permit after its allocation, so no CTA runs a second tile; the
-// grid covers LCAND_MAX candidates and CTAs beyond the list return at once):
+// front criterion) as sweep positions; this kernel runs the network over
+// the candidates and writes each candidate's slot (a prediction, or NaN),
+// in tcgen05 tiles of 128: a persistent grid of INFER_CTAS CTAs, each loading
+// the model image and allocating its tensor memory once and looping over the
+// tiles (CTAs beyond the list return at once):
 // inputs log n_H, log T, x_HII, log of the optically thin photoionisation
 // rate at that TAU_A, log dt; cells predicted to need more than two plain
 // iterations get the predicted time-averaged fraction as their starting
@@ -999,24 +1007,31 @@ __global__ void __launch_bounds__(128) k_learned_infer(Params P, State S, const 
 	if (n > (unsigned)LCAND_MAX || blockIdx.x * 128u >= n) return;  // uniform over the CTA
 	const double dt = h * S.scal[0];
 	const long long sn = S.sw_rad_n;
-	const unsigned t = blockIdx.x * 128u + threadIdx.x;
-	const bool valid = t < n;
-	const int pos = valid ? S.lcand[t] : 0;
-	float f[5] = {0, 0, 0, 0, 0}, y[3];
-	double q_hii = 0;
-	if (valid) {
-		const long long id = cells[pos];
-		const double* sw = S.sw_rad + pos;
-		const double q_den = FLD(S.Q, DEN, id), q_pre = FLD(S.Q, PRE, id);
-		q_hii = sw[3 * sn];
-		const double T = calc_temperature(P, q_hii, q_pre, q_den);
-		learned_features(P, sw[0], T, q_hii, sw[SW_TAU_A * sn], sw[4 * sn], sw[5 * sn], dt, f);
+	const uint32_t tm = mlp::infer_begin(sm_mlp, reinterpret_cast<const uint4*>(S.mlp_img));
+	uint32_t phase = 0;
+	bool ok = true;
+	for (unsigned base = blockIdx.x * 128u; base < n; base += gridDim.x * 128u) {
+		const unsigned t = base + threadIdx.x;
+		const bool valid = t < n;
+		const int pos = valid ? S.lcand[t] : 0;
+		float f[5] = {0, 0, 0, 0, 0}, y[3];
+		double q_hii = 0;
+		if (valid) {
+			const long long id = cells[pos];
+			const double* sw = S.sw_rad + pos;
+			const double q_den = FLD(S.Q, DEN, id), q_pre = FLD(S.Q, PRE, id);
+			q_hii = sw[3 * sn];
+			const double T = calc_temperature(P, q_hii, q_pre, q_den);
+			learned_features(P, sw[0], T, q_hii, sw[SW_TAU_A * sn], sw[4 * sn], sw[5 * sn], dt, f);
+		}
+		ok = mlp::infer_step(sm_mlp, tm, phase, f, y);
+		if (!ok) break;
+		if (valid)
+			S.sw_rad[SW_LSTART * sn + pos] =
+			    y[2] > 1.0f ? inv_logit10(logit10(q_hii) + y[0]) : __longlong_as_double(0x7ff8000000000000LL);
 	}
-	if (!mlp::infer_tile(sm_mlp, reinterpret_cast<const uint4*>(S.mlp_img), f, y)) {
-		if (threadIdx.x == 0) atomicOr(S.err, ERRB_TC);
-		return;
-	}
-	if (valid && y[2] > 1.0f) S.sw_rad[SW_LSTART * sn + pos] = inv_logit10(logit10(q_hii) + y[0]);
+	mlp::infer_end(tm);
+	if (!ok && threadIdx.x == 0) atomicOr(S.err, ERRB_TC);
 }
 
 // The network over a batch's candidates (packed (grid, cell) entries): the
@@ -1028,27 +1043,34 @@ __global__ void __launch_bounds__(128) k_batch_learned_infer(Params Pv, State Sv
 	const unsigned n = *Sv.lcand_n;
 	if (n > (unsigned)LCAND_MAX || blockIdx.x * 128u >= n) return;  // uniform over the CTA
 	const BatchTable& B = *Pv.batch;
-	const unsigned t = blockIdx.x * 128u + threadIdx.x;
-	const bool valid = t < n;
-	const int e = valid ? Sv.lcand[t] : 0;
-	const int g = e >> BATCH_CELL_BITS;
-	const long long id = e & BATCH_CELL_MASK;
-	float f[5] = {0, 0, 0, 0, 0}, y[3];
-	double q_hii = 0;
-	if (valid) {
-		const Params& P = B.P[g];
-		const State& S = B.S[g];
-		const double q_den = FLD(S.Q, DEN, id), q_pre = FLD(S.Q, PRE, id);
-		q_hii = FLD(S.Q, HII, id);
-		const double n_H = P.X * q_den / P.hydrogenMass;
-		const double T = calc_temperature(P, q_hii, q_pre, q_den);
-		learned_features(P, n_H, T, q_hii, RFLD(S.R, R_TAU_A, id), S.ds[id], S.shellVol[id], h * S.scal[0], f);
+	const uint32_t tm = mlp::infer_begin(sm_mlp, reinterpret_cast<const uint4*>(Sv.mlp_img));
+	uint32_t phase = 0;
+	bool ok = true;
+	for (unsigned base = blockIdx.x * 128u; base < n; base += gridDim.x * 128u) {
+		const unsigned t = base + threadIdx.x;
+		const bool valid = t < n;
+		const int e = valid ? Sv.lcand[t] : 0;
+		const int g = e >> BATCH_CELL_BITS;
+		const long long id = e & BATCH_CELL_MASK;
+		float f[5] = {0, 0, 0, 0, 0}, y[3];
+		double q_hii = 0;
+		if (valid) {
+			const Params& P = B.P[g];
+			const State& S = B.S[g];
+			const double q_den = FLD(S.Q, DEN, id), q_pre = FLD(S.Q, PRE, id);
+			q_hii = FLD(S.Q, HII, id);
+			const double n_H = P.X * q_den / P.hydrogenMass;
+			const double T = calc_temperature(P, q_hii, q_pre, q_den);
+			learned_features(P, n_H, T, q_hii, RFLD(S.R, R_TAU_A, id), S.ds[id], S.shellVol[id], h * S.scal[0], f);
+		}
+		ok = mlp::infer_step(sm_mlp, tm, phase, f, y);
+		if (!ok) break;
+		if (valid)
+			B.S[g].lstart[id] =
+			    y[2] > 1.0f ? inv_logit10(logit10(q_hii) + y[0]) : __longlong_as_double(0x7ff8000000000000LL);
 	}
-	if (!mlp::infer_tile(sm_mlp, reinterpret_cast<const uint4*>(Sv.mlp_img), f, y)) {
-		if (threadIdx.x == 0) atomicOr(Sv.err, ERRB_TC);
-		return;
-	}
-	if (valid && y[2] > 1.0f) B.S[g].lstart[id] = inv_logit10(logit10(q_hii) + y[0]);
+	mlp::infer_end(tm);
+	if (!ok && threadIdx.x == 0) atomicOr(Sv.err, ERRB_TC);
 #endif
 }
 
@@ -1078,9 +1100,9 @@ __global__ void __launch_bounds__(256) k_rad_sweep_prep(Params P, State S, const
 		sw[SW_TAU_A * sn] = RFLD(S.R, R_TAU_A, id);
 	}
 	if (S.lstart) {
-		// learned start: no prediction yet; a cell at the front by the
-		// previous sweep's optical depth becomes a candidate (its sweep position)
-		sw[SW_LSTART * sn] = __longlong_as_double(0x7ff8000000000000LL);
+		// learned start: a cell at the front by the previous sweep's optical
+		// depth becomes a candidate (its sweep position); the network writes
+		// every candidate's slot, and no other slot is read
 		const bool cand = front_cell(sw[SW_TAU_A * sn], q_hii);
 		const unsigned ballot = __ballot_sync(__activemask(), cand);
 		if (cand) {
@@ -1129,11 +1151,11 @@ __global__ void TRG_RAD_SHELL_BOUNDS k_rad_shell_fp64_ls(Params P, State S, cons
 	rad_shell<false, false, true>(P.batch->P[g], P.batch->S[g], e & BATCH_CELL_MASK, h);
 #endif
 }
-// Before each radiation sweep of a batch with a network loaded: every cell's
-// prediction slot is cleared, and the cells at the front by the previous
-// sweep's optical depth (TAU_A, kept in R) and x_HII become candidates, listed
-// as packed (grid, cell) entries.  One thread per cell of the padded ranges
-// (a 256-thread block never straddles two grids).
+// Before each radiation sweep of a batch with a network loaded: the cells at
+// the front by the previous sweep's optical depth (TAU_A, kept in R) and x_HII
+// become candidates, listed as packed (grid, cell) entries; the network writes
+// every candidate's slot.  One thread per cell of the padded ranges (a
+// 256-thread block never straddles two grids).
 __global__ void __launch_bounds__(256) k_batch_learned_prep(Params Pv, State Sv) {
 #if TRG_BATCHED
 	const BatchTable& B = *Pv.batch;
@@ -1142,11 +1164,7 @@ __global__ void __launch_bounds__(256) k_batch_learned_prep(Params Pv, State Sv)
 	const long long id = pos - B.cell_off[g];
 	const Params& P = B.P[g];
 	const State& S = B.S[g];
-	bool cand = false;
-	if (id < P.N) {
-		S.lstart[id] = __longlong_as_double(0x7ff8000000000000LL);
-		cand = front_cell(RFLD(S.R, R_TAU_A, id), FLD(S.Q, HII, id));
-	}
+	const bool cand = id < P.N && front_cell(RFLD(S.R, R_TAU_A, id), FLD(S.Q, HII, id));
 	const unsigned ballot = __ballot_sync(0xffffffffu, cand);
 	if (cand) {
 		const int lane = threadIdx.x & 31, leader = __ffs(ballot) - 1;

@@ -191,32 +191,42 @@ __device__ __forceinline__ void sync_tc() {
 	fence_after();
 }
 
-// Forward pass of the CTA's 128-sample tile (all 128 threads, CTA-converged).
-// x: this thread's 5 raw features; y: its 3 raw outputs.  `img` holds the
-// IMG_INFER_BYTES of the model image (16-byte aligned), `sm` INFER_SMEM bytes
-// of shared memory (128-byte aligned).  Returns false if a tensor-core wait
-// expired (then y is garbage).
-__device__ __forceinline__ bool infer_tile(unsigned char* sm, const uint4* __restrict__ img, const float* x, float* y) {
+// Forward passes of 128-sample tiles by one CTA (all 128 threads,
+// CTA-converged): infer_begin copies the model image (IMG_INFER_BYTES at
+// `img`, 16-byte aligned) into shared memory (`sm`, INFER_SMEM bytes, 128-byte
+// aligned), initialises the mbarrier and allocates 64 tensor-memory columns
+// (once per CTA: the allocation gives up the CTA's allocation permit);
+// infer_step runs one tile (x: this thread's 5 raw features, y: its 3 raw
+// outputs; `phase` is the mbarrier phase, carried from tile to tile) and
+// returns false, the same in every thread, if a tensor-core wait expired (y
+// is then garbage and the CTA must stop); infer_end frees the columns.
+__device__ __forceinline__ uint32_t infer_begin(unsigned char* sm, const uint4* __restrict__ img) {
+	const int t = threadIdx.x;
+	unsigned char* W = sm + INFER_SM_W;
+	const uint32_t bar = smem_u32(sm + INFER_SM_BAR);
+	const uint32_t slot = smem_u32(sm + INFER_SM_BAR + 8);
+	for (int i = t; i < IMG_INFER_BYTES / 16; i += blockDim.x) reinterpret_cast<uint4*>(W)[i] = img[i];
+	if (t == 0) mbar_init(bar, 1);
+	if (t < 32) tmem_alloc(slot, 64);
+	sync_tc();
+	return *reinterpret_cast<volatile uint32_t*>(sm + INFER_SM_BAR + 8);
+}
+
+__device__ __forceinline__ bool infer_step(unsigned char* sm, uint32_t tm, uint32_t& phase, const float* x, float* y) {
 	const int t = threadIdx.x;
 	unsigned char* X = sm + INFER_SM_X;
 	unsigned char* H = sm + INFER_SM_H;
 	unsigned char* W = sm + INFER_SM_W;
 	const uint32_t bar = smem_u32(sm + INFER_SM_BAR);
-	const uint32_t slot = smem_u32(sm + INFER_SM_BAR + 8);
-	for (int i = t; i < IMG_INFER_BYTES / 16; i += blockDim.x) reinterpret_cast<uint4*>(W)[i] = img[i];
-	const float* F = reinterpret_cast<const float*>(img) + IMG_F32 / 4;
+	const float* Fs = reinterpret_cast<const float*>(W + IMG_F32);
 	float xv[8] = {0, 0, 0, 0, 0, 0, 0, 0}, zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
-	for (int f = 0; f < IN; ++f) xv[f] = (x[f] - F[F_IN_MEAN + f]) * F[F_IN_SCALE + f];
+	for (int f = 0; f < IN; ++f) xv[f] = (x[f] - Fs[F_IN_MEAN + f]) * Fs[F_IN_SCALE + f];
 	st_chunk(X, t, 0, K1, xv);
 	st_chunk(X, t, 8, K1, zero);
-	if (t == 0) mbar_init(bar, 1);
-	if (t < 32) tmem_alloc(slot, 64);
+	// the previous tile's reads of the accumulator and of X/H are done
 	sync_tc();
-	const uint32_t tm = *reinterpret_cast<volatile uint32_t*>(sm + INFER_SM_BAR + 8);
-	const float* Fs = reinterpret_cast<const float*>(W + IMG_F32);
 	bool ok = true;
-	uint32_t phase = 0;
 	// layer 1 and layer 2: Z = A W, H = relu(Z + b) into the H tile, 16
 	// accumulator columns at a time (few live registers)
 #pragma unroll 1
@@ -246,14 +256,28 @@ __device__ __forceinline__ bool infer_tile(unsigned char* sm, const uint4* __res
 		commit(bar);
 	}
 	ok = mbar_wait(bar, phase) && ok;
+	phase ^= 1;
 	fence_after();
 	float o[16];
 	tmem_ld16(tmem_row_addr(tm, 0), o);
 #pragma unroll
 	for (int k = 0; k < OUT; ++k) y[k] = (o[k] + Fs[F_B3 + k]) / Fs[F_OUT_SCALE + k] + Fs[F_OUT_MEAN + k];
 	fence_before();
+	return __syncthreads_and(ok) != 0;
+}
+
+__device__ __forceinline__ void infer_end(uint32_t tm) {
+	fence_before();
 	__syncthreads();
-	if (t < 32) tmem_dealloc(tm, 64);
+	if (threadIdx.x < 32) tmem_dealloc(tm, 64);
+}
+
+// One tile with its own set-up and release.
+__device__ __forceinline__ bool infer_tile(unsigned char* sm, const uint4* __restrict__ img, const float* x, float* y) {
+	const uint32_t tm = infer_begin(sm, img);
+	uint32_t phase = 0;
+	const bool ok = infer_step(sm, tm, phase, x, y);
+	infer_end(tm);
 	return ok;
 }
 

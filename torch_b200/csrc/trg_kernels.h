@@ -3,8 +3,9 @@
 #pragma once
 #include "trg_device.cuh"
 
-// kernels_fp64.cu, built twice: exact (plain-FP64 form, rounds like the
-// reference) and fast (FP32 form; FMA and CUDA libm)
+// kernels_fp64.cu, built three times: exact (plain-FP64 form, rounds like the
+// reference), fast (FP32 form; FMA and CUDA libm) and fastb (fast, with the
+// batch dispatch, for FP32-form batches)
 #define TRG_FP64_KERNELS \
 	__global__ void k_faces_fp64(Params P, State S, int dim); \
 	__global__ void k_hydro_update_fp64(Params P, State S, double h, int sel_base, int sel_out, int mode); \
@@ -49,6 +50,9 @@ namespace exact {
 TRG_FP64_KERNELS
 }
 namespace fast {
+TRG_FP64_KERNELS
+}
+namespace fastb {  // the fast build with the batch dispatch (FP32-form batches)
 TRG_FP64_KERNELS
 }
 // FP32 form of the hydro pass (kernels_fp32.cu)

@@ -50,6 +50,8 @@ constexpr int THQ_MAX_SUBCYCLES = 1 << 26;
 // candidate list the learned start serves in one sweep.
 constexpr int SW_TAU_A = 6, SW_LSTART = 7, SW_RAD_ROWS = 8;
 constexpr int LCAND_MAX = 1 << 21;
+// persistent grid of the learned-start inference (4 CTAs per SM of a B200)
+constexpr int INFER_CTAS = 148 * 4;
 
 // Planes per CTA of the FP32 form's fallback flag pass (k_fb_flags).
 constexpr int FB_ZCHUNK = 16;
