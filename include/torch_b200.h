@@ -370,6 +370,49 @@ void trg_batch_destroy(trg_batch* b);
 int trg_hydro_step_fp32_noalloc(trg_ctx* c, const double* U_in, double* U_out, double dt, double* dt_next,
                                 void* stream);
 
+/* x-slab decomposition of a hydrodynamics-only run (no radiation, cooling or
+ * star), one slab per GPU, as the reference splits its grid over MPI ranks
+ * (Grid::initialise, src/Fluid/Grid.cpp:446-459; the halo exchange of
+ * Grid::applyBCs PARTITION, :804-833; the minimum time step over ranks,
+ * src/Torch/Torch.cpp:323-335).  trg_create_slab takes the whole grid's
+ * parameters p and the cells of one slab - global x from x0 to x0 + nx - 1,
+ * nx >= 2, every y and z, flat index i + nx*(j + ny*k) - and, for the FP32
+ * form, the whole grid's reference density and pressure f32_scale[2] in
+ * code units (NULL: the slab's own medians; give the same values to every
+ * slab for results equal to the undecomposed run's).  An x face that borders
+ * another slab (or the other end of a periodic grid) takes its ghost layers
+ * from the neighbour (trg_slab_partitions: bit 1 the low x face, bit 2 the
+ * high one).  trg_f32_scales gives the whole grid's f32_scale from its
+ * initial fields (host only).  Before stepping, trg_slab_exchange registers
+ * the host's hook, two device buffers of trg_slab_halo_bytes(c) bytes each,
+ * [side 2][layer 2][field 7][ny*nz] (layer 0 next to the face; doubles, or
+ * floats in the hydro-only FP32 form), and a device buffer dt_buf of three
+ * unsigned 64-bit integers.  The library calls
+ *   fn(user, TRG_EXCHANGE_HALO, stream): halo_send holds this slab's layers,
+ *     packed on `stream`; the hook must make halo_recv hold the neighbours'
+ *     (recv[left] = left neighbour's send[right], recv[right] = right
+ *     neighbour's send[left]) in `stream` order before it returns (e.g. NCCL
+ *     send/recv enqueued on `stream`), and must not let a neighbour's next
+ *     pack overwrite its send buffer before the copy has read it;
+ *   fn(user, TRG_EXCHANGE_DT, stream): dt_buf holds this slab's three
+ *     time-step minima (bit patterns of positive doubles: an integer minimum
+ *     is the minimum of the values); each must become its minimum over all
+ *     slabs, in `stream` order (e.g. an NCCL all-reduce MIN on `stream`);
+ * and a nonzero return makes the step return TRG_ERR_ARG.  Every slab calls
+ * the hook the same number of times in the same order. */
+#define TRG_EXCHANGE_HALO 0
+#define TRG_EXCHANGE_DT 1
+typedef int (*trg_exchange_fn)(void* user, int what, void* stream);
+int trg_create_slab(const trg_params* p, int x0, int nx, const double* f32_scale, const double* den,
+                    const double* pre, const double* hii, const double* v0, const double* v1, const double* v2,
+                    const double* grav, trg_ctx** out);
+int trg_slab_exchange(trg_ctx* c, trg_exchange_fn fn, void* user, void* halo_send, const void* halo_recv,
+                      void* dt_buf);
+long long trg_slab_halo_bytes(const trg_ctx* c);
+int trg_slab_partitions(const trg_ctx* c);
+int trg_f32_scales(const trg_params* p, const double* den, const double* pre, const double* hii, const double* v0,
+                   const double* v1, const double* v2, double* f32_scale);
+
 #ifdef __cplusplus
 }
 #endif

@@ -6,6 +6,7 @@ build (oracle/_ref), i.e. this build container; skipped elsewhere.  The
 linked program is run without arguments, which makes no CUDA call."""
 import os
 import re
+import shutil
 import subprocess
 import tempfile
 
@@ -67,3 +68,27 @@ def test_torchgpu_binding_compiles_and_links():
         assert r.returncode == 0, r.stderr[-3000:]
         out = subprocess.run([os.path.join(d, "binding")], capture_output=True, text=True, timeout=60)
         assert out.returncode == 0 and "binding linked" in out.stdout, out.stderr
+
+
+def test_slab_hook_example_compiles():
+    """The NCCL exchange hook of INTEGRATION.md's decomposed-run example,
+    compiled against the library header and the system NCCL header, with
+    the call it makes to register itself."""
+    if not os.path.exists("/usr/include/nccl.h"):
+        pytest.skip("no NCCL header")
+    text = open(os.path.join(common.ROOT, "INTEGRATION.md")).read()
+    blocks = [b for b in re.findall(r"```cpp\n(.*?)```", text, flags=re.S) if "trg_exchange_fn" in b]
+    assert len(blocks) == 1
+    body = blocks[0].replace("trg_slab_exchange(ctx, exchange, &comm, send, recv, dt);",
+                             "void reg(trg_ctx* ctx, SlabComm& comm, void* send, void* recv, void* dt) {\n"
+                             "    trg_slab_exchange(ctx, exchange, &comm, send, recv, dt);\n}")
+    src = "#include <cuda_runtime.h>\n#include <nccl.h>\n#include \"torch_b200.h\"\n" + body
+    with tempfile.TemporaryDirectory() as d:
+        with open(os.path.join(d, "hook.cpp"), "w") as f:
+            f.write(src)
+        cuda_inc = os.path.join(os.path.dirname(os.path.dirname(shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")),
+                                "include")
+        cmd = ["g++", "-std=c++11", "-c", "-I" + os.path.join(common.ROOT, "include"), "-I" + cuda_inc,
+               os.path.join(d, "hook.cpp"), "-o", os.path.join(d, "hook.o")]
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, r.stderr[-3000:]

@@ -78,6 +78,10 @@ def library_path() -> str:
 _lib = None
 
 # (name, restype, argtypes) for every entry point of include/torch_b200.h
+# the x-slab exchange hook of trg_slab_exchange: int fn(void* user, int what, void* stream)
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_void_p)
+EXCHANGE_HALO, EXCHANGE_DT = 0, 1
+
 _SIGNATURES = [
     ("trg_create", C.c_int, [C.POINTER(TrgParams)] + [C.c_void_p] * 7 + [C.POINTER(C.c_void_p)]),
     ("trg_setup_positions", C.c_int, [C.POINTER(TrgParams)] + [C.c_void_p] * 4),
@@ -141,6 +145,12 @@ _SIGNATURES = [
     ("trg_conservation_history", C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.POINTER(C.c_longlong)]),
     ("trg_hydro_step_fp32_noalloc", C.c_int,
      [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.POINTER(C.c_double), C.c_void_p]),
+    ("trg_create_slab", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p] + [C.c_void_p] * 7
+     + [C.POINTER(C.c_void_p)]),
+    ("trg_slab_exchange", C.c_int, [C.c_void_p, EXCHANGE_FN, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("trg_slab_halo_bytes", C.c_longlong, [C.c_void_p]),
+    ("trg_slab_partitions", C.c_int, [C.c_void_p]),
+    ("trg_f32_scales", C.c_int, [C.c_void_p] + [C.c_void_p] * 6 + [C.c_void_p]),
 ]
 
 
@@ -334,16 +344,32 @@ class Torch:
     reference's DataReader or Lua setup provides them).
     """
 
-    def __init__(self, tp: TorchParameters, ic, precision: int = PRECISION_FP64, device: int = 0):
+    def __init__(self, tp: TorchParameters, ic, precision: int = PRECISION_FP64, device: int = 0, slab=None):
+        """slab = (x0, nx, f32_scale or None): this context holds global x from
+        x0 to x0 + nx - 1 of the grid `ic` describes (trg_create_slab); the
+        hydrodynamics-only step then needs an exchange hook (torch_b200.slabs)."""
         self.lib = load_library()
-        self.N = int(np.prod(ic.ncells))
         p = make_params(tp, ic.side_length, ic.ncells, precision, device)
-        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in
-                (ic.den, ic.pre, ic.hii, ic.vel[0], ic.vel[1], ic.vel[2])]
+        fields = [ic.den, ic.pre, ic.hii, ic.vel[0], ic.vel[1], ic.vel[2]]
         grav = getattr(ic, "grav", None)
+        if slab is not None:
+            x0, nx = int(slab[0]), int(slab[1])
+            shape = (int(ic.ncells[2]), int(ic.ncells[1]), int(ic.ncells[0]))
+            fields = [np.asarray(a, dtype=np.float64).reshape(shape)[:, :, x0:x0 + nx].ravel() for a in fields]
+            if grav is not None:
+                grav = np.asarray(grav, dtype=np.float64).reshape((3,) + shape)[:, :, :, x0:x0 + nx].reshape(3, -1)
+            self.N = nx * shape[0] * shape[1]
+        else:
+            self.N = int(np.prod(ic.ncells))
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in fields]
         garr = None if grav is None else np.ascontiguousarray(grav, dtype=np.float64)
         ctx = C.c_void_p()
-        rc = self.lib.trg_create(C.byref(p), *[_ptr(a) for a in arrs], _ptr(garr), C.byref(ctx))
+        if slab is not None:
+            sc = None if slab[2] is None else np.ascontiguousarray(slab[2], dtype=np.float64)
+            rc = self.lib.trg_create_slab(C.byref(p), x0, nx, _ptr(sc), *[_ptr(a) for a in arrs], _ptr(garr),
+                                          C.byref(ctx))
+        else:
+            rc = self.lib.trg_create(C.byref(p), *[_ptr(a) for a in arrs], _ptr(garr), C.byref(ctx))
         self.ctx = ctx.value
         if rc != 0:
             msg = self.lib.trg_last_error(self.ctx).decode() if self.ctx else "trg_create failed"

@@ -51,6 +51,11 @@ struct trg_ctx {
 	// sub-steps run through the FP32 kernel
 	bool fp32 = false;
 	bool mixed = false;
+	// x-slab decomposition: the host's exchange hook and whether it failed
+	trg_exchange_fn xfn = nullptr;
+	void* xuser = nullptr;
+	unsigned long long* xdt = nullptr;  // the host's device buffer of the three time-step minima
+	bool xfail = false;
 	// FP32 form (either kind): the FP64 kernels come from the fast build
 	int fastk = 0;  // kernel build: 0 exact, 1 fast, 2 fast with the batch dispatch
 	// FP32 form with radiation/cooling: Q already holds the primitives of the
@@ -254,6 +259,26 @@ int download_rt(trg_ctx* c, double* host, const double* dev, int nf) {
 
 void q_from_u(trg_ctx* c, int sel, int fix) { LAUNCH(KF(k_q_from_u_fp64), c->P.N, 256, c->P, c->S, sel, fix); }
 
+// x-slab decomposition: before a flux computation, the layers next to the
+// partition faces of `src` (the state it reads) are packed into the halo send
+// buffer and the host's hook fills the receive buffer from the neighbours
+// (Grid::applyBCs PARTITION, Grid.cpp:804-833), all on the context's stream.
+void halo_exchange(trg_ctx* c, const void* src, bool f32) {
+	if (!c->S.halo_send) return;
+	launch_halo_pack(c->P, src, c->S.halo_send, f32, c->stream);
+	c->launches++;
+	if (c->xfn(c->xuser, TRG_EXCHANGE_HALO, c->stream) != 0) c->xfail = true;
+}
+// ... and before the time step is taken from the per-component minima, their
+// minimum over all slabs (Torch::calculateTimeStep's MPI minimum, Torch.cpp:323-335).
+void dt_exchange(trg_ctx* c) {
+	if (!c->xfn) return;
+	const size_t b = 3 * sizeof(unsigned long long);
+	cudaMemcpyAsync(c->xdt, c->S.scal + 2, b, cudaMemcpyDeviceToDevice, c->stream);
+	if (c->xfn(c->xuser, TRG_EXCHANGE_DT, c->stream) != 0) c->xfail = true;
+	cudaMemcpyAsync(c->S.scal + 2, c->xdt, b, cudaMemcpyDeviceToDevice, c->stream);
+}
+
 void colden_sweep_direct(trg_ctx* c) {
 	const auto& off = c->hs.off_all;
 	const bool sw = c->S.sw_col != nullptr;
@@ -326,6 +351,7 @@ void comp_pre(trg_ctx* c, int comp) {
 }
 
 void hydro_fluxes(trg_ctx* c) {
+	halo_exchange(c, c->S.Q, false);
 	for (int d = 0; d < c->P.nd; ++d) LAUNCH(KF(k_faces_fp64), c->S.nfaces[d], 128, c->P, c->S, d);
 }
 
@@ -554,6 +580,7 @@ void time_step(trg_ctx* c, double dt_next) {
 	LAUNCH_SCALAR(KF(k_dt_reset), c->P, c->S);
 	LAUNCH(KF(k_dt_reduce_fp64), c->P.N, 256, c->P, c->S, first_cell);
 	if (c->cons_on) cons_record(c, true);
+	dt_exchange(c);
 	LAUNCH_SCALAR(KF(k_dt_finalize), c->P, c->S, dt_next, 0, step);
 }
 
@@ -563,10 +590,12 @@ void enqueue_full_step_fp32(trg_ctx* c, double dt_next) {
 	// kernel each.
 	int step = c->steps < c->dt_hist_cap ? (int)c->steps : -1;
 	if (c->cons_on) cons_record(c, false);
+	if (!c->first_time) dt_exchange(c);
 	LAUNCH_SCALAR(KF(k_dt_finalize), c->P, c->S, dt_next, c->first_time, step);
 	c->first_time = 0;
 	LAUNCH_SCALAR(KF(k_dt_reset), c->P, c->S);
 	auto stage = [&](int st, const float* Uq, const float* Ub, float* Uo) {
+		halo_exchange(c, Uq, true);
 		cudaEvent_t ea = nullptr, eb = nullptr;
 		if (c->profiling) { ea = pool_event(c); eb = pool_event(c); cudaEventRecord(ea, c->stream); }
 		launch_hydro_stage_fp32(st, c->P, c->S, Uq, Ub, Uo, c->zchunk, c->stream);
@@ -658,6 +687,10 @@ int check_device_error(trg_ctx* c) {
 	if (e & ERRB_SUBCYCLE)
 		return set_error(c, TRG_ERR_SUBCYCLE, "Thermodynamics::integrate: a cell needs more thermal sub-cycles than "
 		                                      "the work queue runs (2^26)");
+	if (c->xfail) {
+		c->xfail = false;
+		return set_error(c, TRG_ERR_ARG, "slab exchange: the host's exchange hook reported a failure");
+	}
 	return TRG_OK;
 }
 
@@ -705,12 +738,17 @@ int ctx_fp32_zchunk(const trg_ctx* c) {
 	return zc < 16 ? 16 : zc;
 }
 int ctx_fail(trg_ctx* c, int code, const std::string& msg) { return set_error(c, code, msg); }
+// a slab with partition faces and no exchange hook yet
+bool slab_unhooked(const trg_ctx* c) {
+	return (c->P.lbc[0] == BC_PARTITION || c->P.rbc[0] == BC_PARTITION) && !c->xfn;
+}
 }  // namespace trg
 
 extern "C" {
 
-int trg_create(const trg_params* p, const double* den, const double* pre, const double* hii, const double* v0,
-               const double* v1, const double* v2, const double* grav, trg_ctx** out) {
+namespace {
+int create_impl(const trg_params* p, const SlabSpec* slab, const double* den, const double* pre, const double* hii,
+                const double* v0, const double* v1, const double* v2, const double* grav, trg_ctx** out) {
 	if (!p || !out) return TRG_ERR_ARG;
 	*out = nullptr;
 	trg_ctx* c = new trg_ctx();
@@ -720,7 +758,7 @@ int trg_create(const trg_params* p, const double* den, const double* pre, const 
 		*out = c;
 		return TRG_ERR_ARG;
 	}
-	std::string why = host_setup(*p, den, pre, hii, v0, v1, v2, grav, c->hs);
+	std::string why = host_setup(*p, den, pre, hii, v0, v1, v2, grav, c->hs, slab);
 	if (!why.empty()) {
 		c->err = why;
 		*out = c;
@@ -827,9 +865,66 @@ int trg_create(const trg_params* p, const double* den, const double* pre, const 
 	std::vector<double>().swap(c->hs.grav);
 	return check_device_error(c);
 }
+}  // namespace
+
+int trg_create(const trg_params* p, const double* den, const double* pre, const double* hii, const double* v0,
+               const double* v1, const double* v2, const double* grav, trg_ctx** out) {
+	return create_impl(p, nullptr, den, pre, hii, v0, v1, v2, grav, out);
+}
+
+int trg_create_slab(const trg_params* p, int x0, int nx, const double* f32_scale, const double* den,
+                    const double* pre, const double* hii, const double* v0, const double* v1, const double* v2,
+                    const double* grav, trg_ctx** out) {
+	SlabSpec sl;
+	sl.x0 = x0;
+	sl.nx = nx;
+	if (f32_scale) {
+		sl.f32_rho0 = f32_scale[0];
+		sl.f32_p0 = f32_scale[1];
+	}
+	return create_impl(p, &sl, den, pre, hii, v0, v1, v2, grav, out);
+}
+
+int trg_slab_exchange(trg_ctx* c, trg_exchange_fn fn, void* user, void* halo_send, const void* halo_recv,
+                      void* dt_buf) {
+	if (!c) return TRG_ERR_ARG;
+	const bool part = c->P.lbc[0] == BC_PARTITION || c->P.rbc[0] == BC_PARTITION;
+	if (fn && (!dt_buf || (part && (!halo_send || !halo_recv))))
+		return set_error(c, TRG_ERR_ARG, "trg_slab_exchange: the hook needs the time-step buffer and, for a slab "
+		                                 "with partition faces, both halos");
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	c->xfn = fn;
+	c->xuser = user;
+	c->xdt = static_cast<unsigned long long*>(dt_buf);
+	c->S.halo_send = fn && part ? halo_send : nullptr;
+	c->S.halo_recv = fn && part ? halo_recv : nullptr;
+	return TRG_OK;
+}
+
+long long trg_slab_halo_bytes(const trg_ctx* c) {
+	if (!c) return 0;
+	return 4LL * 7 * c->P.ny * c->P.nz * (long long)(c->fp32 ? sizeof(float) : sizeof(double));
+}
+
+int trg_slab_partitions(const trg_ctx* c) {
+	if (!c) return 0;
+	return (c->P.lbc[0] == BC_PARTITION ? 1 : 0) | (c->P.rbc[0] == BC_PARTITION ? 2 : 0);
+}
+
+int trg_f32_scales(const trg_params* p, const double* den, const double* pre, const double* hii, const double* v0,
+                   const double* v1, const double* v2, double* scales) {
+	if (!p || !scales) return TRG_ERR_ARG;
+	HostSetup hs;
+	std::string why = host_setup(*p, den, pre, hii, v0, v1, v2, nullptr, hs);
+	if (!why.empty()) return TRG_ERR_ARG;
+	scales[0] = hs.P.f32_rho0;
+	scales[1] = hs.P.f32_p0;
+	return TRG_OK;
+}
 
 int trg_full_step(trg_ctx* c, double dt_next_checkpoint, double* dt_taken) {
 	if (!c) return TRG_ERR_ARG;
+	if (slab_unhooked(c)) return set_error(c, TRG_ERR_ARG, "a slab steps only after trg_slab_exchange");
 	int rc = ensure_dt_hist(c, c->steps + 1);
 	if (rc) return rc;
 	enqueue_full_step(c, dt_next_checkpoint);
@@ -842,6 +937,7 @@ int trg_full_step(trg_ctx* c, double dt_next_checkpoint, double* dt_taken) {
 
 int trg_run_steps(trg_ctx* c, int nsteps, double dt_next_checkpoint, double* dts_out) {
 	if (!c || nsteps < 0) return TRG_ERR_ARG;
+	if (slab_unhooked(c)) return set_error(c, TRG_ERR_ARG, "a slab steps only after trg_slab_exchange");
 	long long first = c->steps;
 	int rc = ensure_dt_hist(c, c->steps + nsteps);
 	if (rc) return rc;
@@ -854,6 +950,7 @@ int trg_run_steps(trg_ctx* c, int nsteps, double dt_next_checkpoint, double* dts
 
 int trg_enqueue_steps(trg_ctx* c, int nsteps, double dt_next_checkpoint) {
 	if (!c || nsteps < 0) return TRG_ERR_ARG;
+	if (slab_unhooked(c)) return set_error(c, TRG_ERR_ARG, "a slab steps only after trg_slab_exchange");
 	int rc = ensure_dt_hist(c, c->steps + nsteps);
 	if (rc) return rc;
 	for (int s = 0; s < nsteps; ++s) enqueue_full_step(c, dt_next_checkpoint);
@@ -1451,6 +1548,8 @@ int trg_batch_create(trg_ctx* const* grids, int G, trg_batch** out) {
 			return set_error(c, TRG_ERR_ARG, "trg_batch_create: grids differ in physics flags, solver or device");
 		if (c->S.mlp_img || c->S.harvest)
 			return set_error(c, TRG_ERR_ARG, "trg_batch_create: no learned start or harvest in a batch");
+		if (c->P.x0 != 0 || c->P.lbc[0] == BC_PARTITION || c->P.rbc[0] == BC_PARTITION)
+			return set_error(c, TRG_ERR_ARG, "trg_batch_create: slabs of a decomposed grid are not batched");
 	}
 	trg_batch* b = new trg_batch();
 	b->G = G;

@@ -472,7 +472,8 @@ __device__ __forceinline__ void apply_flip(Prim& q, int dim, int cond, int side)
 // the CTA's position only, not on the plane: a thread works out its (at most
 // two) box positions once, before the z march.  Per position: the source
 // offset xs + nx ys within a plane (-1: not staged - a corner, or beyond a
-// ragged grid edge) and the velocity flips the boundary rule applies there.
+// ragged grid edge; below -1: a ghost layer of a slab face, from the halo)
+// and the velocity flips the boundary rule applies there.
 constexpr int STAGE_PER_THREAD = (SX * SY + BX * BY - 1) / (BX * BY);
 struct StageMap {
 	int off[STAGE_PER_THREAD];
@@ -490,9 +491,19 @@ __device__ __forceinline__ StageMap stage_map(const Params& P, int x0, int y0) {
 		const bool xh = lx < HALO || lx >= HALO + BX, yh = ly < HALO || ly >= HALO + BY;
 		if (xh && yh) continue;  // corners: never part of a stencil
 		int xc, xside, yc = -1, yside = 0;
-		const int xs = bc_src(P, 0, x0 + lx - HALO, P.nx, xc, xside);
+		const int gxp = x0 + lx - HALO;
+		const int xs = bc_src(P, 0, gxp, P.nx, xc, xside);
 		const int ys = P.nd > 1 ? bc_src(P, 1, y0 + ly - HALO, P.ny, yc, yside) : 0;
 		if (P.nd <= 1) yc = -1;
+		if (xc == BC_PARTITION) {
+			// ghost layer of a slab face: from the neighbour's halo
+			// ([side][layer][field][ny * nz]), coded as -2 - ((side 2 + layer) ny + ys)
+			if (ys < 0 || ys >= P.ny) continue;
+			const int layer = (xside ? gxp - P.nx + 1 : -gxp) - 1;
+			m.off[j] = -2 - ((xside * 2 + layer) * P.ny + ys);
+			m.flags[j] = ((yc + 1) << 4) | (yside << 7);
+			continue;
+		}
 		if (xs < 0 || xs >= P.nx || ys < 0 || ys >= P.ny) continue;  // tile beyond a ragged grid edge
 		m.off[j] = xs + P.nx * ys;
 		m.flags[j] = (xc + 1) | (xside << 3) | ((yc + 1) << 4) | (yside << 7);
@@ -512,19 +523,31 @@ __device__ __forceinline__ int plane_src(const Params& P, int z, int& zc, int& z
 	return P.nd > 2 ? bc_src(P, 2, z, P.nz, zc, zside) : 0;
 }
 
+// Source of field f of staged position j in source plane zs: the state, or
+// for a ghost layer of a slab face the neighbour's halo.
+template <typename TS>
+__device__ __forceinline__ const TS* stage_src(const Params& P, const TS* Up, const void* halo, int off, int f,
+                                               int zs) {
+	if (off >= 0) return Up + (long long)f * P.N + off;
+	const int code = -2 - off, sl = code / P.ny, ys = code - sl * P.ny;
+	const long long nyz = (long long)P.ny * P.nz;
+	return static_cast<const TS*>(halo) + (long long)(sl * NU + f) * nyz + ys + (long long)P.ny * zs;
+}
+
 // Loads plane z (global index, may be a ghost plane) of the CTA's x/y box into ring slot.
 template <int STAGE, typename TS>
 __device__ __forceinline__ void load_plane(const Params& P, const Scaled& SP, const StoreScale& SC,
-                                           const TS* __restrict__ U, SmemQ& s, int slot, const StageMap& m, int z) {
+                                           const TS* __restrict__ U, const void* halo, SmemQ& s, int slot,
+                                           const StageMap& m, int z) {
 	int zc, zside;
-	const TS* Up = U + (long long)P.nx * P.ny * plane_src(P, z, zc, zside);
-	const long long N = P.N;
+	const int zs = plane_src(P, z, zc, zside);
+	const TS* Up = U + (long long)P.nx * P.ny * zs;
 #pragma unroll
 	for (int j = 0; j < STAGE_PER_THREAD; ++j) {
-		if (m.off[j] < 0) continue;
+		if (m.off[j] == -1) continue;
 		float u[7];
 #pragma unroll
-		for (int f = 0; f < 7; ++f) u[f] = load_u(Up, f * N + m.off[j], SC, f);
+		for (int f = 0; f < 7; ++f) u[f] = load_u(stage_src(P, Up, halo, m.off[j], f, zs), 0, SC, f);
 		Prim q = prim_from_cons(u, (float)P.gamma, P.nd);
 		if (STAGE == 1) fix_prim(SP, q, u[DEN]);
 		apply_flips(P, q, m.flags[j], zc, zside);
@@ -587,17 +610,17 @@ __device__ __forceinline__ bool tma_wait(uint64_t* bar, uint32_t phase) {
 }
 
 template <typename TS>
-__device__ __forceinline__ void plane_fetch(const Params& P, const TS* __restrict__ U, TS* raw, const StageMap& m,
-                                            int z) {
+__device__ __forceinline__ void plane_fetch(const Params& P, const TS* __restrict__ U, const void* halo, TS* raw,
+                                            const StageMap& m, int z) {
 	int zc, zside;
-	const TS* Up = U + (long long)P.nx * P.ny * plane_src(P, z, zc, zside);
-	const long long N = P.N;
+	const int zs = plane_src(P, z, zc, zside);
+	const TS* Up = U + (long long)P.nx * P.ny * zs;
 #pragma unroll
 	for (int j = 0; j < STAGE_PER_THREAD; ++j) {
-		if (m.off[j] < 0) continue;
+		if (m.off[j] == -1) continue;
 		const int idx = threadIdx.x + j * BX * BY;
 #pragma unroll
-		for (int f = 0; f < 7; ++f) cp_async_elem(raw + f * (SX * SY) + idx, Up + f * N + m.off[j]);
+		for (int f = 0; f < 7; ++f) cp_async_elem(raw + f * (SX * SY) + idx, stage_src(P, Up, halo, m.off[j], f, zs));
 	}
 	cp_async_commit();
 }
@@ -608,7 +631,7 @@ __device__ __forceinline__ void plane_convert(const Params& P, const Scaled& SP,
 	plane_src(P, z, zc, zside);
 #pragma unroll
 	for (int j = 0; j < STAGE_PER_THREAD; ++j) {
-		if (m.off[j] < 0) continue;
+		if (m.off[j] == -1) continue;
 		const int idx = threadIdx.x + j * BX * BY;
 		float u[7];
 #pragma unroll
@@ -797,15 +820,15 @@ __device__ __forceinline__ void hydro_stage_body(const Params& P, const State& S
 	// 3-D: the pass starts one plane early (z0 - 1), where it only forms the
 	// flux through z0 - 1/2, so that every z face goes through the same code
 	if (nd > 2) {
-		for (int z = z0 - 2; z <= z0; ++z) load_plane<STAGE>(P, SP, SC, Uq, s, slot_of(z), smap, z);
+		for (int z = z0 - 2; z <= z0; ++z) load_plane<STAGE>(P, SP, SC, Uq, S.halo_recv, s, slot_of(z), smap, z);
 		__syncthreads();
 		if (rec)
 			szc = slope_of(lim, th, get(s, slot_of(z0 - 2), ly, lx), get(s, slot_of(z0 - 1), ly, lx),
 			               get(s, slot_of(z0), ly, lx));
 		__syncthreads();  // plane z0 - 2 is read: its slot takes plane z0 + 1
-		load_plane<STAGE>(P, SP, SC, Uq, s, slot_of(z0 + 1), smap, z0 + 1);
+		load_plane<STAGE>(P, SP, SC, Uq, S.halo_recv, s, slot_of(z0 + 1), smap, z0 + 1);
 	} else {
-		load_plane<STAGE>(P, SP, SC, Uq, s, 0, smap, 0);
+		load_plane<STAGE>(P, SP, SC, Uq, S.halo_recv, s, 0, smap, 0);
 	}
 
 	// Plane z + 3 is staged (cp.async) while plane z is computed and turned into
@@ -824,7 +847,7 @@ __device__ __forceinline__ void hydro_stage_body(const Params& P, const State& S
 					tma_plane(tmap, raw, tbar, x0 - HALO, y0 - HALO, plane_src(P, z + 3, zc, zside));
 				}
 			} else {
-				plane_fetch(P, Uq, raw, smap, z + 3);
+				plane_fetch(P, Uq, S.halo_recv, raw, smap, z + 3);
 			}
 		}
 		// slopes: this cell in x, y and (of the next plane's cell) z; the cells
@@ -1151,6 +1174,31 @@ void launch_hydro_substep_fp32(const Params& P, const State& S, const double* U,
 	bool fast = P.limiter == 6 && P.riemann == RS_ROTATED;
 	if (fast) launch_one<1, double, 6, RS_ROTATED>(P, S, U, U, Uout, h, zchunk, stream);
 	else launch_one<1, double, -1, -1>(P, S, U, U, Uout, h, zchunk, stream);
+}
+
+// x-slab decomposition: the two x layers next to each PARTITION face of a
+// slab, packed [side][layer][field][ny * nz] (layer 0 next to the face) for
+// the neighbour, from the state the next flux computation reads (primitives
+// of the FP64 form, the hydro-only FP32 state): what the reference's
+// applyBCs sends for its partition ghost cells (Grid.cpp:804-833).
+template <typename T>
+__global__ void __launch_bounds__(256) k_halo_pack(Params P, const T* __restrict__ src, T* __restrict__ dst) {
+	const long long nyz = (long long)P.ny * P.nz;
+	const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (i >= 4LL * NU * nyz) return;
+	const long long yz = i % nyz;
+	const int f = (int)((i / nyz) % NU);
+	const int sl = (int)(i / (NU * nyz));  // side * 2 + layer
+	const int side = sl >> 1, layer = sl & 1;
+	if ((side ? P.rbc[0] : P.lbc[0]) != BC_PARTITION) return;
+	const int x = side ? P.nx - 1 - layer : layer;
+	dst[i] = src[(long long)f * P.N + x + (long long)P.nx * yz];
+}
+void launch_halo_pack(const Params& P, const void* src, void* dst, bool f32, cudaStream_t stream) {
+	const long long n = 4LL * NU * P.ny * P.nz;
+	const unsigned g = (unsigned)((n + 255) / 256);
+	if (f32) k_halo_pack<float><<<g, 256, 0, stream>>>(P, static_cast<const float*>(src), static_cast<float*>(dst));
+	else k_halo_pack<double><<<g, 256, 0, stream>>>(P, static_cast<const double*>(src), static_cast<double*>(dst));
 }
 
 // FP64 <-> FP32 state conversion (entry to / exit from the FP32 form), with

@@ -223,8 +223,11 @@ __device__ void rotated_hllc(double* F, const double* Ql, const double* Qr, doub
 // ------------------------------------------------------------- hydro faces
 // Ghost position p (< 0 or >= n) along dim -> interior source index and the
 // velocity rule of Grid::applyBCs (Grid.cpp:649-836).  Layer k = 1 is adjacent.
-__device__ __forceinline__ void load_line(const Params& P, const double* __restrict__ Q, long long base, long long stride,
-                                          int n, int dim, int pos, double* q) {
+// A PARTITION face (x-slab decomposition) takes ghost layer k from the
+// neighbour's halo, S.halo_recv [side][k - 1][field][ny * nz], as the
+// reference's ghost cells take the neighbour's Q (Grid.cpp:804-833).
+__device__ __forceinline__ void load_line(const Params& P, const double* __restrict__ Q, const void* halo,
+                                          long long base, long long stride, int n, int dim, int pos, double* q) {
 	int src = pos, cond = -1, side = 0;
 	if (pos < 0) {
 		int k = -pos;
@@ -235,6 +238,14 @@ __device__ __forceinline__ void load_line(const Params& P, const double* __restr
 		cond = P.rbc[dim];
 		side = 1;
 		src = cond == BC_PERIODIC ? k - 1 : (cond == BC_REFLECTING ? n - 1 - k : n - 1);
+	}
+	if (cond == BC_PARTITION) {  // x faces only: base = (j + ny k) nx
+		const long long nyz = (long long)P.ny * P.nz, trans = base / P.nx;
+		const int layer = (side ? pos - n + 1 : -pos) - 1;
+		const double* h = static_cast<const double*>(halo) + (long long)(side * 2 + layer) * NU * nyz + trans;
+#pragma unroll
+		for (int f = 0; f < NU; ++f) q[f] = h[(long long)f * nyz];
+		return;
 	}
 	long long id = base + (long long)src * stride;
 #pragma unroll
@@ -292,10 +303,10 @@ __device__ __forceinline__ void b_faces_fp64(const Params& P, const State& S, lo
 	double Ls[7], Rs[7], Fv[7];
 	if (P.order == 1) {
 		double a[7], b[7], c[7], e[7];
-		load_line(P, S.Q, base, stride, n, dim, f - 2, a);
-		load_line(P, S.Q, base, stride, n, dim, f - 1, b);
-		load_line(P, S.Q, base, stride, n, dim, f, c);
-		load_line(P, S.Q, base, stride, n, dim, f + 1, e);
+		load_line(P, S.Q, S.halo_recv, base, stride, n, dim, f - 2, a);
+		load_line(P, S.Q, S.halo_recv, base, stride, n, dim, f - 1, b);
+		load_line(P, S.Q, S.halo_recv, base, stride, n, dim, f, c);
+		load_line(P, S.Q, S.halo_recv, base, stride, n, dim, f + 1, e);
 #pragma unroll
 		for (int iq = 0; iq < NU; ++iq) {
 			// QR of the cell at f-1 and QL of the cell at f (Hydro.cpp:44-50)
@@ -305,8 +316,8 @@ __device__ __forceinline__ void b_faces_fp64(const Params& P, const State& S, lo
 			Rs[iq] = c[iq] - 0.5 * sr;
 		}
 	} else {
-		load_line(P, S.Q, base, stride, n, dim, f - 1, Ls);
-		load_line(P, S.Q, base, stride, n, dim, f, Rs);
+		load_line(P, S.Q, S.halo_recv, base, stride, n, dim, f - 1, Ls);
+		load_line(P, S.Q, S.halo_recv, base, stride, n, dim, f, Rs);
 	}
 	double a_l2 = P.gamma * Ls[PRE] / Ls[DEN];
 	double a_r2 = P.gamma * Rs[PRE] / Rs[DEN];

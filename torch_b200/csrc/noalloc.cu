@@ -107,6 +107,8 @@ extern "C" int trg_hydro_step_fp32_noalloc(trg_ctx* c, const double* U_in, doubl
 		                "cooling on");
 	if (!(dt > 0) || !(dt <= 1.0e308))
 		return ctx_fail(c, TRG_ERR_ARG, "trg_hydro_step_fp32_noalloc: dt must be positive and finite");
+	if (P.lbc[0] == BC_PARTITION || P.rbc[0] == BC_PARTITION)
+		return ctx_fail(c, TRG_ERR_ARG, "trg_hydro_step_fp32_noalloc: takes whole grids, not slabs");
 	DeviceGuard guard;
 	cudaError_t e = cudaSetDevice(ctx_device(c));
 	float* base = nullptr;

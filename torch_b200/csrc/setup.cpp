@@ -133,6 +133,7 @@ struct Geo {
 		ijk[1] = (int)((id / P.nx) % P.ny);
 		ijk[2] = (int)(id / ((long long)P.nx * P.ny));
 		for (int i = 0; i < 3; ++i) x[i] = (double)ijk[i];
+		x[0] += (double)P.x0;  // a slab's cells at their global x
 		for (int i = 0; i < P.nd; ++i) x[i] += 0.5;
 	}
 	double volume(double rc) const {
@@ -222,7 +223,7 @@ void neighbour_cells(const Params& P, const int* ijk, const double* xc, long lon
 }  // namespace
 
 std::string host_setup(const trg_params& p, const double* den, const double* pre, const double* hii, const double* v0,
-                       const double* v1, const double* v2, const double* grav, HostSetup& out) {
+                       const double* v1, const double* v2, const double* grav, HostSetup& out, const SlabSpec* slab) {
 	Params& P = out.P;
 	std::memset(&P, 0, sizeof(P));
 	if (p.nd < 1 || p.nd > 3) return "nd must be 1, 2 or 3";
@@ -233,6 +234,12 @@ std::string host_setup(const trg_params& p, const double* den, const double* pre
 		return "spatial_order must be 0 or 1 (Hydrodynamics::calcFluxes, Hydro.cpp:94-112)";
 	if (p.rt_scheme < 0 || p.rt_scheme > 2) return "rt_scheme must be 0 (implicit), 1 (implicit2) or 2 (explicit)";
 	if (!den || !pre || !hii || !v0) return "den, pre, hii and v0 are required";
+	if (slab) {
+		if (p.radiation_on || p.cooling_on || p.star_on)
+			return "slabs take hydrodynamics-only runs (no radiation, cooling or star)";
+		if (slab->nx < 2 || slab->x0 < 0 || slab->x0 + slab->nx > p.ncells[0])
+			return "a slab lies inside the grid and holds at least two x layers";
+	}
 	Converter cv;
 	cv.set_rho_pressure_time(p.dscale, p.pscale, p.tscale);
 	P.hydrogenMass = cv.to_code(1.674e-24, 1, 0, 0);
@@ -267,15 +274,23 @@ std::string host_setup(const trg_params& p, const double* den, const double* pre
 	P.gamma = p.gamma;
 	P.X = p.mass_frac_h;
 	P.nd = p.nd;
-	P.nx = p.ncells[0]; P.ny = p.ncells[1]; P.nz = p.ncells[2];
+	P.nx = slab ? slab->nx : p.ncells[0]; P.ny = p.ncells[1]; P.nz = p.ncells[2];
 	P.N = (long long)P.nx * P.ny * P.nz;
+	P.x0 = slab ? slab->x0 : 0;
+	if (slab) {
+		// Grid.cpp:804-833: a face between two slabs takes its ghosts from the
+		// neighbour (PARTITION); with periodic x the two ends are neighbours too
+		const bool many = slab->nx < p.ncells[0];
+		if (slab->x0 > 0 || (many && P.lbc[0] == BC_PERIODIC)) P.lbc[0] = BC_PARTITION;
+		if (slab->x0 + slab->nx < p.ncells[0] || (many && P.rbc[0] == BC_PERIODIC)) P.rbc[0] = BC_PARTITION;
+	}
 	P.geometry = p.geometry;
 	P.order = p.spatial_order;
 	P.ng = P.order + 1;
 	P.riemann = p.riemann;
 	P.limiter = p.limiter;
 	for (int i = 0; i < 3; ++i) P.dx[i] = 0;
-	for (int i = 0; i < P.nd; ++i) P.dx[i] = side / (double)P.nx;  // Grid.cpp:470-471 (ncells[0] for every dim)
+	for (int i = 0; i < P.nd; ++i) P.dx[i] = side / (double)p.ncells[0];  // Grid.cpp:470-471 (ncells[0] for every dim)
 	for (int d = 0; d < P.nd; ++d) {
 		int n = d == 0 ? P.nx : (d == 1 ? P.ny : P.nz);
 		bool mirror = P.lbc[d] == BC_REFLECTING || P.lbc[d] == BC_PERIODIC || P.rbc[d] == BC_REFLECTING ||
@@ -509,6 +524,10 @@ std::string host_setup(const trg_params& p, const double* den, const double* pre
 		std::nth_element(pr.begin(), pr.begin() + N / 2, pr.end());
 		P.f32_rho0 = d[N / 2] > 0 ? d[N / 2] : 1.0;
 		P.f32_p0 = pr[N / 2] > 0 ? pr[N / 2] : 1.0;
+		if (slab && slab->f32_rho0 > 0 && slab->f32_p0 > 0) {
+			P.f32_rho0 = slab->f32_rho0;
+			P.f32_p0 = slab->f32_p0;
+		}
 		P.f32_v0 = std::sqrt(P.f32_p0 / P.f32_rho0);
 	}
 	out.nactive = 0;

@@ -24,9 +24,19 @@ struct HostSetup {
 	int active[3] = {0, 0, 0};
 };
 
+// One slab of an x-slab decomposition: global x of its first cell, its
+// width, and the FP32 form's reference density and pressure (the whole
+// grid's, so that every slab scales its state alike; 0: this slab's medians).
+struct SlabSpec {
+	int x0 = 0, nx = 0;
+	double f32_rho0 = 0, f32_p0 = 0;
+};
+
 // Returns an empty string on success, else the reason for refusing the input.
+// With `slab`, p describes the whole grid and the arrays hold the slab's cells.
 std::string host_setup(const trg_params& p, const double* den, const double* pre, const double* hii, const double* v0,
-                       const double* v1, const double* v2, const double* grav, HostSetup& out);
+                       const double* v1, const double* v2, const double* grav, HostSetup& out,
+                       const SlabSpec* slab = nullptr);
 
 // Cell and star positions (cgs) as Torch::setUpLua passes them to the Lua
 // setup function; empty string on success.

@@ -60,6 +60,7 @@ __device__ __forceinline__ long long flat_id(const Params& P, int i, int j, int 
 // Grid::buildCells (Grid.cpp:525-548): centre at index + 0.5 for dims < nd, 0 beyond.
 __device__ __forceinline__ void cell_xc(const Params& P, const int* ijk, double* xc) {
 	for (int i = 0; i < 3; ++i) xc[i] = (double)ijk[i];
+	xc[0] += (double)P.x0;  // a slab's cells at their global x
 	#pragma unroll
 	for (int i = 0; i < 3; ++i) if (i < P.nd) xc[i] += 0.5;
 }

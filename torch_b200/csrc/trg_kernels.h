@@ -62,6 +62,9 @@ size_t hydro_stage_fp32_smem();
 void launch_hydro_substep_fp32(const Params& P, const State& S, const double* U, double* Uout, double h, int zchunk,
                                cudaStream_t stream);
 __global__ void k_f64_to_f32(Params P, const double* a, float* b);
+// x-slab decomposition: pack the layers next to the partition faces into dst
+// (kernels_fp32.cu); src is [7][N] doubles, or floats when f32
+void launch_halo_pack(const Params& P, const void* src, void* dst, bool f32, cudaStream_t stream);
 // FP32 form of a batch of 2-D grids: the hydro sub-step of every grid (U -> U1,
 // then U1 copied back to U)
 void launch_hydro_substep_fp32_batch(const Params& Pv, const BatchTable* B, int ntiles, double h, cudaStream_t stream);

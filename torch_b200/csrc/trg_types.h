@@ -31,6 +31,10 @@ TRG_HD inline constexpr long long t_index(long long N, int f, long long id) {
 enum { H_IMLC = 0, H_NMLC, H_RHII, H_CEHI, H_CIEC, H_NMC, H_EUVH, H_FUVH, H_IRH, H_CRH, H_TOT, NH };
 enum { G_CART = 0, G_CYL = 1, G_SPH = 2 };
 enum { BC_FREE = 0, BC_REFLECTING = 1, BC_OUTFLOW = 2, BC_INFLOW = 3, BC_PERIODIC = 4 };
+// an x face that borders another slab of an x-slab decomposition
+// (Condition::PARTITION, Grid.cpp:804-833): its ghost layers come from the
+// neighbour's halo, held in State::halo_recv
+constexpr int BC_PARTITION = 5;
 enum { CP_TTI = 0, CP_NEQ = 1, CP_OFF = 2 };
 enum { RS_HLLC = 0, RS_ROTATED = 1, RS_HLL = 2 };
 
@@ -74,6 +78,9 @@ struct BatchTable;
 struct Params {
 	int nd, nx, ny, nz;
 	long long N;
+	// x-slab decomposition: global x index of this grid's first cell (0 for a
+	// whole grid); cell centres and the geometry use global positions
+	int x0;
 	int geometry, order, ng;
 	int lbc[3], rbc[3];
 	int riemann, limiter;
@@ -121,6 +128,13 @@ struct State {
 	double* ds;     // [N]
 	double* shellVol;
 	double* grav;   // [3][N] or nullptr
+	// x-slab decomposition (caller-owned device buffers, null for a whole
+	// grid): the two boundary x layers of each partition face packed for the
+	// neighbour, and the neighbours' layers received, both
+	// [side 2][layer 2][field 7][ny * nz] (layer 0 next to the face); doubles
+	// (primitives of the FP64 form) or floats (the hydro-only FP32 state)
+	void* halo_send;
+	const void* halo_recv;
 	double* F[3];   // face fluxes per dimension [7][faces]
 	long long nfaces[3];
 	const Tables* tables;
