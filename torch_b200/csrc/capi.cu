@@ -853,6 +853,15 @@ int create_impl(const trg_params* p, const SlabSpec* slab, const double* den, co
 		LAUNCH(k_f64_to_f32, 7 * N, 256, c->P, S.U, c->U32);
 		CUDA_TRY(cudaMemsetAsync(c->U32s, 0, 7 * N * sizeof(float), st));
 	}
+	// TRG_FP64_KERNELS=exact|fast, read when a context is created: the build of
+	// the FP64 kernels (radiation, cooling and time step; the FP64 form's
+	// hydrodynamics too) in place of the form's own (exact for the FP64 form,
+	// fast for the FP32 form), to measure what each build contributes to the
+	// difference between the forms
+	if (const char* kb = std::getenv("TRG_FP64_KERNELS")) {
+		if (!std::strcmp(kb, "exact")) c->fastk = 0;
+		else if (!std::strcmp(kb, "fast")) c->fastk = 1;
+	}
 	// Torch::run prologue (Torch.cpp:245-264): Q from U with floors, and the
 	// column-density ray trace of fillHeatingArrays (Thermodynamics.cpp:420-421).
 	q_from_u(c, 0, 1);
