@@ -370,8 +370,7 @@ void trg_batch_destroy(trg_batch* b);
 int trg_hydro_step_fp32_noalloc(trg_ctx* c, const double* U_in, double* U_out, double dt, double* dt_next,
                                 void* stream);
 
-/* x-slab decomposition of a hydrodynamics-only run (no radiation, cooling or
- * star), one slab per GPU, as the reference splits its grid over MPI ranks
+/* x-slab decomposition, one slab per GPU, as the reference splits its grid over MPI ranks
  * (Grid::initialise, src/Fluid/Grid.cpp:446-459; the halo exchange of
  * Grid::applyBCs PARTITION, :804-833; the minimum time step over ranks,
  * src/Torch/Torch.cpp:323-335).  trg_create_slab takes the whole grid's
@@ -402,6 +401,33 @@ int trg_hydro_step_fp32_noalloc(trg_ctx* c, const double* U_in, double* U_out, d
  * the hook the same number of times in the same order. */
 #define TRG_EXCHANGE_HALO 0
 #define TRG_EXCHANGE_DT 1
+/* Slabs of a run with a star (radiation and/or cooling, FP64 form, no stellar
+ * wind) also sweep slab after slab outwards from the slab that holds the star
+ * (trg_slab_star_side: 0 this slab holds it, 1 it lies at lower x, 2 at
+ * higher x), as the reference's ranks pass their boundary optical depths and
+ * column densities on (Radiation::transferRadiation, src/Integrators/
+ * Radiation.cpp:573-636; Thermodynamics::rayTrace, Thermodynamics.cpp:365-417).
+ * Before stepping, trg_slab_sweep_exchange registers two more device buffers
+ * of trg_slab_sweep_bytes(c) bytes each, [side 2][ny*nz][4] doubles, and the
+ * library calls, around every causal sweep,
+ *   fn(user, TRG_EXCHANGE_SWEEP_IN, stream): before the sweep; sweep_recv
+ *     must hold, in `stream` order, the star-side neighbour's sweep_send of
+ *     its side facing this slab (nothing for the star's own slab), and this
+ *     slab's sweep_send must be free to be overwritten (every neighbour away
+ *     from the star has read its previous contents);
+ *   fn(user, TRG_EXCHANGE_SWEEP_OUT, stream): after the sweep; sweep_send
+ *     holds this slab's boundary layers, packed on `stream`, for the
+ *     neighbours away from the star (the low-x side unless the star lies at
+ *     lower x or this is the first slab, the high-x side unless it lies at
+ *     higher x or this is the last).
+ * Each slab's first causal non-wind cell takes the radiation time step's
+ * one-off form, as each rank's does in the reference (Radiation.cpp:300-316).
+ * The column-density sweep of the Torch::run prologue, which trg_create runs
+ * for a whole grid, runs at the start of a slab's first step (the hook is not
+ * registered yet when the slab is created); trg_heating is a collective call
+ * for slabs, since its ray trace goes through the sweep exchange. */
+#define TRG_EXCHANGE_SWEEP_IN 2
+#define TRG_EXCHANGE_SWEEP_OUT 3
 typedef int (*trg_exchange_fn)(void* user, int what, void* stream);
 int trg_create_slab(const trg_params* p, int x0, int nx, const double* f32_scale, const double* den,
                     const double* pre, const double* hii, const double* v0, const double* v1, const double* v2,
@@ -410,6 +436,9 @@ int trg_slab_exchange(trg_ctx* c, trg_exchange_fn fn, void* user, void* halo_sen
                       void* dt_buf);
 long long trg_slab_halo_bytes(const trg_ctx* c);
 int trg_slab_partitions(const trg_ctx* c);
+int trg_slab_sweep_exchange(trg_ctx* c, void* sweep_send, const void* sweep_recv);
+long long trg_slab_sweep_bytes(const trg_ctx* c);
+int trg_slab_star_side(const trg_ctx* c);
 int trg_f32_scales(const trg_params* p, const double* den, const double* pre, const double* hii, const double* v0,
                    const double* v1, const double* v2, double* f32_scale);
 

@@ -73,7 +73,7 @@ def test_torchgpu_binding_compiles_and_links():
 def test_slab_hook_example_compiles():
     """The NCCL exchange hook of INTEGRATION.md's decomposed-run example,
     compiled against the library header and the system NCCL header, with
-    the call it makes to register itself."""
+    the calls it makes to register itself and the sweep buffers."""
     if not os.path.exists("/usr/include/nccl.h"):
         pytest.skip("no NCCL header")
     text = open(os.path.join(common.ROOT, "INTEGRATION.md")).read()
@@ -82,6 +82,9 @@ def test_slab_hook_example_compiles():
     body = blocks[0].replace("trg_slab_exchange(ctx, exchange, &comm, send, recv, dt);",
                              "void reg(trg_ctx* ctx, SlabComm& comm, void* send, void* recv, void* dt) {\n"
                              "    trg_slab_exchange(ctx, exchange, &comm, send, recv, dt);\n}")
+    body = body.replace("trg_slab_sweep_exchange(ctx, sw_send, sw_recv);",
+                        "void reg_sweeps(trg_ctx* ctx, void* sw_send, void* sw_recv) {\n"
+                        "    trg_slab_sweep_exchange(ctx, sw_send, sw_recv);\n}")
     src = "#include <cuda_runtime.h>\n#include <nccl.h>\n#include \"torch_b200.h\"\n" + body
     with tempfile.TemporaryDirectory() as d:
         with open(os.path.join(d, "hook.cpp"), "w") as f:

@@ -79,3 +79,62 @@ def test_halo_exchange_pattern_on_three_gloo_ranks(periodic):
         assert low == (left * 10 + 1 if left is not None else -1.0)
         assert high == (right * 10 + 0 if right is not None else -1.0)
         assert dt == [100, 48, 7]
+
+
+def _sweep_rank(rank, world, port, star_slab, out):
+    """One rank of a chain of causal sweeps: each 'sweep' adds one to the
+    value received from the star-side neighbour (the star's slab starts from
+    its own rank), as a slab's boundary layer depends on its upstream one."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    import torch
+    import torch.distributed as dist
+    from torch_b200 import slabs
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    star_side = 0 if rank == star_slab else (1 if star_slab < rank else 2)
+    recv = torch.full((2, 3, 4), -1.0)
+    send = torch.zeros_like(recv)
+    seen = []
+    for sweep in range(3):
+        slabs.sweep_receive(recv, rank, world, star_side)
+        up = slabs.sweep_upstream(rank, world, star_side)
+        base = 100.0 * sweep if up is None else float(recv[0 if up < rank else 1].mean())
+        seen.append(base)
+        send.fill_(base + 1.0)
+        slabs.sweep_send(send, rank, world, star_side)
+    dist.barrier()
+    dist.destroy_process_group()
+    out.put((rank, star_side, seen))
+
+
+@pytest.mark.parametrize("star_slab", [0, 1, 3])
+def test_sweep_chain_runs_outwards_from_the_star_on_four_gloo_ranks(star_slab):
+    """The radiation and column-density sweeps of a decomposed run: a slab
+    receives its star-side neighbour's boundary layer before its sweep and
+    hands its own to the slabs away from the star after it
+    (Radiation.cpp:573-636), so slab r's sweep k sees the star slab's sweep k
+    passed on |r - star| times; no slab sends towards the star."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    world = 4
+    ps = [ctx.Process(target=_sweep_rank, args=(r, world, port, star_slab, q)) for r in range(world)]
+    for p in ps:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in ps)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, star_side, seen in res:
+        assert star_side == (0 if rank == star_slab else (1 if star_slab < rank else 2))
+        assert seen == [100.0 * k + abs(rank - star_slab) for k in range(3)]
+
+
+def test_sweep_neighbours():
+    sys.path.insert(0, ROOT)
+    from torch_b200 import slabs
+    # star in slab 1 of 4: slab 1 sends both ways, 0 sends nowhere, 2 sends right, 3 nowhere
+    assert slabs.sweep_downstream(1, 4, 0) == [(0, 0), (2, 1)]
+    assert slabs.sweep_downstream(0, 4, 2) == [] and slabs.sweep_upstream(0, 4, 2) == 1
+    assert slabs.sweep_downstream(2, 4, 1) == [(3, 1)] and slabs.sweep_upstream(2, 4, 1) == 1
+    assert slabs.sweep_downstream(3, 4, 1) == [] and slabs.sweep_upstream(1, 4, 0) is None

@@ -80,7 +80,7 @@ _lib = None
 # (name, restype, argtypes) for every entry point of include/torch_b200.h
 # the x-slab exchange hook of trg_slab_exchange: int fn(void* user, int what, void* stream)
 EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_void_p)
-EXCHANGE_HALO, EXCHANGE_DT = 0, 1
+EXCHANGE_HALO, EXCHANGE_DT, EXCHANGE_SWEEP_IN, EXCHANGE_SWEEP_OUT = 0, 1, 2, 3
 
 _SIGNATURES = [
     ("trg_create", C.c_int, [C.POINTER(TrgParams)] + [C.c_void_p] * 7 + [C.POINTER(C.c_void_p)]),
@@ -150,6 +150,9 @@ _SIGNATURES = [
     ("trg_slab_exchange", C.c_int, [C.c_void_p, EXCHANGE_FN, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("trg_slab_halo_bytes", C.c_longlong, [C.c_void_p]),
     ("trg_slab_partitions", C.c_int, [C.c_void_p]),
+    ("trg_slab_sweep_exchange", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("trg_slab_sweep_bytes", C.c_longlong, [C.c_void_p]),
+    ("trg_slab_star_side", C.c_int, [C.c_void_p]),
     ("trg_f32_scales", C.c_int, [C.c_void_p] + [C.c_void_p] * 6 + [C.c_void_p]),
 ]
 
@@ -347,7 +350,7 @@ class Torch:
     def __init__(self, tp: TorchParameters, ic, precision: int = PRECISION_FP64, device: int = 0, slab=None):
         """slab = (x0, nx, f32_scale or None): this context holds global x from
         x0 to x0 + nx - 1 of the grid `ic` describes (trg_create_slab); the
-        hydrodynamics-only step then needs an exchange hook (torch_b200.slabs)."""
+        step then needs an exchange hook (torch_b200.slabs)."""
         self.lib = load_library()
         p = make_params(tp, ic.side_length, ic.ncells, precision, device)
         fields = [ic.den, ic.pre, ic.hii, ic.vel[0], ic.vel[1], ic.vel[2]]

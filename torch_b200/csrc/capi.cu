@@ -56,6 +56,12 @@ struct trg_ctx {
 	void* xuser = nullptr;
 	unsigned long long* xdt = nullptr;  // the host's device buffer of the three time-step minima
 	bool xfail = false;
+	// ... with a star: the boundary layer packed after each causal sweep for
+	// the neighbour away from the star (the received one is S.sweep_recv)
+	double* sweep_send = nullptr;
+	// ... and the Torch::run prologue's column-density sweep, deferred to the
+	// slab's first step
+	bool prologue_colden = false;
 	// FP32 form (either kind): the FP64 kernels come from the fast build
 	int fastk = 0;  // kernel build: 0 exact, 1 fast, 2 fast with the batch dispatch
 	// FP32 form with radiation/cooling: Q already holds the primitives of the
@@ -279,6 +285,23 @@ void dt_exchange(trg_ctx* c) {
 	cudaMemcpyAsync(c->S.scal + 2, c->xdt, b, cudaMemcpyDeviceToDevice, c->stream);
 }
 
+// x-slab decomposition with a star: the causal sweeps run slab after slab
+// outwards from the star's slab, as the reference's ranks do
+// (Radiation.cpp:573-636, Thermodynamics.cpp:365-417).  Before a sweep the
+// hook makes S.sweep_recv hold the star-side neighbour's boundary layer of
+// the fields that sweep reads (and frees this slab's send buffer); after it,
+// this slab's boundary layers are packed and the hook hands them on.
+void sweep_in(trg_ctx* c) {
+	if (!c->sweep_send) return;
+	if (c->xfn(c->xuser, TRG_EXCHANGE_SWEEP_IN, c->stream) != 0) c->xfail = true;
+}
+void sweep_out(trg_ctx* c, bool colden) {
+	if (!c->sweep_send) return;
+	launch_sweep_pack(c->P, colden ? c->S.T : c->S.R, colden, c->sweep_send, c->stream);
+	c->launches++;
+	if (c->xfn(c->xuser, TRG_EXCHANGE_SWEEP_OUT, c->stream) != 0) c->xfail = true;
+}
+
 void colden_sweep_direct(trg_ctx* c) {
 	const auto& off = c->hs.off_all;
 	const bool sw = c->S.sw_col != nullptr;
@@ -326,8 +349,10 @@ void launch_graph(trg_ctx* c, cudaGraphExec_t ge, long long nodes, const char* n
 void colden_sweep(trg_ctx* c) {
 	if (c->use_graphs && !c->g_colden)
 		c->g_colden = capture_graph(c, [&] { colden_sweep_direct(c); }, c->g_colden_nodes);
+	sweep_in(c);
 	if (c->use_graphs && c->g_colden) launch_graph(c, c->g_colden, c->g_colden_nodes, "graph_colden_sweep");
 	else colden_sweep_direct(c);
+	sweep_out(c, true);
 }
 
 void thermo_pre(trg_ctx* c) {
@@ -418,8 +443,10 @@ void tau_sweep_direct(trg_ctx* c) {
 
 void rad_integrate2(trg_ctx* c, double h) {
 	if (c->use_graphs && !c->g_tau) c->g_tau = capture_graph(c, [&] { tau_sweep_direct(c); }, c->g_tau_nodes);
+	sweep_in(c);
 	if (c->use_graphs && c->g_tau) launch_graph(c, c->g_tau, c->g_tau_nodes, "graph_tau_sweep");
 	else tau_sweep_direct(c);
+	sweep_out(c, false);
 	int n = (int)c->hs.sweep_nonwind.size();
 	LAUNCH(KF(k_rad_solve2), n, 128, c->P, c->S, c->d_sweep_nonwind, n, h);
 }
@@ -435,12 +462,16 @@ void rad_integrate(trg_ctx* c, double h) {
 		int gi = h == 0.5 ? 0 : 1;
 		if (!c->g_rad[gi]) c->g_rad[gi] = capture_graph(c, [&] { rad_sweep_direct(c, h); }, c->g_rad_nodes[gi]);
 		if (c->g_rad[gi]) {
+			sweep_in(c);
 			launch_graph(c, c->g_rad[gi], c->g_rad_nodes[gi], "graph_rad_sweep");
+			sweep_out(c, false);
 			return;
 		}
 	}
 	if (c->P.star_on) {
+		sweep_in(c);
 		rad_sweep_direct(c, h);
+		sweep_out(c, false);
 	} else {
 		LAUNCH(KF(k_rad_no_star_fp64), c->P.N, 256, c->P, c->S, h);
 	}
@@ -616,6 +647,11 @@ void enqueue_full_step(trg_ctx* c, double dt_next) {
 	// Torch::fullStep, Torch.cpp:389-418
 	if (!c->q_fresh) q_from_u(c, 0, 1);
 	c->q_fresh = false;
+	if (c->prologue_colden) {  // a slab's deferred prologue sweep (of this Q: no second sweep below)
+		colden_sweep(c);
+		c->prologue_colden = false;
+		c->colden_valid = true;
+	}
 	if (c->P.cooling_on && c->P.radiation_on && c->P.star_on && c->side) {
 		// Radiation::preTimeStepCalculations (heating rates, reads Q, R) beside
 		// Thermodynamics::preTimeStepCalculations (column densities and rates,
@@ -684,6 +720,9 @@ int check_device_error(trg_ctx* c) {
 	if (e & ERRB_DT) return set_error(c, TRG_ERR_DT, "Radiation::calculateTimeStep: invalid timestep");
 	if (e & ERRB_TC) return set_error(c, TRG_ERR_TC, "learned start: tensor-core wait expired");
 	if (e & ERRB_ASYNC) return set_error(c, TRG_ERR_CUDA, "hydro pass: a TMA plane copy did not complete in time");
+	if (e & ERRB_SLAB)
+		return set_error(c, TRG_ERR_ARG, "slab sweep: a partition-face neighbour was read before any boundary layer "
+		                                 "was exchanged");
 	if (e & ERRB_SUBCYCLE)
 		return set_error(c, TRG_ERR_SUBCYCLE, "Thermodynamics::integrate: a cell needs more thermal sub-cycles than "
 		                                      "the work queue runs (2^26)");
@@ -739,8 +778,10 @@ int ctx_fp32_zchunk(const trg_ctx* c) {
 }
 int ctx_fail(trg_ctx* c, int code, const std::string& msg) { return set_error(c, code, msg); }
 // a slab with partition faces and no exchange hook yet
+// (with a star, also the buffers of the sweep exchange)
 bool slab_unhooked(const trg_ctx* c) {
-	return (c->P.lbc[0] == BC_PARTITION || c->P.rbc[0] == BC_PARTITION) && !c->xfn;
+	const bool part = c->P.lbc[0] == BC_PARTITION || c->P.rbc[0] == BC_PARTITION;
+	return part && (!c->xfn || (c->P.star_on && !c->sweep_send));
 }
 }  // namespace trg
 
@@ -766,6 +807,8 @@ int create_impl(const trg_params* p, const SlabSpec* slab, const double* den, co
 	}
 	*out = c;
 	c->P = c->hs.P;
+	// slabs with a star call the sweep hooks on the context's own stream only
+	if (slab && c->P.star_on) c->colden_overlap = false;
 	const long long N = c->P.N;
 	CUDA_TRY(cudaSetDevice(p->device));
 	CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
@@ -864,8 +907,14 @@ int create_impl(const trg_params* p, const SlabSpec* slab, const double* den, co
 	}
 	// Torch::run prologue (Torch.cpp:245-264): Q from U with floors, and the
 	// column-density ray trace of fillHeatingArrays (Thermodynamics.cpp:420-421).
+	// A slab's sweep needs its neighbours' boundary layers, which the host's
+	// hook can move only once every slab is registered: a slab runs this
+	// prologue sweep at the start of its first step instead (on the same Q).
 	q_from_u(c, 0, 1);
-	if (c->P.star_on) colden_sweep(c);
+	if (c->P.star_on) {
+		if (slab && (c->P.lbc[0] == BC_PARTITION || c->P.rbc[0] == BC_PARTITION)) c->prologue_colden = true;
+		else colden_sweep(c);
+	}
 	// the host copies of the initial fields are no longer needed
 	std::vector<double>().swap(c->hs.U);
 	std::vector<double>().swap(c->hs.Q);
@@ -910,6 +959,32 @@ int trg_slab_exchange(trg_ctx* c, trg_exchange_fn fn, void* user, void* halo_sen
 	return TRG_OK;
 }
 
+static void drop_graphs(trg_ctx* c);
+int trg_slab_sweep_exchange(trg_ctx* c, void* sweep_send, const void* sweep_recv) {
+	if (!c) return TRG_ERR_ARG;
+	const bool part = c->P.lbc[0] == BC_PARTITION || c->P.rbc[0] == BC_PARTITION;
+	if (!part || !c->P.star_on)
+		return set_error(c, TRG_ERR_ARG, "trg_slab_sweep_exchange: only slabs of a run with a star exchange sweeps");
+	if (!sweep_send || !sweep_recv)
+		return set_error(c, TRG_ERR_ARG, "trg_slab_sweep_exchange: needs both sweep buffers");
+	CUDA_TRY(cudaStreamSynchronize(c->stream));
+	c->sweep_send = static_cast<double*>(sweep_send);
+	c->S.sweep_recv = static_cast<const double*>(sweep_recv);
+	drop_graphs(c);  // the captured sweeps hold the state by value
+	return TRG_OK;
+}
+
+long long trg_slab_sweep_bytes(const trg_ctx* c) {
+	if (!c) return 0;
+	return 2LL * 4 * c->P.ny * c->P.nz * (long long)sizeof(double);
+}
+
+int trg_slab_star_side(const trg_ctx* c) {
+	if (!c || !c->P.star_on) return 0;
+	const int sx = c->raw.star_pos[0];
+	return sx < c->P.x0 ? 1 : (sx > c->P.x0 + c->P.nx - 1 ? 2 : 0);
+}
+
 long long trg_slab_halo_bytes(const trg_ctx* c) {
 	if (!c) return 0;
 	return 4LL * 7 * c->P.ny * c->P.nz * (long long)(c->fp32 ? sizeof(float) : sizeof(double));
@@ -933,7 +1008,7 @@ int trg_f32_scales(const trg_params* p, const double* den, const double* pre, co
 
 int trg_full_step(trg_ctx* c, double dt_next_checkpoint, double* dt_taken) {
 	if (!c) return TRG_ERR_ARG;
-	if (slab_unhooked(c)) return set_error(c, TRG_ERR_ARG, "a slab steps only after trg_slab_exchange");
+	if (slab_unhooked(c)) return set_error(c, TRG_ERR_ARG, "a slab steps only after trg_slab_exchange (with a star, also trg_slab_sweep_exchange)");
 	int rc = ensure_dt_hist(c, c->steps + 1);
 	if (rc) return rc;
 	enqueue_full_step(c, dt_next_checkpoint);
@@ -946,7 +1021,7 @@ int trg_full_step(trg_ctx* c, double dt_next_checkpoint, double* dt_taken) {
 
 int trg_run_steps(trg_ctx* c, int nsteps, double dt_next_checkpoint, double* dts_out) {
 	if (!c || nsteps < 0) return TRG_ERR_ARG;
-	if (slab_unhooked(c)) return set_error(c, TRG_ERR_ARG, "a slab steps only after trg_slab_exchange");
+	if (slab_unhooked(c)) return set_error(c, TRG_ERR_ARG, "a slab steps only after trg_slab_exchange (with a star, also trg_slab_sweep_exchange)");
 	long long first = c->steps;
 	int rc = ensure_dt_hist(c, c->steps + nsteps);
 	if (rc) return rc;
@@ -959,7 +1034,7 @@ int trg_run_steps(trg_ctx* c, int nsteps, double dt_next_checkpoint, double* dts
 
 int trg_enqueue_steps(trg_ctx* c, int nsteps, double dt_next_checkpoint) {
 	if (!c || nsteps < 0) return TRG_ERR_ARG;
-	if (slab_unhooked(c)) return set_error(c, TRG_ERR_ARG, "a slab steps only after trg_slab_exchange");
+	if (slab_unhooked(c)) return set_error(c, TRG_ERR_ARG, "a slab steps only after trg_slab_exchange (with a star, also trg_slab_sweep_exchange)");
 	int rc = ensure_dt_hist(c, c->steps + nsteps);
 	if (rc) return rc;
 	for (int s = 0; s < nsteps; ++s) enqueue_full_step(c, dt_next_checkpoint);
@@ -995,6 +1070,11 @@ int trg_component(trg_ctx* c, int comp, int phase, double dt, double* out) {
 	if (c) c->q_fresh = c->colden_valid = false;
 	if (!c) return TRG_ERR_ARG;
 	if (c->fp32 || c->mixed) return set_error(c, TRG_ERR_ARG, "per-component phases are provided by the FP64 form");
+	if (slab_unhooked(c)) return set_error(c, TRG_ERR_ARG, "a slab steps only after trg_slab_exchange (with a star, also trg_slab_sweep_exchange)");
+	if (c->prologue_colden) {  // a slab's deferred prologue sweep
+		colden_sweep(c);
+		c->prologue_colden = false;
+	}
 	// The phase kernels read dt from the device scalar: stage the caller's dt.
 	CUDA_TRY(cudaMemcpyAsync(c->S.scal, &dt, sizeof(double), cudaMemcpyHostToDevice, c->stream));
 	switch (phase) {
@@ -1152,6 +1232,7 @@ int trg_checkpoint_load(trg_ctx* c, const void* buf, long long bytes) {
 	CUDA_TRY(cudaMemset(c->S.UDOT, 0, 7 * N * sizeof(double)));
 	c->q_fresh = h.q_fresh != 0;
 	c->colden_valid = false;
+	c->prologue_colden = false;  // the restored T is the saved run's
 	c->steps = h.steps;
 	c->first_time = h.first_time;
 	c->rad_once_pending = h.rad_once_pending;
@@ -1319,6 +1400,8 @@ int trg_heating_enable(trg_ctx* c, int on) {
 int trg_heating(trg_ctx* c, double* H) {
 	if (!c || !H) return TRG_ERR_ARG;
 	if (!c->S.H) return set_error(c, TRG_ERR_ARG, "trg_heating: call trg_heating_enable before stepping");
+	// (slabs: a collective call, its ray trace runs through the sweep exchange)
+	if (slab_unhooked(c)) return set_error(c, TRG_ERR_ARG, "a slab steps only after trg_slab_exchange (with a star, also trg_slab_sweep_exchange)");
 	// Thermodynamics::fillHeatingArrays: rayTrace, then the per-cell terms
 	if (c->P.star_on) colden_sweep(c);
 	LAUNCH(KF(k_heating_arrays_fp64), c->P.N, 256, c->P, c->S);
@@ -1414,21 +1497,29 @@ int trg_autotune(trg_ctx* c, int* zchunk_out, double* ms_out) {
 		if (c->fp32) launch_hydro_stage_fp32(1, c->P, c->S, c->U32, c->U32, c->U32s, zc, c->stream);
 		else launch_hydro_substep_fp32(c->P, c->S, c->S.U, c->S.U1, 0.5, zc, c->stream);
 	};
+	// Launches before the timed ones bring the SM clock up from idle (the
+	// first candidates would otherwise be timed at a lower clock than the
+	// last), and every candidate is timed in two rounds, keeping its faster.
+	for (int r = 0; r < 8; ++r) trial(cand.back());
+	std::vector<float> cand_ms(cand.size(), 1e30f);
+	for (int round = 0; round < 2; ++round)
+		for (size_t i = 0; i < cand.size(); ++i) {
+			trial(cand[i]);
+			cudaEventRecord(e0, c->stream);
+			for (int r = 0; r < 3; ++r) trial(cand[i]);
+			cudaEventRecord(e1, c->stream);
+			CUDA_TRY(cudaEventSynchronize(e1));
+			float ms = 0;
+			cudaEventElapsedTime(&ms, e0, e1);
+			cand_ms[i] = std::min(cand_ms[i], ms);
+		}
 	int best = c->zchunk;
 	float best_ms = 1e30f;
-	for (int zc : cand) {
-		trial(zc);
-		cudaEventRecord(e0, c->stream);
-		for (int r = 0; r < 3; ++r) trial(zc);
-		cudaEventRecord(e1, c->stream);
-		CUDA_TRY(cudaEventSynchronize(e1));
-		float ms = 0;
-		cudaEventElapsedTime(&ms, e0, e1);
-		if (ms < best_ms) {
-			best_ms = ms;
-			best = zc;
+	for (size_t i = 0; i < cand.size(); ++i)
+		if (cand_ms[i] < best_ms) {
+			best_ms = cand_ms[i];
+			best = cand[i];
 		}
-	}
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
 	CUDA_TRY(cudaMemcpy(c->S.scal, scal, sizeof(scal), cudaMemcpyHostToDevice));

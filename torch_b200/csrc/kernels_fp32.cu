@@ -497,9 +497,13 @@ __device__ __forceinline__ StageMap stage_map(const Params& P, int x0, int y0) {
 		if (P.nd <= 1) yc = -1;
 		if (xc == BC_PARTITION) {
 			// ghost layer of a slab face: from the neighbour's halo
-			// ([side][layer][field][ny * nz]), coded as -2 - ((side 2 + layer) ny + ys)
+			// ([side][layer][field][ny * nz]), coded as -2 - ((side 2 + layer) ny + ys).
+			// Box positions further out than the HALO ghost layers (a tile that
+			// overhangs a slab narrower than BX) are no stencil's cells and are
+			// not staged: the halo holds HALO layers per side only.
 			if (ys < 0 || ys >= P.ny) continue;
 			const int layer = (xside ? gxp - P.nx + 1 : -gxp) - 1;
+			if (layer >= HALO) continue;
 			m.off[j] = -2 - ((xside * 2 + layer) * P.ny + ys);
 			m.flags[j] = ((yc + 1) << 4) | (yside << 7);
 			continue;
@@ -1199,6 +1203,35 @@ void launch_halo_pack(const Params& P, const void* src, void* dst, bool f32, cud
 	const unsigned g = (unsigned)((n + 255) / 256);
 	if (f32) k_halo_pack<float><<<g, 256, 0, stream>>>(P, static_cast<const float*>(src), static_cast<float*>(dst));
 	else k_halo_pack<double><<<g, 256, 0, stream>>>(P, static_cast<const double*>(src), static_cast<double*>(dst));
+}
+
+// x-slab decomposition with a star: the slab's boundary x layer next to each
+// partition face, packed [side][ny * nz][4] for the neighbour on the far side
+// from the star after a causal sweep - the four optical depths of a cell (R
+// quad) or its COL_DEN, DCOL_DEN (T pair) - as the reference sends them after
+// Radiation::transferRadiation and Thermodynamics::rayTrace
+// (Radiation.cpp:614-635, Thermodynamics.cpp:398-416).
+__global__ void __launch_bounds__(256) k_sweep_pack(Params P, const double* __restrict__ src, int colden,
+                                                    double* __restrict__ dst) {
+	const long long nyz = (long long)P.ny * P.nz;
+	const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+	if (i >= 2 * nyz) return;
+	const int side = (int)(i / nyz);
+	const long long yz = i - side * nyz;
+	if ((side ? P.rbc[0] : P.lbc[0]) != BC_PARTITION) return;
+	const long long id = (side ? P.nx - 1 : 0) + (long long)P.nx * yz;
+	double2* d = reinterpret_cast<double2*>(dst + i * 4);
+	if (colden) {
+		d[0] = reinterpret_cast<const double2*>(src + id * 2)[0];
+	} else {
+		const double2* q = reinterpret_cast<const double2*>(src + id * 4);
+		d[0] = q[0];
+		d[1] = q[1];
+	}
+}
+void launch_sweep_pack(const Params& P, const double* src, bool colden, double* dst, cudaStream_t stream) {
+	const long long n = 2LL * P.ny * P.nz;
+	k_sweep_pack<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(P, src, colden ? 1 : 0, dst);
 }
 
 // FP64 <-> FP32 state conversion (entry to / exit from the FP32 form), with

@@ -572,7 +572,12 @@ __device__ __forceinline__ double pick3(double a0, double a1, double a2, int k) 
 // C2-Ray upwind neighbours and weights (Grid::calculateNearestNeighbours,
 // Grid.cpp:922-952) computed on the fly.  A neighbour outside the interior
 // (a ghost cell or none in the reference) contributes zero optical depth and
-// is returned as -1.
+// is returned as -1.  In an x slab, a neighbour one layer beyond a partition
+// face is the reference's partition ghost cell (reached through the grid
+// joins, Grid.cpp:936-943), which holds the star-side neighbour's boundary
+// layer as received before the sweep (Radiation.cpp:578-588,
+// Thermodynamics.cpp:372-380): it is returned as -2 - (side ny nz + j + ny k),
+// its index into S.sweep_recv.
 // The rotated frame (irot) is resolved with selects rather than indexed
 // arrays, so that everything stays in registers.
 __device__ __forceinline__ void neighbours(const Params& P, const int* ijk, const double* xc, long long* nb, double* w) {
@@ -599,8 +604,11 @@ __device__ __forceinline__ void neighbours(const Params& P, const int* ijk, cons
 		const int ti = ijk[0] + (r0 == 0 ? o0 : 0) + (r1 == 0 ? o1 : 0) + (r2 == 0 ? o2 : 0);
 		const int tj = ijk[1] + (r0 == 1 ? o0 : 0) + (r1 == 1 ? o1 : 0) + (r2 == 1 ? o2 : 0);
 		const int tk = ijk[2] + (r0 == 2 ? o0 : 0) + (r1 == 2 ? o1 : 0) + (r2 == 2 ? o2 : 0);
-		bool in = ti >= 0 && ti < P.nx && tj >= 0 && tj < P.ny && tk >= 0 && tk < P.nz;
+		const bool yz = tj >= 0 && tj < P.ny && tk >= 0 && tk < P.nz;
+		const bool in = ti >= 0 && ti < P.nx && yz;
 		nb[n] = in ? flat_id(P, ti, tj, tk) : -1;
+		if (!in && yz && ((ti == -1 && P.lbc[0] == BC_PARTITION) || (ti == P.nx && P.rbc[0] == BC_PARTITION)))
+			nb[n] = -2 - ((ti < 0 ? 0 : (long long)P.ny * P.nz) + tj + (long long)P.ny * tk);
 	}
 	double ic0 = (int)x0 - 0.5 * (s2 * d0 / d2);
 	double ic1 = (int)x1 - 0.5 * (s2 * d1 / d2);
@@ -672,13 +680,31 @@ __device__ __forceinline__ double tau_interp(const Params& P, const double* tau,
 // belong to the shell being swept: it is not read.  Neighbour optical depths
 // written by the previous shell are read past L1, one 16-byte pair (TAU, DTAU
 // or TAU_A, DTAU_A) at a time.
-__device__ __forceinline__ bool nb_read(const long long* nb, const double* w0, int i) { return nb[i] >= 0 && w0[i] != 0; }
+// A slab's boundary-layer neighbour with no received layer (a sweep outside
+// the exchange, which the host does not launch) is reported, never read.
+__device__ __forceinline__ bool nb_read(const State& S, const long long* nb, const double* w0, int i) {
+	if (nb[i] == -1 || w0[i] == 0) return false;
+	if (nb[i] < -1 && !S.sweep_recv) {
+		atomicOr(S.err, ERRB_SLAB);
+		return false;
+	}
+	return true;
+}
+// A neighbour's four optical depths (R quad) and its column densities
+// (COL_DEN, DCOL_DEN): in the state, or across a slab's partition face in
+// the received boundary layer (4 doubles per cell).
+__device__ __forceinline__ const double2* nb_quad(const State& S, long long nb) {
+	return reinterpret_cast<const double2*>(nb >= 0 ? S.R + nb * 4 : S.sweep_recv + (-2 - nb) * 4);
+}
+__device__ __forceinline__ const double2* nb_colden(const State& S, long long nb) {
+	return reinterpret_cast<const double2*>(nb >= 0 ? S.T + nb * 2 : S.sweep_recv + (-2 - nb) * 4);
+}
 // TAU (from TAU + DTAU of the neighbours)
 __device__ __forceinline__ double tau_sc(const Params& P, const State& S, const long long* nb, const double* w0) {
 	double tau[4] = {0, 0, 0, 0};
 	for (int i = 0; i < 4; ++i)
-		if (nb_read(nb, w0, i)) {
-			const double2 a = __ldcg(reinterpret_cast<const double2*>(S.R + nb[i] * 4));
+		if (nb_read(S, nb, w0, i)) {
+			const double2 a = __ldcg(nb_quad(S, nb[i]));
 			tau[i] = a.x + a.y;
 		}
 	return tau_interp(P, tau, w0);
@@ -688,8 +714,8 @@ __device__ __forceinline__ void tau_sc2(const Params& P, const State& S, const l
                                         double& tau_out, double& tau_a_out) {
 	double tau[4] = {0, 0, 0, 0}, tau_a[4] = {0, 0, 0, 0};
 	for (int i = 0; i < 4; ++i)
-		if (nb_read(nb, w0, i)) {
-			const double2* q = reinterpret_cast<const double2*>(S.R + nb[i] * 4);
+		if (nb_read(S, nb, w0, i)) {
+			const double2* q = nb_quad(S, nb[i]);
 			const double2 a = __ldcg(q), b = __ldcg(q + 1);
 			tau[i] = a.x + a.y;
 			tau_a[i] = b.x + b.y;
@@ -1456,8 +1482,8 @@ __device__ __forceinline__ void b_colden_shell_fp64(const Params& P, const State
 		double colden[4] = {0, 0, 0, 0}, w[4];
 #ifdef TRG_FAST_MATH
 		for (int i = 0; i < 4; ++i)
-			if (nb_read(nb, w0, i)) {
-				const double2 c = __ldcg(reinterpret_cast<const double2*>(S.T + nb[i] * 2));  // COL_DEN, DCOL_DEN
+			if (nb_read(S, nb, w0, i)) {
+				const double2 c = __ldcg(nb_colden(S, nb[i]));  // COL_DEN, DCOL_DEN
 				colden[i] = c.x + c.y;
 			}
 		// The interpolation is the weighted harmonic mean sum(w0) / sum(w0 / c)
@@ -1486,8 +1512,8 @@ __device__ __forceinline__ void b_colden_shell_fp64(const Params& P, const State
 		}
 #else
 		for (int i = 0; i < 4; ++i) {
-			if (nb_read(nb, w0, i)) {
-				const double2 c = __ldcg(reinterpret_cast<const double2*>(S.T + nb[i] * 2));  // COL_DEN, DCOL_DEN
+			if (nb_read(S, nb, w0, i)) {
+				const double2 c = __ldcg(nb_colden(S, nb[i]));  // COL_DEN, DCOL_DEN
 				colden[i] = c.x + c.y;
 			}
 			w[i] = colden[i] == 0 ? 0 : w0[i] / colden[i];

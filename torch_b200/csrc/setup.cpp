@@ -235,8 +235,10 @@ std::string host_setup(const trg_params& p, const double* den, const double* pre
 	if (p.rt_scheme < 0 || p.rt_scheme > 2) return "rt_scheme must be 0 (implicit), 1 (implicit2) or 2 (explicit)";
 	if (!den || !pre || !hii || !v0) return "den, pre, hii and v0 are required";
 	if (slab) {
-		if (p.radiation_on || p.cooling_on || p.star_on)
-			return "slabs take hydrodynamics-only runs (no radiation, cooling or star)";
+		if ((p.radiation_on || p.cooling_on || p.star_on) && p.precision != TRG_PRECISION_FP64)
+			return "slabs of a run with radiation, cooling or a star take the FP64 form";
+		if (p.star_on && (p.mass_loss_rate != 0 || p.wind_cell_radius > 0))
+			return "slabs take no stellar wind (its injection volume would be split over slabs)";
 		if (slab->nx < 2 || slab->x0 < 0 || slab->x0 + slab->nx > p.ncells[0])
 			return "a slab lies inside the grid and holds at least two x layers";
 	}
@@ -321,13 +323,17 @@ std::string host_setup(const trg_params& p, const double* den, const double* pre
 	if (P.nd < 3) P.sxc[2] = 0;
 	if (P.nd < 2) P.sxc[1] = 0;
 	Geo g(P);
-	P.star_cell = g.within(p.star_pos) ? p.star_pos[0] + (long long)P.nx * (p.star_pos[1] + (long long)P.ny * p.star_pos[2]) : -1;
+	// the star's cell in this grid's (a slab's) own indices
+	const int sp_loc[3] = {p.star_pos[0] - P.x0, p.star_pos[1], p.star_pos[2]};
+	P.star_cell = g.within(sp_loc) ? sp_loc[0] + (long long)P.nx * (sp_loc[1] + (long long)P.ny * sp_loc[2]) : -1;
 
 	const long long N = P.N;
 	// Causal order (Grid::buildCausal, Grid.cpp:568-574) -> wind list and the
 	// first non-wind cell; wind volume summed in that order (Star.cpp:42-51).
-	int start[3] = {(int)smin(smax(0, p.star_pos[0]), P.nx - 1), (int)smin(smax(0, p.star_pos[1]), P.ny - 1),
-	                (int)smin(smax(0, p.star_pos[2]), P.nz - 1)};
+	// (a slab walks its own cells from the one nearest the star,
+	// Grid::nearestCoord / buildCausal, Grid.cpp:252-258, :568-574)
+	int start[3] = {(int)smin(smax(0, sp_loc[0]), P.nx - 1), (int)smin(smax(0, sp_loc[1]), P.ny - 1),
+	                (int)smin(smax(0, sp_loc[2]), P.nz - 1)};
 	int cur[3] = {start[0], start[1], start[2]}, nxt[3];
 	std::vector<char> wind(N, 0);
 	double wind_volume = 0;
@@ -351,7 +357,8 @@ std::string host_setup(const trg_params& p, const double* den, const double* pre
 		++visited;
 	}
 	if (visited != N) return "causal order does not cover the grid";
-	P.mdot = massLossRate / wind_volume;
+	// (a slab without the star's cell has no wind cells: no injection)
+	P.mdot = (slab && wind_volume == 0) ? 0.0 : massLossRate / wind_volume;
 	P.edot = 0.5 * P.mdot * windVelocity * windVelocity;
 
 	build_tables(cv, out.tables);

@@ -65,6 +65,9 @@ __global__ void k_f64_to_f32(Params P, const double* a, float* b);
 // x-slab decomposition: pack the layers next to the partition faces into dst
 // (kernels_fp32.cu); src is [7][N] doubles, or floats when f32
 void launch_halo_pack(const Params& P, const void* src, void* dst, bool f32, cudaStream_t stream);
+// ... and with a star, the boundary x layer of R's optical depths (colden =
+// false) or T's column densities into dst [side 2][ny * nz][4] after a sweep
+void launch_sweep_pack(const Params& P, const double* src, bool colden, double* dst, cudaStream_t stream);
 // FP32 form of a batch of 2-D grids: the hydro sub-step of every grid (U -> U1,
 // then U1 copied back to U)
 void launch_hydro_substep_fp32_batch(const Params& Pv, const BatchTable* B, int ntiles, double h, cudaStream_t stream);

@@ -42,6 +42,7 @@ enum { RS_HLLC = 0, RS_ROTATED = 1, RS_HLL = 2 };
 enum : unsigned {
 	ERRB_NAN = 1u, ERRB_PICARD = 2u, ERRB_DT = 4u, ERRB_FLUX = 8u, ERRB_TC = 16u, ERRB_SUBCYCLE = 32u,
 	ERRB_ASYNC = 64u,  // an asynchronous (TMA) copy did not complete within its wait limit
+	ERRB_SLAB = 128u,  // a slab's sweep met a partition-face neighbour before any boundary layer was exchanged
 };
 
 // Work queue of the thermal sub-cycles: control words (State::thq_ctl) and
@@ -135,6 +136,12 @@ struct State {
 	// (primitives of the FP64 form) or floats (the hydro-only FP32 state)
 	void* halo_send;
 	const void* halo_recv;
+	// x-slab decomposition with a star: the star-side neighbour's boundary x
+	// layer, received before each causal sweep, [side 2][ny * nz][4] doubles
+	// (the four optical depths in the R quad order, or COL_DEN, DCOL_DEN and
+	// two unused), read where an upwind neighbour lies across a partition
+	// face; null for a whole grid
+	const double* sweep_recv;
 	double* F[3];   // face fluxes per dimension [7][faces]
 	long long nfaces[3];
 	const Tables* tables;
