@@ -291,7 +291,10 @@ def time_form(args, precision, tp, ic, local, pg, profile_names):
         sim.fp32_contrast(args.fp32_contrast)
     if getattr(args, "thermo_queue", 0) and tp.cooling_on:
         sim.thermo_queue(args.thermo_queue)
-    sim.tile = sim.autotune()
+    if getattr(args, "tile_z", 0):
+        sim.tile = (sim.set_tile(args.tile_z), None)
+    else:
+        sim.tile = sim.autotune()
     dt_next = sim.dt_max
     stream = torch.cuda.ExternalStream(sim.stream_handle(), device=f"cuda:{local}")
     sim.run_steps(args.warmup)  # the first step is the reference's dt_max*1e-20 start step
@@ -838,6 +841,8 @@ def main():
     ap.add_argument("--validate", type=int, default=0,
                     help="instead of timing: error of the FP32 form against the FP64 form after this many steps")
     ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--tile-z", type=int, default=0,
+                    help="FP32 hydro kernel tile depth (z planes per CTA) in place of the autotuner's choice")
     ap.add_argument("--precision", choices=["both", "fp32", "fp64"], default="both")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-steps", type=int, default=4)

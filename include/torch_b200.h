@@ -245,6 +245,9 @@ int trg_checkpoint_load(trg_ctx* c, const void* buf, long long bytes);
  * (may be NULL) receive the choice and its time per launch; the FP64 form has
  * nothing to tune (0). */
 int trg_autotune(trg_ctx* c, int* zchunk_out, double* ms_out);
+/* Sets the FP32 form's CTA tile depth directly (1..nz; results do not depend
+ * on it), in place of the autotuner's choice; returns the depth in effect. */
+int trg_fp32_tile(trg_ctx* c, int zchunk);
 
 int trg_stats_enable(trg_ctx* c, int on);
 int trg_stats(trg_ctx* c, unsigned long long* out, int reset);

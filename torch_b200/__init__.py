@@ -151,6 +151,7 @@ _SIGNATURES = [
     ("trg_slab_halo_bytes", C.c_longlong, [C.c_void_p]),
     ("trg_slab_partitions", C.c_int, [C.c_void_p]),
     ("trg_slab_sweep_exchange", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("trg_fp32_tile", C.c_int, [C.c_void_p, C.c_int]),
     ("trg_slab_sweep_bytes", C.c_longlong, [C.c_void_p]),
     ("trg_slab_star_side", C.c_int, [C.c_void_p]),
     ("trg_f32_scales", C.c_int, [C.c_void_p] + [C.c_void_p] * 6 + [C.c_void_p]),
@@ -506,6 +507,10 @@ class Torch:
         ms = C.c_double(0)
         self._check(self.lib.trg_autotune(self.ctx, C.byref(z), C.byref(ms)))
         return z.value, ms.value
+
+    def set_tile(self, zchunk: int) -> int:
+        """Sets the FP32 hydro kernel's tile depth (z planes per CTA); returns the depth in effect."""
+        return int(self.lib.trg_fp32_tile(self.ctx, int(zchunk)))
 
     def stats_enable(self, on: bool):
         self._check(self.lib.trg_stats_enable(self.ctx, int(on)))

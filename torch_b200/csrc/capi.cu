@@ -1531,6 +1531,12 @@ int trg_autotune(trg_ctx* c, int* zchunk_out, double* ms_out) {
 	return TRG_OK;
 }
 
+int trg_fp32_tile(trg_ctx* c, int zchunk) {
+	if (!c) return 0;
+	if (zchunk > 0) c->zchunk = std::min(zchunk, c->P.nz);
+	return c->zchunk;
+}
+
 long long trg_kernel_launches(const trg_ctx* c) { return c ? c->launches : 0; }
 const char* trg_last_error(const trg_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
