@@ -598,6 +598,7 @@ __device__ __forceinline__ void neighbours(const Params& P, const int* ijk, cons
 	const int s0 = d0 < -1.0 / 10.0 ? -1 : 1, s1 = d1 < -1.0 / 10.0 ? -1 : 1, s2 = d2 < -1.0 / 10.0 ? -1 : 1;
 	const int L0 = fabs(d0) < 1.0 / 10.0 ? 0 : s0, L1 = fabs(d1) < 1.0 / 10.0 ? 0 : s1, L2 = fabs(d2) < 1.0 / 10.0 ? 0 : s2;
 	// offsets in the rotated frame: n = 0: (0, 0, -L2), 1: (0, -L1, -L2), 2: (-L0, 0, -L2), 3: (-L0, -L1, -L2)
+	const bool slab = P.lbc[0] == BC_PARTITION || P.rbc[0] == BC_PARTITION;  // the same for every thread
 #pragma unroll
 	for (int n = 0; n < 4; ++n) {
 		const int o0 = (n & 2) ? -L0 : 0, o1 = (n & 1) ? -L1 : 0, o2 = -L2;
@@ -607,7 +608,8 @@ __device__ __forceinline__ void neighbours(const Params& P, const int* ijk, cons
 		const bool yz = tj >= 0 && tj < P.ny && tk >= 0 && tk < P.nz;
 		const bool in = ti >= 0 && ti < P.nx && yz;
 		nb[n] = in ? flat_id(P, ti, tj, tk) : -1;
-		if (!in && yz && ((ti == -1 && P.lbc[0] == BC_PARTITION) || (ti == P.nx && P.rbc[0] == BC_PARTITION)))
+		if (slab && !in && yz &&
+		    ((ti == -1 && P.lbc[0] == BC_PARTITION) || (ti == P.nx && P.rbc[0] == BC_PARTITION)))
 			nb[n] = -2 - ((ti < 0 ? 0 : (long long)P.ny * P.nz) + tj + (long long)P.ny * tk);
 	}
 	double ic0 = (int)x0 - 0.5 * (s2 * d0 / d2);
@@ -676,47 +678,45 @@ __device__ __forceinline__ double tau_interp(const Params& P, const double* tau,
 	return newtau;
 #endif
 }
-// A zero-weight neighbour contributes 0 * tau = 0 whatever its tau, and may
-// belong to the shell being swept: it is not read.  Neighbour optical depths
-// written by the previous shell are read past L1, one 16-byte pair (TAU, DTAU
-// or TAU_A, DTAU_A) at a time.
-// A slab's boundary-layer neighbour with no received layer (a sweep outside
-// the exchange, which the host does not launch) is reported, never read.
-__device__ __forceinline__ bool nb_read(const State& S, const long long* nb, const double* w0, int i) {
-	if (nb[i] == -1 || w0[i] == 0) return false;
-	if (nb[i] < -1 && !S.sweep_recv) {
-		atomicOr(S.err, ERRB_SLAB);
-		return false;
+// Where the inner neighbours' optical depths (R quads, STRIDE 4) or column
+// densities (T pairs, STRIDE 2) are read, resolved before the sweep's wait so
+// that no address arithmetic sits between the wait and the loads: null where
+// a neighbour is not read (outside the grid, or of zero weight: it
+// contributes 0 * tau = 0 whatever its tau, and may belong to the shell being
+// swept); across a slab's partition face, its entry of the received boundary
+// layer (4 doubles per cell).  A slab whose layer was never exchanged (a
+// sweep outside the exchange, which the host does not launch) reports
+// ERRB_SLAB and reads nothing.  Neighbour values written by the previous
+// shell are read past L1, one 16-byte pair at a time.
+template <int STRIDE>
+__device__ __forceinline__ void nb_sources(const State& S, const double* base, const long long* nb, const double* w0,
+                                           const double2** src) {
+#pragma unroll
+	for (int i = 0; i < 4; ++i) {
+		src[i] = nullptr;
+		if (w0[i] == 0 || nb[i] == -1) continue;
+		if (nb[i] >= 0) src[i] = reinterpret_cast<const double2*>(base + nb[i] * STRIDE);
+		else if (S.sweep_recv) src[i] = reinterpret_cast<const double2*>(S.sweep_recv + (-2 - nb[i]) * 4);
+		else atomicOr(S.err, ERRB_SLAB);
 	}
-	return true;
-}
-// A neighbour's four optical depths (R quad) and its column densities
-// (COL_DEN, DCOL_DEN): in the state, or across a slab's partition face in
-// the received boundary layer (4 doubles per cell).
-__device__ __forceinline__ const double2* nb_quad(const State& S, long long nb) {
-	return reinterpret_cast<const double2*>(nb >= 0 ? S.R + nb * 4 : S.sweep_recv + (-2 - nb) * 4);
-}
-__device__ __forceinline__ const double2* nb_colden(const State& S, long long nb) {
-	return reinterpret_cast<const double2*>(nb >= 0 ? S.T + nb * 2 : S.sweep_recv + (-2 - nb) * 4);
 }
 // TAU (from TAU + DTAU of the neighbours)
-__device__ __forceinline__ double tau_sc(const Params& P, const State& S, const long long* nb, const double* w0) {
+__device__ __forceinline__ double tau_sc(const Params& P, const double2* const* src, const double* w0) {
 	double tau[4] = {0, 0, 0, 0};
 	for (int i = 0; i < 4; ++i)
-		if (nb_read(S, nb, w0, i)) {
-			const double2 a = __ldcg(nb_quad(S, nb[i]));
+		if (src[i]) {
+			const double2 a = __ldcg(src[i]);
 			tau[i] = a.x + a.y;
 		}
 	return tau_interp(P, tau, w0);
 }
 // TAU and TAU_A together (each neighbour's four optical depths share a sector)
-__device__ __forceinline__ void tau_sc2(const Params& P, const State& S, const long long* nb, const double* w0,
+__device__ __forceinline__ void tau_sc2(const Params& P, const double2* const* src, const double* w0,
                                         double& tau_out, double& tau_a_out) {
 	double tau[4] = {0, 0, 0, 0}, tau_a[4] = {0, 0, 0, 0};
 	for (int i = 0; i < 4; ++i)
-		if (nb_read(S, nb, w0, i)) {
-			const double2* q = nb_quad(S, nb[i]);
-			const double2 a = __ldcg(q), b = __ldcg(q + 1);
+		if (src[i]) {
+			const double2 a = __ldcg(src[i]), b = __ldcg(src[i] + 1);
 			tau[i] = a.x + a.y;
 			tau_a[i] = b.x + b.y;
 		}
@@ -869,9 +869,11 @@ __device__ __forceinline__ void rad_shell(const Params& P, const State& S, const
 			shellVol = S.shellVol[id];
 		}
 	}
+	const double2* src[4];
+	nb_sources<4>(S, S.R, nb, w, src);
 	sweep_wait();
 	double tau = 0, tau_a = 0;
-	if (inner) tau_sc2(P, S, nb, w, tau, tau_a);
+	if (inner) tau_sc2(P, src, w, tau, tau_a);
 	if (!star) {
 		tau_avg = tau_a;
 		front = front_cell(tau_avg, q_hii);
@@ -1230,8 +1232,10 @@ __device__ __forceinline__ void b_rad_tau_shell(const Params& P, const State& S,
 	const double nH = P.X * FLD(S.Q, DEN, id) / P.hydrogenMass;
 	const double dtau = (1.0 - FLD(S.Q, HII, id)) * nH * P.photoIonXsec * S.ds[id];
 	const double dtau_a = (1.0 - RFLD(S.R, R_HII_A, id)) * nH * P.photoIonXsec * S.ds[id];
+	const double2* src[4] = {nullptr, nullptr, nullptr, nullptr};
+	if (inner) nb_sources<4>(S, S.R, nb, w, src);
 	sweep_wait();
-	RFLD(S.R, R_TAU, id) = inner ? tau_sc(P, S, nb, w) : 0.0;
+	RFLD(S.R, R_TAU, id) = inner ? tau_sc(P, src, w) : 0.0;
 	RFLD(S.R, R_DTAU, id) = dtau;
 	RFLD(S.R, R_DTAU_A, id) = dtau_a;
 }
@@ -1476,14 +1480,16 @@ __device__ __forceinline__ void b_colden_shell_fp64(const Params& P, const State
 	double w0[4];
 	if (inner) neighbours(P, ijk, xc, nb, w0);
 	const double dcolden = own ? *own : (FLD(S.Q, DEN, id) / P.hydrogenMass) * S.ds[id];
+	const double2* src[4] = {nullptr, nullptr, nullptr, nullptr};
+	if (inner) nb_sources<2>(S, S.T, nb, w0, src);
 	sweep_wait();
 	double newcolden = 0.0;
 	if (inner) {
 		double colden[4] = {0, 0, 0, 0}, w[4];
 #ifdef TRG_FAST_MATH
 		for (int i = 0; i < 4; ++i)
-			if (nb_read(S, nb, w0, i)) {
-				const double2 c = __ldcg(nb_colden(S, nb[i]));  // COL_DEN, DCOL_DEN
+			if (src[i]) {
+				const double2 c = __ldcg(src[i]);  // COL_DEN, DCOL_DEN
 				colden[i] = c.x + c.y;
 			}
 		// The interpolation is the weighted harmonic mean sum(w0) / sum(w0 / c)
@@ -1512,8 +1518,8 @@ __device__ __forceinline__ void b_colden_shell_fp64(const Params& P, const State
 		}
 #else
 		for (int i = 0; i < 4; ++i) {
-			if (nb_read(S, nb, w0, i)) {
-				const double2 c = __ldcg(nb_colden(S, nb[i]));  // COL_DEN, DCOL_DEN
+			if (src[i]) {
+				const double2 c = __ldcg(src[i]);  // COL_DEN, DCOL_DEN
 				colden[i] = c.x + c.y;
 			}
 			w[i] = colden[i] == 0 ? 0 : w0[i] / colden[i];
