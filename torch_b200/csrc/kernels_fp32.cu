@@ -66,13 +66,14 @@ __device__ __forceinline__ float fminf_(float a, float b) { return (b < a) ? b :
 // [2^-126, 2^126], which the scaled units keep every divisor of this file in).
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
 __device__ __forceinline__ float frcp(float b) { return __fdividef(1.0f, b); }
-// ... and the correctly rounded ones, kept where the rounding noise of every
-// hydro sub-step feeds the long-run error against the FP64 form most: the
-// reciprocal density of the primitives, and the square roots, reciprocal and
-// sound speeds of the Einfeldt wave-speed estimate.  (Measured on the 256^3
-// HII region after 1000 steps: pressure L1 1.2e-4 with every operation
-// approximate, 4.9e-5 with these five correctly rounded, for 8% more time in
-// this kernel.)
+// ... and the correctly rounded ones, kept in the radiation-hydro form (FP64
+// state, CR = true below) where the rounding noise of every hydro sub-step
+// feeds the long-run error against the FP64 form most: the reciprocal density
+// of the primitives, and the square roots, reciprocal and sound speeds of the
+// Einfeldt wave-speed estimate.  (Measured on the 256^3 HII region after 1000
+// steps: pressure L1 1.2e-4 with every operation approximate, 4.9e-5 with
+// these five correctly rounded, for 8% more time in this kernel.)  The
+// hydro-only form (FP32 state) keeps them all approximate.
 __device__ __forceinline__ float pdiv(float a, float b) { return __fdiv_rn(a, b); }
 __device__ __forceinline__ float prcp(float b) { return __frcp_rn(b); }
 __device__ __forceinline__ float psqrt(float a) { return __fsqrt_rn(a); }
@@ -114,10 +115,11 @@ __device__ __forceinline__ void two_prod(float a, float b, float& p, float& e) {
 }
 
 // Q from U with the compensated E - KE.  KE = 0.5 |m|^2 / rho as a float pair.
+template <bool CR>
 __device__ __forceinline__ Prim prim_from_cons(const float* u, float gamma, int nd) {
 	Prim q;
 	q.d = u[DEN];
-	float inv = prcp(u[DEN]);
+	float inv = CR ? prcp(u[DEN]) : frcp(u[DEN]);
 	float s = 0.f, se = 0.f;
 #pragma unroll
 	for (int k = 0; k < 3; ++k) {
@@ -157,7 +159,7 @@ __device__ __forceinline__ void fix_prim(const Scaled& P, Prim& q, float u_den) 
 // Fluid::fixSolution in FP32 (compensated kinetic energy as in prim_from_cons).
 __device__ __forceinline__ bool fix_cons(const Scaled& P, float* u) {
 	if (!isfinite(u[DEN]) || !isfinite(u[PRE])) return false;
-	float inv = prcp(u[DEN]);
+	float inv = frcp(u[DEN]);
 	float hii = fmaxf_(fminf_(u[HII] * inv, 1.f), 0.f);
 	float adv = fmaxf_(fminf_(u[ADV] * inv, 1.f), 0.f);
 	float den = fmaxf_(u[DEN], P.dfloor);
@@ -165,7 +167,7 @@ __device__ __forceinline__ bool fix_cons(const Scaled& P, float* u) {
 	float v[3];
 #pragma unroll
 	for (int k = 0; k < 3; ++k) v[k] = k < nd ? u[VEL + k] * inv : 0.f;
-	Prim q = prim_from_cons(u, P.gamma, nd);
+	Prim q = prim_from_cons<false>(u, P.gamma, nd);
 	float pre = q.p;
 	float ke = (v[0] * v[0] + v[1] * v[1]) + v[2] * v[2];
 	ke *= 0.5f * den;
@@ -277,14 +279,16 @@ __device__ __forceinline__ void cons_of(const Prim& q, float g1inv, float* U) {
 	U[ADV] = q.d * q.a;
 	for (int k = 0; k < 3; ++k) U[VEL + k] = q.d * q.v[k];
 }
+template <bool CR>
 __device__ __forceinline__ void face_pre(const Prim& L, const Prim& R, float gamma, float g1inv, FacePre& f) {
 	cons_of(L, g1inv, f.UL);
 	cons_of(R, g1inv, f.UR);
-	f.sl = psqrt(L.d);
-	f.sr = psqrt(R.d);
-	f.inv = prcp(f.sl + f.sr);
+	f.sl = CR ? psqrt(L.d) : sqrtf(L.d);
+	f.sr = CR ? psqrt(R.d) : sqrtf(R.d);
+	f.inv = CR ? prcp(f.sl + f.sr) : frcp(f.sl + f.sr);
 	f.nu2 = 0.5f * f.sr * f.sl * f.inv * f.inv;
-	float aL2 = pdiv(gamma * L.p, L.d), aR2 = pdiv(gamma * R.p, R.d);
+	float aL2 = CR ? pdiv(gamma * L.p, L.d) : fdiv(gamma * L.p, L.d);
+	float aR2 = CR ? pdiv(gamma * R.p, R.d) : fdiv(gamma * R.p, R.d);
 	f.c2 = (f.sl * aL2 + f.sr * aR2) * f.inv;
 }
 // Physical flux of a state (conserved U) along unit normal n.
@@ -297,19 +301,21 @@ __device__ __forceinline__ void flux_n(const Prim& q, const float* U, const floa
 	F[ADV] = mflux * q.a;
 	for (int k = 0; k < 3; ++k) F[VEL + k] = mflux * q.v[k] + q.p * n[k];
 }
+template <bool CR>
 __device__ __forceinline__ void speeds_n(const FacePre& f, float unL, float unR, float& SL, float& SR) {
 	float ut = (f.sl * unL + f.sr * unR) * f.inv;
 	float d2 = f.c2 + f.nu2 * (unR - unL) * (unR - unL);
-	float dd = psqrt(d2);
+	float dd = CR ? psqrt(d2) : sqrtf(d2);
 	SL = ut - dd;
 	SR = ut + dd;
 }
 
+template <bool CR>
 __device__ __forceinline__ void hll_n(const Prim& L, const Prim& R, const FacePre& f, const float* n, float* F) {
 	float FL[7], FR[7], unL, unR, SL, SR;
 	flux_n(L, f.UL, n, unL, FL);
 	flux_n(R, f.UR, n, unR, FR);
-	speeds_n(f, unL, unR, SL, SR);
+	speeds_n<CR>(f, unL, unR, SL, SR);
 	if (SR <= 0) {
 		for (int i = 0; i < 7; ++i) F[i] = FR[i];
 	} else if (SL >= 0) {
@@ -320,11 +326,12 @@ __device__ __forceinline__ void hll_n(const Prim& L, const Prim& R, const FacePr
 	}
 }
 
+template <bool CR>
 __device__ __forceinline__ void hllc_n(const Prim& L, const Prim& R, const FacePre& f, const float* n, float* F) {
 	float FL[7], FR[7], unL, unR, SL, SR;
 	flux_n(L, f.UL, n, unL, FL);
 	flux_n(R, f.UR, n, unR, FR);
-	speeds_n(f, unL, unR, SL, SR);
+	speeds_n<CR>(f, unL, unR, SL, SR);
 	if (SL >= 0) {
 		for (int i = 0; i < 7; ++i) F[i] = FL[i];
 	} else if (SR <= 0) {
@@ -361,11 +368,12 @@ __device__ __forceinline__ void hllc_n(const Prim& L, const Prim& R, const FaceP
 // w2 = 0, n1 = d); a solve with weight 0 is skipped, so the exact flux of the
 // pure cases is kept, and each solver is inlined once.
 // No array is indexed with the run-time dim, so everything stays in registers.
+template <bool CR>
 __device__ __forceinline__ void riemann32(int kind, const Prim& L, const Prim& R, int dim, float gamma, float* F) {
 	const float g1inv = 1.f / (gamma - 1.f);
 	const float d[3] = {dim == 0 ? 1.f : 0.f, dim == 1 ? 1.f : 0.f, dim == 2 ? 1.f : 0.f};
 	FacePre f;
-	face_pre(L, R, gamma, g1inv, f);
+	face_pre<CR>(L, R, gamma, g1inv, f);
 	float n1[3] = {d[0], d[1], d[2]}, n2[3] = {d[0], d[1], d[2]};
 	float w1 = kind == RS_HLL ? 1.f : 0.f, w2 = kind == RS_HLLC ? 1.f : 0.f;
 	if (kind == RS_ROTATED) {
@@ -394,8 +402,8 @@ __device__ __forceinline__ void riemann32(int kind, const Prim& L, const Prim& R
 	float F1[7], F2[7];
 #pragma unroll
 	for (int i = 0; i < 7; ++i) F1[i] = F2[i] = 0.f;
-	if (w1 != 0.f) hll_n(L, R, f, n1, F1);
-	if (w2 != 0.f) hllc_n(L, R, f, n2, F2);
+	if (w1 != 0.f) hll_n<CR>(L, R, f, n1, F1);
+	if (w2 != 0.f) hllc_n<CR>(L, R, f, n2, F2);
 #pragma unroll
 	for (int i = 0; i < 7; ++i) F[i] = w1 * F1[i] + w2 * F2[i];
 }
@@ -562,7 +570,7 @@ __device__ __forceinline__ void load_plane(const Params& P, const Scaled& SP, co
 		float u[7];
 #pragma unroll
 		for (int f = 0; f < 7; ++f) u[f] = load_u(stage_src(P, Up, halo, m.off[j], f, zs), 0, SC, f);
-		Prim q = prim_from_cons(u, (float)P.gamma, P.nd);
+		Prim q = prim_from_cons<sizeof(TS) == sizeof(double)>(u, (float)P.gamma, P.nd);
 		if (STAGE == 1) fix_prim(SP, q, u[DEN]);
 		apply_flips(P, q, m.flags[j], zc, zside);
 		put_prim(s, slot, threadIdx.x + j * BX * BY, q);
@@ -650,7 +658,7 @@ __device__ __forceinline__ void plane_convert(const Params& P, const Scaled& SP,
 		float u[7];
 #pragma unroll
 		for (int f = 0; f < 7; ++f) u[f] = scaled_u(raw[f * (SX * SY) + idx], SC, f);
-		Prim q = prim_from_cons(u, (float)P.gamma, P.nd);
+		Prim q = prim_from_cons<sizeof(TS) == sizeof(double)>(u, (float)P.gamma, P.nd);
 		if (STAGE == 1) fix_prim(SP, q, u[DEN]);
 		apply_flips(P, q, m.flags[j], zc, zside);
 		put_prim(s, slot, idx, q);
@@ -732,9 +740,10 @@ __host__ __device__ constexpr size_t hydro_stage_raw_offset() {
 }
 
 // Riemann solve for one face from its reconstructed states.
-template <int RS>
+// CR: the correctly rounded operations of the radiation-hydro form (above).
+template <int RS, bool CR>
 __device__ __forceinline__ void face_flux(int rs_rt, const Prim& L, const Prim& R, int dim, float gamma, float* F) {
-	riemann32(RS >= 0 ? RS : rs_rt, L, R, dim, gamma, F);
+	riemann32<CR>(RS >= 0 ? RS : rs_rt, L, R, dim, gamma, F);
 }
 
 // One Euler stage U_out = fix(U_base + h dt L(Q(U_q))).
@@ -753,6 +762,7 @@ __device__ __forceinline__ void hydro_stage_body(const Params& P, const State& S
                                                  const TS* Ubase, TS* Uout, double hfac, int zchunk,
                                                  const CUtensorMap* tmap, int use_tma, int bx, int by, int bz) {
 	extern __shared__ __align__(128) unsigned char smem_raw[];
+	constexpr bool CR = sizeof(TS) == sizeof(double);  // the radiation-hydro form's correctly rounded operations
 	SmemQ& s = *reinterpret_cast<SmemQ*>(smem_raw);
 	float4* v8 = reinterpret_cast<float4*>(smem_raw + sizeof(SmemQ));
 	const V8 Fx{v8, v8 + N_FX};                      // [BY][BX + 1] x-face fluxes
@@ -949,13 +959,13 @@ __device__ __forceinline__ void hydro_stage_body(const Params& P, const State& S
 			}
 			if (!ok) continue;
 			float f[7];
-			face_flux<RS>(rs_rt, rec ? face_left(ql, sl) : ql, rec ? face_right(qr, sr) : qr, dim, gamma, f);
+			face_flux<RS, CR>(rs_rt, rec ? face_left(ql, sl) : ql, rec ? face_right(qr, sr) : qr, dim, gamma, f);
 			dst.put_f(di, f);
 		}
 		float fz[7];  // flux through this column's face z + 1/2
 		if (nd > 2) {
 			const Prim ql = get(s, sc, ly, lx), qr = get(s, s_z1, ly, lx);
-			face_flux<RS>(rs_rt, rec ? face_left(ql, szc) : ql, rec ? face_right(qr, szn) : qr, 2, gamma, fz);
+			face_flux<RS, CR>(rs_rt, rec ? face_left(ql, szc) : ql, rec ? face_right(qr, szn) : qr, 2, gamma, fz);
 		}
 		// the cell itself for the source terms, read before the barrier: after
 		// it, nothing of this plane is read, so the next plane's load may reuse
@@ -1033,7 +1043,7 @@ __device__ __forceinline__ void hydro_stage_body(const Params& P, const State& S
 			if (STAGE == 2) {
 				// the next step's CFL limit from Q(U1) with floors (Torch::fullStep:
 				// globalQfromU + fixPrimitives, then Hydrodynamics::calculateTimeStep)
-				Prim q = prim_from_cons(u, gamma, nd);
+				Prim q = prim_from_cons<CR>(u, gamma, nd);
 				fix_prim(SP, q, u[DEN]);
 				// velocities are in units of v0: inv_t = (|v| + c) v0 / dx
 				double ss = sqrt(P.gamma * (double)q.p / (double)q.d);
